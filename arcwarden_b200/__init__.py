@@ -1,0 +1,273 @@
+"""arcwarden_b200 — B200-native (sm_100a) ArcWarden PIC hot path.
+
+The product is the C-ABI library ``libarcb200.so`` (declared in
+``include/arcb200.h``). This module is a thin ctypes binding used by the tests
+and the benchmark: it passes device pointers (from torch CUDA tensors or raw
+integers) straight through and turns a non-zero status into ``ArcError``.
+
+There is no CPU fallback: importing works without a GPU, but every compute call
+runs the CUDA kernels in the library, and a missing library raises at load time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libarcb200.so"
+
+AW_OK, AW_ERR_ARG, AW_ERR_CUDA, AW_ERR_CUFFT, AW_ERR_STATE, AW_ERR_DEVICE, AW_ERR_NOMEM = 0, -1, -2, -3, -4, -5, -6
+AW_MODEL_ES, AW_MODEL_DARWIN = 0, 1
+AW_DEV_NONFINITE, AW_DEV_OUT_OF_GRID, AW_DEV_WAIT_LIMIT = 1, 2, 4
+
+
+class ArcError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("ny", C.c_int32), ("Lx", C.c_double), ("Ly", C.c_double)]
+
+
+class Params(C.Structure):
+    _fields_ = [("dt", C.c_double), ("qm", C.c_double), ("eps0", C.c_double), ("n0", C.c_double),
+                ("c", C.c_double), ("B0", C.c_float * 3), ("has_b0", C.c_int32), ("pump", C.c_int32),
+                ("pump_ex", C.c_double), ("pump_ey", C.c_double), ("pump_ez", C.c_double),
+                ("pump_k0", C.c_double), ("pump_w0", C.c_double), ("pump_trmp", C.c_double),
+                ("pump_toff", C.c_double)]
+
+
+class Species(C.Structure):
+    _fields_ = [("ppc", C.c_int32), ("density", C.c_double), ("uth", C.c_double * 3), ("ufl", C.c_double * 3)]
+
+
+SOURCE_NAMES = ("rho", "Jx", "Jy", "Jz", "dcux", "dcuy", "dcuz", "amu0", "amu1", "amu2", "amu3")
+FIELD_NAMES = ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "ELx", "ELy", "ETx", "ETy", "ETz")
+
+
+class SourcePtrs(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in SOURCE_NAMES]
+
+
+class FieldPtrs(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in FIELD_NAMES]
+
+
+class Diag(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("ke", "ee", "charge", "max_e", "px", "py", "pz", "eb")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class Stats(C.Structure):
+    _fields_ = [("chunks", C.c_int64), ("window_overflow", C.c_int64), ("slow_deposits", C.c_int64),
+                ("steps", C.c_int64)]
+
+
+# Exported symbols and their ctypes signatures (must match include/arcb200.h).
+_P, _I32, _I64, _U64, _D, _F = C.c_void_p, C.c_int32, C.c_int64, C.c_uint64, C.c_double, C.c_float
+SIGNATURES = {
+    "aw_ctx_create": [C.POINTER(Grid), C.POINTER(Params), _I32, _P, C.POINTER(_P)],
+    "aw_ctx_destroy": [_P],
+    "aw_set_stream": [_P, _P],
+    "aw_set_params": [_P, C.POINTER(Params)],
+    "aw_particles_bind": [_P, _P, _P, _P, _P, _P, _P, _P, _I64],
+    "aw_sources_bind": [_P, C.POINTER(SourcePtrs)],
+    "aw_fields_bind": [_P, C.POINTER(FieldPtrs)],
+    "aw_load_species": [_P, C.POINTER(Species), _I32, _U64, _I32],
+    "aw_deposit_rho": [_P], "aw_deposit_rho_j": [_P], "aw_deposit_amu": [_P], "aw_deposit_dcu": [_P],
+    "aw_push_es": [_P], "aw_push_em": [_P], "aw_half_step_back": [_P], "aw_migrate": [_P],
+    "aw_sort_tiles": [_P, _I32, _I32, _I32],
+    "aw_tile_bins": [_P, C.POINTER(_P), C.POINTER(_P), C.POINTER(_I32), C.POINTER(_I32)],
+    "aw_solve_es": [_P], "aw_solve_darwin_el_b": [_P], "aw_solve_darwin_et": [_P], "aw_solve_darwin": [_P],
+    "aw_form_e": [_P, _F], "aw_add_b0": [_P], "aw_add_pump": [_P, _D],
+    "aw_fft_r2c": [_P, _P, _P], "aw_fft_c2r": [_P, _P, _P],
+    "aw_init": [_P], "aw_step": [_P, _I64], "aw_run": [_P, _I64, _I64, _I32],
+    "aw_reduce_fp64": [_P, C.POINTER(Diag)], "aw_step_diag": [_P, C.POINTER(Diag)],
+    "aw_step_diag_device": [_P, C.POINTER(_P)],
+    "aw_error_word": [_P, C.POINTER(C.c_uint32)], "aw_stats": [_P, C.POINTER(Stats)],
+    "aw_last_error": [C.c_char_p, _I32],
+}
+
+_lib = None
+
+
+def load_library(path: str | Path | None = None) -> C.CDLL:
+    """Load libarcb200.so (raises if it is missing: there is no fallback)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ArcError(AW_ERR_STATE, f"{p} is missing; build it with `python -m arcwarden_b200.build`")
+    lib = C.CDLL(str(p))
+    for name, argtypes in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = argtypes
+        fn.restype = C.c_int
+    lib.aw_version.restype = C.c_char_p
+    lib.aw_version.argtypes = []
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != AW_OK:
+        buf = C.create_string_buffer(1024)
+        _lib.aw_last_error(buf, 1024)
+        raise ArcError(rc, buf.value.decode(errors="replace"))
+
+
+def _ptr(t) -> int | None:
+    """Device pointer of a torch tensor / int / None."""
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+class Context:
+    """One simulation context (grid, run parameters, bound particle/grid memory)."""
+
+    def __init__(self, nx, ny, Lx, Ly, *, dt, qm=-1.0, eps0=1.0, n0=1.0, c=1.0, B0=(0.0, 0.0, 0.0),
+                 has_b0=True, model=AW_MODEL_ES, stream=None, pump=None):
+        self.lib = load_library()
+        self.grid = Grid(nx, ny, Lx, Ly)
+        self.params = make_params(dt=dt, qm=qm, eps0=eps0, n0=n0, c=c, B0=B0, has_b0=has_b0, pump=pump)
+        self.model = model
+        self._keep = []
+        h = C.c_void_p()
+        _check(self.lib.aw_ctx_create(C.byref(self.grid), C.byref(self.params), model,
+                                      C.c_void_p(stream) if stream else None, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.aw_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- binding ----
+    def bind_particles(self, x, y, ux, uy, uz, w, cell, n=None):
+        n = int(x.numel()) if n is None else int(n)
+        _check(self.lib.aw_particles_bind(self.h, _ptr(x), _ptr(y), _ptr(ux), _ptr(uy), _ptr(uz), _ptr(w),
+                                          _ptr(cell), n))
+        self._keep.append((x, y, ux, uy, uz, w, cell))
+
+    def bind_sources(self, **arrays):
+        s = SourcePtrs(*[_ptr(arrays.get(k)) for k in SOURCE_NAMES])
+        _check(self.lib.aw_sources_bind(self.h, C.byref(s)))
+        self._keep.append(arrays)
+
+    def bind_fields(self, **arrays):
+        f = FieldPtrs(*[_ptr(arrays.get(k)) for k in FIELD_NAMES])
+        _check(self.lib.aw_fields_bind(self.h, C.byref(f)))
+        self._keep.append(arrays)
+
+    def set_params(self, **kw):
+        self.params = make_params(**kw)
+        _check(self.lib.aw_set_params(self.h, C.byref(self.params)))
+
+    def set_stream(self, stream):
+        _check(self.lib.aw_set_stream(self.h, C.c_void_p(stream) if stream else None))
+
+    # ---- loader / operators ----
+    def load_species(self, species, seed=0, noisy=True):
+        arr = (Species * len(species))()
+        for i, s in enumerate(species):
+            arr[i].ppc = int(s["ppc"])
+            arr[i].density = float(s["density"])
+            for d in range(3):
+                arr[i].uth[d] = float(s["uth"][d])
+                arr[i].ufl[d] = float(s["ufl"][d])
+        _check(self.lib.aw_load_species(self.h, arr, len(species), int(seed), int(bool(noisy))))
+
+    def __getattr__(self, name):
+        # operator pass-through: ctx.deposit_rho(), ctx.solve_es(), ...
+        if name in _OPS:
+            fn = getattr(self.lib, "aw_" + name)
+            return lambda *a: _check(fn(self.h, *a))
+        raise AttributeError(name)
+
+    def sort_tiles(self, tx=16, ty=16, physical=False):
+        _check(self.lib.aw_sort_tiles(self.h, tx, ty, int(bool(physical))))
+
+    def tile_bins(self):
+        off, idx, nt, ntx = C.c_void_p(), C.c_void_p(), C.c_int32(), C.c_int32()
+        _check(self.lib.aw_tile_bins(self.h, C.byref(off), C.byref(idx), C.byref(nt), C.byref(ntx)))
+        return off.value, idx.value, nt.value, ntx.value
+
+    def fft_r2c(self, src, dst):
+        _check(self.lib.aw_fft_r2c(self.h, _ptr(src), _ptr(dst)))
+
+    def fft_c2r(self, src, dst):
+        _check(self.lib.aw_fft_c2r(self.h, _ptr(src), _ptr(dst)))
+
+    def form_e(self, s):
+        _check(self.lib.aw_form_e(self.h, C.c_float(s)))
+
+    def add_pump(self, t):
+        _check(self.lib.aw_add_pump(self.h, C.c_double(t)))
+
+    def step(self, n):
+        _check(self.lib.aw_step(self.h, int(n)))
+
+    def run(self, n0, nsteps, graph=True):
+        _check(self.lib.aw_run(self.h, int(n0), int(nsteps), int(bool(graph))))
+
+    def reduce(self) -> dict:
+        d = Diag()
+        _check(self.lib.aw_reduce_fp64(self.h, C.byref(d)))
+        return d.as_dict()
+
+    def step_diag(self) -> dict:
+        d = Diag()
+        _check(self.lib.aw_step_diag(self.h, C.byref(d)))
+        return d.as_dict()
+
+    def step_diag_device(self) -> int:
+        p = C.c_void_p()
+        _check(self.lib.aw_step_diag_device(self.h, C.byref(p)))
+        return p.value
+
+    def error_word(self) -> int:
+        v = C.c_uint32()
+        _check(self.lib.aw_error_word(self.h, C.byref(v)))
+        return v.value
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(self.lib.aw_stats(self.h, C.byref(s)))
+        return {n: getattr(s, n) for n, _ in s._fields_}
+
+
+_OPS = {"deposit_rho", "deposit_rho_j", "deposit_amu", "deposit_dcu", "push_es", "push_em",
+        "half_step_back", "migrate", "solve_es", "solve_darwin_el_b", "solve_darwin_et", "solve_darwin",
+        "add_b0", "init"}
+
+
+def make_params(*, dt, qm=-1.0, eps0=1.0, n0=1.0, c=1.0, B0=(0.0, 0.0, 0.0), has_b0=True, pump=None) -> Params:
+    p = Params()
+    p.dt, p.qm, p.eps0, p.n0, p.c = dt, qm, eps0, n0, c
+    for d in range(3):
+        p.B0[d] = float(B0[d])
+    p.has_b0 = int(bool(has_b0))
+    if pump:
+        p.pump = 1
+        for k in ("ex", "ey", "ez", "k0", "w0", "trmp", "toff"):
+            setattr(p, "pump_" + k, float(pump[k]))
+    return p
+
+
+def version() -> str:
+    return load_library().aw_version().decode()

@@ -1,0 +1,704 @@
+// aw_abi.cu — the extern "C" entry points of libarcb200 (declared in
+// include/arcb200.h) and the host orchestration of the fused step.
+//
+// The fused ES step (Simulation<Cfg>::step, include/pic/simulation.hpp:85-92):
+//   finalize(rho) -> R2C -> k-space E -> C2R x2 (batched) -> fields_es
+//   -> push+migrate+deposit(rho of the new state) -> diagnostics reduce
+// The fused Darwin step (include/pic/simulation.hpp:81-84, 103-119):
+//   finalize(rho,J,amu) -> R2C x8 -> k-space E_L,B -> C2R x5 -> fields_dcu
+//   -> dcu deposit -> finalize(dcu) -> R2C x3 -> k-space E_T -> C2R x3
+//   -> fields_push -> push+migrate+deposit(rho,J,amu of the new state) -> reduce
+// The source deposit of step n is made by the push of step n-1 (or by aw_init),
+// which is exactly the reference's "deposit the current state first".
+#include "aw_internal.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+
+namespace aw {
+
+thread_local std::string g_last_error;
+
+void check_cuda(cudaError_t e, const char* what, const char* file, int line) {
+    if (e != cudaSuccess) {
+        char buf[512];
+        std::snprintf(buf, sizeof(buf), "%s:%d: CUDA error in `%s`: %s (%s)", file, line, what,
+                      cudaGetErrorName(e), cudaGetErrorString(e));
+        throw Error(AW_ERR_CUDA, buf);
+    }
+}
+void check_cufft(cufftResult r, const char* what, const char* file, int line) {
+    if (r != CUFFT_SUCCESS) {
+        char buf[512];
+        std::snprintf(buf, sizeof(buf), "%s:%d: cuFFT error %d in `%s`", file, line, static_cast<int>(r), what);
+        throw Error(AW_ERR_CUFFT, buf);
+    }
+}
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return AW_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return AW_ERR_STATE;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return AW_ERR_STATE;
+    }
+}
+
+template <class T>
+void dalloc(T*& p, size_t n) {
+    if (n == 0) { p = nullptr; return; }
+    AW_CUDA(cudaMalloc(reinterpret_cast<void**>(&p), n * sizeof(T)));
+}
+
+void need(bool ok, int code, const char* msg) {
+    if (!ok) throw Error(code, msg);
+}
+
+void make_plan(cufftHandle& h, int ny, int nx, cufftType type, int batch, size_t& ws) {
+    AW_CUFFT(cufftCreate(&h));
+    AW_CUFFT(cufftSetAutoAllocation(h, 0));
+    int n[2] = {ny, nx};
+    const int nkx = nx / 2 + 1;
+    const int rdist = nx * ny, cdist = nkx * ny;
+    size_t w = 0;
+    if (type == CUFFT_R2C)
+        AW_CUFFT(cufftMakePlanMany(h, 2, n, nullptr, 1, rdist, nullptr, 1, cdist, type, batch, &w));
+    else
+        AW_CUFFT(cufftMakePlanMany(h, 2, n, nullptr, 1, cdist, nullptr, 1, rdist, type, batch, &w));
+    if (w > ws) ws = w;
+}
+
+void free_all(Ctx& c) {
+    if (c.gexec) cudaGraphExecDestroy(c.gexec);
+    if (c.graph) cudaGraphDestroy(c.graph);
+    cufftHandle* plans[] = {&c.p_r2c1, &c.p_c2r1, &c.p_r2cS, &c.p_c2rO, &c.p_r2c3, &c.p_c2r3, &c.p_r2c4};
+    for (cufftHandle* h : plans) if (*h) cufftDestroy(*h);
+    void* bufs[] = {c.st, c.acc_src, c.acc_dcu, c.r_src, c.r_out, c.r_dcu, c.r_et, c.k_src, c.k_out,
+                    c.k_dcu, c.k_et, c.gb_es, c.gb_dcu, c.gb_push, c.part_p, c.part_g, c.diag,
+                    c.bin_count, c.bin_off, c.bin_cursor, c.bin_idx, c.sort_tmp, c.fft_work};
+    for (void* b : bufs) if (b) cudaFree(b);
+    if (c.own_stream) cudaStreamDestroy(c.own_stream);
+}
+
+void drop_graph(Ctx& c) {
+    if (c.gexec) { cudaGraphExecDestroy(c.gexec); c.gexec = nullptr; }
+    if (c.graph) { cudaGraphDestroy(c.graph); c.graph = nullptr; }
+}
+
+void set_fft_stream(Ctx& c) {
+    cufftHandle plans[] = {c.p_r2c1, c.p_c2r1, c.p_r2cS, c.p_c2rO, c.p_r2c3, c.p_c2r3, c.p_r2c4};
+    for (cufftHandle h : plans) if (h) AW_CUFFT(cufftSetStream(h, c.stream));
+}
+
+void require_parts(Ctx& c) { need(c.parts.x != nullptr, AW_ERR_STATE, "particles not bound"); }
+
+// Deposit scales for unfused deposits: maxima of the current state, then scales.
+void static_scales(Ctx& c) {
+    launch_particle_max(c);
+    launch_make_scales(c);
+}
+
+// Fresh accumulators for an unfused operation (drops a pending fused deposit).
+void reset_acc(Ctx& c, unsigned long long* acc, int nf) {
+    AW_CUDA(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * static_cast<size_t>(nf) * c.geo.ncell, c.stream));
+    if (acc == c.acc_src) c.pending_valid = false;
+}
+
+// ---- the step body (no host syncs; capturable) --------------------------------
+void es_fields_from_pending(Ctx& c, bool step_begin) {
+    float* api[1] = {c.src.rho};
+    launch_finalize(c, c.acc_src, 0, 1, c.st->S_pend, c.r_src, api, false, true, step_begin);
+    AW_CUFFT(cufftExecR2C(c.p_r2cS, c.r_src, c.k_src));
+    launch_kspace_es(c, c.k_src, c.k_out);
+    AW_CUFFT(cufftExecC2R(c.p_c2rO, c.k_out, c.r_out));
+    launch_fields_es(c);
+}
+
+void darwin_fields_from_pending(Ctx& c, bool step_begin) {
+    float* api[8] = {c.src.rho, c.src.Jx, c.src.Jy, c.src.Jz, c.src.amu0, c.src.amu1, c.src.amu2, c.src.amu3};
+    launch_finalize(c, c.acc_src, 0, 8, c.st->S_pend, c.r_src, api, false, true, step_begin);
+    AW_CUFFT(cufftExecR2C(c.p_r2cS, c.r_src, c.k_src));
+    launch_kspace_elb(c, c.k_src, c.k_out);
+    AW_CUFFT(cufftExecC2R(c.p_c2rO, c.k_out, c.r_out));
+    launch_fields_dcu(c);
+    launch_deposit_dcu(c, c.gb_dcu);
+    float* apid[3] = {c.src.dcux, c.src.dcuy, c.src.dcuz};
+    launch_finalize(c, c.acc_dcu, 0, 3, c.st->S_dcu, c.r_dcu, apid, false, false, false);
+    AW_CUFFT(cufftExecR2C(c.p_r2c3, c.r_dcu, c.k_dcu));
+    launch_kspace_et(c, c.k_dcu, c.k_src + static_cast<size_t>(4) * c.sg.nk, c.k_et);
+    AW_CUFFT(cufftExecC2R(c.p_c2r3, c.k_et, c.r_et));
+    launch_fields_push(c);
+}
+
+void step_body(Ctx& c) {
+    if (c.model == AW_MODEL_ES) {
+        es_fields_from_pending(c, true);
+        launch_push_deposit_es(c);
+    } else {
+        darwin_fields_from_pending(c, true);
+        launch_push_deposit_em(c);
+    }
+    launch_diag_reduce(c, true);
+}
+
+void ensure_pending(Ctx& c) {
+    if (c.pending_valid) return;
+    // scales S_pend / S_next were set by aw_init or the last unfused deposit
+    launch_deposit_src(c, c.model == AW_MODEL_ES ? 1 : 8);
+    c.pending_valid = true;
+}
+
+}  // namespace
+}  // namespace aw
+
+using aw::Ctx;
+using aw::Error;
+using aw::guarded;
+
+struct aw_ctx { Ctx c; };
+
+extern "C" {
+
+const char* aw_version(void) { return "arcb200 0.1.0 (sm_100a)"; }
+
+int aw_last_error(char* buf, int32_t n) {
+    if (!buf || n <= 0) return AW_ERR_ARG;
+    std::snprintf(buf, static_cast<size_t>(n), "%s", aw::g_last_error.c_str());
+    return AW_OK;
+}
+
+int aw_ctx_create(const aw_grid* g, const aw_params* p, int32_t model, void* stream, aw_ctx** out) {
+    return guarded([&] {
+        aw::need(g && p && out, AW_ERR_ARG, "ctx_create: null argument");
+        aw::need(g->nx > 0 && g->ny > 0 && g->Lx > 0 && g->Ly > 0, AW_ERR_ARG, "ctx_create: bad grid");
+        aw::need(model == AW_MODEL_ES || model == AW_MODEL_DARWIN, AW_ERR_ARG, "ctx_create: bad model");
+        aw::need(static_cast<long long>(g->nx) * g->ny <= (1LL << 28), AW_ERR_ARG, "ctx_create: grid too large");
+        *out = nullptr;
+        std::unique_ptr<aw_ctx> h(new aw_ctx());
+        Ctx& c = h->c;
+        c.grid = *g;
+        c.prm = *p;
+        c.model = model;
+        c.geo.nx = g->nx; c.geo.ny = g->ny;
+        c.geo.nxf = static_cast<float>(g->nx); c.geo.nyf = static_cast<float>(g->ny);
+        c.geo.dx = g->Lx / g->nx; c.geo.dy = g->Ly / g->ny;
+        c.geo.ncell = g->nx * g->ny;
+        c.sg.nx = g->nx; c.sg.ny = g->ny; c.sg.nkx = g->nx / 2 + 1; c.sg.nk = c.sg.nkx * g->ny;
+        c.sg.dkx = 6.28318530717958647692 / g->Lx;
+        c.sg.dky = 6.28318530717958647692 / g->Ly;
+        c.sg.invN = 1.0f / static_cast<float>(c.geo.ncell);
+        if (stream) {
+            c.stream = static_cast<cudaStream_t>(stream);
+        } else {
+            AW_CUDA(cudaStreamCreate(&c.own_stream));
+            c.stream = c.own_stream;
+        }
+        try {
+            const size_t nc = c.geo.ncell, nk = c.sg.nk;
+            const int ns = c.nsrc(), no = c.nout();
+            aw::dalloc(c.st, 1);
+            AW_CUDA(cudaMemset(c.st, 0, sizeof(aw::DevState)));
+            aw::dalloc(c.diag, 1);
+            AW_CUDA(cudaMemset(c.diag, 0, sizeof(aw_diag)));
+            c.npart_g = aw::grid_partial_blocks();
+            aw::dalloc(c.part_g, static_cast<size_t>(c.npart_g) * 5);
+            AW_CUDA(cudaMemset(c.part_g, 0, sizeof(double) * c.npart_g * 5));
+            aw::dalloc(c.acc_src, static_cast<size_t>(ns) * nc);
+            AW_CUDA(cudaMemset(c.acc_src, 0, sizeof(unsigned long long) * ns * nc));
+            aw::dalloc(c.r_src, static_cast<size_t>(ns) * nc);
+            aw::dalloc(c.r_out, static_cast<size_t>(no) * nc);
+            aw::dalloc(c.k_src, static_cast<size_t>(ns) * nk);
+            aw::dalloc(c.k_out, static_cast<size_t>(no) * nk);
+            if (model == AW_MODEL_DARWIN) {
+                aw::dalloc(c.acc_dcu, 3 * nc);
+                AW_CUDA(cudaMemset(c.acc_dcu, 0, sizeof(unsigned long long) * 3 * nc));
+                aw::dalloc(c.r_dcu, 3 * nc);
+                aw::dalloc(c.r_et, 3 * nc);
+                aw::dalloc(c.k_dcu, 3 * nk);
+                aw::dalloc(c.k_et, 3 * nk);
+                aw::dalloc(c.gb_dcu, 8 * nc);
+                aw::dalloc(c.gb_push, 8 * nc);
+            } else {
+                aw::dalloc(c.gb_es, 2 * nc);
+                aw::dalloc(c.gb_dcu, 8 * nc);   // used by an unfused dcu deposit only
+            }
+            size_t ws = 0;
+            aw::make_plan(c.p_r2c1, g->ny, g->nx, CUFFT_R2C, 1, ws);
+            aw::make_plan(c.p_c2r1, g->ny, g->nx, CUFFT_C2R, 1, ws);
+            aw::make_plan(c.p_r2cS, g->ny, g->nx, CUFFT_R2C, ns, ws);
+            aw::make_plan(c.p_c2rO, g->ny, g->nx, CUFFT_C2R, no, ws);
+            if (model == AW_MODEL_DARWIN) {
+                aw::make_plan(c.p_r2c3, g->ny, g->nx, CUFFT_R2C, 3, ws);
+                aw::make_plan(c.p_c2r3, g->ny, g->nx, CUFFT_C2R, 3, ws);
+            }
+            if (ws) AW_CUDA(cudaMalloc(&c.fft_work, ws));
+            cufftHandle plans[] = {c.p_r2c1, c.p_c2r1, c.p_r2cS, c.p_c2rO, c.p_r2c3, c.p_c2r3};
+            for (cufftHandle ph : plans) if (ph) AW_CUFFT(cufftSetWorkArea(ph, c.fft_work));
+            c.plans_made = true;
+            aw::set_fft_stream(c);
+        } catch (...) {
+            aw::free_all(c);
+            throw;
+        }
+        *out = h.release();
+    });
+}
+
+int aw_ctx_destroy(aw_ctx* ctx) {
+    if (!ctx) return AW_OK;
+    aw::free_all(ctx->c);
+    delete ctx;
+    return AW_OK;
+}
+
+int aw_set_stream(aw_ctx* ctx, void* stream) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        aw::need(stream != nullptr || c.own_stream != nullptr, AW_ERR_ARG, "set_stream: null stream");
+        if (stream) c.stream = static_cast<cudaStream_t>(stream);
+        else c.stream = c.own_stream;
+        aw::set_fft_stream(c);
+    });
+}
+
+int aw_set_params(aw_ctx* ctx, const aw_params* p) {
+    return guarded([&] {
+        aw::need(ctx && p, AW_ERR_ARG, "null argument");
+        ctx->c.prm = *p;
+        aw::drop_graph(ctx->c);
+    });
+}
+
+int aw_particles_bind(aw_ctx* ctx, float* x, float* y, float* ux, float* uy, float* uz, float* w,
+                      int32_t* cell, int64_t n) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::need(n >= 0, AW_ERR_ARG, "particles_bind: negative n");
+        aw::need(n == 0 || (x && y && ux && uy && uz && w), AW_ERR_ARG, "particles_bind: null array");
+        aw::need(n < (1LL << 40), AW_ERR_ARG, "particles_bind: n too large");
+        Ctx& c = ctx->c;
+        c.parts.x = x; c.parts.y = y; c.parts.ux = ux; c.parts.uy = uy; c.parts.uz = uz;
+        c.parts.w = w; c.parts.cell = cell; c.parts.n = n;
+        auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+        c.parts.vec_ok = (al(x) && al(y) && al(ux) && al(uy) && al(uz) && al(w) && (!cell || al(cell))) ? 1 : 0;
+        const int nb = static_cast<int>(std::max<long long>(1, (n + aw::kChunk - 1) / aw::kChunk));
+        if (nb > c.npart_p) {
+            if (c.part_p) cudaFree(c.part_p);
+            c.part_p = nullptr;
+            aw::dalloc(c.part_p, static_cast<size_t>(nb) * 5);
+        }
+        c.npart_p = nb;
+        AW_CUDA(cudaMemsetAsync(c.part_p, 0, sizeof(double) * 5 * nb, c.stream));
+        c.pending_valid = false;
+        c.inited = false;
+        aw::drop_graph(c);
+    });
+}
+
+int aw_sources_bind(aw_ctx* ctx, const aw_source_ptrs* s) {
+    return guarded([&] {
+        aw::need(ctx && s, AW_ERR_ARG, "null argument");
+        ctx->c.src = *s;
+        aw::drop_graph(ctx->c);
+    });
+}
+
+int aw_fields_bind(aw_ctx* ctx, const aw_field_ptrs* f) {
+    return guarded([&] {
+        aw::need(ctx && f, AW_ERR_ARG, "null argument");
+        ctx->c.fld = *f;
+        aw::drop_graph(ctx->c);
+    });
+}
+
+int aw_load_species(aw_ctx* ctx, const aw_species* sp, int32_t nspecies, uint64_t seed, int32_t noisy) {
+    return guarded([&] {
+        aw::need(ctx && (sp || nspecies == 0), AW_ERR_ARG, "null argument");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        long long total = 0;
+        for (int i = 0; i < nspecies; ++i) {
+            aw::need(sp[i].ppc > 0, AW_ERR_ARG, "load_species: ppc must be positive");
+            total += static_cast<long long>(sp[i].ppc) * c.geo.ncell;
+        }
+        aw::need(total == c.parts.n, AW_ERR_ARG, "load_species: bound n != sum(ppc)*nx*ny");
+        long long base = 0;
+        for (int i = 0; i < nspecies; ++i) {
+            aw::launch_load_species(c, sp[i], i, base, seed, noisy);
+            base += static_cast<long long>(sp[i].ppc) * c.geo.ncell;
+        }
+        c.pending_valid = false;
+        c.inited = false;
+    });
+}
+
+// ---- unfused operators ---------------------------------------------------------
+
+int aw_deposit_rho(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        aw::need(c.src.rho != nullptr, AW_ERR_STATE, "deposit_rho: rho not bound");
+        aw::static_scales(c);
+        aw::reset_acc(c, c.acc_src, 1);
+        aw::launch_deposit_src(c, 1);
+        float* api[1] = {c.src.rho};
+        aw::launch_finalize(c, c.acc_src, 0, 1, c.st->S_pend, c.r_src, api, true, false, false);
+    });
+}
+
+int aw_deposit_rho_j(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        aw::need(c.model == AW_MODEL_DARWIN, AW_ERR_STATE, "deposit_rho_j: Darwin context required");
+        aw::need(c.src.rho && c.src.Jx && c.src.Jy && c.src.Jz, AW_ERR_STATE, "deposit_rho_j: rho/J not bound");
+        aw::static_scales(c);
+        aw::reset_acc(c, c.acc_src, 4);
+        aw::launch_deposit_src(c, 4);
+        float* api[4] = {c.src.rho, c.src.Jx, c.src.Jy, c.src.Jz};
+        aw::launch_finalize(c, c.acc_src, 0, 4, c.st->S_pend, c.r_src, api, true, false, false);
+    });
+}
+
+int aw_deposit_amu(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        aw::need(c.model == AW_MODEL_DARWIN, AW_ERR_STATE, "deposit_amu: Darwin context required");
+        aw::need(c.src.amu0 && c.src.amu1 && c.src.amu2 && c.src.amu3, AW_ERR_STATE, "deposit_amu: amu not bound");
+        aw::static_scales(c);
+        AW_CUDA(cudaMemsetAsync(c.acc_src + static_cast<size_t>(4) * c.geo.ncell, 0,
+                                sizeof(unsigned long long) * 4 * c.geo.ncell, c.stream));
+        c.pending_valid = false;
+        aw::launch_deposit_src(c, -4);
+        float* api[4] = {c.src.amu0, c.src.amu1, c.src.amu2, c.src.amu3};
+        aw::launch_finalize(c, c.acc_src, 4, 4, c.st->S_pend, c.r_src + static_cast<size_t>(4) * c.geo.ncell,
+                            api, true, false, false);
+    });
+}
+
+int aw_deposit_dcu(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        aw::need(c.model == AW_MODEL_DARWIN, AW_ERR_STATE, "deposit_dcu: Darwin context required");
+        aw::need(c.src.dcux && c.src.dcuy && c.src.dcuz, AW_ERR_STATE, "deposit_dcu: dcu not bound");
+        aw::launch_particle_max(c);
+        aw::launch_pack_em(c);
+        aw::reset_acc(c, c.acc_dcu, 3);
+        aw::launch_deposit_dcu(c, c.gb_dcu);
+        float* api[3] = {c.src.dcux, c.src.dcuy, c.src.dcuz};
+        aw::launch_finalize(c, c.acc_dcu, 0, 3, c.st->S_dcu, c.r_dcu, api, true, false, false);
+    });
+}
+
+int aw_push_es(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::require_parts(ctx->c);
+        aw::launch_push_es_plain(ctx->c, nullptr, 1.0f, true);
+        ctx->c.pending_valid = false;
+    });
+}
+
+int aw_push_em(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::require_parts(ctx->c);
+        aw::launch_push_em_plain(ctx->c, nullptr);
+        ctx->c.pending_valid = false;
+    });
+}
+
+int aw_half_step_back(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::require_parts(ctx->c);
+        aw::launch_push_es_plain(ctx->c, nullptr, -0.5f, false);
+    });
+}
+
+int aw_migrate(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::require_parts(ctx->c);
+        aw::launch_migrate(ctx->c);
+        ctx->c.pending_valid = false;
+    });
+}
+
+int aw_sort_tiles(aw_ctx* ctx, int32_t tx, int32_t ty, int32_t physical) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::need(tx > 0 && ty > 0, AW_ERR_ARG, "sort_tiles: bad tile size");
+        aw::require_parts(ctx->c);
+        aw::launch_sort_tiles(ctx->c, tx, ty, physical != 0);
+    });
+}
+
+int aw_tile_bins(aw_ctx* ctx, const int32_t** off, const int32_t** idx, int32_t* ntiles, int32_t* ntx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        aw::need(c.bin_ntiles > 0, AW_ERR_STATE, "tile_bins: no binning yet");
+        if (off) *off = c.bin_off;
+        if (idx) *idx = c.bin_physical ? nullptr : c.bin_idx;
+        if (ntiles) *ntiles = c.bin_ntiles;
+        if (ntx) *ntx = c.bin_ntx;
+    });
+}
+
+int aw_fft_r2c(aw_ctx* ctx, const float* in, void* kspace) {
+    return guarded([&] {
+        aw::need(ctx && in && kspace, AW_ERR_ARG, "null argument");
+        AW_CUFFT(cufftExecR2C(ctx->c.p_r2c1, const_cast<float*>(in), static_cast<cufftComplex*>(kspace)));
+    });
+}
+
+int aw_fft_c2r(aw_ctx* ctx, void* kspace, float* out) {
+    return guarded([&] {
+        aw::need(ctx && kspace && out, AW_ERR_ARG, "null argument");
+        Ctx& c = ctx->c;
+        AW_CUFFT(cufftExecC2R(c.p_c2r1, static_cast<cufftComplex*>(kspace), out));
+        aw::launch_scale_copy(c, out, out, c.geo.ncell, c.sg.invN);
+    });
+}
+
+int aw_solve_es(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        aw::need(c.src.rho && c.fld.Ex && c.fld.Ey, AW_ERR_STATE, "solve_es: rho/Ex/Ey not bound");
+        AW_CUFFT(cufftExecR2C(c.p_r2c1, c.src.rho, c.k_src));
+        aw::launch_es_solve_k(c, c.k_src, c.k_out, c.k_out + c.sg.nk);
+        AW_CUFFT(cufftExecC2R(c.p_c2r1, c.k_out, c.fld.Ex));
+        AW_CUFFT(cufftExecC2R(c.p_c2r1, c.k_out + c.sg.nk, c.fld.Ey));
+    });
+}
+
+static void solve_el_b_into(Ctx& c, float* ex, float* ey) {
+    const aw_source_ptrs& s = c.src;
+    aw::need(c.model == AW_MODEL_DARWIN, AW_ERR_STATE, "Darwin context required");
+    aw::need(s.rho && s.Jx && s.Jy && s.Jz, AW_ERR_STATE, "rho/J not bound");
+    aw::need(ex && ey && c.fld.Bx && c.fld.By && c.fld.Bz, AW_ERR_STATE, "E/B fields not bound");
+    const size_t nk = c.sg.nk;
+    AW_CUFFT(cufftExecR2C(c.p_r2c1, s.rho, c.k_src));
+    AW_CUFFT(cufftExecR2C(c.p_r2c1, s.Jx, c.k_src + nk));
+    AW_CUFFT(cufftExecR2C(c.p_r2c1, s.Jy, c.k_src + 2 * nk));
+    AW_CUFFT(cufftExecR2C(c.p_r2c1, s.Jz, c.k_src + 3 * nk));
+    aw::launch_kspace_elb(c, c.k_src, c.k_out);
+    float* outs[5] = {ex, ey, c.fld.Bx, c.fld.By, c.fld.Bz};
+    for (int f = 0; f < 5; ++f) AW_CUFFT(cufftExecC2R(c.p_c2r1, c.k_out + f * nk, outs[f]));
+}
+
+int aw_solve_darwin_el_b(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        solve_el_b_into(ctx->c, ctx->c.fld.ELx, ctx->c.fld.ELy);
+    });
+}
+
+int aw_solve_darwin(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        solve_el_b_into(c, c.fld.Ex, c.fld.Ey);
+        aw::need(c.fld.Ez != nullptr, AW_ERR_STATE, "solve_darwin: Ez not bound");
+        AW_CUDA(cudaMemsetAsync(c.fld.Ez, 0, sizeof(float) * c.geo.ncell, c.stream));
+    });
+}
+
+int aw_solve_darwin_et(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        const aw_source_ptrs& s = c.src;
+        aw::need(c.model == AW_MODEL_DARWIN, AW_ERR_STATE, "Darwin context required");
+        aw::need(s.dcux && s.dcuy && s.dcuz && s.amu0 && s.amu1 && s.amu2 && s.amu3, AW_ERR_STATE,
+                 "solve_darwin_et: dcu/amu not bound");
+        aw::need(c.fld.ETx && c.fld.ETy && c.fld.ETz, AW_ERR_STATE, "solve_darwin_et: ET not bound");
+        const size_t nk = c.sg.nk;
+        const float* ins[3] = {s.dcux, s.dcuy, s.dcuz};
+        for (int f = 0; f < 3; ++f) AW_CUFFT(cufftExecR2C(c.p_r2c1, const_cast<float*>(ins[f]), c.k_dcu + f * nk));
+        const float* am[4] = {s.amu0, s.amu1, s.amu2, s.amu3};
+        for (int f = 0; f < 4; ++f)
+            AW_CUFFT(cufftExecR2C(c.p_r2c1, const_cast<float*>(am[f]), c.k_src + (4 + f) * nk));
+        aw::launch_kspace_et(c, c.k_dcu, c.k_src + 4 * nk, c.k_et);
+        float* outs[3] = {c.fld.ETx, c.fld.ETy, c.fld.ETz};
+        for (int f = 0; f < 3; ++f) AW_CUFFT(cufftExecC2R(c.p_c2r1, c.k_et + f * nk, outs[f]));
+    });
+}
+
+int aw_form_e(aw_ctx* ctx, float et_scale) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::launch_form_e(ctx->c, et_scale);
+    });
+}
+
+int aw_add_b0(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::launch_add_b0(ctx->c);
+    });
+}
+
+int aw_add_pump(aw_ctx* ctx, double t) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::launch_add_pump(ctx->c, t);
+    });
+}
+
+// ---- the fused step -------------------------------------------------------------
+
+int aw_init(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        aw::drop_graph(c);
+        aw::launch_set_step(c, 0);
+        aw::launch_particle_max(c);
+        aw::launch_copy_umax(c);     // the step-begin copies umax -> ucur
+        aw::launch_make_scales(c);
+        aw::reset_acc(c, c.acc_src, c.nsrc());
+        if (c.model == AW_MODEL_ES) {
+            aw::launch_deposit_src(c, 1);
+            aw::es_fields_from_pending(c, false);
+            // u -> u(-dt/2), gathering E(x^0) from the solve's output
+            aw::launch_push_es_from(c, c.r_out, c.r_out + c.geo.ncell, -0.5f, false);
+            aw::launch_particle_max(c);
+            aw::launch_copy_umax(c);
+            aw::launch_deposit_src(c, 1);    // pending rho(x^0) for step 0
+        } else {
+            aw::launch_deposit_src(c, 8);
+            aw::darwin_fields_from_pending(c, true);   // t = 0 fields
+            aw::launch_copy_umax(c);
+            aw::launch_deposit_src(c, 8);              // pending rho,J,amu for step 0
+        }
+        c.pending_valid = true;
+        aw::launch_set_step(c, 0);
+        AW_CUDA(cudaStreamSynchronize(c.stream));
+        c.inited = true;
+    });
+}
+
+int aw_step(aw_ctx* ctx, int64_t n) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        aw::ensure_pending(c);
+        aw::launch_set_step(c, n);
+        aw::step_body(c);
+    });
+}
+
+int aw_run(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::need(nsteps >= 0, AW_ERR_ARG, "run: negative nsteps");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        aw::ensure_pending(c);
+        aw::launch_set_step(c, n0);
+        if (!use_graph) {
+            for (int64_t i = 0; i < nsteps; ++i) aw::step_body(c);
+            return;
+        }
+        if (!c.gexec) {
+            AW_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+            try {
+                aw::step_body(c);
+            } catch (...) {
+                cudaGraph_t g = nullptr;
+                cudaStreamEndCapture(c.stream, &g);
+                if (g) cudaGraphDestroy(g);
+                throw;
+            }
+            AW_CUDA(cudaStreamEndCapture(c.stream, &c.graph));
+            AW_CUDA(cudaGraphInstantiate(&c.gexec, c.graph, 0));
+        }
+        for (int64_t i = 0; i < nsteps; ++i) AW_CUDA(cudaGraphLaunch(c.gexec, c.stream));
+    });
+}
+
+// ---- diagnostics / status -----------------------------------------------------------
+
+int aw_reduce_fp64(aw_ctx* ctx, aw_diag* out) {
+    return guarded([&] {
+        aw::need(ctx && out, AW_ERR_ARG, "null argument");
+        Ctx& c = ctx->c;
+        const bool parts = c.parts.x != nullptr && c.parts.n > 0;
+        if (parts) aw::launch_particle_diag(c);
+        aw::launch_grid_diag(c);
+        aw::launch_diag_reduce(c, parts);
+        AW_CUDA(cudaMemcpyAsync(out, c.diag, sizeof(aw_diag), cudaMemcpyDeviceToHost, c.stream));
+        AW_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int aw_step_diag(aw_ctx* ctx, aw_diag* out) {
+    return guarded([&] {
+        aw::need(ctx && out, AW_ERR_ARG, "null argument");
+        Ctx& c = ctx->c;
+        AW_CUDA(cudaMemcpyAsync(out, c.diag, sizeof(aw_diag), cudaMemcpyDeviceToHost, c.stream));
+        AW_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int aw_step_diag_device(aw_ctx* ctx, const aw_diag** dev_ptr) {
+    return guarded([&] {
+        aw::need(ctx && dev_ptr, AW_ERR_ARG, "null argument");
+        *dev_ptr = ctx->c.diag;
+    });
+}
+
+int aw_error_word(aw_ctx* ctx, uint32_t* out) {
+    return guarded([&] {
+        aw::need(ctx && out, AW_ERR_ARG, "null argument");
+        Ctx& c = ctx->c;
+        unsigned v = 0;
+        AW_CUDA(cudaMemcpyAsync(&v, &c.st->err, sizeof(unsigned), cudaMemcpyDeviceToHost, c.stream));
+        AW_CUDA(cudaMemsetAsync(&c.st->err, 0, sizeof(unsigned), c.stream));
+        AW_CUDA(cudaStreamSynchronize(c.stream));
+        *out = v;
+    });
+}
+
+int aw_stats(aw_ctx* ctx, aw_stats_t* out) {
+    return guarded([&] {
+        aw::need(ctx && out, AW_ERR_ARG, "null argument");
+        Ctx& c = ctx->c;
+        aw::DevState h{};
+        AW_CUDA(cudaMemcpyAsync(&h, c.st, sizeof(h), cudaMemcpyDeviceToHost, c.stream));
+        AW_CUDA(cudaStreamSynchronize(c.stream));
+        out->chunks = static_cast<int64_t>(h.chunks);
+        out->window_overflow = static_cast<int64_t>(h.overflow);
+        out->slow_deposits = static_cast<int64_t>(h.slow);
+        out->steps = h.step;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,414 @@
+// aw_device.cuh — device-side building blocks of the B200 PIC hot path.
+//
+// Contents:
+//   * Geo / DevState        — POD kernel arguments and the small device-resident
+//                             state block that lets a captured CUDA graph run step
+//                             after step without host involvement.
+//   * cic / gather / boris  — the CIC stencil and Boris arithmetic, written as
+//                             explicit FP32 operation sequences (__fmaf_rn,
+//                             __fmul_rn, ...) so the C oracle can restate them
+//                             bit for bit.
+//   * fixed-point deposit   — contributions are rounded to integers
+//                             q = rint(v * S) with a per-field power-of-two scale
+//                             S and summed in 64-bit integers, so a deposit is a
+//                             function of the particle SET, independent of order,
+//                             thread mapping or atomics scheduling.
+//   * WinDep                — the chunk-window deposit engine: one CTA owns a
+//                             chunk of CHUNK consecutive particles, reduces the
+//                             bounding box of their cells, privatises that window
+//                             of cells in shared memory as int64 accumulators,
+//                             adds register-accumulated runs of same-cell
+//                             contributions with shared atomics and flushes the
+//                             window to the global int64 accumulators with
+//                             red.global.add.u64.
+//
+// Reference arithmetic being mirrored (paths relative to the ArcWarden tree):
+//   CIC weights           include/pic/grid.hpp:135-155, depositor.hpp:136-146
+//   gather                include/pic/pusher.hpp:35-43, 247-250
+//   Boris                 include/pic/pusher.hpp:47-109
+//   move (double product) include/pic/pusher.hpp:126-127, 255-256
+//   migrate               include/pic/particles.hpp:294-315
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace aw {
+
+constexpr int kThreads = 256;          // CTA size of every particle kernel
+constexpr int kPPT     = 8;            // consecutive particles per thread
+constexpr int kChunk   = kThreads * kPPT;   // particles per CTA chunk (2048)
+
+// Fast-path range of one quantised contribution: |v*S| < 2^22 rounds exactly
+// with one FADD against 1.5*2^23 and fits a 32-bit run accumulator.
+constexpr float kFastLim   = 4194304.0f;      // 2^22
+constexpr float kMagic     = 12582912.0f;     // 1.5 * 2^23
+constexpr int   kMagicBits = 0x4B400000;
+
+// Geometry passed by value into every kernel.
+struct Geo {
+    int    nx, ny;
+    float  nxf, nyf;
+    double dx, dy;
+    int    ncell;
+};
+
+// Device-resident state block (one per context). The fused step's kernels hand
+// values to each other through it so the whole step can be replayed from a CUDA
+// graph: scales, maxima, the step counter and the error word.
+struct DevState {
+    long long step;            // index n of the next fused step
+    double    t;               // n * dt of the step being computed
+    unsigned  err;             // AW_DEV_* bits
+    unsigned  umax_bits[3];    // max |u_d| of the state written by the last push
+    unsigned  ucur_bits[3];    // max |u_d| of the current particle state (copied)
+    unsigned  emax_bits;       // max |E component| of the dcu gather field
+    unsigned  bmax_bits;       // max |B component|
+    float     S_next[8];       // scales the next source deposit will use
+    float     S_pend[8];       // scales of the pending (not yet finalised) deposit
+    float     S_dcu[4];        // scale of the pending dcu deposit (x3, same value)
+    float     coef_max;        // max |qm w / (dx dy)| over particles
+    float     pad0;
+    unsigned long long chunks, overflow, slow;
+};
+
+// ---------------------------------------------------------------------------
+// small helpers
+__device__ __forceinline__ int wrap_once(int i, int n) {
+    if (i >= n) i -= n;
+    if (i < 0) i += n;
+    return i;
+}
+__device__ __forceinline__ int wrap_far(int i, int n) {
+    i %= n;
+    if (i < 0) i += n;
+    return i;
+}
+// signed offset in [-n/2, n/2) for |d| < n
+__device__ __forceinline__ int wrap_signed(int d, int n) {
+    if (d >= (n >> 1)) d -= n;
+    if (d < -(n >> 1)) d += n;
+    return d;
+}
+__device__ __forceinline__ void atomic_max_abs(unsigned* p, float v) {
+    atomicMax(p, __float_as_uint(fabsf(v)));   // |v| >= 0: uint order == float order
+}
+__device__ __forceinline__ void set_err(DevState* st, unsigned bits) {
+    atomicOr(&st->err, bits);
+}
+
+// Power-of-two scale S such that bound * S < 2^22 (the fast path), from a
+// positive bound. Deterministic: a pure function of the bound.
+__host__ __device__ inline float scale_for_bound(float bound) {
+    if (!(bound > 0.0f) || !(bound < 3.0e38f)) return 1.0f;
+    int e;
+    frexpf(bound, &e);            // bound in [2^(e-1), 2^e)
+    int k = 22 - e;               // bound * 2^k < 2^22
+    if (k > 120) k = 120;
+    if (k < -120) k = -120;
+    return ldexpf(1.0f, k);
+}
+
+// ---------------------------------------------------------------------------
+// CIC stencil — include/pic/grid.hpp:135-155. Positions are in cell units and
+// already inside [0,nx)x[0,ny), so the int conversion is the floor.
+struct Cic {
+    int   i0, j0;
+    float w0, w1, w2, w3;
+};
+__device__ __forceinline__ Cic cic(float x, float y) {
+    Cic s;
+    s.i0 = static_cast<int>(x);
+    s.j0 = static_cast<int>(y);
+    const float fx = __fsub_rn(x, static_cast<float>(s.i0));
+    const float fy = __fsub_rn(y, static_cast<float>(s.j0));
+    const float gx = __fsub_rn(1.0f, fx);
+    const float gy = __fsub_rn(1.0f, fy);
+    s.w0 = __fmul_rn(gx, gy);
+    s.w1 = __fmul_rn(fx, gy);
+    s.w2 = __fmul_rn(gx, fy);
+    s.w3 = __fmul_rn(fx, fy);
+    return s;
+}
+// four-term gather in the reference order: ((w0 a + w1 b) + w2 c) + w3 d
+__device__ __forceinline__ float gather4(const Cic& s, float a, float b, float c, float d) {
+    float r = __fmul_rn(s.w0, a);
+    r = __fmaf_rn(s.w1, b, r);
+    r = __fmaf_rn(s.w2, c, r);
+    r = __fmaf_rn(s.w3, d, r);
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// Boris rotation about (bx,by,bz) with qmh = (q/m) dt/2 — pusher.hpp:85-97.
+__device__ __forceinline__ void boris_rotate(float& ux, float& uy, float& uz,
+                                             float bx, float by, float bz, float qmh) {
+    const float tx = __fmul_rn(qmh, bx), ty = __fmul_rn(qmh, by), tz = __fmul_rn(qmh, bz);
+    const float t2 = __fmaf_rn(tz, tz, __fmaf_rn(ty, ty, __fmul_rn(tx, tx)));
+    const float sf = __fdiv_rn(2.0f, __fadd_rn(1.0f, t2));
+    const float sx = __fmul_rn(sf, tx), sy = __fmul_rn(sf, ty), sz = __fmul_rn(sf, tz);
+    const float upx = __fadd_rn(ux, __fmaf_rn(uy, tz, -__fmul_rn(uz, ty)));
+    const float upy = __fadd_rn(uy, __fmaf_rn(uz, tx, -__fmul_rn(ux, tz)));
+    const float upz = __fadd_rn(uz, __fmaf_rn(ux, ty, -__fmul_rn(uy, tx)));
+    ux = __fadd_rn(ux, __fmaf_rn(upy, sz, -__fmul_rn(upz, sy)));
+    uy = __fadd_rn(uy, __fmaf_rn(upz, sx, -__fmul_rn(upx, sz)));
+    uz = __fadd_rn(uz, __fmaf_rn(upx, sy, -__fmul_rn(upy, sx)));
+}
+// ES velocity update over dt_eff with uniform B0 — pusher.hpp:47-80 (Ez = 0).
+__device__ __forceinline__ void boris_es(float& ux, float& uy, float& uz, float ex, float ey,
+                                         float qmh, bool has_b0, float b0x, float b0y, float b0z) {
+    ux = __fmaf_rn(qmh, ex, ux);
+    uy = __fmaf_rn(qmh, ey, uy);
+    if (has_b0) boris_rotate(ux, uy, uz, b0x, b0y, b0z, qmh);
+    ux = __fmaf_rn(qmh, ex, ux);
+    uy = __fmaf_rn(qmh, ey, uy);
+}
+// Full Boris with gathered E and B — pusher.hpp:103-109.
+__device__ __forceinline__ void boris_em(float& ux, float& uy, float& uz,
+                                         float ex, float ey, float ez,
+                                         float bx, float by, float bz, float qmh) {
+    ux = __fmaf_rn(qmh, ex, ux); uy = __fmaf_rn(qmh, ey, uy); uz = __fmaf_rn(qmh, ez, uz);
+    boris_rotate(ux, uy, uz, bx, by, bz, qmh);
+    ux = __fmaf_rn(qmh, ex, ux); uy = __fmaf_rn(qmh, ey, uy); uz = __fmaf_rn(qmh, ez, uz);
+}
+// Move in cell units: x += float(double(u) * dt / dx) — pusher.hpp:126-127.
+__device__ __forceinline__ float move1(float x, float u, double dt, double d) {
+    return __fadd_rn(x, __double2float_rn(__ddiv_rn(__dmul_rn(static_cast<double>(u), dt), d)));
+}
+// Periodic wrap of a position — particles.hpp:301-306.
+__device__ __forceinline__ float wrap_pos(float x, float n) {
+    x = fmodf(x, n);
+    if (x < 0.0f) x = __fadd_rn(x, n);
+    if (x >= n) x = 0.0f;
+    return x;
+}
+// Owning cell index of a wrapped position — particles.hpp:310-314.
+__device__ __forceinline__ int cell_of(float x, float y, int nx, int ny) {
+    int ci = static_cast<int>(floorf(x));
+    int cj = static_cast<int>(floorf(y));
+    if (ci >= nx) ci = nx - 1;
+    if (cj >= ny) cj = ny - 1;
+    return cj * nx + ci;
+}
+
+// ---------------------------------------------------------------------------
+// Fixed-point rounding. q = rint(t) with t = v*S already scaled; exact for the
+// fast path (|t| < 2^22) and identical to llrintf(t) in the C oracle.
+__device__ __forceinline__ int quant_fast(float t) {
+    return __float_as_int(__fadd_rn(t, kMagic)) - kMagicBits;
+}
+
+// ---------------------------------------------------------------------------
+// Particle SoA pointers.
+struct Parts {
+    float *x, *y, *ux, *uy, *uz, *w;
+    int*   cell;
+    long long n;
+    int   vec_ok;     // all arrays 16-byte aligned
+};
+
+// Load / store kPPT consecutive floats starting at `base` (vectorised when the
+// whole run is in range and aligned; scalar and bounds-checked otherwise).
+__device__ __forceinline__ void load8(const float* __restrict__ a, long long base, long long n,
+                                      bool vec, float (&v)[kPPT]) {
+    if (vec && base + kPPT <= n) {
+        const float4 p = __ldg(reinterpret_cast<const float4*>(a + base));
+        const float4 q = __ldg(reinterpret_cast<const float4*>(a + base + 4));
+        v[0] = p.x; v[1] = p.y; v[2] = p.z; v[3] = p.w;
+        v[4] = q.x; v[5] = q.y; v[6] = q.z; v[7] = q.w;
+    } else {
+#pragma unroll
+        for (int k = 0; k < kPPT; ++k) v[k] = (base + k < n) ? a[base + k] : 0.0f;
+    }
+}
+__device__ __forceinline__ void store8(float* __restrict__ a, long long base, long long n,
+                                       bool vec, const float (&v)[kPPT]) {
+    if (vec && base + kPPT <= n) {
+        reinterpret_cast<float4*>(a + base)[0] = make_float4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<float4*>(a + base)[1] = make_float4(v[4], v[5], v[6], v[7]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kPPT; ++k) if (base + k < n) a[base + k] = v[k];
+    }
+}
+__device__ __forceinline__ void store8i(int* __restrict__ a, long long base, long long n,
+                                        bool vec, const int (&v)[kPPT]) {
+    if (vec && base + kPPT <= n) {
+        reinterpret_cast<int4*>(a + base)[0] = make_int4(v[0], v[1], v[2], v[3]);
+        reinterpret_cast<int4*>(a + base)[1] = make_int4(v[4], v[5], v[6], v[7]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kPPT; ++k) if (base + k < n) a[base + k] = v[k];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Chunk-window deposit engine.
+//
+// NF fields are deposited. Per particle the caller supplies the base cell
+// (i0, j0), the four CIC weights and NF coefficients already multiplied by the
+// field scales; contribution (f, corner c) = rint(coef[f] * w[c]).
+//
+// Shared memory: WMAXC cells x NF int64, AoS [cell][NF].
+template <int NF, int WMAXC>
+struct WinDep {
+    static constexpr int kSmemBytes = WMAXC * NF * 8;
+
+    long long* sacc;      // shared accumulators
+    int  ir, jr;          // reference cell (any cell near the chunk)
+    int  mi, mj;          // window origin offset (min wrapped offset)
+    int  W, H;            // window extent in cells
+    bool use;             // window fits shared memory
+
+    // Block-wide bounding box of the wrapped cell offsets of the valid particles.
+    // `red` is 8 ints of shared scratch per warp (kThreads/32 * 4).
+    __device__ void setup(const int (&ci)[kPPT], const int (&cj)[kPPT], const bool (&ok)[kPPT],
+                          int ir_, int jr_, const Geo& g, int* red) {
+        ir = ir_; jr = jr_;
+        int lo_i = 1 << 30, lo_j = 1 << 30, hi_i = -(1 << 30), hi_j = -(1 << 30);
+#pragma unroll
+        for (int k = 0; k < kPPT; ++k) {
+            if (ok[k]) {
+                const int di = wrap_signed(ci[k] - ir, g.nx);
+                const int dj = wrap_signed(cj[k] - jr, g.ny);
+                lo_i = min(lo_i, di); hi_i = max(hi_i, di);
+                lo_j = min(lo_j, dj); hi_j = max(hi_j, dj);
+            }
+        }
+        lo_i = __reduce_min_sync(0xffffffffu, lo_i);
+        lo_j = __reduce_min_sync(0xffffffffu, lo_j);
+        hi_i = __reduce_max_sync(0xffffffffu, hi_i);
+        hi_j = __reduce_max_sync(0xffffffffu, hi_j);
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (lane == 0) {
+            red[warp * 4 + 0] = lo_i; red[warp * 4 + 1] = lo_j;
+            red[warp * 4 + 2] = hi_i; red[warp * 4 + 3] = hi_j;
+        }
+        __syncthreads();
+        lo_i = red[0]; lo_j = red[1]; hi_i = red[2]; hi_j = red[3];
+#pragma unroll
+        for (int w = 1; w < kThreads / 32; ++w) {
+            lo_i = min(lo_i, red[w * 4 + 0]); lo_j = min(lo_j, red[w * 4 + 1]);
+            hi_i = max(hi_i, red[w * 4 + 2]); hi_j = max(hi_j, red[w * 4 + 3]);
+        }
+        if (hi_i < lo_i) { lo_i = hi_i = 0; lo_j = hi_j = 0; }   // no valid particle
+        mi = lo_i; mj = lo_j;
+        W = hi_i - lo_i + 2;
+        H = hi_j - lo_j + 2;
+        use = (static_cast<long long>(W) * H <= WMAXC);
+    }
+    // zero the used part of the window; caller syncs afterwards
+    __device__ void zero() {
+        if (!use) return;
+        const int m = W * H * NF;
+        for (int i = threadIdx.x; i < m; i += kThreads) sacc[i] = 0;
+    }
+    __device__ __forceinline__ int wcell(int ci, int cj, const Geo& g) const {
+        return (wrap_signed(cj - jr, g.ny) - mj) * W + (wrap_signed(ci - ir, g.nx) - mi);
+    }
+    // Flush the window into the global accumulators acc[f*ncell + cell].
+    // Caller syncs before calling.
+    __device__ void flush(unsigned long long* __restrict__ acc, const Geo& g) {
+        if (!use) return;
+        const int m = W * H;
+        for (int c = threadIdx.x; c < m; c += kThreads) {
+            const int wi = c % W, wj = c / W;
+            const int gc = wrap_far(jr + mj + wj, g.ny) * g.nx + wrap_far(ir + mi + wi, g.nx);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const long long v = sacc[c * NF + f];
+                if (v != 0) atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gc,
+                                      static_cast<unsigned long long>(v));
+            }
+        }
+    }
+};
+
+// Per-thread run accumulator: contributions of consecutive particles that share
+// the same base cell are summed exactly in 32-bit registers (each fast-path value
+// is < 2^22 in magnitude and a run holds at most kPPT particles).
+template <int NF>
+struct Run {
+    int cw;              // window cell of the run's base corner, -1 = empty
+    int a[NF][4];
+
+    __device__ __forceinline__ void clear() {
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) a[f][c] = 0;
+    }
+    // Add the run into the shared window. Corners are visited in a lane-rotated
+    // order so lanes that flush the same cell at once touch different addresses.
+    __device__ __forceinline__ void flush(long long* __restrict__ s, int W) {
+        if (cw < 0) return;
+        const int r = threadIdx.x & 3;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = (q + r) & 3;
+            const int off = (c == 0) ? 0 : (c == 1) ? 1 : (c == 2) ? W : W + 1;
+            long long* base = s + static_cast<size_t>(cw + off) * NF;
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const int v = (c == 0) ? a[f][0] : (c == 1) ? a[f][1] : (c == 2) ? a[f][2] : a[f][3];
+                if (v != 0)
+                    atomicAdd(reinterpret_cast<unsigned long long*>(base + f),
+                              static_cast<unsigned long long>(static_cast<long long>(v)));
+            }
+        }
+    }
+};
+
+// Deposit one particle through the window (or, when the window is unused, the
+// exact global slow path). coefS[f] = coefficient * scale; cells c0..c3 are the
+// wrapped global corner cells (needed only for the slow path).
+template <int NF, int WMAXC>
+__device__ __forceinline__ void deposit_particle(WinDep<NF, WMAXC>& win, Run<NF>& run,
+                                                 const Cic& s, const float (&coefS)[NF],
+                                                 int gc0, int gc1, int gc2, int gc3,
+                                                 unsigned long long* __restrict__ gacc,
+                                                 const Geo& g, DevState* st,
+                                                 unsigned long long& nslow) {
+    const float wv[4] = {s.w0, s.w1, s.w2, s.w3};
+    const int   gcs[4] = {gc0, gc1, gc2, gc3};
+    if (win.use) {
+        const int cw = win.wcell(s.i0, s.j0, g);
+        if (cw != run.cw) {
+            run.flush(win.sacc, win.W);
+            run.cw = cw;
+            run.clear();
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float t = __fmul_rn(coefS[f], wv[c]);
+                if (fabsf(t) < kFastLim) {
+                    run.a[f][c] += quant_fast(t);
+                } else {
+                    if (!isfinite(t)) set_err(st, 1u);
+                    ++nslow;
+                    atomicAdd(gacc + static_cast<size_t>(f) * g.ncell + gcs[c],
+                              static_cast<unsigned long long>(__float2ll_rn(t)));
+                }
+            }
+        }
+    } else {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float t = __fmul_rn(coefS[f], wv[c]);
+                if (!isfinite(t)) set_err(st, 1u);
+                ++nslow;
+                const long long q = (fabsf(t) < kFastLim) ? static_cast<long long>(quant_fast(t))
+                                                          : __float2ll_rn(t);
+                if (q != 0)
+                    atomicAdd(gacc + static_cast<size_t>(f) * g.ncell + gcs[c],
+                              static_cast<unsigned long long>(q));
+            }
+        }
+    }
+}
+
+}  // namespace aw

@@ -1,0 +1,157 @@
+// aw_internal.h — host-side context of libarcb200 and the kernel launchers the
+// C ABI (aw_abi.cu) sequences. Not part of the public interface.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/arcb200.h"
+#include "aw_device.cuh"
+
+namespace aw {
+
+// Error carrying an aw status code; converted to the return value at the ABI.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+void check_cuda(cudaError_t e, const char* what, const char* file, int line);
+void check_cufft(cufftResult r, const char* what, const char* file, int line);
+#define AW_CUDA(x) ::aw::check_cuda((x), #x, __FILE__, __LINE__)
+#define AW_CUFFT(x) ::aw::check_cufft((x), #x, __FILE__, __LINE__)
+#define AW_LAUNCH() ::aw::check_cuda(cudaPeekAtLastError(), "kernel launch", __FILE__, __LINE__)
+
+// Field-kernel parameters (k-space + real-space finalisers).
+struct SpecGeo {
+    int    nx, ny, nkx, nk;      // nk = nkx*ny complex elements
+    double dkx, dky;
+    float  invN;                 // 1/(nx*ny), a power of two for the config grids
+};
+
+// Pump parameters (RunParams pump_*; include/pic/pump.hpp:27-47).
+struct PumpP {
+    int    on;
+    double ex, ey, ez, k0, w0, trmp, toff;
+};
+
+// Gather buffers: interleaved per-cell field values, 8 floats per cell for the
+// EM path ([Ex Ey Ez Bx | By Bz 0 0]) and 2 floats per cell for ES ([Ex Ey]).
+// One 32-byte sector per cell, read with two LDG.128 per CIC corner.
+
+struct Ctx {
+    // configuration
+    aw_grid   grid{};
+    aw_params prm{};
+    int       model = AW_MODEL_ES;
+    Geo       geo{};
+    SpecGeo   sg{};
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+
+    // bound caller memory
+    Parts           parts{};
+    aw_source_ptrs  src{};
+    aw_field_ptrs   fld{};
+
+    // device state
+    DevState* st = nullptr;
+
+    // fixed-point accumulators [NF][ncell] int64 (sources: rho,Jx,Jy,Jz,amu0..3)
+    unsigned long long* acc_src = nullptr;   // 8 * ncell
+    unsigned long long* acc_dcu = nullptr;   // 3 * ncell
+    // real staging (contiguous for batched cuFFT)
+    float* r_src = nullptr;     // 8 * ncell
+    float* r_out = nullptr;     // 5 * ncell (ES: Ex,Ey; Darwin: ELx,ELy,Bx,By,Bz)
+    float* r_dcu = nullptr;     // 3 * ncell
+    float* r_et  = nullptr;     // 3 * ncell
+    // k-space
+    cufftComplex* k_src = nullptr;   // 8 * nk
+    cufftComplex* k_out = nullptr;   // 5 * nk
+    cufftComplex* k_dcu = nullptr;   // 3 * nk
+    cufftComplex* k_et  = nullptr;   // 3 * nk
+    // gather buffers
+    float* gb_es   = nullptr;   // 2 * ncell
+    float* gb_dcu  = nullptr;   // 8 * ncell
+    float* gb_push = nullptr;   // 8 * ncell
+    // diagnostics partials and result
+    double* part_p = nullptr;   // particle partials [nblk][5]
+    double* part_g = nullptr;   // grid partials [nblk][5]
+    int     npart_p = 0, npart_g = 0;
+    aw_diag* diag = nullptr;    // device aw_diag
+    // tile binning scratch
+    int* bin_count = nullptr; int* bin_off = nullptr; int* bin_cursor = nullptr;
+    int* bin_idx = nullptr;   long long bin_idx_n = 0;
+    int  bin_ntiles = 0, bin_ntx = 0, bin_tx = 0, bin_ty = 0, bin_cap = 0;
+    bool bin_physical = false;
+    float* sort_tmp = nullptr; long long sort_tmp_n = 0;   // 7 arrays of n
+    // scales for unfused deposits
+    bool have_static_scales = false;
+
+    // cuFFT plans
+    cufftHandle p_r2c1 = 0, p_c2r1 = 0;     // single field
+    cufftHandle p_r2cS = 0;                 // sources batch (ES 1, Darwin 8)
+    cufftHandle p_c2rO = 0;                 // outputs batch (ES 2, Darwin 5)
+    cufftHandle p_r2c3 = 0, p_c2r3 = 0;     // dcu / E_T batch 3
+    cufftHandle p_r2c4 = 0;                 // rho+J batch 4 (unfused solve)
+    void* fft_work = nullptr;
+    bool plans_made = false;
+
+    // graph
+    cudaGraph_t     graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    bool inited = false;
+    bool pending_valid = false;       // acc_src holds the deposit of the current state
+    long long host_step = 0;
+    int write_cell = 1;
+
+    int nsrc() const { return model == AW_MODEL_DARWIN ? 8 : 1; }
+    int nout() const { return model == AW_MODEL_DARWIN ? 5 : 2; }
+};
+
+// ---- launchers (aw_particles.cu) -------------------------------------------
+void launch_load_species(Ctx& c, const aw_species& sp, int index, long long base,
+                         uint64_t seed, int noisy);
+void launch_migrate(Ctx& c);
+// Gathers from the caller's Ex/Ey; dt_scale = 1 (push) or -0.5 (half-step back).
+void launch_push_es_plain(Ctx& c, const float* unused, float dt_scale, bool move);
+void launch_push_es_from(Ctx& c, const float* ex, const float* ey, float dt_scale, bool move);
+void launch_push_em_plain(Ctx& c, const float* unused);
+void launch_particle_max(Ctx& c);                  // ucur_bits, coef_max
+void launch_sort_tiles(Ctx& c, int tx, int ty, bool physical);
+void launch_particle_diag(Ctx& c);                 // KE, P partials -> part_p
+
+// ---- launchers (aw_deposit.cu) --------------------------------------------
+// which: 1 = rho, 4 = rho+J, -4 = amu (fields 4..7), 8 = rho+J+amu
+void launch_deposit_src(Ctx& c, int which);
+void launch_deposit_dcu(Ctx& c, const float* gb);
+void launch_push_deposit_es(Ctx& c);
+void launch_push_deposit_em(Ctx& c);
+
+// ---- launchers (aw_spectral.cu) -------------------------------------------
+int  grid_partial_blocks();
+void launch_make_scales(Ctx& c);
+void launch_finalize(Ctx& c, unsigned long long* acc, int first, int nf, const float* S, float* r,
+                     float* const* api, bool accumulate, bool charge_partials, bool step_begin);
+void launch_kspace_es(Ctx& c, const cufftComplex* rho_k, cufftComplex* e_k);
+void launch_es_solve_k(Ctx& c, const cufftComplex* rho_k, cufftComplex* ex_k, cufftComplex* ey_k);
+void launch_kspace_elb(Ctx& c, const cufftComplex* src_k, cufftComplex* out_k);
+void launch_kspace_et(Ctx& c, const cufftComplex* dcu_k, const cufftComplex* amu_k, cufftComplex* et_k);
+void launch_fields_es(Ctx& c);
+void launch_fields_dcu(Ctx& c);
+void launch_fields_push(Ctx& c);
+void launch_diag_reduce(Ctx& c, bool with_particles);
+void launch_scale_copy(Ctx& c, float* dst, const float* src, int n, float s);
+void launch_form_e(Ctx& c, float et_scale);
+void launch_add_b0(Ctx& c);
+void launch_add_pump(Ctx& c, double t);
+void launch_pack_em(Ctx& c);
+void launch_grid_diag(Ctx& c);
+void launch_set_step(Ctx& c, long long n);
+void launch_copy_umax(Ctx& c);
+
+}  // namespace aw

@@ -1,0 +1,586 @@
+// aw_spectral.cu — grid-side kernels of the step.
+//
+//   k_finalize       int64 fixed-point accumulators -> FP32 grids (contiguous
+//                    staging for the batched R2C, plus the caller's Sources
+//                    arrays), accumulators reset, charge partials; in the fused
+//                    step the first block also advances the device step state
+//                    (time, deposit scales) so a CUDA graph can replay steps.
+//   k_kspace_es      phi_k = rho_k/(eps0 k^2); E_k = -i k phi_k; DC and Nyquist
+//                    zeroed; the 1/(nx ny) inverse-FFT scale is folded in
+//                    (solver_es.hpp:40-78, spectral.hpp:124-132).
+//   k_kspace_elb     fused E_L and B_k = i mu0 (k x J)/k^2 (solver_darwin.hpp:38-75).
+//   k_kspace_et      E_T = -green_et (dcu - i S(amu))_T (solver_darwin.hpp:83-129).
+//   k_fields_*       real-space finalisers: B += B0, E = E_L (+E_T) + pump
+//                    (pump.hpp:27-54, solver_darwin.hpp:134-144), the caller's
+//                    Fields arrays, the interleaved gather buffers the particle
+//                    kernels read, field maxima and FP64 energy partials.
+//   k_diag_reduce    fixed-order FP64 reduction of all partials (diagnostics.hpp).
+//
+// Scale folding is exact: nx*ny is a power of two for every grid this path is
+// run on, and multiplying by 2^-k commutes with FP32 rounding.
+#include "aw_internal.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace aw {
+namespace {
+
+constexpr int kGridBlocks = 592;   // 4 x 148 SMs; fixed so partials reduce in a fixed order
+
+__device__ __forceinline__ double kx_of(int i, double dkx) { return i * dkx; }
+__device__ __forceinline__ double ky_of(int j, int ny, double dky) {
+    const int m = (j <= ny / 2) ? j : j - ny;
+    return m * dky;
+}
+__device__ __forceinline__ bool nyquist(int i, int j, int nx, int ny) {
+    return ((nx % 2 == 0) && i == nx / 2) || ((ny % 2 == 0) && j == ny / 2);
+}
+
+// Trapezoidal pump ramp — include/pic/pump.hpp:27-32.
+__device__ __forceinline__ double pump_ramp(double t, double trmp, double toff) {
+    if (t >= toff) return 0.0;
+    if (t < trmp) return t / trmp;
+    if (t > toff - trmp) return (toff - t) / trmp;
+    return 1.0;
+}
+
+// Deposit scales for the next source deposit from the current |u| maxima.
+// |u_d| bound U_d = max(1.25 max|u_d|, 0.01 cref); see aw_device.cuh for the
+// fast-path contract.
+__device__ void make_src_scales(const DevState* st, float cref, float (&S)[8]) {
+    float U[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+        U[d] = fmaxf(__fmul_rn(1.25f, __uint_as_float(st->ucur_bits[d])), __fmul_rn(0.01f, cref));
+    const float cm = st->coef_max;
+    S[0] = scale_for_bound(cm);
+    S[1] = scale_for_bound(__fmul_rn(cm, U[0]));
+    S[2] = scale_for_bound(__fmul_rn(cm, U[1]));
+    S[3] = scale_for_bound(__fmul_rn(cm, U[2]));
+    S[4] = scale_for_bound(__fmul_rn(__fmul_rn(cm, 0.5f), fmaxf(__fmul_rn(U[0], U[0]), __fmul_rn(U[1], U[1]))));
+    S[5] = scale_for_bound(__fmul_rn(__fmul_rn(cm, U[0]), U[1]));
+    S[6] = scale_for_bound(__fmul_rn(__fmul_rn(cm, U[2]), U[0]));
+    S[7] = scale_for_bound(__fmul_rn(__fmul_rn(cm, U[2]), U[1]));
+}
+
+__global__ void k_make_scales(DevState* st, float cref) {
+    float S[8];
+    make_src_scales(st, cref, S);
+#pragma unroll
+    for (int f = 0; f < 8; ++f) { st->S_next[f] = S[f]; st->S_pend[f] = S[f]; }
+}
+
+// Finalise nf fields of the accumulator block acc[f*ncell + c] (f = first..first+nf-1)
+// into real staging r[(f-first)*ncell + c] and optional caller arrays.
+struct FinOut { float* p[8]; };
+__global__ void k_finalize(unsigned long long* __restrict__ acc, int first, int nf, int ncell,
+                           const float* __restrict__ Sdev, float* __restrict__ r,
+                           FinOut api, int accumulate, double* __restrict__ part,
+                           DevState* st, int step_begin, double dt, float cref, int darwin) {
+    double qsum = 0.0;
+    double invS[8];
+    for (int f = 0; f < nf; ++f) invS[f] = 1.0 / static_cast<double>(Sdev[first + f]);
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        for (int f = 0; f < nf; ++f) {
+            unsigned long long* a = acc + static_cast<size_t>(first + f) * ncell + c;
+            const long long v = static_cast<long long>(*a);
+            *a = 0ull;
+            const float val = __double2float_rn(static_cast<double>(v) * invS[f]);
+            r[static_cast<size_t>(f) * ncell + c] = val;
+            float* o = api.p[f];
+            if (o) o[c] = accumulate ? __fadd_rn(o[c], val) : val;
+            if (first + f == 0) qsum += val;
+        }
+    }
+    if (part) {
+        __shared__ double sh[kThreads / 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) qsum += __shfl_down_sync(0xffffffffu, qsum, o);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = qsum;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double s = 0;
+            for (int w = 0; w < kThreads / 32; ++w) s += sh[w];
+            part[blockIdx.x * 5 + 2] = s;
+        }
+    }
+    if (step_begin && blockIdx.x == 0 && threadIdx.x == 0) {
+        st->t = static_cast<double>(st->step) * dt;
+        // the particle state is the last push's output: its |u| maxima
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { st->ucur_bits[d] = st->umax_bits[d]; st->umax_bits[d] = 0u; }
+        st->emax_bits = 0u; st->bmax_bits = 0u;
+        if (darwin) {
+            float S[8];
+            make_src_scales(st, cref, S);
+#pragma unroll
+            for (int f = 0; f < 8; ++f) st->S_next[f] = S[f];
+        }
+    }
+}
+
+// ---- k-space -------------------------------------------------------------
+__device__ __forceinline__ void es_k(cufftComplex r, int i, int j, const SpecGeo& g, double eps0,
+                                     cufftComplex& ex, cufftComplex& ey) {
+    const double kxi = kx_of(i, g.dkx);
+    const double kyj = ky_of(j, g.ny, g.dky);
+    const double k2 = kxi * kxi + kyj * kyj;
+    const double gr = (k2 > 0.0 ? 1.0 / (eps0 * k2) : 0.0) * 1.0;
+    cufftComplex phi;
+    phi.x = static_cast<float>(r.x * gr);
+    phi.y = static_cast<float>(r.y * gr);
+    if (nyquist(i, j, g.nx, g.ny)) {
+        ex.x = ex.y = ey.x = ey.y = 0.0f;
+    } else {
+        const double kx = kx_of(i, g.dkx);
+        const double ky = ky_of(j, g.ny, g.dky);
+        ex.x = static_cast<float>( kx * phi.y) * g.invN;
+        ex.y = static_cast<float>(-kx * phi.x) * g.invN;
+        ey.x = static_cast<float>( ky * phi.y) * g.invN;
+        ey.y = static_cast<float>(-ky * phi.x) * g.invN;
+    }
+}
+
+__global__ void k_kspace_es(const cufftComplex* __restrict__ rho_k, cufftComplex* __restrict__ ex_k,
+                            cufftComplex* __restrict__ ey_k, SpecGeo g, double eps0) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.nk) return;
+    const int i = t % g.nkx, j = t / g.nkx;
+    cufftComplex ex, ey;
+    es_k(rho_k[t], i, j, g, eps0, ex, ey);
+    ex_k[t] = ex;
+    ey_k[t] = ey;
+}
+
+// src_k = [rho, Jx, Jy, Jz, ...] (stride nk); out_k = [ELx, ELy, Bx, By, Bz].
+__global__ void k_kspace_elb(const cufftComplex* __restrict__ src_k, cufftComplex* __restrict__ out_k,
+                             SpecGeo g, double eps0, double c) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.nk) return;
+    const int i = t % g.nkx, j = t / g.nkx;
+    const size_t nk = g.nk;
+    cufftComplex ex, ey;
+    es_k(src_k[t], i, j, g, eps0, ex, ey);
+    out_k[t] = ex;
+    out_k[nk + t] = ey;
+
+    const double kxi = kx_of(i, g.dkx), kyj = ky_of(j, g.ny, g.dky);
+    const double k2 = kxi * kxi + kyj * kyj;
+    const double G = k2 > 0.0 ? 1.0 / (eps0 * c * c * k2) : 0.0;
+    cufftComplex bx, by, bz;
+    if (nyquist(i, j, g.nx, g.ny) || k2 == 0.0) {
+        bx.x = bx.y = by.x = by.y = bz.x = bz.y = 0.0f;
+    } else {
+        const double kx = kx_of(i, g.dkx), ky = ky_of(j, g.ny, g.dky);
+        const cufftComplex Jx = src_k[nk + t], Jy = src_k[2 * nk + t], Jz = src_k[3 * nk + t];
+        bx.x = static_cast<float>(-G * ky * Jz.y) * g.invN;
+        bx.y = static_cast<float>( G * ky * Jz.x) * g.invN;
+        by.x = static_cast<float>( G * kx * Jz.y) * g.invN;
+        by.y = static_cast<float>(-G * kx * Jz.x) * g.invN;
+        const double Cx = kx * Jy.x - ky * Jx.x;
+        const double Cy = kx * Jy.y - ky * Jx.y;
+        bz.x = static_cast<float>(-G * Cy) * g.invN;
+        bz.y = static_cast<float>( G * Cx) * g.invN;
+    }
+    out_k[2 * nk + t] = bx;
+    out_k[3 * nk + t] = by;
+    out_k[4 * nk + t] = bz;
+}
+
+// dcu_k = [dcux, dcuy, dcuz], amu_k = [amu0..amu3] (stride nk); et_k = [ETx, ETy, ETz].
+__global__ void k_kspace_et(const cufftComplex* __restrict__ dcu_k, const cufftComplex* __restrict__ amu_k,
+                            cufftComplex* __restrict__ et_k, SpecGeo g, double eps0, double c, double n0) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= g.nk) return;
+    const int i = t % g.nkx, j = t / g.nkx;
+    const size_t nk = g.nk;
+    const double kxi = kx_of(i, g.dkx), kyj = ky_of(j, g.ny, g.dky);
+    const double k2 = kxi * kxi + kyj * kyj;
+    const double G = k2 > 0.0 ? 1.0 / (eps0 * c * c * k2 + n0) : 0.0;
+    cufftComplex ex, ey, ez;
+    if (nyquist(i, j, g.nx, g.ny) || k2 == 0.0) {
+        ex.x = ex.y = ey.x = ey.y = ez.x = ez.y = 0.0f;
+    } else {
+        const double kx = kx_of(i, g.dkx), ky = ky_of(j, g.ny, g.dky);
+        const cufftComplex a0 = amu_k[t], a1 = amu_k[nk + t], a2 = amu_k[2 * nk + t], a3 = amu_k[3 * nk + t];
+        const double Sx_r = kx*a0.x + ky*a1.x, Sx_i = kx*a0.y + ky*a1.y;
+        const double Sy_r = kx*a1.x - ky*a0.x, Sy_i = kx*a1.y - ky*a0.y;
+        const double Sz_r = kx*a2.x + ky*a3.x, Sz_i = kx*a2.y + ky*a3.y;
+        const cufftComplex dcx = dcu_k[t], dcy = dcu_k[nk + t], dcz = dcu_k[2 * nk + t];
+        double Jx_r = dcx.x + Sx_i, Jx_i = dcx.y - Sx_r;
+        double Jy_r = dcy.x + Sy_i, Jy_i = dcy.y - Sy_r;
+        double Jz_r = dcz.x + Sz_i, Jz_i = dcz.y - Sz_r;
+        const double inv = 1.0 / k2;
+        const double kd_r = (kx*Jx_r + ky*Jy_r) * inv;
+        const double kd_i = (kx*Jx_i + ky*Jy_i) * inv;
+        Jx_r -= kx*kd_r; Jx_i -= kx*kd_i;
+        Jy_r -= ky*kd_r; Jy_i -= ky*kd_i;
+        ex.x = static_cast<float>(-G*Jx_r) * g.invN; ex.y = static_cast<float>(-G*Jx_i) * g.invN;
+        ey.x = static_cast<float>(-G*Jy_r) * g.invN; ey.y = static_cast<float>(-G*Jy_i) * g.invN;
+        ez.x = static_cast<float>(-G*Jz_r) * g.invN; ez.y = static_cast<float>(-G*Jz_i) * g.invN;
+    }
+    et_k[t] = ex;
+    et_k[nk + t] = ey;
+    et_k[2 * nk + t] = ez;
+}
+
+// ---- real-space finalisers ----------------------------------------------------
+// Partials layout per block: [sum e2, max e2, sum rho, sum b2, unused].
+__device__ void grid_partials(double se2, double me2, double sb2, double* __restrict__ part) {
+    __shared__ double sh[3][kThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        se2 += __shfl_down_sync(0xffffffffu, se2, o);
+        me2 = fmax(me2, __shfl_down_sync(0xffffffffu, me2, o));
+        sb2 += __shfl_down_sync(0xffffffffu, sb2, o);
+    }
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) { sh[0][warp] = se2; sh[1][warp] = me2; sh[2][warp] = sb2; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0, m = 0, b = 0;
+        for (int w = 0; w < kThreads / 32; ++w) { a += sh[0][w]; m = fmax(m, sh[1][w]); b += sh[2][w]; }
+        part[blockIdx.x * 5 + 0] = a;
+        part[blockIdx.x * 5 + 1] = m;
+        part[blockIdx.x * 5 + 3] = b;
+    }
+}
+
+// ES: r = [Ex, Ey] -> gather buffer [ncell][2], caller Ex/Ey, energy partials.
+__global__ void k_fields_es(const float* __restrict__ r, float* __restrict__ gb, float* ex_api,
+                            float* ey_api, int ncell, double* __restrict__ part) {
+    double se2 = 0, me2 = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        const float ex = r[c], ey = r[ncell + c];
+        reinterpret_cast<float2*>(gb)[c] = make_float2(ex, ey);
+        if (ex_api) ex_api[c] = ex;
+        if (ey_api) ey_api[c] = ey;
+        const double e2 = double(ex) * ex + double(ey) * ey;
+        se2 += e2;
+        me2 = fmax(me2, e2);
+    }
+    grid_partials(se2, me2, 0.0, part);
+}
+
+struct PumpArgs {
+    int    on;
+    double ex, ey, ez, k0, w0, trmp, toff;
+    double dx;
+};
+// Pump E at grid column i and time t, added in float like add_pump_kernel.
+__device__ __forceinline__ void pump_add(const PumpArgs& pa, int i, double t,
+                                         float& ex, float& ey, float& ez) {
+    if (!pa.on || t >= pa.toff) return;
+    const double x  = i * pa.dx;
+    const double th = pa.k0 * x - pa.w0 * t;
+    const double rr = pump_ramp(t, pa.trmp, pa.toff);
+    const double ct = cos(th), st = sin(th);
+    ex += static_cast<float>(pa.ex * ct * rr);
+    ey += static_cast<float>(-pa.ey * st * rr);
+    ez += static_cast<float>(pa.ez * ct * rr);
+}
+
+struct FieldAPI { float *Ex, *Ey, *Ez, *Bx, *By, *Bz, *ELx, *ELy, *ETx, *ETy, *ETz; };
+
+// Darwin, after the E_L/B solve: r = [ELx, ELy, Bx, By, Bz] (self fields).
+// gb_dcu[c] = [E_L + pump (3), B + B0 (3), 0, 0]; caller EL and B; field maxima.
+__global__ void k_fields_dcu(const float* __restrict__ r, float* __restrict__ gb, FieldAPI api,
+                             int nx, int ncell, float b0x, float b0y, float b0z, PumpArgs pa,
+                             DevState* st) {
+    const double t = st->t;
+    float emax = 0.f, bmax = 0.f;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        const float elx = r[c], ely = r[ncell + c];
+        const float bx = r[2 * ncell + c] + b0x;
+        const float by = r[3 * ncell + c] + b0y;
+        const float bz = r[4 * ncell + c] + b0z;
+        float ex = elx, ey = ely, ez = 0.0f;
+        pump_add(pa, c % nx, t, ex, ey, ez);
+        float4* q = reinterpret_cast<float4*>(gb) + 2 * static_cast<size_t>(c);
+        q[0] = make_float4(ex, ey, ez, bx);
+        q[1] = make_float4(by, bz, 0.f, 0.f);
+        if (api.ELx) api.ELx[c] = elx;
+        if (api.ELy) api.ELy[c] = ely;
+        if (api.Bx) api.Bx[c] = bx;
+        if (api.By) api.By[c] = by;
+        if (api.Bz) api.Bz[c] = bz;
+        emax = fmaxf(emax, fmaxf(fabsf(ex), fmaxf(fabsf(ey), fabsf(ez))));
+        bmax = fmaxf(bmax, fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
+    }
+    emax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(emax)));
+    bmax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(bmax)));
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&st->emax_bits, __float_as_uint(emax));
+        atomicMax(&st->bmax_bits, __float_as_uint(bmax));
+    }
+}
+
+// Darwin, after the E_T solve: r_et = [ETx, ETy, ETz], r_el = [ELx, ELy, ...].
+// E = E_L + E_T + pump -> caller E and ET, gather buffer for the push (B from
+// gb_dcu), energy partials.
+__global__ void k_fields_push(const float* __restrict__ r_et, const float* __restrict__ r_el,
+                              const float* __restrict__ gb_dcu, float* __restrict__ gb, FieldAPI api,
+                              int nx, int ncell, PumpArgs pa, const DevState* st,
+                              double* __restrict__ part) {
+    const double t = st->t;
+    double se2 = 0, me2 = 0, sb2 = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        const float etx = r_et[c], ety = r_et[ncell + c], etz = r_et[2 * ncell + c];
+        float ex = r_el[c] + 1.0f * etx;
+        float ey = r_el[ncell + c] + 1.0f * ety;
+        float ez = 1.0f * etz;
+        pump_add(pa, c % nx, t, ex, ey, ez);
+        const float4* qd = reinterpret_cast<const float4*>(gb_dcu) + 2 * static_cast<size_t>(c);
+        const float4 b1 = qd[0], b2 = qd[1];
+        float4* q = reinterpret_cast<float4*>(gb) + 2 * static_cast<size_t>(c);
+        q[0] = make_float4(ex, ey, ez, b1.w);
+        q[1] = make_float4(b2.x, b2.y, 0.f, 0.f);
+        if (api.Ex) api.Ex[c] = ex;
+        if (api.Ey) api.Ey[c] = ey;
+        if (api.Ez) api.Ez[c] = ez;
+        if (api.ETx) api.ETx[c] = etx;
+        if (api.ETy) api.ETy[c] = ety;
+        if (api.ETz) api.ETz[c] = etz;
+        const double e2 = double(ex) * ex + double(ey) * ey;
+        se2 += e2;
+        me2 = fmax(me2, e2);
+        sb2 += double(b1.w) * b1.w + double(b2.x) * b2.x + double(b2.y) * b2.y;
+    }
+    grid_partials(se2, me2, sb2, part);
+}
+
+// Fixed-order reduction of particle (ke, px, py, pz) and grid partials.
+__global__ void k_diag_reduce(const double* __restrict__ pp, int np, const double* __restrict__ pg,
+                              int ng, double eps0, double dxdy, aw_diag* out) {
+    __shared__ double sh[8][32];
+    const int l = threadIdx.x;   // 32 threads
+    double ke = 0, px = 0, py = 0, pz = 0, se2 = 0, me2 = 0, q = 0, sb2 = 0;
+    for (int b = l; b < np; b += 32) {
+        ke += pp[b * 5 + 0]; px += pp[b * 5 + 1]; py += pp[b * 5 + 2]; pz += pp[b * 5 + 3];
+    }
+    for (int b = l; b < ng; b += 32) {
+        se2 += pg[b * 5 + 0]; me2 = fmax(me2, pg[b * 5 + 1]); q += pg[b * 5 + 2]; sb2 += pg[b * 5 + 3];
+    }
+    sh[0][l] = ke; sh[1][l] = px; sh[2][l] = py; sh[3][l] = pz;
+    sh[4][l] = se2; sh[5][l] = me2; sh[6][l] = q; sh[7][l] = sb2;
+    __syncwarp();
+    if (l == 0) {
+        double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int i = 0; i < 32; ++i) {
+            for (int k = 0; k < 8; ++k) s[k] = (k == 5) ? fmax(s[k], sh[k][i]) : s[k] + sh[k][i];
+        }
+        out->ke = 0.5 * s[0];
+        out->px = s[1]; out->py = s[2]; out->pz = s[3];
+        out->ee = 0.5 * eps0 * s[4] * dxdy;
+        out->max_e = sqrt(s[5]);
+        out->charge = s[6] * dxdy;
+        out->eb = 0.5 * s[7] * dxdy;
+    }
+}
+
+// ---- unfused helpers on caller arrays ---------------------------------------
+__global__ void k_scale_copy(float* dst, const float* src, int n, float s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = src[i] * s;
+}
+__global__ void k_form_e(FieldAPI f, int n, float s) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f.Ex[i] = f.ELx[i] + s * f.ETx[i];
+    f.Ey[i] = f.ELy[i] + s * f.ETy[i];
+    f.Ez[i] = s * f.ETz[i];
+}
+__global__ void k_add_b0(FieldAPI f, int n, float bx, float by, float bz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f.Bx[i] += bx; f.By[i] += by; f.Bz[i] += bz;
+}
+__global__ void k_add_pump(FieldAPI f, int nx, int n, PumpArgs pa, double t) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    float ex = f.Ex[c], ey = f.Ey[c], ez = f.Ez[c];
+    pump_add(pa, c % nx, t, ex, ey, ez);
+    f.Ex[c] = ex; f.Ey[c] = ey; f.Ez[c] = ez;
+}
+
+// Pack caller E/B arrays into the [ncell][8] gather layout (unfused dcu
+// deposit) and record the field maxima its deposit scale needs.
+__global__ void k_pack_em(FieldAPI f, float* __restrict__ gb, int ncell, DevState* st) {
+    float emax = 0.f, bmax = 0.f;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        const float ex = f.Ex[c], ey = f.Ey[c], ez = f.Ez[c];
+        const float bx = f.Bx[c], by = f.By[c], bz = f.Bz[c];
+        float4* q = reinterpret_cast<float4*>(gb) + 2 * static_cast<size_t>(c);
+        q[0] = make_float4(ex, ey, ez, bx);
+        q[1] = make_float4(by, bz, 0.f, 0.f);
+        emax = fmaxf(emax, fmaxf(fabsf(ex), fmaxf(fabsf(ey), fabsf(ez))));
+        bmax = fmaxf(bmax, fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
+    }
+    emax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(emax)));
+    bmax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(bmax)));
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&st->emax_bits, __float_as_uint(emax));
+        atomicMax(&st->bmax_bits, __float_as_uint(bmax));
+    }
+}
+
+// Energy / charge partials from caller arrays (any may be null).
+__global__ void k_grid_diag(const float* ex, const float* ey, const float* bx, const float* by,
+                            const float* bz, const float* rho, int ncell, double* __restrict__ part) {
+    double se2 = 0, me2 = 0, sb2 = 0, q = 0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        const double a = ex ? ex[c] : 0.0f, b = ey ? ey[c] : 0.0f;
+        const double e2 = a * a + b * b;
+        se2 += e2; me2 = fmax(me2, e2);
+        if (bx) sb2 += double(bx[c]) * bx[c] + double(by[c]) * by[c] + double(bz[c]) * bz[c];
+        if (rho) q += rho[c];
+    }
+    __shared__ double sh[kThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) q += __shfl_down_sync(0xffffffffu, q, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = q;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0;
+        for (int w = 0; w < kThreads / 32; ++w) s += sh[w];
+        part[blockIdx.x * 5 + 2] = s;
+    }
+    __syncthreads();
+    grid_partials(se2, me2, sb2, part);
+}
+
+__global__ void k_set_step(DevState* st, long long n) { st->step = n; }
+__global__ void k_copy_umax(DevState* st) {
+    for (int d = 0; d < 3; ++d) st->umax_bits[d] = st->ucur_bits[d];
+}
+
+inline int blocks_for(int n) { return std::max(1, (n + kThreads - 1) / kThreads); }
+
+FieldAPI api_of(const aw_field_ptrs& f) {
+    return FieldAPI{f.Ex, f.Ey, f.Ez, f.Bx, f.By, f.Bz, f.ELx, f.ELy, f.ETx, f.ETy, f.ETz};
+}
+PumpArgs pump_of(const Ctx& c) {
+    PumpArgs pa{};
+    pa.on = c.prm.pump;
+    pa.ex = c.prm.pump_ex; pa.ey = c.prm.pump_ey; pa.ez = c.prm.pump_ez;
+    pa.k0 = c.prm.pump_k0; pa.w0 = c.prm.pump_w0; pa.trmp = c.prm.pump_trmp; pa.toff = c.prm.pump_toff;
+    pa.dx = c.geo.dx;
+    return pa;
+}
+float cref_of(const Ctx& c) { return c.model == AW_MODEL_DARWIN ? static_cast<float>(c.prm.c) : 1.0f; }
+
+}  // namespace
+
+int grid_partial_blocks() { return kGridBlocks; }
+
+// ===========================================================================
+void launch_make_scales(Ctx& c) {
+    k_make_scales<<<1, 1, 0, c.stream>>>(c.st, cref_of(c));
+    AW_LAUNCH();
+}
+
+// Finalise acc fields [first, first+nf) with scales S_pend into r (+ api arrays).
+void launch_finalize(Ctx& c, unsigned long long* acc, int first, int nf, const float* S, float* r,
+                     float* const* api, bool accumulate, bool charge_partials, bool step_begin) {
+    FinOut o{};
+    for (int f = 0; f < nf && f < 8; ++f) o.p[f] = api ? api[f] : nullptr;
+    k_finalize<<<kGridBlocks, kThreads, 0, c.stream>>>(acc, first, nf, c.geo.ncell, S, r, o,
+                                                       accumulate ? 1 : 0,
+                                                       charge_partials ? c.part_g : nullptr, c.st,
+                                                       step_begin ? 1 : 0, c.prm.dt, cref_of(c),
+                                                       c.model == AW_MODEL_DARWIN ? 1 : 0);
+    AW_LAUNCH();
+}
+
+void launch_kspace_es(Ctx& c, const cufftComplex* rho_k, cufftComplex* e_k) {
+    k_kspace_es<<<blocks_for(c.sg.nk), kThreads, 0, c.stream>>>(rho_k, e_k, e_k + c.sg.nk, c.sg,
+                                                                 c.prm.eps0);
+    AW_LAUNCH();
+}
+void launch_es_solve_k(Ctx& c, const cufftComplex* rho_k, cufftComplex* ex_k, cufftComplex* ey_k) {
+    k_kspace_es<<<blocks_for(c.sg.nk), kThreads, 0, c.stream>>>(rho_k, ex_k, ey_k, c.sg, c.prm.eps0);
+    AW_LAUNCH();
+}
+void launch_kspace_elb(Ctx& c, const cufftComplex* src_k, cufftComplex* out_k) {
+    k_kspace_elb<<<blocks_for(c.sg.nk), kThreads, 0, c.stream>>>(src_k, out_k, c.sg, c.prm.eps0, c.prm.c);
+    AW_LAUNCH();
+}
+void launch_kspace_et(Ctx& c, const cufftComplex* dcu_k, const cufftComplex* amu_k, cufftComplex* et_k) {
+    k_kspace_et<<<blocks_for(c.sg.nk), kThreads, 0, c.stream>>>(dcu_k, amu_k, et_k, c.sg, c.prm.eps0,
+                                                                 c.prm.c, c.prm.n0);
+    AW_LAUNCH();
+}
+void launch_fields_es(Ctx& c) {
+    k_fields_es<<<kGridBlocks, kThreads, 0, c.stream>>>(c.r_out, c.gb_es, c.fld.Ex, c.fld.Ey,
+                                                        c.geo.ncell, c.part_g);
+    AW_LAUNCH();
+}
+void launch_fields_dcu(Ctx& c) {
+    k_fields_dcu<<<kGridBlocks, kThreads, 0, c.stream>>>(c.r_out, c.gb_dcu, api_of(c.fld), c.geo.nx,
+                                                         c.geo.ncell, c.prm.B0[0], c.prm.B0[1],
+                                                         c.prm.B0[2], pump_of(c), c.st);
+    AW_LAUNCH();
+}
+void launch_fields_push(Ctx& c) {
+    k_fields_push<<<kGridBlocks, kThreads, 0, c.stream>>>(c.r_et, c.r_out, c.gb_dcu, c.gb_push,
+                                                          api_of(c.fld), c.geo.nx, c.geo.ncell,
+                                                          pump_of(c), c.st, c.part_g);
+    AW_LAUNCH();
+}
+void launch_diag_reduce(Ctx& c, bool with_particles) {
+    k_diag_reduce<<<1, 32, 0, c.stream>>>(c.part_p, with_particles ? c.npart_p : 0, c.part_g,
+                                          kGridBlocks, c.prm.eps0, c.geo.dx * c.geo.dy, c.diag);
+    AW_LAUNCH();
+}
+void launch_scale_copy(Ctx& c, float* dst, const float* src, int n, float s) {
+    k_scale_copy<<<blocks_for(n), kThreads, 0, c.stream>>>(dst, src, n, s);
+    AW_LAUNCH();
+}
+void launch_form_e(Ctx& c, float et_scale) {
+    const aw_field_ptrs& f = c.fld;
+    if (!f.Ex || !f.Ey || !f.Ez || !f.ELx || !f.ELy || !f.ETx || !f.ETy || !f.ETz)
+        throw Error(AW_ERR_STATE, "form_e: E, E_L and E_T fields must be bound");
+    k_form_e<<<blocks_for(c.geo.ncell), kThreads, 0, c.stream>>>(api_of(f), c.geo.ncell, et_scale);
+    AW_LAUNCH();
+}
+void launch_add_b0(Ctx& c) {
+    const aw_field_ptrs& f = c.fld;
+    if (!f.Bx || !f.By || !f.Bz) throw Error(AW_ERR_STATE, "add_b0: B fields not bound");
+    k_add_b0<<<blocks_for(c.geo.ncell), kThreads, 0, c.stream>>>(api_of(f), c.geo.ncell, c.prm.B0[0],
+                                                                 c.prm.B0[1], c.prm.B0[2]);
+    AW_LAUNCH();
+}
+void launch_add_pump(Ctx& c, double t) {
+    if (!c.prm.pump || t >= c.prm.pump_toff) return;
+    const aw_field_ptrs& f = c.fld;
+    if (!f.Ex || !f.Ey || !f.Ez) throw Error(AW_ERR_STATE, "add_pump: E fields not bound");
+    k_add_pump<<<blocks_for(c.geo.ncell), kThreads, 0, c.stream>>>(api_of(f), c.geo.nx, c.geo.ncell,
+                                                                   pump_of(c), t);
+    AW_LAUNCH();
+}
+
+void launch_pack_em(Ctx& c) {
+    const aw_field_ptrs& f = c.fld;
+    if (!f.Ex || !f.Ey || !f.Ez || !f.Bx || !f.By || !f.Bz)
+        throw Error(AW_ERR_STATE, "deposit_dcu: fields E and B must be bound");
+    AW_CUDA(cudaMemsetAsync(&c.st->emax_bits, 0, 2 * sizeof(unsigned), c.stream));
+    k_pack_em<<<kGridBlocks, kThreads, 0, c.stream>>>(api_of(f), c.gb_dcu, c.geo.ncell, c.st);
+    AW_LAUNCH();
+}
+void launch_grid_diag(Ctx& c) {
+    const aw_field_ptrs& f = c.fld;
+    k_grid_diag<<<kGridBlocks, kThreads, 0, c.stream>>>(f.Ex, f.Ey, f.Bx, f.By, f.Bz, c.src.rho,
+                                                        c.geo.ncell, c.part_g);
+    AW_LAUNCH();
+}
+void launch_set_step(Ctx& c, long long n) {
+    k_set_step<<<1, 1, 0, c.stream>>>(c.st, n);
+    AW_LAUNCH();
+}
+void launch_copy_umax(Ctx& c) {
+    k_copy_umax<<<1, 1, 0, c.stream>>>(c.st);
+    AW_LAUNCH();
+}
+
+}  // namespace aw

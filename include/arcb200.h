@@ -1,0 +1,228 @@
+/*
+ * arcb200.h — C ABI of the B200-native ArcWarden PIC hot path (libarcb200.so).
+ *
+ * Plain C: pointers, sizes and POD structs only; no C++ or torch types. Every
+ * entry point returns an int status (AW_OK == 0, negative on error);
+ * aw_last_error() returns the text of the most recent error on the calling thread.
+ *
+ * Each entry point replaces one reference interface. The citations name the
+ * file:line (relative to the ArcWarden source tree) whose behaviour it
+ * reproduces.
+ *
+ * Memory model. The caller owns the particle SoA and (optionally) the real-space
+ * source/field grids. It binds them with aw_particles_bind / aw_sources_bind /
+ * aw_fields_bind, and the library never frees them. Layout is the reference's:
+ * particles are FP32 SoA (x, y in cell units, ux, uy, uz = momentum u with
+ * gamma == 1, w = macro weight) plus int32 cell; grids are row-major [ny][nx] FP32
+ * (include/pic/grid.hpp:14-30, include/pic/particles.hpp:453-458).
+ * The context owns its k-space workspace, its 64-bit fixed-point deposit
+ * accumulators and its cuFFT plans; aw_ctx_destroy releases them.
+ *
+ * Threading. A context is used from one host thread. All work is enqueued on
+ * the context's stream (aw_ctx_create / aw_set_stream), and the library never
+ * synchronises except in aw_init, aw_stats and the diagnostic read-back calls
+ * that return host values.
+ */
+#ifndef ARCB200_H
+#define ARCB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+enum {
+    AW_OK            = 0,
+    AW_ERR_ARG       = -1,  /* invalid argument (null, size, alignment)        */
+    AW_ERR_CUDA      = -2,  /* CUDA runtime error                               */
+    AW_ERR_CUFFT     = -3,  /* cuFFT error                                      */
+    AW_ERR_STATE     = -4,  /* call out of order (e.g. nothing bound)           */
+    AW_ERR_DEVICE    = -5,  /* device-side error word set (see aw_error_word)   */
+    AW_ERR_NOMEM     = -6   /* allocation failed                                */
+};
+
+/* Device-side error-word bits (aw_error_word). Kernels set them and never trap. */
+enum {
+    AW_DEV_NONFINITE   = 1u << 0,  /* a deposit contribution was NaN or Inf      */
+    AW_DEV_OUT_OF_GRID = 1u << 1,  /* a position outside [0,nx)x[0,ny) was seen  */
+    AW_DEV_WAIT_LIMIT  = 1u << 2   /* a bounded device-side wait gave up          */
+};
+
+/* Field models (include/pic/config.hpp:72, FieldModel). */
+enum { AW_MODEL_ES = 0, AW_MODEL_DARWIN = 1 };
+
+/* ---- POD descriptions ---------------------------------------------------- */
+
+/* Grid geometry, include/pic/grid.hpp:44-57 (Grid(nx, ny, Lx, Ly); dx = Lx/nx). */
+typedef struct aw_grid {
+    int32_t nx, ny;
+    double  Lx, Ly;
+} aw_grid;
+
+/* The RunParams fields this path reads (include/pic/config.hpp:127-313). */
+typedef struct aw_params {
+    double  dt;
+    double  qm;        /* q/m, electrons -1                                    */
+    double  eps0;
+    double  n0;        /* background density (Darwin E_T resummation)         */
+    double  c;         /* speed of light (Darwin mu0 = 1/(eps0 c^2))           */
+    float   B0[3];     /* uniform external B                                   */
+    int32_t has_b0;    /* ES push rotates about B0 (SimConfig HasB0)           */
+    int32_t pump;      /* external whistler pump on (include/pic/pump.hpp)     */
+    double  pump_ex, pump_ey, pump_ez, pump_k0, pump_w0, pump_trmp, pump_toff;
+} aw_params;
+
+/* One species (include/pic/species.hpp:20-45) for the device loader. */
+typedef struct aw_species {
+    int32_t ppc;
+    double  density;
+    double  uth[3];
+    double  ufl[3];
+} aw_species;
+
+/* Real-space grids. Any pointer may be NULL (not bound); all are [ny][nx]. */
+typedef struct aw_source_ptrs {
+    float *rho, *Jx, *Jy, *Jz, *dcux, *dcuy, *dcuz, *amu0, *amu1, *amu2, *amu3;
+} aw_source_ptrs;
+
+typedef struct aw_field_ptrs {
+    float *Ex, *Ey, *Ez, *Bx, *By, *Bz, *ELx, *ELy, *ETx, *ETy, *ETz;
+} aw_field_ptrs;
+
+/* Per-step diagnostics, FP64 on the GPU (include/pic/diagnostics.hpp:58-108,
+ * plus momentum and the magnetic/z-field energies the diag modules use). */
+typedef struct aw_diag {
+    double ke;        /* 1/2 sum w |u|^2                                      */
+    double ee;        /* 1/2 eps0 sum (Ex^2 + Ey^2) dx dy                      */
+    double charge;    /* sum rho dx dy                                         */
+    double max_e;     /* max sqrt(Ex^2 + Ey^2)                                 */
+    double px, py, pz;/* sum w u                                               */
+    double eb;        /* 1/2 sum (Bx^2 + By^2 + Bz^2) dx dy  (Darwin)          */
+} aw_diag;
+
+/* Counters the fused kernels keep (read by aw_stats; a host sync). */
+typedef struct aw_stats_t {
+    int64_t chunks;           /* particle chunks processed by window kernels   */
+    int64_t window_overflow;  /* chunks whose cell window exceeded shared mem  */
+    int64_t slow_deposits;    /* contributions that took the exact slow path   */
+    int64_t steps;            /* fused steps taken                             */
+} aw_stats_t;
+
+typedef struct aw_ctx aw_ctx;
+
+/* ---- context --------------------------------------------------------------
+ * Replaces the owner set-up of Simulation<Cfg> (include/pic/simulation.hpp:41-52):
+ * the SpectralEngine plans/workspace (include/pic/spectral.hpp:106-149,
+ * include/pic/fft.hpp:26-93) and the per-step scratch. `stream` is a
+ * cudaStream_t (NULL = legacy default stream). */
+int aw_ctx_create(const aw_grid* g, const aw_params* p, int32_t model,
+                  void* stream, aw_ctx** out);
+int aw_ctx_destroy(aw_ctx* ctx);
+int aw_set_stream(aw_ctx* ctx, void* stream);
+/* Replace the run parameters (RunParams is passed by value each call in the
+ * reference; here it is context state). */
+int aw_set_params(aw_ctx* ctx, const aw_params* p);
+
+/* ---- binding caller-owned device memory ----------------------------------
+ * Particles: the reference Particles SoA (include/pic/particles.hpp:453-516).
+ * `cell` may be NULL only if the caller never calls aw_migrate/aw_sort_tiles. */
+int aw_particles_bind(aw_ctx* ctx, float* x, float* y, float* ux, float* uy,
+                      float* uz, float* w, int32_t* cell, int64_t n);
+/* Sources (include/pic/sources.hpp:23-86) and Fields (include/pic/fields.hpp:24-73). */
+int aw_sources_bind(aw_ctx* ctx, const aw_source_ptrs* s);
+int aw_fields_bind(aw_ctx* ctx, const aw_field_ptrs* f);
+
+/* ---- loader ----------------------------------------------------------------
+ * Particles::initialize(SpeciesList, Grid, RunParams, stream) with
+ * species_init_kernel, include/pic/particles.hpp:333-379 and 533-559. Writes the
+ * bound SoA; n must equal sum(ppc) * nx * ny. Same hashed RNG / van der Corput
+ * streams, so the reference and this loader give identical particles. */
+int aw_load_species(aw_ctx* ctx, const aw_species* sp, int32_t nspecies,
+                    uint64_t seed, int32_t noisy);
+
+/* ---- operators (unfused; each matches one reference launch sequence) ------ */
+
+/* Depositor<Cfg>::charge, include/pic/depositor.hpp:440-496: rho += deposit. */
+int aw_deposit_rho(aw_ctx* ctx);
+/* Depositor::charge_current[_sorted], include/pic/depositor.hpp:369-408: rho, J += deposit. */
+int aw_deposit_rho_j(aw_ctx* ctx);
+/* Depositor::deposit_amu, include/pic/depositor.hpp:412-422: amu0..3 += deposit. */
+int aw_deposit_amu(aw_ctx* ctx);
+/* Depositor::deposit_dcu, include/pic/depositor.hpp:426-437: dcu += deposit,
+ * gathering the bound fields Ex,Ey,Ez,Bx,By,Bz. */
+int aw_deposit_dcu(aw_ctx* ctx);
+
+/* Pusher<Cfg>::boris, include/pic/pusher.hpp:265-275 (gather Ex,Ey; Boris about
+ * B0 when has_b0; move; no wrap). */
+int aw_push_es(aw_ctx* ctx);
+/* Pusher<Cfg>::boris_em, include/pic/pusher.hpp:300-317 (gather E and B). */
+int aw_push_em(aw_ctx* ctx);
+/* Pusher<Cfg>::half_step_back, include/pic/pusher.hpp:321-330. */
+int aw_half_step_back(aw_ctx* ctx);
+/* Particles::migrate, include/pic/particles.hpp:294-315 and 615-621. */
+int aw_migrate(aw_ctx* ctx);
+/* Particles::build_tile_bins (physical == 0) / sort_by_tile (physical != 0),
+ * include/pic/particles.hpp:632-726: keys tile = (j/ty)*ntx + i/tx from cell.
+ * The permutation (physical == 0) or the tile offsets are kept in the context. */
+int aw_sort_tiles(aw_ctx* ctx, int32_t tx, int32_t ty, int32_t physical);
+/* Device pointers to the last tile binning: off[ntiles+1], idx[n] (idx is NULL
+ * after a physical sort), and the tile geometry (BinViews, particles.hpp:63-69). */
+int aw_tile_bins(aw_ctx* ctx, const int32_t** off, const int32_t** idx,
+                 int32_t* ntiles, int32_t* ntx);
+
+/* ElectrostaticSpectralSolver::solve, include/pic/solver_es.hpp:238-259. */
+int aw_solve_es(aw_ctx* ctx);
+/* DarwinSpectralSolver::solve_el_b, include/pic/solver_darwin.hpp:188-216. */
+int aw_solve_darwin_el_b(aw_ctx* ctx);
+/* DarwinSpectralSolver::solve_et, include/pic/solver_darwin.hpp:235-263. */
+int aw_solve_darwin_et(aw_ctx* ctx);
+/* DarwinSpectralSolver::solve (E_L + B into Ex,Ey,Bx..z; Ez = 0),
+ * include/pic/solver_darwin.hpp:153-184. */
+int aw_solve_darwin(aw_ctx* ctx);
+/* DarwinSpectralSolver::form_e, include/pic/solver_darwin.hpp:220-231. */
+int aw_form_e(aw_ctx* ctx, float et_scale);
+/* add_background_b0 / add_pump_field, include/pic/pump.hpp:59-79. */
+int aw_add_b0(aw_ctx* ctx);
+int aw_add_pump(aw_ctx* ctx, double t);
+/* R2C / C2R of one [ny][nx] field (SpectralEngine::r2c / c2r with the 1/(nx*ny)
+ * scale, include/pic/spectral.hpp:118-132). `kspace` holds ny*(nx/2+1) complex
+ * FP32 values; c2r overwrites its input like cuFFT. */
+int aw_fft_r2c(aw_ctx* ctx, const float* in, void* kspace);
+int aw_fft_c2r(aw_ctx* ctx, void* kspace, float* out);
+
+/* ---- the fused, graph-capturable step (the product hot path) -------------
+ * Simulation<Cfg>::init, include/pic/simulation.hpp:56-77: ES deposits, solves
+ * and rolls u back half a step; Darwin computes the t = 0 fields. Synchronises. */
+int aw_init(aw_ctx* ctx);
+/* Simulation<Cfg>::step(n), include/pic/simulation.hpp:80-93, without the host
+ * diagnostics: one PIC step through the fused kernels. Time t = n*dt. */
+int aw_step(aw_ctx* ctx, int64_t n);
+/* `nsteps` steps starting at step n0. use_graph != 0 captures one step into a
+ * CUDA graph (once per context) and replays it; the step index lives in device
+ * memory so the same graph serves every step. */
+int aw_run(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph);
+
+/* ---- diagnostics and status ----------------------------------------------- */
+/* Diagnostics::compute, include/pic/diagnostics.hpp:58-108, reduced on the GPU
+ * in FP64 from the bound particles / sources / fields (synchronises). */
+int aw_reduce_fp64(aw_ctx* ctx, aw_diag* out);
+/* Diagnostics of the most recent fused step (computed inside its kernels) into a
+ * host struct; synchronises. */
+int aw_step_diag(aw_ctx* ctx, aw_diag* out);
+/* Device pointer to the per-step diagnostics the fused step writes (one aw_diag,
+ * updated every step; for a caller that copies it asynchronously). */
+int aw_step_diag_device(aw_ctx* ctx, const aw_diag** dev_ptr);
+int aw_error_word(aw_ctx* ctx, uint32_t* out);   /* reads and clears; syncs */
+int aw_stats(aw_ctx* ctx, aw_stats_t* out);      /* syncs */
+int aw_last_error(char* buf, int32_t n);
+/* Library version string (static storage). */
+const char* aw_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ARCB200_H */
