@@ -14,11 +14,18 @@
 //                        (pusher.hpp:212-258 + particles.hpp:294-315 +
 //                        depositor.hpp:161-270), KE/momentum partials, |u| max.
 //
-// Every kernel processes one chunk of kChunk consecutive particles per CTA; a
-// thread owns kPPT consecutive particles (two LDG.128 per array). Deposits go
-// through the shared-memory cell window of WinDep (aw_device.cuh). No kernel
-// sorts particles: the array order is whatever the caller holds, so the ES path
-// keeps the reference's particle order.
+// Structure of every kernel (one CTA = one chunk of kChunk consecutive
+// particles; no kernel sorts particles, so the ES path keeps the reference's
+// particle order):
+//   pass 1  coalesced 128-bit loads (4 consecutive particles per thread per
+//           iteration), per-particle work (gather / push / wrap), coalesced
+//           128-bit stores of the new state, and a copy of what the deposit
+//           needs into a shared-memory stage; bounding box of the cells.
+//   window  block-wide bounding box -> int32 shared window [NF][W*H].
+//   pass 2  lane l of warp w deposits stage slot j*256 + 32w + l, so a warp
+//           holds 32 consecutive particles (usually one or two cells) and
+//           win_deposit sums them with redux.sync before one shared atomic.
+//   flush   window -> global int64 accumulators (red.global.add.u64).
 #include "aw_internal.h"
 
 #include <algorithm>
@@ -30,27 +37,20 @@ namespace {
 enum { SET_RHO = 0, SET_RHOJ = 1, SET_AMU = 2, SET_ALL = 3 };
 
 template <int SET> struct SetNF;
-template <> struct SetNF<SET_RHO>  { static constexpr int NF = 1; };
-template <> struct SetNF<SET_RHOJ> { static constexpr int NF = 4; };
-template <> struct SetNF<SET_AMU>  { static constexpr int NF = 4; };
-template <> struct SetNF<SET_ALL>  { static constexpr int NF = 8; };
+template <> struct SetNF<SET_RHO>  { static constexpr int NF = 1, NS = 3; };   // stage: x y w
+template <> struct SetNF<SET_RHOJ> { static constexpr int NF = 4, NS = 6; };   // x y w ux uy uz
+template <> struct SetNF<SET_AMU>  { static constexpr int NF = 4, NS = 6; };
+template <> struct SetNF<SET_ALL>  { static constexpr int NF = 8, NS = 6; };
 
-// Window capacity in cells for NF fields (dynamic shared memory ~64 KB).
-inline int wmax_cells(int nf) {
-    switch (nf) {
-        case 1: return 4096;
-        case 3: return 2560;
-        case 4: return 2048;
-        default: return 1024;
-    }
-}
-inline size_t smem_bytes(int nf) {
-    return static_cast<size_t>(wmax_cells(nf)) * nf * 8 + kThreads / 32 * 4 * sizeof(int);
+// Window capacity in cells for NF int32 planes (~48 KB per CTA).
+constexpr int wmax_cells(int nf) { return nf == 1 ? 8192 : (nf == 3 ? 4096 : (nf == 4 ? 3072 : 1536)); }
+constexpr size_t smem_bytes(int nf, int ns) {
+    return static_cast<size_t>(ns) * kChunk * 4 + static_cast<size_t>(wmax_cells(nf)) * nf * 4
+           + kThreads / 32 * 4 * sizeof(int);
 }
 
-// Reference cell for the window: the chunk's first particle (any cell works).
 __device__ __forceinline__ void ref_cell(const Parts& p, long long c0, const Geo& g, int& ir, int& jr) {
-    const float x = p.x[c0], y = p.y[c0];
+    const float x = __ldg(p.x + c0), y = __ldg(p.y + c0);
     ir = (x >= 0.0f && x < g.nxf) ? static_cast<int>(x) : 0;
     jr = (y >= 0.0f && y < g.nyf) ? static_cast<int>(y) : 0;
 }
@@ -63,11 +63,8 @@ __device__ __forceinline__ void cell_ij(float x, float y, const Geo& g, int& ci,
     if (cj >= g.ny) cj = g.ny - 1;
 }
 
-// Wrapped global corner cells of a stencil (slow path only).
-__device__ __forceinline__ void corner_cells(const Cic& s, const Geo& g, int& c0, int& c1, int& c2, int& c3) {
-    const int i1 = wrap_once(s.i0 + 1, g.nx);
-    const int r0 = s.j0 * g.nx, r1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
-    c0 = r0 + s.i0; c1 = r0 + i1; c2 = r1 + s.i0; c3 = r1 + i1;
+__device__ __forceinline__ bool in_grid(float x, float y, const Geo& g) {
+    return x >= 0.0f && x < g.nxf && y >= 0.0f && y < g.nyf;
 }
 
 // Per-particle source coefficients (unscaled), in the deposit's field order.
@@ -120,81 +117,130 @@ __device__ void block_sum4(double a, double b, double c, double d, double* __res
     if (threadIdx.x == 4) part[blockIdx.x * 5 + 4] = 0.0;
 }
 
+// 4 consecutive floats at a[i..i+3] (vectorised when aligned and in range).
+__device__ __forceinline__ float4 ld4(const float* __restrict__ a, long long i, long long n, bool vec) {
+    if (vec && i + 4 <= n) return __ldg(reinterpret_cast<const float4*>(a + i));
+    float4 v;
+    v.x = (i + 0 < n) ? a[i + 0] : 0.0f;
+    v.y = (i + 1 < n) ? a[i + 1] : 0.0f;
+    v.z = (i + 2 < n) ? a[i + 2] : 0.0f;
+    v.w = (i + 3 < n) ? a[i + 3] : 0.0f;
+    return v;
+}
+__device__ __forceinline__ void st4(float* __restrict__ a, long long i, long long n, bool vec, float4 v) {
+    if (vec && i + 4 <= n) { *reinterpret_cast<float4*>(a + i) = v; return; }
+    if (i + 0 < n) a[i + 0] = v.x;
+    if (i + 1 < n) a[i + 1] = v.y;
+    if (i + 2 < n) a[i + 2] = v.z;
+    if (i + 3 < n) a[i + 3] = v.w;
+}
+__device__ __forceinline__ void st4i(int* __restrict__ a, long long i, long long n, bool vec, int4 v) {
+    if (vec && i + 4 <= n) { *reinterpret_cast<int4*>(a + i) = v; return; }
+    if (i + 0 < n) a[i + 0] = v.x;
+    if (i + 1 < n) a[i + 1] = v.y;
+    if (i + 2 < n) a[i + 2] = v.z;
+    if (i + 3 < n) a[i + 3] = v.w;
+}
+__device__ __forceinline__ float& comp(float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
+__device__ __forceinline__ float compc(const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
+__device__ __forceinline__ int& compi(int4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
+
+// Running bounding box of wrapped cell offsets.
+struct BBox {
+    int lo_i = 1 << 30, lo_j = 1 << 30, hi_i = -(1 << 30), hi_j = -(1 << 30);
+    __device__ __forceinline__ void add(int ci, int cj, int ir, int jr, const Geo& g) {
+        const int di = win_off(ci, ir, g.nx), dj = win_off(cj, jr, g.ny);
+        lo_i = min(lo_i, di); hi_i = max(hi_i, di);
+        lo_j = min(lo_j, dj); hi_j = max(hi_j, dj);
+    }
+};
+
+// Stage plane f, slot s.
+__device__ __forceinline__ float& stg(float* st, int f, int s) { return st[f * kChunk + s]; }
+__device__ __forceinline__ float4& stg4(float* st, int f, int s) { return reinterpret_cast<float4*>(st + f * kChunk)[s >> 2]; }
+
+__device__ __forceinline__ void weights(const Cic& s, float (&wv)[4]) {
+    wv[0] = s.w0; wv[1] = s.w1; wv[2] = s.w2; wv[3] = s.w3;
+}
+
 // ---------------------------------------------------------------------------
+// Standalone source deposit at the current positions.
 template <int SET>
 __global__ void __launch_bounds__(kThreads)
 k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st) {
-    constexpr int NF = SetNF<SET>::NF;
+    constexpr int NF = SetNF<SET>::NF, NS = SetNF<SET>::NS;
     extern __shared__ __align__(16) unsigned char smem[];
-    long long* sacc = reinterpret_cast<long long*>(smem);
-    int* red = reinterpret_cast<int*>(smem + static_cast<size_t>(wmaxc) * NF * 8);
+    float* stage = reinterpret_cast<float*>(smem);
+    int* win = reinterpret_cast<int*>(smem + static_cast<size_t>(NS) * kChunk * 4);
+    int* red = win + wmaxc * NF;
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
-    const long long base = c0 + static_cast<long long>(threadIdx.x) * kPPT;
     const bool vec = p.vec_ok != 0;
-    float x[kPPT], y[kPPT], w[kPPT], ux[kPPT], uy[kPPT], uz[kPPT];
-    load8(p.x, base, p.n, vec, x);
-    load8(p.y, base, p.n, vec, y);
-    load8(p.w, base, p.n, vec, w);
-    if constexpr (SET != SET_RHO) {
-        load8(p.ux, base, p.n, vec, ux);
-        load8(p.uy, base, p.n, vec, uy);
-        load8(p.uz, base, p.n, vec, uz);
+    int ir, jr;
+    ref_cell(p, c0, g, ir, jr);
+    BBox bb;
+    // pass 1: load into the stage (x, y, w[, ux, uy, uz]); an invalid slot has x = -1
+#pragma unroll 1
+    for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
+        const int s0 = it * 4 * kThreads + 4 * threadIdx.x;
+        const long long i = c0 + s0;
+        float4 x = ld4(p.x, i, p.n, vec), y = ld4(p.y, i, p.n, vec), w = ld4(p.w, i, p.n, vec);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            float& xe = comp(x, e);
+            const float ye = compc(y, e);
+            if (i + e < p.n && in_grid(xe, ye, g)) {
+                bb.add(static_cast<int>(xe), static_cast<int>(ye), ir, jr, g);
+            } else {
+                if (i + e < p.n) set_err(st, AW_DEV_OUT_OF_GRID);
+                xe = -1.0f;
+            }
+        }
+        stg4(stage, 0, s0) = x; stg4(stage, 1, s0) = y; stg4(stage, 2, s0) = w;
+        if constexpr (NS == 6) {
+            stg4(stage, 3, s0) = ld4(p.ux, i, p.n, vec);
+            stg4(stage, 4, s0) = ld4(p.uy, i, p.n, vec);
+            stg4(stage, 5, s0) = ld4(p.uz, i, p.n, vec);
+        }
     }
+    Win wn;
+    win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, red);   // syncs
+    win_zero<NF>(win, wn);
+    __syncthreads();
+
     float S[NF];
     const int foff = (SET == SET_AMU) ? 4 : 0;
 #pragma unroll
     for (int f = 0; f < NF; ++f) S[f] = Sdev[foff + f];
-
-    int ci[kPPT], cj[kPPT];
-    bool ok[kPPT];
-#pragma unroll
-    for (int k = 0; k < kPPT; ++k) {
-        const bool valid = base + k < p.n;
-        ok[k] = valid && x[k] >= 0.0f && x[k] < g.nxf && y[k] >= 0.0f && y[k] < g.nyf;
-        if (valid && !ok[k]) set_err(st, AW_DEV_OUT_OF_GRID);
-        ci[k] = ok[k] ? static_cast<int>(x[k]) : 0;
-        cj[k] = ok[k] ? static_cast<int>(y[k]) : 0;
-    }
-    int ir, jr;
-    ref_cell(p, c0, g, ir, jr);
-    WinDep<NF, 1 << 30> win;
-    win.sacc = sacc;
-    win.setup(ci, cj, ok, ir, jr, g, red);
-    win.use = static_cast<long long>(win.W) * win.H <= wmaxc;
-    win.zero();
-    __syncthreads();
-
-    Run<NF> run;
-    run.cw = -1;
-    run.clear();
-    unsigned long long nslow = 0;
-#pragma unroll
-    for (int k = 0; k < kPPT; ++k) {
-        if (!ok[k]) continue;
-        const Cic s = cic(x[k], y[k]);
-        const float coef = __double2float_rn(qoa * static_cast<double>(w[k]));
+    unsigned nslow = 0;
+#pragma unroll 1
+    for (int j = 0; j < kChunk / kThreads; ++j) {
+        const int s = j * kThreads + threadIdx.x;
+        const float x = stg(stage, 0, s), y = stg(stage, 1, s);
+        const bool valid = x >= 0.0f;
+        const Cic c = cic(valid ? x : 0.0f, valid ? y : 0.0f);
+        const float coef = __double2float_rn(qoa * static_cast<double>(stg(stage, 2, s)));
         float cf[NF];
-        src_coefs<SET>(coef, ux[k], uy[k], uz[k], cf);
+        if constexpr (NS == 6) src_coefs<SET>(coef, stg(stage, 3, s), stg(stage, 4, s), stg(stage, 5, s), cf);
+        else src_coefs<SET>(coef, 0.f, 0.f, 0.f, cf);
 #pragma unroll
         for (int f = 0; f < NF; ++f) cf[f] = __fmul_rn(cf[f], S[f]);
-        int g0, g1, g2, g3;
-        corner_cells(s, g, g0, g1, g2, g3);
-        deposit_particle<NF, 1 << 30>(win, run, s, cf, g0, g1, g2, g3, acc, g, st, nslow);
+        float wv[4];
+        weights(c, wv);
+        win_deposit<NF>(win, wn, valid, c.i0, c.j0, wv, cf, acc, g, nslow);
     }
-    if (win.use) run.flush(sacc, win.W);
     __syncthreads();
-    win.flush(acc, g);
-    if (nslow) atomicAdd(&st->slow, nslow);
+    win_flush<NF>(win, wn, acc, g);
+    if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
     if (threadIdx.x == 0) {
         atomicAdd(&st->chunks, 1ull);
-        if (!win.use) atomicAdd(&st->overflow, 1ull);
+        if (!wn.use) atomicAdd(&st->overflow, 1ull);
     }
 }
 
 // ---------------------------------------------------------------------------
-// dcu deposit. gb: [ncell][8] = Ex Ey Ez Bx | By Bz . . (E = E_L + pump, B total)
+// EM gather from the interleaved buffer gb[ncell][8] = Ex Ey Ez Bx | By Bz . .
 __device__ __forceinline__ void gather_em(const float* __restrict__ gb, const Cic& s, const Geo& g,
                                           float& ex, float& ey, float& ez,
                                           float& bx, float& by, float& bz) {
@@ -224,76 +270,78 @@ __device__ __forceinline__ float dcu_scale(const DevState* st, float abs_qm) {
     return scale_for_bound(bound);
 }
 
-__global__ void __launch_bounds__(kThreads)
+// dcu deposit: stage = x, y, ax, ay, az (the three scaled coefficients).
+__global__ void __launch_bounds__(kThreads, 2)
 k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restrict__ gb,
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st) {
-    constexpr int NF = 3;
+    constexpr int NF = 3, NS = 5;
     extern __shared__ __align__(16) unsigned char smem[];
-    long long* sacc = reinterpret_cast<long long*>(smem);
-    int* red = reinterpret_cast<int*>(smem + static_cast<size_t>(wmaxc) * NF * 8);
+    float* stage = reinterpret_cast<float*>(smem);
+    int* win = reinterpret_cast<int*>(smem + static_cast<size_t>(NS) * kChunk * 4);
+    int* red = win + wmaxc * NF;
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
-    const long long base = c0 + static_cast<long long>(threadIdx.x) * kPPT;
     const bool vec = p.vec_ok != 0;
-    float x[kPPT], y[kPPT], w[kPPT], ux[kPPT], uy[kPPT], uz[kPPT];
-    load8(p.x, base, p.n, vec, x);
-    load8(p.y, base, p.n, vec, y);
-    load8(p.w, base, p.n, vec, w);
-    load8(p.ux, base, p.n, vec, ux);
-    load8(p.uy, base, p.n, vec, uy);
-    load8(p.uz, base, p.n, vec, uz);
     const float S = dcu_scale(st, abs_qm);
     if (blockIdx.x == 0 && threadIdx.x == 0) { st->S_dcu[0] = S; st->S_dcu[1] = S; st->S_dcu[2] = S; }
-
-    int ci[kPPT], cj[kPPT];
-    bool ok[kPPT];
-#pragma unroll
-    for (int k = 0; k < kPPT; ++k) {
-        const bool valid = base + k < p.n;
-        ok[k] = valid && x[k] >= 0.0f && x[k] < g.nxf && y[k] >= 0.0f && y[k] < g.nyf;
-        if (valid && !ok[k]) set_err(st, AW_DEV_OUT_OF_GRID);
-        ci[k] = ok[k] ? static_cast<int>(x[k]) : 0;
-        cj[k] = ok[k] ? static_cast<int>(y[k]) : 0;
-    }
     int ir, jr;
     ref_cell(p, c0, g, ir, jr);
-    WinDep<NF, 1 << 30> win;
-    win.sacc = sacc;
-    win.setup(ci, cj, ok, ir, jr, g, red);
-    win.use = static_cast<long long>(win.W) * win.H <= wmaxc;
-    win.zero();
-    __syncthreads();
-
-    Run<NF> run;
-    run.cw = -1;
-    run.clear();
-    unsigned long long nslow = 0;
+    BBox bb;
+#pragma unroll 1
+    for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
+        const int s0 = it * 4 * kThreads + 4 * threadIdx.x;
+        const long long i = c0 + s0;
+        float4 x = ld4(p.x, i, p.n, vec);
+        const float4 y = ld4(p.y, i, p.n, vec), w = ld4(p.w, i, p.n, vec);
+        const float4 ux = ld4(p.ux, i, p.n, vec), uy = ld4(p.uy, i, p.n, vec), uz = ld4(p.uz, i, p.n, vec);
+        float4 ax = make_float4(0.f, 0.f, 0.f, 0.f), ay = ax, az = ax;
 #pragma unroll
-    for (int k = 0; k < kPPT; ++k) {
-        if (!ok[k]) continue;
-        const Cic s = cic(x[k], y[k]);
-        float ex, ey, ez, bx, by, bz;
-        gather_em(gb, s, g, ex, ey, ez, bx, by, bz);
-        const float vx = ux[k], vy = uy[k], vz = uz[k];
-        const float coef = __double2float_rn(qm2oa * static_cast<double>(w[k]));
-        const float cx = __fmaf_rn(vy, bz, -__fmul_rn(vz, by));
-        const float cy = __fmaf_rn(vz, bx, -__fmul_rn(vx, bz));
-        const float cz = __fmaf_rn(vx, by, -__fmul_rn(vy, bx));
-        float cf[NF];
-        cf[0] = __fmul_rn(__fmul_rn(coef, __fadd_rn(ex, cx)), S);
-        cf[1] = __fmul_rn(__fmul_rn(coef, __fadd_rn(ey, cy)), S);
-        cf[2] = __fmul_rn(__fmul_rn(coef, __fadd_rn(ez, cz)), S);
-        int g0, g1, g2, g3;
-        corner_cells(s, g, g0, g1, g2, g3);
-        deposit_particle<NF, 1 << 30>(win, run, s, cf, g0, g1, g2, g3, acc, g, st, nslow);
+        for (int e = 0; e < 4; ++e) {
+            float& xe = comp(x, e);
+            const float ye = compc(y, e);
+            if (i + e < p.n && in_grid(xe, ye, g)) {
+                const Cic s = cic(xe, ye);
+                bb.add(s.i0, s.j0, ir, jr, g);
+                float ex, ey, ez, bx, by, bz;
+                gather_em(gb, s, g, ex, ey, ez, bx, by, bz);
+                const float vx = compc(ux, e), vy = compc(uy, e), vz = compc(uz, e);
+                const float coef = __double2float_rn(qm2oa * static_cast<double>(compc(w, e)));
+                const float cx = __fmaf_rn(vy, bz, -__fmul_rn(vz, by));
+                const float cy = __fmaf_rn(vz, bx, -__fmul_rn(vx, bz));
+                const float cz = __fmaf_rn(vx, by, -__fmul_rn(vy, bx));
+                comp(ax, e) = __fmul_rn(__fmul_rn(coef, __fadd_rn(ex, cx)), S);
+                comp(ay, e) = __fmul_rn(__fmul_rn(coef, __fadd_rn(ey, cy)), S);
+                comp(az, e) = __fmul_rn(__fmul_rn(coef, __fadd_rn(ez, cz)), S);
+            } else {
+                if (i + e < p.n) set_err(st, AW_DEV_OUT_OF_GRID);
+                xe = -1.0f;
+            }
+        }
+        stg4(stage, 0, s0) = x; stg4(stage, 1, s0) = y;
+        stg4(stage, 2, s0) = ax; stg4(stage, 3, s0) = ay; stg4(stage, 4, s0) = az;
     }
-    if (win.use) run.flush(sacc, win.W);
+    Win wn;
+    win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, red);
+    win_zero<NF>(win, wn);
     __syncthreads();
-    win.flush(acc, g);
-    if (nslow) atomicAdd(&st->slow, nslow);
+    unsigned nslow = 0;
+#pragma unroll 1
+    for (int j = 0; j < kChunk / kThreads; ++j) {
+        const int s = j * kThreads + threadIdx.x;
+        const float x = stg(stage, 0, s), y = stg(stage, 1, s);
+        const bool valid = x >= 0.0f;
+        const Cic c = cic(valid ? x : 0.0f, valid ? y : 0.0f);
+        const float cf[NF] = {stg(stage, 2, s), stg(stage, 3, s), stg(stage, 4, s)};
+        float wv[4];
+        weights(c, wv);
+        win_deposit<NF>(win, wn, valid, c.i0, c.j0, wv, cf, acc, g, nslow);
+    }
+    __syncthreads();
+    win_flush<NF>(win, wn, acc, g);
+    if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
     if (threadIdx.x == 0) {
         atomicAdd(&st->chunks, 1ull);
-        if (!win.use) atomicAdd(&st->overflow, 1ull);
+        if (!wn.use) atomicAdd(&st->overflow, 1ull);
     }
 }
 
@@ -306,100 +354,95 @@ struct PushP {
     int    write_cell;
 };
 
-// Fused ES step kernel.
-__global__ void __launch_bounds__(kThreads)
+// Fused ES step kernel: stage = new x, y, w.
+__global__ void __launch_bounds__(kThreads, 3)
 k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                   double qoa, unsigned long long* __restrict__ acc, int wmaxc,
                   double* __restrict__ part, DevState* st) {
-    constexpr int NF = 1;
+    constexpr int NF = 1, NS = 3;
     extern __shared__ __align__(16) unsigned char smem[];
-    long long* sacc = reinterpret_cast<long long*>(smem);
-    int* red = reinterpret_cast<int*>(smem + static_cast<size_t>(wmaxc) * NF * 8);
+    float* stage = reinterpret_cast<float*>(smem);
+    int* win = reinterpret_cast<int*>(smem + static_cast<size_t>(NS) * kChunk * 4);
+    int* red = win + wmaxc * NF;
     __shared__ double dsh[4 * (kThreads / 32)];
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
-    const long long base = c0 + static_cast<long long>(threadIdx.x) * kPPT;
     const bool vec = p.vec_ok != 0;
-    float x[kPPT], y[kPPT], w[kPPT], ux[kPPT], uy[kPPT], uz[kPPT];
-    load8(p.x, base, p.n, vec, x);
-    load8(p.y, base, p.n, vec, y);
-    load8(p.ux, base, p.n, vec, ux);
-    load8(p.uy, base, p.n, vec, uy);
-    load8(p.uz, base, p.n, vec, uz);
-    load8(p.w, base, p.n, vec, w);
     const float S = st->S_next[0];
     int ir, jr;
     ref_cell(p, c0, g, ir, jr);
-
-    int ci[kPPT], cj[kPPT];
-    bool ok[kPPT];
+    BBox bb;
     double ke = 0, px = 0, py = 0, pz = 0;
     const float2* q = reinterpret_cast<const float2*>(gb);
+#pragma unroll 1
+    for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
+        const int s0 = it * 4 * kThreads + 4 * threadIdx.x;
+        const long long i = c0 + s0;
+        float4 x = ld4(p.x, i, p.n, vec), y = ld4(p.y, i, p.n, vec);
+        float4 ux = ld4(p.ux, i, p.n, vec), uy = ld4(p.uy, i, p.n, vec), uz = ld4(p.uz, i, p.n, vec);
+        const float4 w = ld4(p.w, i, p.n, vec);
+        int4 cell = make_int4(0, 0, 0, 0);
+        float4 xs = x;
 #pragma unroll
-    for (int k = 0; k < kPPT; ++k) {
-        const bool valid = base + k < p.n;
-        ok[k] = false;
-        ci[k] = cj[k] = 0;
-        if (!valid) continue;
-        const bool inb = x[k] >= 0.0f && x[k] < g.nxf && y[k] >= 0.0f && y[k] < g.nyf;
-        if (!inb) { set_err(st, AW_DEV_OUT_OF_GRID); continue; }
-        const Cic s = cic(x[k], y[k]);
-        const int i1 = wrap_once(s.i0 + 1, g.nx);
-        const int r0 = s.j0 * g.nx, r1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
-        const float2 e0 = __ldg(q + r0 + s.i0), e1 = __ldg(q + r0 + i1);
-        const float2 e2 = __ldg(q + r1 + s.i0), e3 = __ldg(q + r1 + i1);
-        const float ex = gather4(s, e0.x, e1.x, e2.x, e3.x);
-        const float ey = gather4(s, e0.y, e1.y, e2.y, e3.y);
-        boris_es(ux[k], uy[k], uz[k], ex, ey, pp.qmh, pp.has_b0 != 0, pp.b0x, pp.b0y, pp.b0z);
-        x[k] = wrap_pos(move1(x[k], ux[k], pp.dt, g.dx), g.nxf);
-        y[k] = wrap_pos(move1(y[k], uy[k], pp.dt, g.dy), g.nyf);
-        cell_ij(x[k], y[k], g, ci[k], cj[k]);
-        ok[k] = x[k] >= 0.0f && x[k] < g.nxf && y[k] >= 0.0f && y[k] < g.nyf;   // false for NaN
-        const double dw = w[k], du = ux[k], dv = uy[k], dz = uz[k];
-        ke += dw * (du * du + dv * dv + dz * dz);
-        px += dw * du; py += dw * dv; pz += dw * dz;
+        for (int e = 0; e < 4; ++e) {
+            comp(xs, e) = -1.0f;
+            if (i + e >= p.n) continue;
+            float& xe = comp(x, e);
+            float& ye = comp(y, e);
+            if (!in_grid(xe, ye, g)) { set_err(st, AW_DEV_OUT_OF_GRID); continue; }
+            const Cic s = cic(xe, ye);
+            const int i1 = wrap_once(s.i0 + 1, g.nx);
+            const int r0 = s.j0 * g.nx, r1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
+            const float2 e0 = __ldg(q + r0 + s.i0), e1 = __ldg(q + r0 + i1);
+            const float2 e2 = __ldg(q + r1 + s.i0), e3 = __ldg(q + r1 + i1);
+            const float ex = gather4(s, e0.x, e1.x, e2.x, e3.x);
+            const float ey = gather4(s, e0.y, e1.y, e2.y, e3.y);
+            float& u = comp(ux, e); float& v = comp(uy, e); float& wz = comp(uz, e);
+            boris_es(u, v, wz, ex, ey, pp.qmh, pp.has_b0 != 0, pp.b0x, pp.b0y, pp.b0z);
+            xe = wrap_pos(move1(xe, u, pp.dt, g.dx), g.nxf);
+            ye = wrap_pos(move1(ye, v, pp.dt, g.dy), g.nyf);
+            int ci, cj;
+            cell_ij(xe, ye, g, ci, cj);
+            compi(cell, e) = cj * g.nx + ci;
+            if (in_grid(xe, ye, g)) {
+                bb.add(ci, cj, ir, jr, g);
+                comp(xs, e) = xe;
+            }
+            const double dw = compc(w, e), du = u, dv = v, dz = wz;
+            ke += dw * (du * du + dv * dv + dz * dz);
+            px += dw * du; py += dw * dv; pz += dw * dz;
+        }
+        st4(p.x, i, p.n, vec, x);
+        st4(p.y, i, p.n, vec, y);
+        st4(p.ux, i, p.n, vec, ux);
+        st4(p.uy, i, p.n, vec, uy);
+        st4(p.uz, i, p.n, vec, uz);
+        if (pp.write_cell && p.cell) st4i(p.cell, i, p.n, vec, cell);
+        stg4(stage, 0, s0) = xs; stg4(stage, 1, s0) = y; stg4(stage, 2, s0) = w;
     }
-    store8(p.x, base, p.n, vec, x);
-    store8(p.y, base, p.n, vec, y);
-    store8(p.ux, base, p.n, vec, ux);
-    store8(p.uy, base, p.n, vec, uy);
-    store8(p.uz, base, p.n, vec, uz);
-    if (pp.write_cell && p.cell) {
-        int cell[kPPT];
-#pragma unroll
-        for (int k = 0; k < kPPT; ++k) cell[k] = cj[k] * g.nx + ci[k];
-        store8i(p.cell, base, p.n, vec, cell);
-    }
-
-    WinDep<NF, 1 << 30> win;
-    win.sacc = sacc;
-    win.setup(ci, cj, ok, ir, jr, g, red);
-    win.use = static_cast<long long>(win.W) * win.H <= wmaxc;
-    win.zero();
+    Win wn;
+    win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, red);
+    win_zero<NF>(win, wn);
     __syncthreads();
-
-    Run<NF> run;
-    run.cw = -1;
-    run.clear();
-    unsigned long long nslow = 0;
-#pragma unroll
-    for (int k = 0; k < kPPT; ++k) {
-        if (!ok[k]) continue;
-        const Cic s = cic(x[k], y[k]);
-        float cf[NF];
-        cf[0] = __fmul_rn(__double2float_rn(qoa * static_cast<double>(w[k])), S);
-        int g0, g1, g2, g3;
-        corner_cells(s, g, g0, g1, g2, g3);
-        deposit_particle<NF, 1 << 30>(win, run, s, cf, g0, g1, g2, g3, acc, g, st, nslow);
+    unsigned nslow = 0;
+#pragma unroll 2
+    for (int j = 0; j < kChunk / kThreads; ++j) {
+        const int s = j * kThreads + threadIdx.x;
+        const float x = stg(stage, 0, s), y = stg(stage, 1, s);
+        const bool valid = x >= 0.0f;
+        const Cic c = cic(valid ? x : 0.0f, valid ? y : 0.0f);
+        const float cf[NF] = {__fmul_rn(__double2float_rn(qoa * static_cast<double>(stg(stage, 2, s))), S)};
+        float wv[4];
+        weights(c, wv);
+        win_deposit<NF>(win, wn, valid, c.i0, c.j0, wv, cf, acc, g, nslow);
     }
-    if (win.use) run.flush(sacc, win.W);
     __syncthreads();
-    win.flush(acc, g);
+    win_flush<NF>(win, wn, acc, g);
     block_sum4(ke, px, py, pz, part, dsh);
-    if (nslow) atomicAdd(&st->slow, nslow);
+    if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
     if (threadIdx.x == 0) {
         atomicAdd(&st->chunks, 1ull);
-        if (!win.use) atomicAdd(&st->overflow, 1ull);
+        if (!wn.use) atomicAdd(&st->overflow, 1ull);
         if (blockIdx.x == 0) {
             st->S_pend[0] = S;
             st->step += 1;
@@ -407,111 +450,114 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     }
 }
 
-// Fused Darwin step kernel. gb: [ncell][8] = E_total (3), B total (3).
-__global__ void __launch_bounds__(kThreads)
+// Fused Darwin step kernel: stage = new x, y, w, ux, uy, uz.
+__global__ void __launch_bounds__(kThreads, 2)
 k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                   double qoa, unsigned long long* __restrict__ acc, int wmaxc,
                   double* __restrict__ part, DevState* st) {
-    constexpr int NF = 8;
+    constexpr int NF = 8, NS = 6;
     extern __shared__ __align__(16) unsigned char smem[];
-    long long* sacc = reinterpret_cast<long long*>(smem);
-    int* red = reinterpret_cast<int*>(smem + static_cast<size_t>(wmaxc) * NF * 8);
+    float* stage = reinterpret_cast<float*>(smem);
+    int* win = reinterpret_cast<int*>(smem + static_cast<size_t>(NS) * kChunk * 4);
+    int* red = win + wmaxc * NF;
     __shared__ double dsh[4 * (kThreads / 32)];
+    __shared__ unsigned umx[3][kThreads / 32];
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
-    const long long base = c0 + static_cast<long long>(threadIdx.x) * kPPT;
     const bool vec = p.vec_ok != 0;
-    float x[kPPT], y[kPPT], w[kPPT], ux[kPPT], uy[kPPT], uz[kPPT];
-    load8(p.x, base, p.n, vec, x);
-    load8(p.y, base, p.n, vec, y);
-    load8(p.ux, base, p.n, vec, ux);
-    load8(p.uy, base, p.n, vec, uy);
-    load8(p.uz, base, p.n, vec, uz);
-    load8(p.w, base, p.n, vec, w);
     int ir, jr;
     ref_cell(p, c0, g, ir, jr);
-
-    int ci[kPPT], cj[kPPT];
-    bool ok[kPPT];
+    BBox bb;
     double ke = 0, px = 0, py = 0, pz = 0;
     float m0 = 0.f, m1 = 0.f, m2 = 0.f;
+#pragma unroll 1
+    for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
+        const int s0 = it * 4 * kThreads + 4 * threadIdx.x;
+        const long long i = c0 + s0;
+        float4 x = ld4(p.x, i, p.n, vec), y = ld4(p.y, i, p.n, vec);
+        float4 ux = ld4(p.ux, i, p.n, vec), uy = ld4(p.uy, i, p.n, vec), uz = ld4(p.uz, i, p.n, vec);
+        const float4 w = ld4(p.w, i, p.n, vec);
+        int4 cell = make_int4(0, 0, 0, 0);
+        float4 xs = x;
 #pragma unroll
-    for (int k = 0; k < kPPT; ++k) {
-        const bool valid = base + k < p.n;
-        ok[k] = false;
-        ci[k] = cj[k] = 0;
-        if (!valid) continue;
-        const bool inb = x[k] >= 0.0f && x[k] < g.nxf && y[k] >= 0.0f && y[k] < g.nyf;
-        if (!inb) { set_err(st, AW_DEV_OUT_OF_GRID); continue; }
-        const Cic s = cic(x[k], y[k]);
-        float ex, ey, ez, bx, by, bz;
-        gather_em(gb, s, g, ex, ey, ez, bx, by, bz);
-        boris_em(ux[k], uy[k], uz[k], ex, ey, ez, bx, by, bz, pp.qmh);
-        x[k] = wrap_pos(move1(x[k], ux[k], pp.dt, g.dx), g.nxf);
-        y[k] = wrap_pos(move1(y[k], uy[k], pp.dt, g.dy), g.nyf);
-        cell_ij(x[k], y[k], g, ci[k], cj[k]);
-        ok[k] = x[k] >= 0.0f && x[k] < g.nxf && y[k] >= 0.0f && y[k] < g.nyf;
-        m0 = fmaxf(m0, fabsf(ux[k])); m1 = fmaxf(m1, fabsf(uy[k])); m2 = fmaxf(m2, fabsf(uz[k]));
-        const double dw = w[k], du = ux[k], dv = uy[k], dz = uz[k];
-        ke += dw * (du * du + dv * dv + dz * dz);
-        px += dw * du; py += dw * dv; pz += dw * dz;
+        for (int e = 0; e < 4; ++e) {
+            comp(xs, e) = -1.0f;
+            if (i + e >= p.n) continue;
+            float& xe = comp(x, e);
+            float& ye = comp(y, e);
+            if (!in_grid(xe, ye, g)) { set_err(st, AW_DEV_OUT_OF_GRID); continue; }
+            const Cic s = cic(xe, ye);
+            float ex, ey, ez, bx, by, bz;
+            gather_em(gb, s, g, ex, ey, ez, bx, by, bz);
+            float& u = comp(ux, e); float& v = comp(uy, e); float& wz = comp(uz, e);
+            boris_em(u, v, wz, ex, ey, ez, bx, by, bz, pp.qmh);
+            xe = wrap_pos(move1(xe, u, pp.dt, g.dx), g.nxf);
+            ye = wrap_pos(move1(ye, v, pp.dt, g.dy), g.nyf);
+            int ci, cj;
+            cell_ij(xe, ye, g, ci, cj);
+            compi(cell, e) = cj * g.nx + ci;
+            if (in_grid(xe, ye, g)) {
+                bb.add(ci, cj, ir, jr, g);
+                comp(xs, e) = xe;
+            }
+            m0 = fmaxf(m0, fabsf(u)); m1 = fmaxf(m1, fabsf(v)); m2 = fmaxf(m2, fabsf(wz));
+            const double dw = compc(w, e), du = u, dv = v, dz = wz;
+            ke += dw * (du * du + dv * dv + dz * dz);
+            px += dw * du; py += dw * dv; pz += dw * dz;
+        }
+        st4(p.x, i, p.n, vec, x);
+        st4(p.y, i, p.n, vec, y);
+        st4(p.ux, i, p.n, vec, ux);
+        st4(p.uy, i, p.n, vec, uy);
+        st4(p.uz, i, p.n, vec, uz);
+        if (pp.write_cell && p.cell) st4i(p.cell, i, p.n, vec, cell);
+        stg4(stage, 0, s0) = xs; stg4(stage, 1, s0) = y; stg4(stage, 2, s0) = w;
+        stg4(stage, 3, s0) = ux; stg4(stage, 4, s0) = uy; stg4(stage, 5, s0) = uz;
     }
-    store8(p.x, base, p.n, vec, x);
-    store8(p.y, base, p.n, vec, y);
-    store8(p.ux, base, p.n, vec, ux);
-    store8(p.uy, base, p.n, vec, uy);
-    store8(p.uz, base, p.n, vec, uz);
-    if (pp.write_cell && p.cell) {
-        int cell[kPPT];
-#pragma unroll
-        for (int k = 0; k < kPPT; ++k) cell[k] = cj[k] * g.nx + ci[k];
-        store8i(p.cell, base, p.n, vec, cell);
-    }
+    // |u| maxima of the new state (next step's deposit scales): one atomic per block
     m0 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m0)));
     m1 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m1)));
     m2 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m2)));
     if ((threadIdx.x & 31) == 0) {
-        atomicMax(&st->umax_bits[0], __float_as_uint(m0));
-        atomicMax(&st->umax_bits[1], __float_as_uint(m1));
-        atomicMax(&st->umax_bits[2], __float_as_uint(m2));
+        umx[0][threadIdx.x >> 5] = __float_as_uint(m0);
+        umx[1][threadIdx.x >> 5] = __float_as_uint(m1);
+        umx[2][threadIdx.x >> 5] = __float_as_uint(m2);
     }
-
+    Win wn;
+    win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, red);   // syncs
+    win_zero<NF>(win, wn);
+    if (threadIdx.x < 3) {
+        unsigned m = 0;
+        for (int k = 0; k < kThreads / 32; ++k) m = max(m, umx[threadIdx.x][k]);
+        atomicMax(&st->umax_bits[threadIdx.x], m);
+    }
+    __syncthreads();
     float S[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) S[f] = st->S_next[f];
-
-    WinDep<NF, 1 << 30> win;
-    win.sacc = sacc;
-    win.setup(ci, cj, ok, ir, jr, g, red);
-    win.use = static_cast<long long>(win.W) * win.H <= wmaxc;
-    win.zero();
-    __syncthreads();
-
-    Run<NF> run;
-    run.cw = -1;
-    run.clear();
-    unsigned long long nslow = 0;
-#pragma unroll
-    for (int k = 0; k < kPPT; ++k) {
-        if (!ok[k]) continue;
-        const Cic s = cic(x[k], y[k]);
-        const float coef = __double2float_rn(qoa * static_cast<double>(w[k]));
+    unsigned nslow = 0;
+#pragma unroll 1
+    for (int j = 0; j < kChunk / kThreads; ++j) {
+        const int s = j * kThreads + threadIdx.x;
+        const float x = stg(stage, 0, s), y = stg(stage, 1, s);
+        const bool valid = x >= 0.0f;
+        const Cic c = cic(valid ? x : 0.0f, valid ? y : 0.0f);
+        const float coef = __double2float_rn(qoa * static_cast<double>(stg(stage, 2, s)));
         float cf[NF];
-        src_coefs<SET_ALL>(coef, ux[k], uy[k], uz[k], cf);
+        src_coefs<SET_ALL>(coef, stg(stage, 3, s), stg(stage, 4, s), stg(stage, 5, s), cf);
 #pragma unroll
         for (int f = 0; f < NF; ++f) cf[f] = __fmul_rn(cf[f], S[f]);
-        int g0, g1, g2, g3;
-        corner_cells(s, g, g0, g1, g2, g3);
-        deposit_particle<NF, 1 << 30>(win, run, s, cf, g0, g1, g2, g3, acc, g, st, nslow);
+        float wv[4];
+        weights(c, wv);
+        win_deposit<NF>(win, wn, valid, c.i0, c.j0, wv, cf, acc, g, nslow);
     }
-    if (win.use) run.flush(sacc, win.W);
     __syncthreads();
-    win.flush(acc, g);
+    win_flush<NF>(win, wn, acc, g);
     block_sum4(ke, px, py, pz, part, dsh);
-    if (nslow) atomicAdd(&st->slow, nslow);
+    if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
     if (threadIdx.x == 0) {
         atomicAdd(&st->chunks, 1ull);
-        if (!win.use) atomicAdd(&st->overflow, 1ull);
+        if (!wn.use) atomicAdd(&st->overflow, 1ull);
         if (blockIdx.x == 0) {
 #pragma unroll
             for (int f = 0; f < NF; ++f) st->S_pend[f] = S[f];
@@ -524,7 +570,7 @@ inline int nchunks(long long n) { return static_cast<int>(std::max<long long>(1,
 
 // Opt a kernel into its dynamic shared-memory size once per process (never
 // inside a stream capture: aw_init launches every kernel before any capture).
-// Keyed by the kernel's address; the table holds every kernel of this file.
+// Keyed by the kernel's address.
 template <class K>
 void prep_smem(K kern, size_t bytes) {
     static std::mutex mu;
@@ -542,58 +588,38 @@ void prep_smem(K kern, size_t bytes) {
     if (nkeys < 16) { keys[nkeys] = key; vals[nkeys] = bytes; ++nkeys; }
 }
 
+template <int SET>
+void launch_src(Ctx& c, unsigned long long* acc) {
+    constexpr int NF = SetNF<SET>::NF, NS = SetNF<SET>::NS;
+    const size_t sh = smem_bytes(NF, NS);
+    prep_smem(k_deposit_src<SET>, sh);
+    const double qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
+    k_deposit_src<SET><<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(c.parts, c.geo, qoa, c.st->S_pend, acc,
+                                                                        wmax_cells(NF), c.st);
+    AW_LAUNCH();
+}
+
 }  // namespace
 
 // ===========================================================================
 void launch_deposit_src(Ctx& c, int which) {
     if (c.parts.n == 0) return;
-    const double qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
-    const float* S = c.st->S_pend;
-    const int nb = nchunks(c.parts.n);
     switch (which) {
-        case 1: {
-            const size_t sh = smem_bytes(1);
-            prep_smem(k_deposit_src<SET_RHO>, sh);
-            k_deposit_src<SET_RHO><<<nb, kThreads, sh, c.stream>>>(c.parts, c.geo, qoa, S, c.acc_src,
-                                                                   wmax_cells(1), c.st);
-            break;
-        }
-        case 4: {
-            const size_t sh = smem_bytes(4);
-            prep_smem(k_deposit_src<SET_RHOJ>, sh);
-            k_deposit_src<SET_RHOJ><<<nb, kThreads, sh, c.stream>>>(c.parts, c.geo, qoa, S, c.acc_src,
-                                                                    wmax_cells(4), c.st);
-            break;
-        }
-        case -4: {
-            const size_t sh = smem_bytes(4);
-            prep_smem(k_deposit_src<SET_AMU>, sh);
-            // amu accumulators are fields 4..7 of acc_src
-            k_deposit_src<SET_AMU><<<nb, kThreads, sh, c.stream>>>(
-                c.parts, c.geo, qoa, S, c.acc_src + static_cast<size_t>(4) * c.geo.ncell,
-                wmax_cells(4), c.st);
-            break;
-        }
-        case 8: {
-            const size_t sh = smem_bytes(8);
-            prep_smem(k_deposit_src<SET_ALL>, sh);
-            k_deposit_src<SET_ALL><<<nb, kThreads, sh, c.stream>>>(c.parts, c.geo, qoa, S, c.acc_src,
-                                                                   wmax_cells(8), c.st);
-            break;
-        }
+        case 1: launch_src<SET_RHO>(c, c.acc_src); break;
+        case 4: launch_src<SET_RHOJ>(c, c.acc_src); break;
+        case -4: launch_src<SET_AMU>(c, c.acc_src + static_cast<size_t>(4) * c.geo.ncell); break;
+        case 8: launch_src<SET_ALL>(c, c.acc_src); break;
         default: throw Error(AW_ERR_ARG, "deposit_src: bad field set");
     }
-    AW_LAUNCH();
 }
 
 void launch_deposit_dcu(Ctx& c, const float* gb) {
     if (c.parts.n == 0) return;
     const double qm2oa = c.prm.qm * c.prm.qm / (c.geo.dx * c.geo.dy);
-    const size_t sh = smem_bytes(3);
+    const size_t sh = smem_bytes(3, 5);
     prep_smem(k_deposit_dcu, sh);
     k_deposit_dcu<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(
-        c.parts, c.geo, qm2oa, static_cast<float>(std::fabs(c.prm.qm)), gb, c.acc_dcu,
-        wmax_cells(3), c.st);
+        c.parts, c.geo, qm2oa, static_cast<float>(std::fabs(c.prm.qm)), gb, c.acc_dcu, wmax_cells(3), c.st);
     AW_LAUNCH();
 }
 
@@ -606,7 +632,7 @@ void launch_push_deposit_es(Ctx& c) {
     pp.dt = c.prm.dt;
     pp.write_cell = c.write_cell;
     const double qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
-    const size_t sh = smem_bytes(1);
+    const size_t sh = smem_bytes(1, 3);
     prep_smem(k_push_deposit_es, sh);
     k_push_deposit_es<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(
         c.parts, c.geo, pp, c.gb_es, qoa, c.acc_src, wmax_cells(1), c.part_p, c.st);
@@ -620,7 +646,7 @@ void launch_push_deposit_em(Ctx& c) {
     pp.dt = c.prm.dt;
     pp.write_cell = c.write_cell;
     const double qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
-    const size_t sh = smem_bytes(8);
+    const size_t sh = smem_bytes(8, 6);
     prep_smem(k_push_deposit_em, sh);
     k_push_deposit_em<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(
         c.parts, c.geo, pp, c.gb_push, qoa, c.acc_src, wmax_cells(8), c.part_p, c.st);

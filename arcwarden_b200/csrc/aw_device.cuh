@@ -13,14 +13,14 @@
 //                             S and summed in 64-bit integers, so a deposit is a
 //                             function of the particle SET, independent of order,
 //                             thread mapping or atomics scheduling.
-//   * WinDep                — the chunk-window deposit engine: one CTA owns a
-//                             chunk of CHUNK consecutive particles, reduces the
-//                             bounding box of their cells, privatises that window
-//                             of cells in shared memory as int64 accumulators,
-//                             adds register-accumulated runs of same-cell
-//                             contributions with shared atomics and flushes the
-//                             window to the global int64 accumulators with
-//                             red.global.add.u64.
+//   * window deposit engine — one CTA owns a chunk of kChunk consecutive
+//                             particles, reduces the bounding box of their cells,
+//                             privatises that window of cells in shared memory as
+//                             int32 accumulators ([NF][W*H]), sums the
+//                             contributions of warp lanes that share a cell with
+//                             one redux.sync per value (exact integer sums) and
+//                             flushes the window into the global int64
+//                             accumulators with red.global.add.u64.
 //
 // Reference arithmetic being mirrored (paths relative to the ArcWarden tree):
 //   CIC weights           include/pic/grid.hpp:135-155, depositor.hpp:136-146
@@ -39,11 +39,14 @@ constexpr int kThreads = 256;          // CTA size of every particle kernel
 constexpr int kPPT     = 8;            // consecutive particles per thread
 constexpr int kChunk   = kThreads * kPPT;   // particles per CTA chunk (2048)
 
-// Fast-path range of one quantised contribution: |v*S| < 2^22 rounds exactly
-// with one FADD against 1.5*2^23 and fits a 32-bit run accumulator.
-constexpr float kFastLim   = 4194304.0f;      // 2^22
+// Fast-path range of one quantised contribution: |v*S| < 2^20 rounds exactly
+// with one FADD against 1.5*2^23, and a chunk of kChunk = 2048 particles adds at
+// most 2048 such values into one shared-window cell, so the int32 window sums
+// cannot overflow (2048 * 2^20 = 2^31).
+constexpr float kFastLim   = 1048576.0f;      // 2^20
 constexpr float kMagic     = 12582912.0f;     // 1.5 * 2^23
 constexpr int   kMagicBits = 0x4B400000;
+constexpr unsigned kMagicU  = 0x4B400000u;
 
 // Geometry passed by value into every kernel.
 struct Geo {
@@ -97,13 +100,13 @@ __device__ __forceinline__ void set_err(DevState* st, unsigned bits) {
     atomicOr(&st->err, bits);
 }
 
-// Power-of-two scale S such that bound * S < 2^22 (the fast path), from a
+// Power-of-two scale S such that bound * S < 2^20 (the fast path), from a
 // positive bound. Deterministic: a pure function of the bound.
 __host__ __device__ inline float scale_for_bound(float bound) {
     if (!(bound > 0.0f) || !(bound < 3.0e38f)) return 1.0f;
     int e;
     frexpf(bound, &e);            // bound in [2^(e-1), 2^e)
-    int k = 22 - e;               // bound * 2^k < 2^22
+    int k = 20 - e;               // bound * 2^k < 2^20
     if (k > 120) k = 120;
     if (k < -120) k = -120;
     return ldexpf(1.0f, k);
@@ -193,7 +196,7 @@ __device__ __forceinline__ int cell_of(float x, float y, int nx, int ny) {
 
 // ---------------------------------------------------------------------------
 // Fixed-point rounding. q = rint(t) with t = v*S already scaled; exact for the
-// fast path (|t| < 2^22) and identical to llrintf(t) in the C oracle.
+// fast path (|t| < 2^20) and identical to llrintf(t) in the C oracle.
 __device__ __forceinline__ int quant_fast(float t) {
     return __float_as_int(__fadd_rn(t, kMagic)) - kMagicBits;
 }
@@ -243,171 +246,135 @@ __device__ __forceinline__ void store8i(int* __restrict__ a, long long base, lon
 }
 
 // ---------------------------------------------------------------------------
-// Chunk-window deposit engine.
+// Window deposit engine.
 //
-// NF fields are deposited. Per particle the caller supplies the base cell
-// (i0, j0), the four CIC weights and NF coefficients already multiplied by the
-// field scales; contribution (f, corner c) = rint(coef[f] * w[c]).
-//
-// Shared memory: WMAXC cells x NF int64, AoS [cell][NF].
-template <int NF, int WMAXC>
-struct WinDep {
-    static constexpr int kSmemBytes = WMAXC * NF * 8;
-
-    long long* sacc;      // shared accumulators
-    int  ir, jr;          // reference cell (any cell near the chunk)
-    int  mi, mj;          // window origin offset (min wrapped offset)
-    int  W, H;            // window extent in cells
-    bool use;             // window fits shared memory
-
-    // Block-wide bounding box of the wrapped cell offsets of the valid particles.
-    // `red` is 8 ints of shared scratch per warp (kThreads/32 * 4).
-    __device__ void setup(const int (&ci)[kPPT], const int (&cj)[kPPT], const bool (&ok)[kPPT],
-                          int ir_, int jr_, const Geo& g, int* red) {
-        ir = ir_; jr = jr_;
-        int lo_i = 1 << 30, lo_j = 1 << 30, hi_i = -(1 << 30), hi_j = -(1 << 30);
-#pragma unroll
-        for (int k = 0; k < kPPT; ++k) {
-            if (ok[k]) {
-                const int di = wrap_signed(ci[k] - ir, g.nx);
-                const int dj = wrap_signed(cj[k] - jr, g.ny);
-                lo_i = min(lo_i, di); hi_i = max(hi_i, di);
-                lo_j = min(lo_j, dj); hi_j = max(hi_j, dj);
-            }
-        }
-        lo_i = __reduce_min_sync(0xffffffffu, lo_i);
-        lo_j = __reduce_min_sync(0xffffffffu, lo_j);
-        hi_i = __reduce_max_sync(0xffffffffu, hi_i);
-        hi_j = __reduce_max_sync(0xffffffffu, hi_j);
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        if (lane == 0) {
-            red[warp * 4 + 0] = lo_i; red[warp * 4 + 1] = lo_j;
-            red[warp * 4 + 2] = hi_i; red[warp * 4 + 3] = hi_j;
-        }
-        __syncthreads();
-        lo_i = red[0]; lo_j = red[1]; hi_i = red[2]; hi_j = red[3];
-#pragma unroll
-        for (int w = 1; w < kThreads / 32; ++w) {
-            lo_i = min(lo_i, red[w * 4 + 0]); lo_j = min(lo_j, red[w * 4 + 1]);
-            hi_i = max(hi_i, red[w * 4 + 2]); hi_j = max(hi_j, red[w * 4 + 3]);
-        }
-        if (hi_i < lo_i) { lo_i = hi_i = 0; lo_j = hi_j = 0; }   // no valid particle
-        mi = lo_i; mj = lo_j;
-        W = hi_i - lo_i + 2;
-        H = hi_j - lo_j + 2;
-        use = (static_cast<long long>(W) * H <= WMAXC);
-    }
-    // zero the used part of the window; caller syncs afterwards
-    __device__ void zero() {
-        if (!use) return;
-        const int m = W * H * NF;
-        for (int i = threadIdx.x; i < m; i += kThreads) sacc[i] = 0;
-    }
-    __device__ __forceinline__ int wcell(int ci, int cj, const Geo& g) const {
-        return (wrap_signed(cj - jr, g.ny) - mj) * W + (wrap_signed(ci - ir, g.nx) - mi);
-    }
-    // Flush the window into the global accumulators acc[f*ncell + cell].
-    // Caller syncs before calling.
-    __device__ void flush(unsigned long long* __restrict__ acc, const Geo& g) {
-        if (!use) return;
-        const int m = W * H;
-        for (int c = threadIdx.x; c < m; c += kThreads) {
-            const int wi = c % W, wj = c / W;
-            const int gc = wrap_far(jr + mj + wj, g.ny) * g.nx + wrap_far(ir + mi + wi, g.nx);
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const long long v = sacc[c * NF + f];
-                if (v != 0) atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gc,
-                                      static_cast<unsigned long long>(v));
-            }
-        }
-    }
+// A chunk's window is the bounding box of its particles' base cells, taken as
+// wrapped offsets from a reference cell (any cell near the chunk), plus one cell
+// for the +1 CIC corner. Window cell (di, dj) maps back to grid cell
+// (wrap(ir + mi + di), wrap(jr + mj + dj)), so correctness never depends on the
+// reference cell; only the window size does.
+struct Win {
+    int ir, jr;      // reference cell
+    int mi, mj;      // min wrapped offsets
+    int W, H;        // extent in cells (incl. the +1 corner)
+    int WH;
+    bool use;        // fits the shared window capacity
 };
 
-// Per-thread run accumulator: contributions of consecutive particles that share
-// the same base cell are summed exactly in 32-bit registers (each fast-path value
-// is < 2^22 in magnitude and a run holds at most kPPT particles).
-template <int NF>
-struct Run {
-    int cw;              // window cell of the run's base corner, -1 = empty
-    int a[NF][4];
+// Block-wide min/max of the offsets, then the window geometry. `red` is
+// kThreads/32*4 ints of shared scratch. Every thread of the block calls it.
+__device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, int hi_j, int ir, int jr,
+                                          int wmaxc, int* red) {
+    lo_i = __reduce_min_sync(0xffffffffu, lo_i);
+    lo_j = __reduce_min_sync(0xffffffffu, lo_j);
+    hi_i = __reduce_max_sync(0xffffffffu, hi_i);
+    hi_j = __reduce_max_sync(0xffffffffu, hi_j);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        red[warp * 4 + 0] = lo_i; red[warp * 4 + 1] = lo_j;
+        red[warp * 4 + 2] = hi_i; red[warp * 4 + 3] = hi_j;
+    }
+    __syncthreads();
+    lo_i = red[0]; lo_j = red[1]; hi_i = red[2]; hi_j = red[3];
+#pragma unroll
+    for (int k = 1; k < kThreads / 32; ++k) {
+        lo_i = min(lo_i, red[k * 4 + 0]); lo_j = min(lo_j, red[k * 4 + 1]);
+        hi_i = max(hi_i, red[k * 4 + 2]); hi_j = max(hi_j, red[k * 4 + 3]);
+    }
+    if (hi_i < lo_i) { lo_i = hi_i = 0; lo_j = hi_j = 0; }   // no valid particle
+    w.ir = ir; w.jr = jr;
+    w.mi = lo_i; w.mj = lo_j;
+    w.W = hi_i - lo_i + 2;
+    w.H = hi_j - lo_j + 2;
+    w.use = static_cast<long long>(w.W) * w.H <= wmaxc;
+    w.WH = w.use ? w.W * w.H : 0;
+}
 
-    __device__ __forceinline__ void clear() {
+// Zero NF window planes; the caller syncs afterwards.
+template <int NF>
+__device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
+    const int m = NF * w.WH;
+    for (int i = threadIdx.x; i < m; i += kThreads) s[i] = 0;
+}
+
+// Flush the window into the global int64 accumulators acc[f*ncell + cell].
+// The caller syncs before calling.
+template <int NF>
+__device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& w,
+                                          unsigned long long* __restrict__ acc, const Geo& g) {
+    for (int c = threadIdx.x; c < w.WH; c += kThreads) {
+        const int wi = c % w.W, wj = c / w.W;
+        const int gc = wrap_far(w.jr + w.mj + wj, g.ny) * g.nx + wrap_far(w.ir + w.mi + wi, g.nx);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            const int v = s[f * w.WH + c];
+            if (v != 0)
+                atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gc,
+                          static_cast<unsigned long long>(static_cast<long long>(v)));
+        }
+    }
+}
+
+// Wrapped offset of a cell from the window's reference cell.
+__device__ __forceinline__ int win_off(int c, int r, int n) { return wrap_signed(c - r, n); }
+
+// Deposit one particle per lane. All 32 lanes of the warp must call this
+// together (invalid lanes pass valid = false). cs[f] = coefficient * scale;
+// the contribution of field f at corner c is rint(cs[f] * w[c]).
+//
+// Lanes whose particles share a base cell are summed with one redux.sync per
+// value and the group leader adds the sum to the window; when the warp holds
+// more than 8 distinct cells each lane adds its own values. Values outside the
+// fast range (and every value when the window is unused) go straight to the
+// global accumulators as exact 64-bit integers.
+template <int NF>
+__device__ __forceinline__ void win_deposit(int* __restrict__ s, const Win& w, bool valid,
+                                            int ci, int cj, const float (&wv)[4], const float (&cs)[NF],
+                                            unsigned long long* __restrict__ gacc, const Geo& g,
+                                            unsigned& nslow) {
+    const int lane = threadIdx.x & 31;
+    bool fast = valid && w.use;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) fast = fast && (fabsf(cs[f]) < kFastLim);
+    const int cw = fast ? (win_off(cj, w.jr, g.ny) - w.mj) * w.W + (win_off(ci, w.ir, g.nx) - w.mi) : -1;
+    const unsigned peers = __match_any_sync(0xffffffffu, cw);
+    const int leader = __ffs(peers) - 1;
+    const unsigned leaders = __ballot_sync(0xffffffffu, lane == leader);
+    const bool agg = __popc(leaders) <= 8;
+    const unsigned ngroup = static_cast<unsigned>(__popc(peers));
+    const int offs[4] = {0, 1, w.W, w.W + 1};
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            // fast lanes: bits of t + 1.5*2^23 (their integer sum minus
+            // count * magic bits is the exact sum of rint(t)); others add 0.
+            const float t = __fmul_rn(cs[f], wv[c]);
+            const unsigned bits = fast ? __float_as_uint(__fadd_rn(t, kMagic)) : kMagicU;
+            if (agg) {
+                // modular (wrapping) unsigned sum; the true sum fits in int32
+                const int sum = static_cast<int>(__reduce_add_sync(peers, bits) - ngroup * kMagicU);
+                if (lane == leader && cw >= 0 && sum != 0) atomicAdd(s + f * w.WH + cw + offs[c], sum);
+            } else if (cw >= 0) {
+                const int q = static_cast<int>(bits - kMagicU);
+                if (q != 0) atomicAdd(s + f * w.WH + cw + offs[c], q);
+            }
+        }
+    }
+    if (valid && !fast) {
+        // exact slow path (window too small, or a value beyond the fast range)
+        const int i1 = wrap_once(ci + 1, g.nx);
+        const int r0 = cj * g.nx, r1 = wrap_once(cj + 1, g.ny) * g.nx;
+        const int gcs[4] = {r0 + ci, r0 + i1, r1 + ci, r1 + i1};
 #pragma unroll
         for (int f = 0; f < NF; ++f)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) a[f][c] = 0;
-    }
-    // Add the run into the shared window. Corners are visited in a lane-rotated
-    // order so lanes that flush the same cell at once touch different addresses.
-    __device__ __forceinline__ void flush(long long* __restrict__ s, int W) {
-        if (cw < 0) return;
-        const int r = threadIdx.x & 3;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int c = (q + r) & 3;
-            const int off = (c == 0) ? 0 : (c == 1) ? 1 : (c == 2) ? W : W + 1;
-            long long* base = s + static_cast<size_t>(cw + off) * NF;
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const int v = (c == 0) ? a[f][0] : (c == 1) ? a[f][1] : (c == 2) ? a[f][2] : a[f][3];
-                if (v != 0)
-                    atomicAdd(reinterpret_cast<unsigned long long*>(base + f),
-                              static_cast<unsigned long long>(static_cast<long long>(v)));
-            }
-        }
-    }
-};
-
-// Deposit one particle through the window (or, when the window is unused, the
-// exact global slow path). coefS[f] = coefficient * scale; cells c0..c3 are the
-// wrapped global corner cells (needed only for the slow path).
-template <int NF, int WMAXC>
-__device__ __forceinline__ void deposit_particle(WinDep<NF, WMAXC>& win, Run<NF>& run,
-                                                 const Cic& s, const float (&coefS)[NF],
-                                                 int gc0, int gc1, int gc2, int gc3,
-                                                 unsigned long long* __restrict__ gacc,
-                                                 const Geo& g, DevState* st,
-                                                 unsigned long long& nslow) {
-    const float wv[4] = {s.w0, s.w1, s.w2, s.w3};
-    const int   gcs[4] = {gc0, gc1, gc2, gc3};
-    if (win.use) {
-        const int cw = win.wcell(s.i0, s.j0, g);
-        if (cw != run.cw) {
-            run.flush(win.sacc, win.W);
-            run.cw = cw;
-            run.clear();
-        }
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-#pragma unroll
             for (int c = 0; c < 4; ++c) {
-                const float t = __fmul_rn(coefS[f], wv[c]);
-                if (fabsf(t) < kFastLim) {
-                    run.a[f][c] += quant_fast(t);
-                } else {
-                    if (!isfinite(t)) set_err(st, 1u);
-                    ++nslow;
-                    atomicAdd(gacc + static_cast<size_t>(f) * g.ncell + gcs[c],
-                              static_cast<unsigned long long>(__float2ll_rn(t)));
-                }
-            }
-        }
-    } else {
-#pragma unroll
-        for (int f = 0; f < NF; ++f) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const float t = __fmul_rn(coefS[f], wv[c]);
-                if (!isfinite(t)) set_err(st, 1u);
-                ++nslow;
-                const long long q = (fabsf(t) < kFastLim) ? static_cast<long long>(quant_fast(t))
-                                                          : __float2ll_rn(t);
+                const long long q = __float2ll_rn(__fmul_rn(cs[f], wv[c]));
                 if (q != 0)
-                    atomicAdd(gacc + static_cast<size_t>(f) * g.ncell + gcs[c],
-                              static_cast<unsigned long long>(q));
+                    atomicAdd(gacc + static_cast<size_t>(f) * g.ncell + gcs[c], static_cast<unsigned long long>(q));
             }
-        }
+        ++nslow;
     }
 }
 

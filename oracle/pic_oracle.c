@@ -15,7 +15,7 @@
 #include <omp.h>
 #endif
 
-#define FAST_LIM 4194304.0f
+#define FAST_LIM 1048576.0f
 static const double kTwoPi = 6.28318530717958647692;
 
 static inline int wrap_once(int i, int n) { if (i >= n) i -= n; if (i < 0) i += n; return i; }
@@ -216,7 +216,7 @@ float or_scale_for_bound(float b) {
     if (!(b > 0.0f) || !(b < 3.0e38f)) return 1.0f;
     int e;
     frexpf(b, &e);
-    int k = 22 - e;
+    int k = 20 - e;
     if (k > 120) k = 120;
     if (k < -120) k = -120;
     return ldexpf(1.0f, k);
