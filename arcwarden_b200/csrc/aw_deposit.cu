@@ -22,9 +22,10 @@
 //           128-bit stores of the new state, and a copy of what the deposit
 //           needs into a shared-memory stage; bounding box of the cells.
 //   window  block-wide bounding box -> int32 shared window [NF][W*H].
-//   pass 2  lane l of warp w deposits stage slot j*256 + 32w + l, so a warp
-//           holds 32 consecutive particles (usually one or two cells) and
-//           win_deposit sums them with redux.sync before one shared atomic.
+//   pass 2  each lane deposits 8 consecutive particles from the stage,
+//           summing same-cell runs exactly in integer registers; the lanes of a
+//           warp sit 64 particles apart (different cells), so each run's flush
+//           is a set of conflict-free int32 shared atomics.
 //   flush   window -> global int64 accumulators (red.global.add.u64).
 #include "aw_internal.h"
 
@@ -155,9 +156,43 @@ struct BBox {
     }
 };
 
-// Stage plane f, slot s.
-__device__ __forceinline__ float& stg(float* st, int f, int s) { return st[f * kChunk + s]; }
-__device__ __forceinline__ float4& stg4(float* st, int f, int s) { return reinterpret_cast<float4*>(st + f * kChunk)[s >> 2]; }
+// Stage plane f, quad q (4 consecutive particles), stored swizzled.
+__device__ __forceinline__ float4& stq(float* st, int f, int q) {
+    return reinterpret_cast<float4*>(st + f * kChunk)[stage_quad(q)];
+}
+
+// Pass 2: lane l of warp w deposits quads 16l + 2w + {0,1}, i.e. the 8
+// consecutive particles 64l + 8w .. 64l + 8w + 7, accumulating same-cell runs
+// in registers; lanes sit 64 particles apart, so their flushes rarely collide.
+// coef(v, e, cs) fills the scaled coefficients of element e of the quad planes v.
+template <int NF, int NS, class CoefFn>
+__device__ __forceinline__ void pass2(float* stage, int* win, const Win& wn,
+                                      unsigned long long* __restrict__ gacc, const Geo& g,
+                                      DevState* st, unsigned& nslow, CoefFn coef) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Run<NF> run;
+    run.cw = -1;
+    run.cnt = 0;
+#pragma unroll 1
+    for (int jq = 0; jq < 2; ++jq) {
+        const int q = 16 * lane + 2 * warp + jq;
+        float4 v[NS];
+#pragma unroll
+        for (int f = 0; f < NS; ++f) v[f] = stq(stage, f, q);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float x = compc(v[0], e), y = compc(v[1], e);
+            if (!(x >= 0.0f)) continue;
+            const Cic c = cic(x, y);
+            float cs[NF];
+            coef(v, e, cs);
+            float wv[4];
+            wv[0] = c.w0; wv[1] = c.w1; wv[2] = c.w2; wv[3] = c.w3;
+            run_deposit<NF>(run, win, wn, c.i0, c.j0, wv, cs, gacc, g, nslow, st);
+        }
+    }
+    run.flush(win, wn);
+}
 
 __device__ __forceinline__ void weights(const Cic& s, float (&wv)[4]) {
     wv[0] = s.w0; wv[1] = s.w1; wv[2] = s.w2; wv[3] = s.w3;
@@ -197,11 +232,11 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
                 xe = -1.0f;
             }
         }
-        stg4(stage, 0, s0) = x; stg4(stage, 1, s0) = y; stg4(stage, 2, s0) = w;
+        stq(stage, 0, s0 >> 2) = x; stq(stage, 1, s0 >> 2) = y; stq(stage, 2, s0 >> 2) = w;
         if constexpr (NS == 6) {
-            stg4(stage, 3, s0) = ld4(p.ux, i, p.n, vec);
-            stg4(stage, 4, s0) = ld4(p.uy, i, p.n, vec);
-            stg4(stage, 5, s0) = ld4(p.uz, i, p.n, vec);
+            stq(stage, 3, s0 >> 2) = ld4(p.ux, i, p.n, vec);
+            stq(stage, 4, s0 >> 2) = ld4(p.uy, i, p.n, vec);
+            stq(stage, 5, s0 >> 2) = ld4(p.uz, i, p.n, vec);
         }
     }
     Win wn;
@@ -214,22 +249,13 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
 #pragma unroll
     for (int f = 0; f < NF; ++f) S[f] = Sdev[foff + f];
     unsigned nslow = 0;
-#pragma unroll 1
-    for (int j = 0; j < kChunk / kThreads; ++j) {
-        const int s = j * kThreads + threadIdx.x;
-        const float x = stg(stage, 0, s), y = stg(stage, 1, s);
-        const bool valid = x >= 0.0f;
-        const Cic c = cic(valid ? x : 0.0f, valid ? y : 0.0f);
-        const float coef = __double2float_rn(qoa * static_cast<double>(stg(stage, 2, s)));
-        float cf[NF];
-        if constexpr (NS == 6) src_coefs<SET>(coef, stg(stage, 3, s), stg(stage, 4, s), stg(stage, 5, s), cf);
-        else src_coefs<SET>(coef, 0.f, 0.f, 0.f, cf);
+    pass2<NF, NS>(stage, win, wn, acc, g, st, nslow, [&](const float4 (&v)[NS], int e, float (&cs)[NF]) {
+        const float coef = __double2float_rn(qoa * static_cast<double>(compc(v[2], e)));
+        if constexpr (NS == 6) src_coefs<SET>(coef, compc(v[3], e), compc(v[4], e), compc(v[5], e), cs);
+        else src_coefs<SET>(coef, 0.f, 0.f, 0.f, cs);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) cf[f] = __fmul_rn(cf[f], S[f]);
-        float wv[4];
-        weights(c, wv);
-        win_deposit<NF>(win, wn, valid, c.i0, c.j0, wv, cf, acc, g, nslow);
-    }
+        for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cs[f], S[f]);
+    });
     __syncthreads();
     win_flush<NF>(win, wn, acc, g);
     if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
@@ -317,25 +343,17 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
                 xe = -1.0f;
             }
         }
-        stg4(stage, 0, s0) = x; stg4(stage, 1, s0) = y;
-        stg4(stage, 2, s0) = ax; stg4(stage, 3, s0) = ay; stg4(stage, 4, s0) = az;
+        stq(stage, 0, s0 >> 2) = x; stq(stage, 1, s0 >> 2) = y;
+        stq(stage, 2, s0 >> 2) = ax; stq(stage, 3, s0 >> 2) = ay; stq(stage, 4, s0 >> 2) = az;
     }
     Win wn;
     win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, red);
     win_zero<NF>(win, wn);
     __syncthreads();
     unsigned nslow = 0;
-#pragma unroll 1
-    for (int j = 0; j < kChunk / kThreads; ++j) {
-        const int s = j * kThreads + threadIdx.x;
-        const float x = stg(stage, 0, s), y = stg(stage, 1, s);
-        const bool valid = x >= 0.0f;
-        const Cic c = cic(valid ? x : 0.0f, valid ? y : 0.0f);
-        const float cf[NF] = {stg(stage, 2, s), stg(stage, 3, s), stg(stage, 4, s)};
-        float wv[4];
-        weights(c, wv);
-        win_deposit<NF>(win, wn, valid, c.i0, c.j0, wv, cf, acc, g, nslow);
-    }
+    pass2<NF, NS>(stage, win, wn, acc, g, st, nslow, [&](const float4 (&v)[NS], int e, float (&cs)[NF]) {
+        cs[0] = compc(v[2], e); cs[1] = compc(v[3], e); cs[2] = compc(v[4], e);
+    });
     __syncthreads();
     win_flush<NF>(win, wn, acc, g);
     if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
@@ -418,24 +436,16 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
         st4(p.uy, i, p.n, vec, uy);
         st4(p.uz, i, p.n, vec, uz);
         if (pp.write_cell && p.cell) st4i(p.cell, i, p.n, vec, cell);
-        stg4(stage, 0, s0) = xs; stg4(stage, 1, s0) = y; stg4(stage, 2, s0) = w;
+        stq(stage, 0, s0 >> 2) = xs; stq(stage, 1, s0 >> 2) = y; stq(stage, 2, s0 >> 2) = w;
     }
     Win wn;
     win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, red);
     win_zero<NF>(win, wn);
     __syncthreads();
     unsigned nslow = 0;
-#pragma unroll 2
-    for (int j = 0; j < kChunk / kThreads; ++j) {
-        const int s = j * kThreads + threadIdx.x;
-        const float x = stg(stage, 0, s), y = stg(stage, 1, s);
-        const bool valid = x >= 0.0f;
-        const Cic c = cic(valid ? x : 0.0f, valid ? y : 0.0f);
-        const float cf[NF] = {__fmul_rn(__double2float_rn(qoa * static_cast<double>(stg(stage, 2, s))), S)};
-        float wv[4];
-        weights(c, wv);
-        win_deposit<NF>(win, wn, valid, c.i0, c.j0, wv, cf, acc, g, nslow);
-    }
+    pass2<NF, NS>(stage, win, wn, acc, g, st, nslow, [&](const float4 (&v)[NS], int e, float (&cs)[NF]) {
+        cs[0] = __fmul_rn(__double2float_rn(qoa * static_cast<double>(compc(v[2], e))), S);
+    });
     __syncthreads();
     win_flush<NF>(win, wn, acc, g);
     block_sum4(ke, px, py, pz, part, dsh);
@@ -511,8 +521,8 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
         st4(p.uy, i, p.n, vec, uy);
         st4(p.uz, i, p.n, vec, uz);
         if (pp.write_cell && p.cell) st4i(p.cell, i, p.n, vec, cell);
-        stg4(stage, 0, s0) = xs; stg4(stage, 1, s0) = y; stg4(stage, 2, s0) = w;
-        stg4(stage, 3, s0) = ux; stg4(stage, 4, s0) = uy; stg4(stage, 5, s0) = uz;
+        stq(stage, 0, s0 >> 2) = xs; stq(stage, 1, s0 >> 2) = y; stq(stage, 2, s0 >> 2) = w;
+        stq(stage, 3, s0 >> 2) = ux; stq(stage, 4, s0 >> 2) = uy; stq(stage, 5, s0 >> 2) = uz;
     }
     // |u| maxima of the new state (next step's deposit scales): one atomic per block
     m0 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m0)));
@@ -536,21 +546,12 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
 #pragma unroll
     for (int f = 0; f < NF; ++f) S[f] = st->S_next[f];
     unsigned nslow = 0;
-#pragma unroll 1
-    for (int j = 0; j < kChunk / kThreads; ++j) {
-        const int s = j * kThreads + threadIdx.x;
-        const float x = stg(stage, 0, s), y = stg(stage, 1, s);
-        const bool valid = x >= 0.0f;
-        const Cic c = cic(valid ? x : 0.0f, valid ? y : 0.0f);
-        const float coef = __double2float_rn(qoa * static_cast<double>(stg(stage, 2, s)));
-        float cf[NF];
-        src_coefs<SET_ALL>(coef, stg(stage, 3, s), stg(stage, 4, s), stg(stage, 5, s), cf);
+    pass2<NF, NS>(stage, win, wn, acc, g, st, nslow, [&](const float4 (&v)[NS], int e, float (&cs)[NF]) {
+        const float coef = __double2float_rn(qoa * static_cast<double>(compc(v[2], e)));
+        src_coefs<SET_ALL>(coef, compc(v[3], e), compc(v[4], e), compc(v[5], e), cs);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) cf[f] = __fmul_rn(cf[f], S[f]);
-        float wv[4];
-        weights(c, wv);
-        win_deposit<NF>(win, wn, valid, c.i0, c.j0, wv, cf, acc, g, nslow);
-    }
+        for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cs[f], S[f]);
+    });
     __syncthreads();
     win_flush<NF>(win, wn, acc, g);
     block_sum4(ke, px, py, pz, part, dsh);

@@ -318,64 +318,96 @@ __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& 
 // Wrapped offset of a cell from the window's reference cell.
 __device__ __forceinline__ int win_off(int c, int r, int n) { return wrap_signed(c - r, n); }
 
-// Deposit one particle per lane. All 32 lanes of the warp must call this
-// together (invalid lanes pass valid = false). cs[f] = coefficient * scale;
-// the contribution of field f at corner c is rint(cs[f] * w[c]).
-//
-// Lanes whose particles share a base cell are summed with one redux.sync per
-// value and the group leader adds the sum to the window; when the warp holds
-// more than 8 distinct cells each lane adds its own values. Values outside the
-// fast range (and every value when the window is unused) go straight to the
-// global accumulators as exact 64-bit integers.
+// Stage layout. The pass-1 writes (one float4 = 4 consecutive particles per
+// thread, consecutive quads across lanes) and the pass-2 reads (lane l reads
+// quads 16l + c, i.e. lanes 64 particles apart) are both conflict-free when
+// quad q is stored at quad position q ^ ((q >> 4) & 7).
+__device__ __forceinline__ int stage_quad(int q) { return q ^ ((q >> 4) & 7); }
+
+// Exact quantisation of the product a*b: rint(a*b) via one FFMA against
+// 1.5*2^23 (|a*b| < 2^20); the raw bits are summed and the magic removed later.
+__device__ __forceinline__ unsigned qbits(float a, float b) {
+    return __float_as_uint(__fmaf_rn(a, b, kMagic));
+}
+
+// Per-lane run accumulator: contributions of consecutive particles that share
+// a base window cell, as sums of qbits (mod 2^32). A run holds at most 8
+// particles, so the exact sum fits in int32 after removing cnt * magic.
 template <int NF>
-__device__ __forceinline__ void win_deposit(int* __restrict__ s, const Win& w, bool valid,
-                                            int ci, int cj, const float (&wv)[4], const float (&cs)[NF],
-                                            unsigned long long* __restrict__ gacc, const Geo& g,
-                                            unsigned& nslow) {
-    const int lane = threadIdx.x & 31;
-    bool fast = valid && w.use;
-#pragma unroll
-    for (int f = 0; f < NF; ++f) fast = fast && (fabsf(cs[f]) < kFastLim);
-    const int cw = fast ? (win_off(cj, w.jr, g.ny) - w.mj) * w.W + (win_off(ci, w.ir, g.nx) - w.mi) : -1;
-    const unsigned peers = __match_any_sync(0xffffffffu, cw);
-    const int leader = __ffs(peers) - 1;
-    const unsigned leaders = __ballot_sync(0xffffffffu, lane == leader);
-    const bool agg = __popc(leaders) <= 8;
-    const unsigned ngroup = static_cast<unsigned>(__popc(peers));
-    const int offs[4] = {0, 1, w.W, w.W + 1};
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            // fast lanes: bits of t + 1.5*2^23 (their integer sum minus
-            // count * magic bits is the exact sum of rint(t)); others add 0.
-            const float t = __fmul_rn(cs[f], wv[c]);
-            const unsigned bits = fast ? __float_as_uint(__fadd_rn(t, kMagic)) : kMagicU;
-            if (agg) {
-                // modular (wrapping) unsigned sum; the true sum fits in int32
-                const int sum = static_cast<int>(__reduce_add_sync(peers, bits) - ngroup * kMagicU);
-                if (lane == leader && cw >= 0 && sum != 0) atomicAdd(s + f * w.WH + cw + offs[c], sum);
-            } else if (cw >= 0) {
-                const int q = static_cast<int>(bits - kMagicU);
-                if (q != 0) atomicAdd(s + f * w.WH + cw + offs[c], q);
-            }
-        }
-    }
-    if (valid && !fast) {
-        // exact slow path (window too small, or a value beyond the fast range)
-        const int i1 = wrap_once(ci + 1, g.nx);
-        const int r0 = cj * g.nx, r1 = wrap_once(cj + 1, g.ny) * g.nx;
-        const int gcs[4] = {r0 + ci, r0 + i1, r1 + ci, r1 + i1};
+struct Run {
+    int cw;                 // window cell of the run's base corner (-1 = empty)
+    unsigned cnt;
+    unsigned a[NF][4];
+    __device__ __forceinline__ void start(int c) {
+        cw = c; cnt = 0;
 #pragma unroll
         for (int f = 0; f < NF; ++f)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const long long q = __float2ll_rn(__fmul_rn(cs[f], wv[c]));
-                if (q != 0)
-                    atomicAdd(gacc + static_cast<size_t>(f) * g.ncell + gcs[c], static_cast<unsigned long long>(q));
-            }
-        ++nslow;
+            for (int k = 0; k < 4; ++k) a[f][k] = 0u;
     }
+    __device__ __forceinline__ void add(const float (&cs)[NF], const float (&wv)[4]) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a[f][k] += qbits(cs[f], wv[k]);
+        ++cnt;
+    }
+    // Add the run into the window planes s[f*WH + cell].
+    __device__ __forceinline__ void flush(int* __restrict__ s, const Win& w) {
+        if (cw < 0) return;
+        const unsigned m = cnt * kMagicU;
+        const int offs[4] = {0, 1, w.W, w.W + 1};
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int v = static_cast<int>(a[f][k] - m);
+                if (v != 0) atomicAdd(s + f * w.WH + cw + offs[k], v);
+            }
+    }
+};
+
+// Exact slow path: every contribution straight into the global int64 planes.
+template <int NF>
+__device__ __forceinline__ void deposit_global(int ci, int cj, const float (&wv)[4], const float (&cs)[NF],
+                                            unsigned long long* __restrict__ gacc, const Geo& g) {
+    const int i1 = wrap_once(ci + 1, g.nx);
+    const int r0 = cj * g.nx, r1 = wrap_once(cj + 1, g.ny) * g.nx;
+    const int gcs[4] = {r0 + ci, r0 + i1, r1 + ci, r1 + i1};
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const long long q = __double2ll_rn(__dmul_rn(static_cast<double>(cs[f]), static_cast<double>(wv[k])));
+            if (q != 0)
+                atomicAdd(gacc + static_cast<size_t>(f) * g.ncell + gcs[k], static_cast<unsigned long long>(q));
+        }
+}
+
+// Deposit one particle into the lane's run (flushing the previous run when the
+// base cell changes), or through the exact slow path when the window is unused
+// or a coefficient is outside the fast range.
+template <int NF>
+__device__ __forceinline__ void run_deposit(Run<NF>& run, int* __restrict__ s, const Win& w,
+                                            int ci, int cj, const float (&wv)[4], const float (&cs)[NF],
+                                            unsigned long long* __restrict__ gacc, const Geo& g,
+                                            unsigned& nslow, DevState* st) {
+    bool fast = w.use;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) fast = fast && (fabsf(cs[f]) < kFastLim);
+    if (!fast) {
+        for (int f = 0; f < NF; ++f)
+            if (!isfinite(cs[f])) { set_err(st, 1u); return; }   // AW_DEV_NONFINITE
+        deposit_global<NF>(ci, cj, wv, cs, gacc, g);
+        ++nslow;
+        return;
+    }
+    const int cw = (win_off(cj, w.jr, g.ny) - w.mj) * w.W + (win_off(ci, w.ir, g.nx) - w.mi);
+    if (cw != run.cw) {
+        run.flush(s, w);
+        run.start(cw);
+    }
+    run.add(cs, wv);
 }
 
 }  // namespace aw

@@ -71,26 +71,56 @@ __global__ void k_make_scales(DevState* st, float cref) {
     for (int f = 0; f < 8; ++f) { st->S_next[f] = S[f]; st->S_pend[f] = S[f]; }
 }
 
-// Finalise nf fields of the accumulator block acc[f*ncell + c] (f = first..first+nf-1)
-// into real staging r[(f-first)*ncell + c] and optional caller arrays.
+// Finalise NF fields of the accumulator block acc[f*ncell + c] (f = first..)
+// into real staging r[(f-first)*ncell + c] and optional caller arrays; two
+// cells per thread so every field's loads are in flight together.
 struct FinOut { float* p[8]; };
-__global__ void k_finalize(unsigned long long* __restrict__ acc, int first, int nf, int ncell,
-                           const float* __restrict__ Sdev, float* __restrict__ r,
-                           FinOut api, int accumulate, double* __restrict__ part,
-                           DevState* st, int step_begin, double dt, float cref, int darwin) {
+template <int NF>
+__global__ void __launch_bounds__(kThreads)
+k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
+           const float* __restrict__ Sdev, float* __restrict__ r, FinOut api, int accumulate,
+           double* __restrict__ part, DevState* st, int step_begin, double dt, float cref, int darwin) {
+    double invS[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) invS[f] = 1.0 / static_cast<double>(Sdev[first + f]);
     double qsum = 0.0;
-    double invS[8];
-    for (int f = 0; f < nf; ++f) invS[f] = 1.0 / static_cast<double>(Sdev[first + f]);
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
-        for (int f = 0; f < nf; ++f) {
+    const int npair = (ncell + 1) >> 1;
+    for (int pi = blockIdx.x * blockDim.x + threadIdx.x; pi < npair; pi += gridDim.x * blockDim.x) {
+        const int c = 2 * pi;
+        const bool two = (c + 1 < ncell);
+        const bool vec = two && ((ncell & 1) == 0);   // planes 16-byte aligned
+        long long v[NF][2];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
             unsigned long long* a = acc + static_cast<size_t>(first + f) * ncell + c;
-            const long long v = static_cast<long long>(*a);
-            *a = 0ull;
-            const float val = __double2float_rn(static_cast<double>(v) * invS[f]);
-            r[static_cast<size_t>(f) * ncell + c] = val;
+            if (vec) {
+                const longlong2 q = *reinterpret_cast<const longlong2*>(a);
+                v[f][0] = q.x; v[f][1] = q.y;
+                *reinterpret_cast<longlong2*>(a) = make_longlong2(0, 0);
+            } else {
+                v[f][0] = static_cast<long long>(a[0]); a[0] = 0ull;
+                v[f][1] = 0;
+                if (two) { v[f][1] = static_cast<long long>(a[1]); a[1] = 0ull; }
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            const float a0 = __double2float_rn(static_cast<double>(v[f][0]) * invS[f]);
+            const float a1 = __double2float_rn(static_cast<double>(v[f][1]) * invS[f]);
+            float* rf = r + static_cast<size_t>(f) * ncell + c;
             float* o = api.p[f];
-            if (o) o[c] = accumulate ? __fadd_rn(o[c], val) : val;
-            if (first + f == 0) qsum += val;
+            if (two) {
+                if (vec) *reinterpret_cast<float2*>(rf) = make_float2(a0, a1);
+                else { rf[0] = a0; rf[1] = a1; }
+                if (o) {
+                    if (accumulate) { o[c] = __fadd_rn(o[c], a0); o[c + 1] = __fadd_rn(o[c + 1], a1); }
+                    else { o[c] = a0; o[c + 1] = a1; }
+                }
+            } else {
+                rf[0] = a0;
+                if (o) o[c] = accumulate ? __fadd_rn(o[c], a0) : a0;
+            }
+            if (first + f == 0) qsum += static_cast<double>(a0) + (two ? static_cast<double>(a1) : 0.0);
         }
     }
     if (part) {
@@ -350,32 +380,38 @@ __global__ void k_fields_push(const float* __restrict__ r_et, const float* __res
     grid_partials(se2, me2, sb2, part);
 }
 
-// Fixed-order reduction of particle (ke, px, py, pz) and grid partials.
-__global__ void k_diag_reduce(const double* __restrict__ pp, int np, const double* __restrict__ pg,
-                              int ng, double eps0, double dxdy, aw_diag* out) {
-    __shared__ double sh[8][32];
-    const int l = threadIdx.x;   // 32 threads
-    double ke = 0, px = 0, py = 0, pz = 0, se2 = 0, me2 = 0, q = 0, sb2 = 0;
-    for (int b = l; b < np; b += 32) {
-        ke += pp[b * 5 + 0]; px += pp[b * 5 + 1]; py += pp[b * 5 + 2]; pz += pp[b * 5 + 3];
+// Fixed-order reduction of particle (ke, px, py, pz) and grid partials:
+// thread t sums blocks t, t+256, ... then a fixed shared-memory tree.
+__global__ void __launch_bounds__(256)
+k_diag_reduce(const double* __restrict__ pp, int np, const double* __restrict__ pg,
+              int ng, double eps0, double dxdy, aw_diag* out) {
+    __shared__ double sh[8][256];
+    const int t = threadIdx.x;
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // ke px py pz se2 me2 q sb2
+    for (int b = t; b < np; b += 256) {
+        a[0] += pp[b * 5 + 0]; a[1] += pp[b * 5 + 1]; a[2] += pp[b * 5 + 2]; a[3] += pp[b * 5 + 3];
     }
-    for (int b = l; b < ng; b += 32) {
-        se2 += pg[b * 5 + 0]; me2 = fmax(me2, pg[b * 5 + 1]); q += pg[b * 5 + 2]; sb2 += pg[b * 5 + 3];
+    for (int b = t; b < ng; b += 256) {
+        a[4] += pg[b * 5 + 0]; a[5] = fmax(a[5], pg[b * 5 + 1]); a[6] += pg[b * 5 + 2]; a[7] += pg[b * 5 + 3];
     }
-    sh[0][l] = ke; sh[1][l] = px; sh[2][l] = py; sh[3][l] = pz;
-    sh[4][l] = se2; sh[5][l] = me2; sh[6][l] = q; sh[7][l] = sb2;
-    __syncwarp();
-    if (l == 0) {
-        double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int i = 0; i < 32; ++i) {
-            for (int k = 0; k < 8; ++k) s[k] = (k == 5) ? fmax(s[k], sh[k][i]) : s[k] + sh[k][i];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sh[k][t] = a[k];
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (t < s) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                sh[k][t] = (k == 5) ? fmax(sh[k][t], sh[k][t + s]) : sh[k][t] + sh[k][t + s];
         }
-        out->ke = 0.5 * s[0];
-        out->px = s[1]; out->py = s[2]; out->pz = s[3];
-        out->ee = 0.5 * eps0 * s[4] * dxdy;
-        out->max_e = sqrt(s[5]);
-        out->charge = s[6] * dxdy;
-        out->eb = 0.5 * s[7] * dxdy;
+        __syncthreads();
+    }
+    if (t == 0) {
+        out->ke = 0.5 * sh[0][0];
+        out->px = sh[1][0]; out->py = sh[2][0]; out->pz = sh[3][0];
+        out->ee = 0.5 * eps0 * sh[4][0] * dxdy;
+        out->max_e = sqrt(sh[5][0]);
+        out->charge = sh[6][0] * dxdy;
+        out->eb = 0.5 * sh[7][0] * dxdy;
     }
 }
 
@@ -480,16 +516,24 @@ void launch_make_scales(Ctx& c) {
     AW_LAUNCH();
 }
 
-// Finalise acc fields [first, first+nf) with scales S_pend into r (+ api arrays).
+// Finalise acc fields [first, first+nf) with scales S into r (+ api arrays).
 void launch_finalize(Ctx& c, unsigned long long* acc, int first, int nf, const float* S, float* r,
                      float* const* api, bool accumulate, bool charge_partials, bool step_begin) {
     FinOut o{};
     for (int f = 0; f < nf && f < 8; ++f) o.p[f] = api ? api[f] : nullptr;
-    k_finalize<<<kGridBlocks, kThreads, 0, c.stream>>>(acc, first, nf, c.geo.ncell, S, r, o,
-                                                       accumulate ? 1 : 0,
-                                                       charge_partials ? c.part_g : nullptr, c.st,
-                                                       step_begin ? 1 : 0, c.prm.dt, cref_of(c),
-                                                       c.model == AW_MODEL_DARWIN ? 1 : 0);
+    const int blocks = std::max(kGridBlocks, std::min(4096, (c.geo.ncell / 2 + kThreads - 1) / kThreads));
+    double* part = charge_partials ? c.part_g : nullptr;
+    const int acc_ = accumulate ? 1 : 0, sb = step_begin ? 1 : 0, dw = c.model == AW_MODEL_DARWIN ? 1 : 0;
+    const float cref = cref_of(c);
+    if (charge_partials && blocks != kGridBlocks) throw Error(AW_ERR_STATE, "finalize: partials need the fixed grid");
+    const int nb = charge_partials ? kGridBlocks : blocks;
+    switch (nf) {
+        case 1: k_finalize<1><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw); break;
+        case 3: k_finalize<3><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw); break;
+        case 4: k_finalize<4><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw); break;
+        case 8: k_finalize<8><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw); break;
+        default: throw Error(AW_ERR_ARG, "finalize: unsupported field count");
+    }
     AW_LAUNCH();
 }
 
@@ -529,7 +573,7 @@ void launch_fields_push(Ctx& c) {
     AW_LAUNCH();
 }
 void launch_diag_reduce(Ctx& c, bool with_particles) {
-    k_diag_reduce<<<1, 32, 0, c.stream>>>(c.part_p, with_particles ? c.npart_p : 0, c.part_g,
+    k_diag_reduce<<<1, 256, 0, c.stream>>>(c.part_p, with_particles ? c.npart_p : 0, c.part_g,
                                           kGridBlocks, c.prm.eps0, c.geo.dx * c.geo.dy, c.diag);
     AW_LAUNCH();
 }

@@ -68,7 +68,9 @@ static inline float wrap_pos(float x, float n) {
     return x;
 }
 
-/* ---- deposit: include/pic/depositor.hpp (fixed-point contract of the kernels) -- */
+/* ---- deposit: include/pic/depositor.hpp (fixed-point contract of the kernels) --
+ * contribution (field f, corner k) = rint(cs_f * w_k) of the EXACT product
+ * (a float*float product is exact in double), summed in int64. */
 int or_nf(int set) { return set == 0 ? 1 : (set == 3 ? 8 : 4); }
 
 static inline void src_coefs(int set, float coef, float ux, float uy, float uz, float* cf) {
@@ -131,7 +133,7 @@ void or_deposit(const or_geo* g, const float* x, const float* y, const float* ux
             src_coefs(set, coef, ux ? ux[p] : 0.0f, uy ? uy[p] : 0.0f, uz ? uz[p] : 0.0f, cf);
             for (int f = 0; f < nf; ++f) {
                 const float cs = cf[f] * S[soff + f];
-                for (int k = 0; k < 4; ++k) a[(size_t)f * ncell + c[k]] += llrintf(cs * s.w[k]);
+                for (int k = 0; k < 4; ++k) a[(size_t)f * ncell + c[k]] += llrint((double)cs * (double)s.w[k]);
             }
         }
     }
@@ -188,7 +190,7 @@ void or_deposit_dcu(const or_geo* g, const float* x, const float* y, const float
             cf[1] = (coef * (ey + cy)) * S;
             cf[2] = (coef * (ez + cz)) * S;
             for (int f = 0; f < 3; ++f)
-                for (int k = 0; k < 4; ++k) a[(size_t)f * ncell + c[k]] += llrintf(cf[f] * s.w[k]);
+                for (int k = 0; k < 4; ++k) a[(size_t)f * ncell + c[k]] += llrint((double)cf[f] * (double)s.w[k]);
         }
     }
     if (priv) {
