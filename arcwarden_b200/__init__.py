@@ -64,7 +64,7 @@ class Diag(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("chunks", C.c_int64), ("window_overflow", C.c_int64), ("slow_deposits", C.c_int64),
-                ("steps", C.c_int64)]
+                ("steps", C.c_int64), ("kernels_per_step", C.c_int64)]
 
 
 # Exported symbols and their ctypes signatures (must match include/arcb200.h).
@@ -90,6 +90,8 @@ SIGNATURES = {
     "aw_step_diag_device": [_P, C.POINTER(_P)],
     "aw_error_word": [_P, C.POINTER(C.c_uint32)], "aw_stats": [_P, C.POINTER(Stats)],
     "aw_last_error": [C.c_char_p, _I32],
+    "aw_step_profile": [_P, _I64, C.POINTER(C.c_float), _I32, C.POINTER(_I32)],
+    "aw_run_diag": [_P, _I64, _I64, _I32, _P],
 }
 
 _lib = None
@@ -110,6 +112,8 @@ def load_library(path: str | Path | None = None) -> C.CDLL:
         fn.restype = C.c_int
     lib.aw_version.restype = C.c_char_p
     lib.aw_version.argtypes = []
+    lib.aw_step_phase_name.restype = C.c_char_p
+    lib.aw_step_phase_name.argtypes = [_I32, _I32]
     if path is None:
         _lib = lib
     return lib
@@ -224,6 +228,17 @@ class Context:
 
     def run(self, n0, nsteps, graph=True):
         _check(self.lib.aw_run(self.h, int(n0), int(nsteps), int(bool(graph))))
+
+    def step_profile(self, n) -> dict:
+        """One fused step with per-phase CUDA-event timings {phase: ms}."""
+        ms = (C.c_float * 16)()
+        npc = C.c_int32()
+        _check(self.lib.aw_step_profile(self.h, int(n), ms, 16, C.byref(npc)))
+        return {self.lib.aw_step_phase_name(self.model, i).decode(): ms[i] for i in range(npc.value)}
+
+    def run_diag(self, n0, nsteps, host_ptr, graph=True):
+        """Run nsteps steps, copying each step's aw_diag to host_ptr[i] (async)."""
+        _check(self.lib.aw_run_diag(self.h, int(n0), int(nsteps), int(bool(graph)), host_ptr))
 
     def reduce(self) -> dict:
         d = Diag()

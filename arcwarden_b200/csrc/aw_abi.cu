@@ -119,41 +119,63 @@ void reset_acc(Ctx& c, unsigned long long* acc, int nf) {
 }
 
 // ---- the step body (no host syncs; capturable) --------------------------------
-void es_fields_from_pending(Ctx& c, bool step_begin) {
+// A step is a fixed list of phases; `mark(i)` runs after phase i (used by
+// aw_step_profile to record CUDA events between phases).
+constexpr int kPhasesES = 7, kPhasesDarwin = 13;
+const char* const kPhaseNamesES[kPhasesES] = {
+    "finalize_rho", "fft_r2c_rho", "kspace_es", "fft_c2r_e", "fields_es", "push_deposit_es", "diag_reduce"};
+const char* const kPhaseNamesDarwin[kPhasesDarwin] = {
+    "finalize_src", "fft_r2c_src8", "kspace_elb", "fft_c2r_elb5", "fields_dcu", "deposit_dcu",
+    "finalize_dcu", "fft_r2c_dcu3", "kspace_et", "fft_c2r_et3", "fields_push", "push_deposit_em",
+    "diag_reduce"};
+
+struct NoMark { void operator()(int) const {} };
+
+template <class Mark>
+void es_fields_from_pending(Ctx& c, bool step_begin, Mark mark) {
     float* api[1] = {c.src.rho};
-    launch_finalize(c, c.acc_src, 0, 1, c.st->S_pend, c.r_src, api, false, true, step_begin);
-    AW_CUFFT(cufftExecR2C(c.p_r2cS, c.r_src, c.k_src));
-    launch_kspace_es(c, c.k_src, c.k_out);
-    AW_CUFFT(cufftExecC2R(c.p_c2rO, c.k_out, c.r_out));
-    launch_fields_es(c);
+    launch_finalize(c, c.acc_src, 0, 1, c.st->S_pend, c.r_src, api, false, true, step_begin); mark(0);
+    AW_CUFFT(cufftExecR2C(c.p_r2cS, c.r_src, c.k_src)); mark(1);
+    launch_kspace_es(c, c.k_src, c.k_out); mark(2);
+    AW_CUFFT(cufftExecC2R(c.p_c2rO, c.k_out, c.r_out)); mark(3);
+    launch_fields_es(c); mark(4);
 }
+void es_fields_from_pending(Ctx& c, bool step_begin) { es_fields_from_pending(c, step_begin, NoMark{}); }
 
-void darwin_fields_from_pending(Ctx& c, bool step_begin) {
+template <class Mark>
+void darwin_fields_from_pending(Ctx& c, bool step_begin, Mark mark) {
     float* api[8] = {c.src.rho, c.src.Jx, c.src.Jy, c.src.Jz, c.src.amu0, c.src.amu1, c.src.amu2, c.src.amu3};
-    launch_finalize(c, c.acc_src, 0, 8, c.st->S_pend, c.r_src, api, false, true, step_begin);
-    AW_CUFFT(cufftExecR2C(c.p_r2cS, c.r_src, c.k_src));
-    launch_kspace_elb(c, c.k_src, c.k_out);
-    AW_CUFFT(cufftExecC2R(c.p_c2rO, c.k_out, c.r_out));
-    launch_fields_dcu(c);
-    launch_deposit_dcu(c, c.gb_dcu);
+    launch_finalize(c, c.acc_src, 0, 8, c.st->S_pend, c.r_src, api, false, true, step_begin); mark(0);
+    AW_CUFFT(cufftExecR2C(c.p_r2cS, c.r_src, c.k_src)); mark(1);
+    launch_kspace_elb(c, c.k_src, c.k_out); mark(2);
+    AW_CUFFT(cufftExecC2R(c.p_c2rO, c.k_out, c.r_out)); mark(3);
+    launch_fields_dcu(c); mark(4);
+    launch_deposit_dcu(c, c.gb_dcu); mark(5);
     float* apid[3] = {c.src.dcux, c.src.dcuy, c.src.dcuz};
-    launch_finalize(c, c.acc_dcu, 0, 3, c.st->S_dcu, c.r_dcu, apid, false, false, false);
-    AW_CUFFT(cufftExecR2C(c.p_r2c3, c.r_dcu, c.k_dcu));
-    launch_kspace_et(c, c.k_dcu, c.k_src + static_cast<size_t>(4) * c.sg.nk, c.k_et);
-    AW_CUFFT(cufftExecC2R(c.p_c2r3, c.k_et, c.r_et));
-    launch_fields_push(c);
+    launch_finalize(c, c.acc_dcu, 0, 3, c.st->S_dcu, c.r_dcu, apid, false, false, false); mark(6);
+    AW_CUFFT(cufftExecR2C(c.p_r2c3, c.r_dcu, c.k_dcu)); mark(7);
+    launch_kspace_et(c, c.k_dcu, c.k_src + static_cast<size_t>(4) * c.sg.nk, c.k_et); mark(8);
+    AW_CUFFT(cufftExecC2R(c.p_c2r3, c.k_et, c.r_et)); mark(9);
+    launch_fields_push(c); mark(10);
 }
+void darwin_fields_from_pending(Ctx& c, bool step_begin) { darwin_fields_from_pending(c, step_begin, NoMark{}); }
 
-void step_body(Ctx& c) {
+template <class Mark>
+void step_body(Ctx& c, Mark mark) {
     if (c.model == AW_MODEL_ES) {
-        es_fields_from_pending(c, true);
-        launch_push_deposit_es(c);
+        es_fields_from_pending(c, true, mark);
+        launch_push_deposit_es(c); mark(5);
+        launch_diag_reduce(c, true); mark(6);
     } else {
-        darwin_fields_from_pending(c, true);
-        launch_push_deposit_em(c);
+        darwin_fields_from_pending(c, true, mark);
+        launch_push_deposit_em(c); mark(11);
+        launch_diag_reduce(c, true); mark(12);
     }
-    launch_diag_reduce(c, true);
 }
+void step_body(Ctx& c) { step_body(c, NoMark{}); }
+
+// Kernels of this library one fused step launches (cuFFT's own not counted).
+int kernels_per_step(const Ctx& c) { return c.model == AW_MODEL_ES ? 5 : 9; }
 
 void ensure_pending(Ctx& c) {
     if (c.pending_valid) return;
@@ -644,6 +666,48 @@ int aw_run(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph) {
     });
 }
 
+int aw_run_diag(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph, aw_diag* host_out) {
+    return guarded([&] {
+        aw::need(ctx && host_out, AW_ERR_ARG, "null argument");
+        Ctx& c = ctx->c;
+        for (int64_t i = 0; i < nsteps; ++i) {
+            const int rc = aw_run(ctx, n0 + i, 1, use_graph);
+            if (rc != AW_OK) throw Error(rc, aw::g_last_error);
+            AW_CUDA(cudaMemcpyAsync(host_out + i, c.diag, sizeof(aw_diag), cudaMemcpyDeviceToHost, c.stream));
+        }
+    });
+}
+
+int aw_step_profile(aw_ctx* ctx, int64_t n, float* ms, int32_t cap, int32_t* nphase) {
+    return guarded([&] {
+        aw::need(ctx && ms && nphase, AW_ERR_ARG, "null argument");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        const int np = c.model == AW_MODEL_ES ? aw::kPhasesES : aw::kPhasesDarwin;
+        aw::need(cap >= np, AW_ERR_ARG, "step_profile: ms array too small");
+        aw::ensure_pending(c);
+        aw::launch_set_step(c, n);
+        cudaEvent_t ev[aw::kPhasesDarwin + 1];
+        for (int i = 0; i <= np; ++i) AW_CUDA(cudaEventCreate(&ev[i]));
+        try {
+            AW_CUDA(cudaEventRecord(ev[0], c.stream));
+            aw::step_body(c, [&](int i) { AW_CUDA(cudaEventRecord(ev[i + 1], c.stream)); });
+            AW_CUDA(cudaEventSynchronize(ev[np]));
+            for (int i = 0; i < np; ++i) AW_CUDA(cudaEventElapsedTime(&ms[i], ev[i], ev[i + 1]));
+        } catch (...) {
+            for (int i = 0; i <= np; ++i) cudaEventDestroy(ev[i]);
+            throw;
+        }
+        for (int i = 0; i <= np; ++i) cudaEventDestroy(ev[i]);
+        *nphase = np;
+    });
+}
+
+const char* aw_step_phase_name(int32_t model, int32_t i) {
+    if (model == AW_MODEL_ES) return (i >= 0 && i < aw::kPhasesES) ? aw::kPhaseNamesES[i] : "";
+    return (i >= 0 && i < aw::kPhasesDarwin) ? aw::kPhaseNamesDarwin[i] : "";
+}
+
 // ---- diagnostics / status -----------------------------------------------------------
 
 int aw_reduce_fp64(aw_ctx* ctx, aw_diag* out) {
@@ -698,6 +762,7 @@ int aw_stats(aw_ctx* ctx, aw_stats_t* out) {
         out->window_overflow = static_cast<int64_t>(h.overflow);
         out->slow_deposits = static_cast<int64_t>(h.slow);
         out->steps = h.step;
+        out->kernels_per_step = aw::kernels_per_step(c);
     });
 }
 

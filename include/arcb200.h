@@ -109,6 +109,7 @@ typedef struct aw_stats_t {
     int64_t window_overflow;  /* chunks whose cell window exceeded shared mem  */
     int64_t slow_deposits;    /* contributions that took the exact slow path   */
     int64_t steps;            /* fused steps taken                             */
+    int64_t kernels_per_step; /* this library's kernels in one fused step      */
 } aw_stats_t;
 
 typedef struct aw_ctx aw_ctx;
@@ -204,6 +205,18 @@ int aw_step(aw_ctx* ctx, int64_t n);
  * CUDA graph (once per context) and replays it; the step index lives in device
  * memory so the same graph serves every step. */
 int aw_run(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph);
+
+/* `nsteps` fused steps (as aw_run) with this step's diagnostics copied into
+ * host_out[i] after step i (cudaMemcpyAsync on the context's stream; pinned
+ * host memory makes the copies asynchronous). The caller synchronises the
+ * stream before reading host_out. */
+int aw_run_diag(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph, aw_diag* host_out);
+
+/* One fused step (like aw_step) with CUDA events recorded on the context's
+ * stream between its phases; ms[i] = duration of phase i, *nphase = number of
+ * phases (cap >= 13). Synchronises. Phase names: aw_step_phase_name. */
+int aw_step_profile(aw_ctx* ctx, int64_t n, float* ms, int32_t cap, int32_t* nphase);
+const char* aw_step_phase_name(int32_t model, int32_t i);
 
 /* ---- diagnostics and status ----------------------------------------------- */
 /* Diagnostics::compute, include/pic/diagnostics.hpp:58-108, reduced on the GPU
