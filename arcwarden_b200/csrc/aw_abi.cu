@@ -88,7 +88,7 @@ void free_all(Ctx& c) {
     cufftHandle* plans[] = {&c.p_r2c1, &c.p_c2r1, &c.p_r2cS, &c.p_c2rO, &c.p_r2c3, &c.p_c2r3, &c.p_r2c4};
     for (cufftHandle* h : plans) if (*h) cufftDestroy(*h);
     void* bufs[] = {c.st, c.acc_src, c.acc_dcu, c.r_src, c.r_out, c.r_dcu, c.r_et, c.k_src, c.k_out,
-                    c.k_dcu, c.k_et, c.gb_es, c.gb_dcu, c.gb_push, c.part_p, c.part_g, c.diag,
+                    c.k_dcu, c.k_et, c.gb_es, c.gb_dcu, c.gb_push, c.part_p, c.part_c, c.part_d, c.part_g, c.diag,
                     c.bin_count, c.bin_off, c.bin_cursor, c.bin_idx, c.sort_tmp, c.fft_work};
     for (void* b : bufs) if (b) cudaFree(b);
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
@@ -121,7 +121,7 @@ void reset_acc(Ctx& c, unsigned long long* acc, int nf) {
 // ---- the step body (no host syncs; capturable) --------------------------------
 // A step is a fixed list of phases; `mark(i)` runs after phase i (used by
 // aw_step_profile to record CUDA events between phases).
-constexpr int kPhasesES = 7, kPhasesDarwin = 13;
+constexpr int kPhasesES = 7, kPhasesDarwin = 14;
 const char* const kPhaseNamesES[kPhasesES] = {
     "finalize_rho", "fft_r2c_rho", "kspace_es", "fft_c2r_e", "fields_es", "push_deposit_es", "diag_reduce"};
 const char* const kPhaseNamesDarwin[kPhasesDarwin] = {
@@ -150,7 +150,7 @@ void darwin_fields_from_pending(Ctx& c, bool step_begin, Mark mark) {
     launch_kspace_elb(c, c.k_src, c.k_out); mark(2);
     AW_CUFFT(cufftExecC2R(c.p_c2rO, c.k_out, c.r_out)); mark(3);
     launch_fields_dcu(c); mark(4);
-    launch_deposit_dcu(c, c.gb_dcu); mark(5);
+    launch_deposit_dcu(c, c.gb_dcu, true); mark(5);
     float* apid[3] = {c.src.dcux, c.src.dcuy, c.src.dcuz};
     launch_finalize(c, c.acc_dcu, 0, 3, c.st->S_dcu, c.r_dcu, apid, false, false, false); mark(6);
     AW_CUFFT(cufftExecR2C(c.p_r2c3, c.r_dcu, c.k_dcu)); mark(7);
@@ -169,13 +169,14 @@ void step_body(Ctx& c, Mark mark) {
     } else {
         darwin_fields_from_pending(c, true, mark);
         launch_push_deposit_em(c); mark(11);
-        launch_diag_reduce(c, true); mark(12);
+        launch_rms_reduce(c, true, true); mark(12);
+        launch_diag_reduce(c, true); mark(13);
     }
 }
 void step_body(Ctx& c) { step_body(c, NoMark{}); }
 
 // Kernels of this library one fused step launches (cuFFT's own not counted).
-int kernels_per_step(const Ctx& c) { return c.model == AW_MODEL_ES ? 5 : 9; }
+int kernels_per_step(const Ctx& c) { return c.model == AW_MODEL_ES ? 5 : 10; }
 
 void ensure_pending(Ctx& c) {
     if (c.pending_valid) return;
@@ -321,8 +322,12 @@ int aw_particles_bind(aw_ctx* ctx, float* x, float* y, float* ux, float* uy, flo
         const int nb = static_cast<int>(std::max<long long>(1, (n + aw::kChunk - 1) / aw::kChunk));
         if (nb > c.npart_p) {
             if (c.part_p) cudaFree(c.part_p);
-            c.part_p = nullptr;
+            if (c.part_c) cudaFree(c.part_c);
+            if (c.part_d) cudaFree(c.part_d);
+            c.part_p = nullptr; c.part_c = nullptr; c.part_d = nullptr;
             aw::dalloc(c.part_p, static_cast<size_t>(nb) * 5);
+            aw::dalloc(c.part_c, static_cast<size_t>(nb) * 9);
+            aw::dalloc(c.part_d, static_cast<size_t>(nb) * 4);
         }
         c.npart_p = nb;
         AW_CUDA(cudaMemsetAsync(c.part_p, 0, sizeof(double) * 5 * nb, c.stream));
@@ -428,7 +433,7 @@ int aw_deposit_dcu(aw_ctx* ctx) {
         aw::launch_particle_max(c);
         aw::launch_pack_em(c);
         aw::reset_acc(c, c.acc_dcu, 3);
-        aw::launch_deposit_dcu(c, c.gb_dcu);
+        aw::launch_deposit_dcu(c, c.gb_dcu, false);
         float* api[3] = {c.src.dcux, c.src.dcuy, c.src.dcuz};
         aw::launch_finalize(c, c.acc_dcu, 0, 3, c.st->S_dcu, c.r_dcu, api, true, false, false);
     });
@@ -601,6 +606,7 @@ int aw_init(aw_ctx* ctx) {
         aw::require_parts(c);
         aw::drop_graph(c);
         aw::launch_set_step(c, 0);
+        AW_CUDA(cudaMemsetAsync(&c.st->have_rms, 0, sizeof(int), c.stream));
         aw::launch_particle_max(c);
         aw::launch_copy_umax(c);     // the step-begin copies umax -> ucur
         aw::launch_make_scales(c);
@@ -618,6 +624,7 @@ int aw_init(aw_ctx* ctx) {
             aw::darwin_fields_from_pending(c, true);   // t = 0 fields
             aw::launch_copy_umax(c);
             aw::launch_deposit_src(c, 8);              // pending rho,J,amu for step 0
+            aw::launch_rms_reduce(c, true, true);
         }
         c.pending_valid = true;
         aw::launch_set_step(c, 0);

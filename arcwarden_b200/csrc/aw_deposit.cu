@@ -43,10 +43,11 @@ template <> struct SetNF<SET_RHOJ> { static constexpr int NF = 4, NS = 6; };   /
 template <> struct SetNF<SET_AMU>  { static constexpr int NF = 4, NS = 6; };
 template <> struct SetNF<SET_ALL>  { static constexpr int NF = 8, NS = 6; };
 
-// Window capacity in cells for NF int32 planes (~48 KB per CTA).
-constexpr int wmax_cells(int nf) { return nf == 1 ? 8192 : (nf == 3 ? 4096 : (nf == 4 ? 3072 : 1536)); }
+// Window capacity in cells for NF int64 planes (<= 56 KB per CTA, so the
+// NF = 8 push kernel keeps two CTAs per SM with its 48 KB stage).
+constexpr int wmax_cells(int nf) { return nf == 1 ? 4096 : (nf == 3 ? 2048 : (nf == 4 ? 1536 : 896)); }
 constexpr size_t smem_bytes(int nf, int ns) {
-    return static_cast<size_t>(ns) * kChunk * 4 + static_cast<size_t>(wmax_cells(nf)) * nf * 4
+    return static_cast<size_t>(ns) * kChunk * 4 + static_cast<size_t>(wmax_cells(nf)) * nf * 8
            + kThreads / 32 * 4 * sizeof(int);
 }
 
@@ -118,6 +119,32 @@ __device__ void block_sum4(double a, double b, double c, double d, double* __res
     if (threadIdx.x == 4) part[blockIdx.x * 5 + 4] = 0.0;
 }
 
+// Block-wide fixed-order sum of NF floats (plus the valid-particle count in
+// slot NF) into part[blockIdx.x * (NF + 1) + f]. Deterministic for a fixed
+// launch shape.
+template <int NF>
+__device__ void block_sumsq(float (&sq)[NF], float cnt, float* __restrict__ part, float* sh /* (NF+1) * warps */) {
+    constexpr int NW = kThreads / 32;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) sq[f] += __shfl_down_sync(0xffffffffu, sq[f], o);
+        cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+    }
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) sh[f * NW + warp] = sq[f];
+        sh[NF * NW + warp] = cnt;
+    }
+    __syncthreads();
+    if (threadIdx.x <= NF) {
+        float s = 0.f;
+        for (int w = 0; w < NW; ++w) s += sh[threadIdx.x * NW + w];
+        part[blockIdx.x * (NF + 1) + threadIdx.x] = s;
+    }
+}
+
 // 4 consecutive floats at a[i..i+3] (vectorised when aligned and in range).
 __device__ __forceinline__ float4 ld4(const float* __restrict__ a, long long i, long long n, bool vec) {
     if (vec && i + 4 <= n) return __ldg(reinterpret_cast<const float4*>(a + i));
@@ -166,7 +193,7 @@ __device__ __forceinline__ float4& stq(float* st, int f, int q) {
 // in registers; lanes sit 64 particles apart, so their flushes rarely collide.
 // coef(v, e, cs) fills the scaled coefficients of element e of the quad planes v.
 template <int NF, int NS, class CoefFn>
-__device__ __forceinline__ void pass2(float* stage, int* win, const Win& wn,
+__device__ __forceinline__ void pass2(float* stage, long long* win, const Win& wn,
                                       unsigned long long* __restrict__ gacc, const Geo& g,
                                       DevState* st, unsigned& nslow, CoefFn coef) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -203,18 +230,20 @@ __device__ __forceinline__ void weights(const Cic& s, float (&wv)[4]) {
 template <int SET>
 __global__ void __launch_bounds__(kThreads)
 k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
-              unsigned long long* __restrict__ acc, int wmaxc, DevState* st) {
+              unsigned long long* __restrict__ acc, int wmaxc, DevState* st, float* __restrict__ psq) {
     constexpr int NF = SetNF<SET>::NF, NS = SetNF<SET>::NS;
     extern __shared__ __align__(16) unsigned char smem[];
     float* stage = reinterpret_cast<float*>(smem);
-    int* win = reinterpret_cast<int*>(smem + static_cast<size_t>(NS) * kChunk * 4);
-    int* red = win + wmaxc * NF;
+    long long* win = reinterpret_cast<long long*>(smem + static_cast<size_t>(NS) * kChunk * 4);
+    int* red = reinterpret_cast<int*>(win + static_cast<size_t>(wmaxc) * NF);
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
     const bool vec = p.vec_ok != 0;
     int ir, jr;
     ref_cell(p, c0, g, ir, jr);
     BBox bb;
+    float sq[NF] = {};
+    float cnt = 0.f;
     // pass 1: load into the stage (x, y, w[, ux, uy, uz]); an invalid slot has x = -1
 #pragma unroll 1
     for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
@@ -234,9 +263,22 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
         }
         stq(stage, 0, s0 >> 2) = x; stq(stage, 1, s0 >> 2) = y; stq(stage, 2, s0 >> 2) = w;
         if constexpr (NS == 6) {
-            stq(stage, 3, s0 >> 2) = ld4(p.ux, i, p.n, vec);
-            stq(stage, 4, s0 >> 2) = ld4(p.uy, i, p.n, vec);
-            stq(stage, 5, s0 >> 2) = ld4(p.uz, i, p.n, vec);
+            const float4 ux = ld4(p.ux, i, p.n, vec), uy = ld4(p.uy, i, p.n, vec), uz = ld4(p.uz, i, p.n, vec);
+            stq(stage, 3, s0 >> 2) = ux;
+            stq(stage, 4, s0 >> 2) = uy;
+            stq(stage, 5, s0 >> 2) = uz;
+            if (psq) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    if (!(compc(x, e) >= 0.0f)) continue;
+                    float cf[NF];
+                    src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(compc(w, e))), compc(ux, e),
+                                   compc(uy, e), compc(uz, e), cf);
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
+                    cnt += 1.0f;
+                }
+            }
         }
     }
     Win wn;
@@ -258,6 +300,10 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
     });
     __syncthreads();
     win_flush<NF>(win, wn, acc, g);
+    if (psq) {
+        __shared__ float ssq[(NF + 1) * (kThreads / 32)];
+        block_sumsq<NF>(sq, cnt, psq, ssq);
+    }
     if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
     if (threadIdx.x == 0) {
         atomicAdd(&st->chunks, 1ull);
@@ -285,34 +331,45 @@ __device__ __forceinline__ void gather_em(const float* __restrict__ gb, const Ci
     bz = gather4(s, b0.y, b1.y, b2.y, b3.y);
 }
 
-// dcu scale: |coef_dcu (E + v x B)| <= |qm| coef_max (Emax + 2 Umax Bmax).
-__device__ __forceinline__ float dcu_scale(const DevState* st, float abs_qm) {
+// dcu scales: |coef_dcu (E + v x B)| <= |qm| coef_max (Emax + 2 Umax Bmax); in
+// the fused step the bound per component is also capped at 8 x the rms the
+// previous step's dcu coefficients had.
+__device__ __forceinline__ void dcu_scales(const DevState* st, float abs_qm, bool use_rms, float (&S)[3]) {
     const float umax = fmaxf(__uint_as_float(st->ucur_bits[0]),
                              fmaxf(__uint_as_float(st->ucur_bits[1]), __uint_as_float(st->ucur_bits[2])));
     const float U = __fmul_rn(umax, 1.25f);
     const float bound = __fmul_rn(__fmul_rn(abs_qm, st->coef_max),
                                   __fmaf_rn(__fmul_rn(2.0f, U), __uint_as_float(st->bmax_bits),
                                             __uint_as_float(st->emax_bits)));
-    return scale_for_bound(bound);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float b = bound;
+        if (use_rms && st->have_rms && st->rms_dcu[k] > 0.0f) b = fminf(b, __fmul_rn(8.0f, st->rms_dcu[k]));
+        S[k] = scale_for_bound(b);
+    }
 }
 
 // dcu deposit: stage = x, y, ax, ay, az (the three scaled coefficients).
 __global__ void __launch_bounds__(kThreads, 2)
 k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restrict__ gb,
-              unsigned long long* __restrict__ acc, int wmaxc, DevState* st) {
+              unsigned long long* __restrict__ acc, int wmaxc, DevState* st, int use_rms,
+              float* __restrict__ psq) {
     constexpr int NF = 3, NS = 5;
     extern __shared__ __align__(16) unsigned char smem[];
     float* stage = reinterpret_cast<float*>(smem);
-    int* win = reinterpret_cast<int*>(smem + static_cast<size_t>(NS) * kChunk * 4);
-    int* red = win + wmaxc * NF;
+    long long* win = reinterpret_cast<long long*>(smem + static_cast<size_t>(NS) * kChunk * 4);
+    int* red = reinterpret_cast<int*>(win + static_cast<size_t>(wmaxc) * NF);
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
     const bool vec = p.vec_ok != 0;
-    const float S = dcu_scale(st, abs_qm);
-    if (blockIdx.x == 0 && threadIdx.x == 0) { st->S_dcu[0] = S; st->S_dcu[1] = S; st->S_dcu[2] = S; }
+    float S[3];
+    dcu_scales(st, abs_qm, use_rms != 0, S);
+    if (blockIdx.x == 0 && threadIdx.x == 0) { st->S_dcu[0] = S[0]; st->S_dcu[1] = S[1]; st->S_dcu[2] = S[2]; }
     int ir, jr;
     ref_cell(p, c0, g, ir, jr);
     BBox bb;
+    float sq[NF] = {};
+    float cnt = 0.f;
 #pragma unroll 1
     for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
         const int s0 = it * 4 * kThreads + 4 * threadIdx.x;
@@ -335,9 +392,14 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
                 const float cx = __fmaf_rn(vy, bz, -__fmul_rn(vz, by));
                 const float cy = __fmaf_rn(vz, bx, -__fmul_rn(vx, bz));
                 const float cz = __fmaf_rn(vx, by, -__fmul_rn(vy, bx));
-                comp(ax, e) = __fmul_rn(__fmul_rn(coef, __fadd_rn(ex, cx)), S);
-                comp(ay, e) = __fmul_rn(__fmul_rn(coef, __fadd_rn(ey, cy)), S);
-                comp(az, e) = __fmul_rn(__fmul_rn(coef, __fadd_rn(ez, cz)), S);
+                const float a0 = __fmul_rn(coef, __fadd_rn(ex, cx));
+                const float a1 = __fmul_rn(coef, __fadd_rn(ey, cy));
+                const float a2 = __fmul_rn(coef, __fadd_rn(ez, cz));
+                comp(ax, e) = __fmul_rn(a0, S[0]);
+                comp(ay, e) = __fmul_rn(a1, S[1]);
+                comp(az, e) = __fmul_rn(a2, S[2]);
+                sq[0] = __fmaf_rn(a0, a0, sq[0]); sq[1] = __fmaf_rn(a1, a1, sq[1]); sq[2] = __fmaf_rn(a2, a2, sq[2]);
+                cnt += 1.0f;
             } else {
                 if (i + e < p.n) set_err(st, AW_DEV_OUT_OF_GRID);
                 xe = -1.0f;
@@ -356,6 +418,10 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
     });
     __syncthreads();
     win_flush<NF>(win, wn, acc, g);
+    if (psq) {
+        __shared__ float ssq[(NF + 1) * (kThreads / 32)];
+        block_sumsq<NF>(sq, cnt, psq, ssq);
+    }
     if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
     if (threadIdx.x == 0) {
         atomicAdd(&st->chunks, 1ull);
@@ -380,8 +446,8 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     constexpr int NF = 1, NS = 3;
     extern __shared__ __align__(16) unsigned char smem[];
     float* stage = reinterpret_cast<float*>(smem);
-    int* win = reinterpret_cast<int*>(smem + static_cast<size_t>(NS) * kChunk * 4);
-    int* red = win + wmaxc * NF;
+    long long* win = reinterpret_cast<long long*>(smem + static_cast<size_t>(NS) * kChunk * 4);
+    int* red = reinterpret_cast<int*>(win + static_cast<size_t>(wmaxc) * NF);
     __shared__ double dsh[4 * (kThreads / 32)];
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
@@ -464,12 +530,12 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
 __global__ void __launch_bounds__(kThreads, 2)
 k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                   double qoa, unsigned long long* __restrict__ acc, int wmaxc,
-                  double* __restrict__ part, DevState* st) {
+                  double* __restrict__ part, DevState* st, float* __restrict__ psq) {
     constexpr int NF = 8, NS = 6;
     extern __shared__ __align__(16) unsigned char smem[];
     float* stage = reinterpret_cast<float*>(smem);
-    int* win = reinterpret_cast<int*>(smem + static_cast<size_t>(NS) * kChunk * 4);
-    int* red = win + wmaxc * NF;
+    long long* win = reinterpret_cast<long long*>(smem + static_cast<size_t>(NS) * kChunk * 4);
+    int* red = reinterpret_cast<int*>(win + static_cast<size_t>(wmaxc) * NF);
     __shared__ double dsh[4 * (kThreads / 32)];
     __shared__ unsigned umx[3][kThreads / 32];
 
@@ -480,6 +546,8 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     BBox bb;
     double ke = 0, px = 0, py = 0, pz = 0;
     float m0 = 0.f, m1 = 0.f, m2 = 0.f;
+    float sq[NF] = {};
+    float cnt = 0.f;
 #pragma unroll 1
     for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
         const int s0 = it * 4 * kThreads + 4 * threadIdx.x;
@@ -511,6 +579,13 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                 comp(xs, e) = xe;
             }
             m0 = fmaxf(m0, fabsf(u)); m1 = fmaxf(m1, fabsf(v)); m2 = fmaxf(m2, fabsf(wz));
+            {
+                float cf[NF];
+                src_coefs<SET_ALL>(__double2float_rn(qoa * static_cast<double>(compc(w, e))), u, v, wz, cf);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
+                cnt += 1.0f;
+            }
             const double dw = compc(w, e), du = u, dv = v, dz = wz;
             ke += dw * (du * du + dv * dv + dz * dz);
             px += dw * du; py += dw * dv; pz += dw * dz;
@@ -546,14 +621,26 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
 #pragma unroll
     for (int f = 0; f < NF; ++f) S[f] = st->S_next[f];
     unsigned nslow = 0;
-    pass2<NF, NS>(stage, win, wn, acc, g, st, nslow, [&](const float4 (&v)[NS], int e, float (&cs)[NF]) {
+    // two 4-field sub-passes (rho, J then amu) keep the register runs small
+    pass2<4, NS>(stage, win, wn, acc, g, st, nslow, [&](const float4 (&v)[NS], int e, float (&cs)[4]) {
         const float coef = __double2float_rn(qoa * static_cast<double>(compc(v[2], e)));
-        src_coefs<SET_ALL>(coef, compc(v[3], e), compc(v[4], e), compc(v[5], e), cs);
+        src_coefs<SET_RHOJ>(coef, compc(v[3], e), compc(v[4], e), compc(v[5], e), cs);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cs[f], S[f]);
+        for (int f = 0; f < 4; ++f) cs[f] = __fmul_rn(cs[f], S[f]);
+    });
+    pass2<4, NS>(stage, win + 4 * wn.WH, wn, acc + static_cast<size_t>(4) * g.ncell, g, st, nslow,
+                 [&](const float4 (&v)[NS], int e, float (&cs)[4]) {
+        const float coef = __double2float_rn(qoa * static_cast<double>(compc(v[2], e)));
+        src_coefs<SET_AMU>(coef, compc(v[3], e), compc(v[4], e), compc(v[5], e), cs);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) cs[f] = __fmul_rn(cs[f], S[4 + f]);
     });
     __syncthreads();
     win_flush<NF>(win, wn, acc, g);
+    {
+        __shared__ float ssq[(NF + 1) * (kThreads / 32)];
+        block_sumsq<NF>(sq, cnt, psq, ssq);
+    }
     block_sum4(ke, px, py, pz, part, dsh);
     if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
     if (threadIdx.x == 0) {
@@ -596,7 +683,8 @@ void launch_src(Ctx& c, unsigned long long* acc) {
     prep_smem(k_deposit_src<SET>, sh);
     const double qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
     k_deposit_src<SET><<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(c.parts, c.geo, qoa, c.st->S_pend, acc,
-                                                                        wmax_cells(NF), c.st);
+                                                                        wmax_cells(NF), c.st,
+                                                                        SET == SET_ALL ? c.part_c : nullptr);
     AW_LAUNCH();
 }
 
@@ -614,13 +702,14 @@ void launch_deposit_src(Ctx& c, int which) {
     }
 }
 
-void launch_deposit_dcu(Ctx& c, const float* gb) {
+void launch_deposit_dcu(Ctx& c, const float* gb, bool fused) {
     if (c.parts.n == 0) return;
     const double qm2oa = c.prm.qm * c.prm.qm / (c.geo.dx * c.geo.dy);
     const size_t sh = smem_bytes(3, 5);
     prep_smem(k_deposit_dcu, sh);
     k_deposit_dcu<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(
-        c.parts, c.geo, qm2oa, static_cast<float>(std::fabs(c.prm.qm)), gb, c.acc_dcu, wmax_cells(3), c.st);
+        c.parts, c.geo, qm2oa, static_cast<float>(std::fabs(c.prm.qm)), gb, c.acc_dcu, wmax_cells(3), c.st,
+        fused ? 1 : 0, fused ? c.part_d : nullptr);
     AW_LAUNCH();
 }
 
@@ -650,7 +739,7 @@ void launch_push_deposit_em(Ctx& c) {
     const size_t sh = smem_bytes(8, 6);
     prep_smem(k_push_deposit_em, sh);
     k_push_deposit_em<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(
-        c.parts, c.geo, pp, c.gb_push, qoa, c.acc_src, wmax_cells(8), c.part_p, c.st);
+        c.parts, c.geo, pp, c.gb_push, qoa, c.acc_src, wmax_cells(8), c.part_p, c.st, c.part_c);
     AW_LAUNCH();
 }
 

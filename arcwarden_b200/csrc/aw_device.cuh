@@ -16,11 +16,10 @@
 //   * window deposit engine — one CTA owns a chunk of kChunk consecutive
 //                             particles, reduces the bounding box of their cells,
 //                             privatises that window of cells in shared memory as
-//                             int32 accumulators ([NF][W*H]), sums the
-//                             contributions of warp lanes that share a cell with
-//                             one redux.sync per value (exact integer sums) and
-//                             flushes the window into the global int64
-//                             accumulators with red.global.add.u64.
+//                             int64 accumulators ([NF][W*H]), sums each lane's
+//                             same-cell runs exactly in int32 registers, adds the
+//                             runs with shared atomics and flushes the window into
+//                             the global int64 accumulators (red.global.add.u64).
 //
 // Reference arithmetic being mirrored (paths relative to the ArcWarden tree):
 //   CIC weights           include/pic/grid.hpp:135-155, depositor.hpp:136-146
@@ -39,11 +38,10 @@ constexpr int kThreads = 256;          // CTA size of every particle kernel
 constexpr int kPPT     = 8;            // consecutive particles per thread
 constexpr int kChunk   = kThreads * kPPT;   // particles per CTA chunk (2048)
 
-// Fast-path range of one quantised contribution: |v*S| < 2^20 rounds exactly
-// with one FADD against 1.5*2^23, and a chunk of kChunk = 2048 particles adds at
-// most 2048 such values into one shared-window cell, so the int32 window sums
-// cannot overflow (2048 * 2^20 = 2^31).
-constexpr float kFastLim   = 1048576.0f;      // 2^20
+// Fast-path range of one quantised contribution: |v*S| < 2^22 rounds exactly
+// with one FFMA against 1.5*2^23; a register run of at most 8 particles sums to
+// < 2^25 (int32), and the shared window planes are int64.
+constexpr float kFastLim   = 4194304.0f;      // 2^22
 constexpr float kMagic     = 12582912.0f;     // 1.5 * 2^23
 constexpr int   kMagicBits = 0x4B400000;
 constexpr unsigned kMagicU  = 0x4B400000u;
@@ -71,7 +69,9 @@ struct DevState {
     float     S_pend[8];       // scales of the pending (not yet finalised) deposit
     float     S_dcu[4];        // scale of the pending dcu deposit (x3, same value)
     float     coef_max;        // max |qm w / (dx dy)| over particles
-    float     pad0;
+    int       have_rms;        // rms_src / rms_dcu hold measured values
+    float     rms_src[8];      // rms of the source deposit coefficients (unscaled)
+    float     rms_dcu[4];      // rms of the dcu coefficients (unscaled)
     unsigned long long chunks, overflow, slow;
 };
 
@@ -100,13 +100,13 @@ __device__ __forceinline__ void set_err(DevState* st, unsigned bits) {
     atomicOr(&st->err, bits);
 }
 
-// Power-of-two scale S such that bound * S < 2^20 (the fast path), from a
+// Power-of-two scale S such that bound * S < 2^22 (the fast path), from a
 // positive bound. Deterministic: a pure function of the bound.
 __host__ __device__ inline float scale_for_bound(float bound) {
     if (!(bound > 0.0f) || !(bound < 3.0e38f)) return 1.0f;
     int e;
     frexpf(bound, &e);            // bound in [2^(e-1), 2^e)
-    int k = 20 - e;               // bound * 2^k < 2^20
+    int k = 22 - e;               // bound * 2^k < 2^22
     if (k > 120) k = 120;
     if (k < -120) k = -120;
     return ldexpf(1.0f, k);
@@ -196,7 +196,7 @@ __device__ __forceinline__ int cell_of(float x, float y, int nx, int ny) {
 
 // ---------------------------------------------------------------------------
 // Fixed-point rounding. q = rint(t) with t = v*S already scaled; exact for the
-// fast path (|t| < 2^20) and identical to llrintf(t) in the C oracle.
+// fast path (|t| < 2^22) and identical to llrintf(t) in the C oracle.
 __device__ __forceinline__ int quant_fast(float t) {
     return __float_as_int(__fadd_rn(t, kMagic)) - kMagicBits;
 }
@@ -292,7 +292,7 @@ __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, 
 
 // Zero NF window planes; the caller syncs afterwards.
 template <int NF>
-__device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
+__device__ __forceinline__ void win_zero(long long* __restrict__ s, const Win& w) {
     const int m = NF * w.WH;
     for (int i = threadIdx.x; i < m; i += kThreads) s[i] = 0;
 }
@@ -300,17 +300,16 @@ __device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
 // Flush the window into the global int64 accumulators acc[f*ncell + cell].
 // The caller syncs before calling.
 template <int NF>
-__device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& w,
+__device__ __forceinline__ void win_flush(const long long* __restrict__ s, const Win& w,
                                           unsigned long long* __restrict__ acc, const Geo& g) {
     for (int c = threadIdx.x; c < w.WH; c += kThreads) {
         const int wi = c % w.W, wj = c / w.W;
         const int gc = wrap_far(w.jr + w.mj + wj, g.ny) * g.nx + wrap_far(w.ir + w.mi + wi, g.nx);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            const int v = s[f * w.WH + c];
+            const long long v = s[f * w.WH + c];
             if (v != 0)
-                atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gc,
-                          static_cast<unsigned long long>(static_cast<long long>(v)));
+                atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gc, static_cast<unsigned long long>(v));
         }
     }
 }
@@ -353,7 +352,7 @@ struct Run {
         ++cnt;
     }
     // Add the run into the window planes s[f*WH + cell].
-    __device__ __forceinline__ void flush(int* __restrict__ s, const Win& w) {
+    __device__ __forceinline__ void flush(long long* __restrict__ s, const Win& w) {
         if (cw < 0) return;
         const unsigned m = cnt * kMagicU;
         const int offs[4] = {0, 1, w.W, w.W + 1};
@@ -362,7 +361,9 @@ struct Run {
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int v = static_cast<int>(a[f][k] - m);
-                if (v != 0) atomicAdd(s + f * w.WH + cw + offs[k], v);
+                if (v != 0)
+                    atomicAdd(reinterpret_cast<unsigned long long*>(s + f * w.WH + cw + offs[k]),
+                              static_cast<unsigned long long>(static_cast<long long>(v)));
             }
     }
 };
@@ -388,7 +389,7 @@ __device__ __forceinline__ void deposit_global(int ci, int cj, const float (&wv)
 // base cell changes), or through the exact slow path when the window is unused
 // or a coefficient is outside the fast range.
 template <int NF>
-__device__ __forceinline__ void run_deposit(Run<NF>& run, int* __restrict__ s, const Win& w,
+__device__ __forceinline__ void run_deposit(Run<NF>& run, long long* __restrict__ s, const Win& w,
                                             int ci, int cj, const float (&wv)[4], const float (&cs)[NF],
                                             unsigned long long* __restrict__ gacc, const Geo& g,
                                             unsigned& nslow, DevState* st) {

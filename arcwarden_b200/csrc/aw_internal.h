@@ -80,6 +80,8 @@ struct Ctx {
     float* gb_push = nullptr;   // 8 * ncell
     // diagnostics partials and result
     double* part_p = nullptr;   // particle partials [nblk][5]
+    float*  part_c = nullptr;   // source-coefficient sums of squares [nblk][9]
+    float*  part_d = nullptr;   // dcu-coefficient sums of squares [nblk][4]
     double* part_g = nullptr;   // grid partials [nblk][5]
     int     npart_p = 0, npart_g = 0;
     aw_diag* diag = nullptr;    // device aw_diag
@@ -128,7 +130,7 @@ void launch_particle_diag(Ctx& c);                 // KE, P partials -> part_p
 // ---- launchers (aw_deposit.cu) --------------------------------------------
 // which: 1 = rho, 4 = rho+J, -4 = amu (fields 4..7), 8 = rho+J+amu
 void launch_deposit_src(Ctx& c, int which);
-void launch_deposit_dcu(Ctx& c, const float* gb);
+void launch_deposit_dcu(Ctx& c, const float* gb, bool fused);
 void launch_push_deposit_es(Ctx& c);
 void launch_push_deposit_em(Ctx& c);
 
@@ -153,5 +155,6 @@ void launch_pack_em(Ctx& c);
 void launch_grid_diag(Ctx& c);
 void launch_set_step(Ctx& c, long long n);
 void launch_copy_umax(Ctx& c);
+void launch_rms_reduce(Ctx& c, bool src, bool dcu);
 
 }  // namespace aw

@@ -45,10 +45,13 @@ __device__ __forceinline__ double pump_ramp(double t, double trmp, double toff) 
     return 1.0;
 }
 
-// Deposit scales for the next source deposit from the current |u| maxima.
-// |u_d| bound U_d = max(1.25 max|u_d|, 0.01 cref); see aw_device.cuh for the
-// fast-path contract.
-__device__ void make_src_scales(const DevState* st, float cref, float (&S)[8]) {
+// Deposit scales for the next source deposit from the current |u| maxima:
+// |u_d| bound U_d = max(1.25 max|u_d|, 0.01 cref). With use_rms (the fused
+// step), the bound of each velocity-dependent field is also capped at 8 x the
+// rms its coefficients had in the previous deposit; the few contributions
+// beyond that take the exact slow path. See aw_device.cuh for the fast-path
+// contract.
+__device__ void make_src_scales(const DevState* st, float cref, float (&S)[8], bool use_rms) {
     float U[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d)
@@ -62,11 +65,20 @@ __device__ void make_src_scales(const DevState* st, float cref, float (&S)[8]) {
     S[5] = scale_for_bound(__fmul_rn(__fmul_rn(cm, U[0]), U[1]));
     S[6] = scale_for_bound(__fmul_rn(__fmul_rn(cm, U[2]), U[0]));
     S[7] = scale_for_bound(__fmul_rn(__fmul_rn(cm, U[2]), U[1]));
+    if (use_rms && st->have_rms) {
+        float b[8] = {0.f, __fmul_rn(cm, U[0]), __fmul_rn(cm, U[1]), __fmul_rn(cm, U[2]),
+                      __fmul_rn(__fmul_rn(cm, 0.5f), fmaxf(__fmul_rn(U[0], U[0]), __fmul_rn(U[1], U[1]))),
+                      __fmul_rn(__fmul_rn(cm, U[0]), U[1]), __fmul_rn(__fmul_rn(cm, U[2]), U[0]),
+                      __fmul_rn(__fmul_rn(cm, U[2]), U[1])};
+#pragma unroll
+        for (int f = 1; f < 8; ++f)
+            if (st->rms_src[f] > 0.0f) S[f] = scale_for_bound(fminf(b[f], __fmul_rn(8.0f, st->rms_src[f])));
+    }
 }
 
 __global__ void k_make_scales(DevState* st, float cref) {
     float S[8];
-    make_src_scales(st, cref, S);
+    make_src_scales(st, cref, S, false);
 #pragma unroll
     for (int f = 0; f < 8; ++f) { st->S_next[f] = S[f]; st->S_pend[f] = S[f]; }
 }
@@ -143,7 +155,7 @@ k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
         st->emax_bits = 0u; st->bmax_bits = 0u;
         if (darwin) {
             float S[8];
-            make_src_scales(st, cref, S);
+            make_src_scales(st, cref, S, true);
 #pragma unroll
             for (int f = 0; f < 8; ++f) st->S_next[f] = S[f];
         }
@@ -486,6 +498,41 @@ __global__ void k_grid_diag(const float* ex, const float* ey, const float* bx, c
     grid_partials(se2, me2, sb2, part);
 }
 
+// RMS of the (unscaled) deposit coefficients from the fixed-order block
+// partials of sum coef^2 and the particle count: rms_f = sqrt(sum / n).
+__global__ void __launch_bounds__(256)
+k_rms_reduce(const float* __restrict__ pc, int nbc, const float* __restrict__ pd, int nbd, DevState* st) {
+    __shared__ double sh[12][256];
+    const int t = threadIdx.x;
+    double a[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};   // 8 src + count, 3 dcu... (see below)
+    if (pc) for (int b = t; b < nbc; b += 256) for (int k = 0; k < 9; ++k) a[k] += pc[b * 9 + k];
+    double ad[4] = {0, 0, 0, 0};
+    if (pd) for (int b = t; b < nbd; b += 256) for (int k = 0; k < 4; ++k) ad[k] += pd[b * 4 + k];
+    for (int k = 0; k < 9; ++k) sh[k][t] = a[k];
+    for (int k = 0; k < 3; ++k) sh[9 + k][t] = ad[k];
+    __shared__ double shn[256];
+    shn[t] = ad[3];
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (t < s) {
+            for (int k = 0; k < 12; ++k) sh[k][t] += sh[k][t + s];
+            shn[t] += shn[t + s];
+        }
+        __syncthreads();
+    }
+    if (t == 0) {
+        if (pc && sh[8][0] > 0.0) {
+            for (int f = 0; f < 8; ++f)
+                st->rms_src[f] = static_cast<float>(sqrt(sh[f][0] / sh[8][0]));
+        }
+        if (pd && shn[0] > 0.0) {
+            for (int k = 0; k < 3; ++k)
+                st->rms_dcu[k] = static_cast<float>(sqrt(sh[9 + k][0] / shn[0]));
+        }
+        st->have_rms = 1;
+    }
+}
+
 __global__ void k_set_step(DevState* st, long long n) { st->step = n; }
 __global__ void k_copy_umax(DevState* st) {
     for (int d = 0; d < 3; ++d) st->umax_bits[d] = st->ucur_bits[d];
@@ -620,6 +667,11 @@ void launch_grid_diag(Ctx& c) {
 }
 void launch_set_step(Ctx& c, long long n) {
     k_set_step<<<1, 1, 0, c.stream>>>(c.st, n);
+    AW_LAUNCH();
+}
+void launch_rms_reduce(Ctx& c, bool src, bool dcu) {
+    k_rms_reduce<<<1, 256, 0, c.stream>>>(src ? c.part_c : nullptr, c.npart_p, dcu ? c.part_d : nullptr,
+                                          c.npart_p, c.st);
     AW_LAUNCH();
 }
 void launch_copy_umax(Ctx& c) {

@@ -214,7 +214,7 @@ int aw_run_diag(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph, aw_d
 
 /* One fused step (like aw_step) with CUDA events recorded on the context's
  * stream between its phases; ms[i] = duration of phase i, *nphase = number of
- * phases (cap >= 13). Synchronises. Phase names: aw_step_phase_name. */
+ * phases (cap >= 14). Synchronises. Phase names: aw_step_phase_name. */
 int aw_step_profile(aw_ctx* ctx, int64_t n, float* ms, int32_t cap, int32_t* nphase);
 const char* aw_step_phase_name(int32_t model, int32_t i);
 

@@ -46,7 +46,7 @@ class _State(C.Structure):
         ("etz", C.c_void_p),
         ("ke", C.c_double), ("ee", C.c_double), ("charge", C.c_double), ("px", C.c_double),
         ("py", C.c_double), ("pz", C.c_double), ("eb", C.c_double), ("max_e", C.c_double),
-        ("nthreads", C.c_int),
+        ("nthreads", C.c_int), ("exact", C.c_int),
     ]
 
 
@@ -71,6 +71,8 @@ def lib():
                            C.c_int, _i64],
             "or_deposit_dcu": [G, _f32, _f32, _f32, _f32, _f32, _f32, C.c_int64, C.c_double, _f32, C.c_float, _i64],
             "or_finalize": [_i64, C.c_int, C.c_int32, _f32, _f32],
+            "or_deposit_f64": [G, _f32, _f32, C.c_void_p, C.c_void_p, C.c_void_p, _f32, C.c_int64, C.c_double,
+                               C.c_int, _f64],
             "or_src_scales": [C.c_float, _f32, C.c_float, _f32],
             "or_particle_max": [_f32, _f32, _f32, _f32, C.c_int64, C.c_double, _f32, C.POINTER(C.c_float)],
             "or_push_es": [G, _f32, _f32, _f32, _f32, _f32, C.c_int64, _f32, C.c_float, C.c_int, _f32, C.c_double,
@@ -146,6 +148,18 @@ def deposit(g, x, y, ux, uy, uz, w, qm, S, fset):
     uzz = None if uz is None else _c32(uz)
     lib().or_deposit(C.byref(g), _c32(x), _c32(y), _opt(uxx), _opt(uyy), _opt(uzz), _c32(w), len(x), qm,
                      _c32(S), fset, acc)
+    return acc.reshape(nf, g.ny, g.nx)
+
+
+def deposit_f64(g, x, y, ux, uy, uz, w, qm, fset):
+    """FP64 deposit of the same FP32 contributions; returns [nf, ny, nx] doubles."""
+    nf = lib().or_nf(fset)
+    acc = np.zeros(nf * g.nx * g.ny, np.float64)
+    uxx = None if ux is None else _c32(ux)
+    uyy = None if uy is None else _c32(uy)
+    uzz = None if uz is None else _c32(uz)
+    lib().or_deposit_f64(C.byref(g), _c32(x), _c32(y), _opt(uxx), _opt(uyy), _opt(uzz), _c32(w), len(x), qm,
+                         fset, acc)
     return acc.reshape(nf, g.ny, g.nx)
 
 
@@ -266,7 +280,7 @@ class State:
     """One simulation run on the CPU oracle (same step ordering as the fused GPU step)."""
 
     def __init__(self, g, parts, *, dt, qm=-1.0, eps0=1.0, n0=1.0, c=1.0, B0=(0, 0, 0), has_b0=True,
-                 darwin=False, pump=None):
+                 darwin=False, pump=None, exact=False):
         self.g = g
         self.darwin = darwin
         ncell = g.nx * g.ny
@@ -288,6 +302,7 @@ class State:
             s.pump_ex, s.pump_ey, s.pump_ez = pump["ex"], pump["ey"], pump["ez"]
             s.pump_k0, s.pump_w0, s.pump_trmp, s.pump_toff = pump["k0"], pump["w0"], pump["trmp"], pump["toff"]
         s.n = len(self.p["x"])
+        s.exact = int(bool(exact))
         for k in ("x", "y", "ux", "uy", "uz", "w"):
             setattr(s, k, self.p[k].ctypes.data)
         s.acc = self.acc.ctypes.data

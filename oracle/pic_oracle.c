@@ -15,7 +15,7 @@
 #include <omp.h>
 #endif
 
-#define FAST_LIM 1048576.0f
+#define FAST_LIM 4194304.0f
 static const double kTwoPi = 6.28318530717958647692;
 
 static inline int wrap_once(int i, int n) { if (i >= n) i -= n; if (i < 0) i += n; return i; }
@@ -205,6 +205,52 @@ void or_deposit_dcu(const or_geo* g, const float* x, const float* y, const float
     }
 }
 
+/* FP64 deposits: the same FP32 per-particle coefficients and CIC weights, summed
+ * as exact double products (the FP64 host oracle's sources). Single-threaded. */
+void or_deposit_f64(const or_geo* g, const float* x, const float* y, const float* ux, const float* uy,
+                    const float* uz, const float* w, int64_t n, double qm, int set, double* acc) {
+    const int nf = or_nf(set);
+    const int nx = g->nx, ny = g->ny;
+    const int64_t ncell = (int64_t)nx * ny;
+    const double qoa = qm / ((g->Lx / nx) * (g->Ly / ny));
+    for (int64_t p = 0; p < n; ++p) {
+        const float px = x[p], py = y[p];
+        if (!(px >= 0.0f && px < (float)nx && py >= 0.0f && py < (float)ny)) continue;
+        const cic_t s = cic(px, py);
+        int c[4];
+        corners(&s, nx, ny, c);
+        float cf[8];
+        src_coefs(set, (float)(qoa * (double)w[p]), ux ? ux[p] : 0.0f, uy ? uy[p] : 0.0f, uz ? uz[p] : 0.0f, cf);
+        for (int f = 0; f < nf; ++f)
+            for (int k = 0; k < 4; ++k) acc[(size_t)f * ncell + c[k]] += (double)cf[f] * (double)s.w[k];
+    }
+}
+
+void or_deposit_dcu_f64(const or_geo* g, const float* x, const float* y, const float* ux, const float* uy,
+                        const float* uz, const float* w, int64_t n, double qm, const float* gb, double* acc) {
+    const int nx = g->nx, ny = g->ny;
+    const int64_t ncell = (int64_t)nx * ny;
+    const double qm2oa = qm * qm / ((g->Lx / nx) * (g->Ly / ny));
+    for (int64_t p = 0; p < n; ++p) {
+        const float px = x[p], py = y[p];
+        if (!(px >= 0.0f && px < (float)nx && py >= 0.0f && py < (float)ny)) continue;
+        const cic_t s = cic(px, py);
+        int c[4];
+        corners(&s, nx, ny, c);
+        float v[6];
+        for (int q = 0; q < 6; ++q)
+            v[q] = gather4(&s, gb[(size_t)c[0] * 8 + q], gb[(size_t)c[1] * 8 + q], gb[(size_t)c[2] * 8 + q],
+                           gb[(size_t)c[3] * 8 + q]);
+        const float vx = ux[p], vy = uy[p], vz = uz[p];
+        const float coef = (float)(qm2oa * (double)w[p]);
+        const float a[3] = {coef * (v[0] + fmaf(vy, v[5], -(vz * v[4]))),
+                            coef * (v[1] + fmaf(vz, v[3], -(vx * v[5]))),
+                            coef * (v[2] + fmaf(vx, v[4], -(vy * v[3])))};
+        for (int f = 0; f < 3; ++f)
+            for (int k = 0; k < 4; ++k) acc[(size_t)f * ncell + c[k]] += (double)a[f] * (double)s.w[k];
+    }
+}
+
 void or_finalize(const int64_t* acc, int nf, int32_t ncell, const float* S, float* out) {
     for (int f = 0; f < nf; ++f) {
         const double inv = 1.0 / (double)S[f];
@@ -218,7 +264,7 @@ float or_scale_for_bound(float b) {
     if (!(b > 0.0f) || !(b < 3.0e38f)) return 1.0f;
     int e;
     frexpf(b, &e);
-    int k = 20 - e;
+    int k = 22 - e;
     if (k > 120) k = 120;
     if (k < -120) k = -120;
     return ldexpf(1.0f, k);
@@ -632,11 +678,18 @@ static void diag_particles(or_state* s) {
 static void es_fields(or_state* s, float* gb) {
     const int32_t nc = s->g.nx * s->g.ny;
     const double dxdy = (s->g.Lx / s->g.nx) * (s->g.Ly / s->g.ny);
-    or_finalize(s->acc, 1, nc, s->S_pend, s->rho);
+    double* r = (double*)calloc(3 * (size_t)nc, sizeof(double));
+    if (s->exact) {
+        /* FP64 oracle: exact deposit of the current particles */
+        or_deposit_f64(&s->g, s->x, s->y, NULL, NULL, NULL, s->w, s->n, s->qm, 0, r);
+        for (int32_t c = 0; c < nc; ++c) s->rho[c] = (float)r[c];
+    } else {
+        or_finalize(s->acc, 1, nc, s->S_pend, s->rho);
+        for (int32_t c = 0; c < nc; ++c) r[c] = s->rho[c];
+    }
     memset(s->acc, 0, sizeof(int64_t) * nc);
-    double* r = (double*)malloc(sizeof(double) * 3 * nc);
     double q = 0;
-    for (int32_t c = 0; c < nc; ++c) { r[c] = s->rho[c]; q += s->rho[c]; }
+    for (int32_t c = 0; c < nc; ++c) q += r[c];
     or_solve_es(&s->g, s->eps0, r, r + nc, r + 2 * nc);
     double se2 = 0, me2 = 0;
     for (int32_t c = 0; c < nc; ++c) {
@@ -661,17 +714,22 @@ static void darwin_fields(or_state* s, float* gb_push, int step_begin) {
         or_src_scales(s->coef_max, s->ucur, (float)s->c, s->S_next);
     }
     float* srcf = (float*)malloc(sizeof(float) * 8 * (size_t)nc);
-    or_finalize(s->acc, 8, nc, s->S_pend, srcf);
+    double* d = (double*)calloc(16 * (size_t)nc, sizeof(double));
+    if (s->exact) {
+        or_deposit_f64(&s->g, s->x, s->y, s->ux, s->uy, s->uz, s->w, s->n, s->qm, 3, d);
+        for (size_t c = 0; c < 8 * (size_t)nc; ++c) srcf[c] = (float)d[c];
+    } else {
+        or_finalize(s->acc, 8, nc, s->S_pend, srcf);
+        for (size_t c = 0; c < 8 * (size_t)nc; ++c) d[c] = srcf[c];
+    }
     memset(s->acc, 0, sizeof(int64_t) * 8 * (size_t)nc);
     memcpy(s->rho, srcf, sizeof(float) * nc);
     memcpy(s->jx, srcf + nc, sizeof(float) * nc);
     memcpy(s->jy, srcf + 2 * (size_t)nc, sizeof(float) * nc);
     memcpy(s->jz, srcf + 3 * (size_t)nc, sizeof(float) * nc);
     memcpy(s->amu, srcf + 4 * (size_t)nc, sizeof(float) * 4 * nc);
-    double* d = (double*)malloc(sizeof(double) * 16 * (size_t)nc);
     double q = 0;
-    for (size_t c = 0; c < 8 * (size_t)nc; ++c) d[c] = srcf[c];
-    for (int32_t c = 0; c < nc; ++c) q += srcf[c];
+    for (int32_t c = 0; c < nc; ++c) q += d[c];
     double* el = d + 8 * (size_t)nc;   /* elx, ely, bx, by, bz */
     or_solve_elb(&s->g, s->eps0, s->c, d, d + nc, d + 2 * (size_t)nc, d + 3 * (size_t)nc, el, el + nc,
                  el + 2 * (size_t)nc, el + 3 * (size_t)nc, el + 4 * (size_t)nc);
@@ -691,15 +749,21 @@ static void darwin_fields(or_state* s, float* gb_push, int step_begin) {
         emax = fmaxf(emax, fmaxf(fabsf(ex), fmaxf(fabsf(ey), fabsf(ez))));
         bmax = fmaxf(bmax, fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
     }
-    const float Sd = or_dcu_scale((float)fabs(s->qm), s->coef_max, s->ucur, emax, bmax);
-    int64_t* acc = (int64_t*)calloc(3 * (size_t)nc, sizeof(int64_t));
-    or_deposit_dcu(&s->g, s->x, s->y, s->ux, s->uy, s->uz, s->w, s->n, s->qm, gb, Sd, acc);
-    const float S3[3] = {Sd, Sd, Sd};
-    or_finalize(acc, 3, nc, S3, s->dcu);
-    free(acc);
-    double* dd = (double*)malloc(sizeof(double) * 10 * (size_t)nc);
-    for (size_t c = 0; c < 3 * (size_t)nc; ++c) dd[c] = s->dcu[c];
-    for (size_t c = 0; c < 4 * (size_t)nc; ++c) dd[3 * (size_t)nc + c] = s->amu[c];
+    double* dd = (double*)calloc(10 * (size_t)nc, sizeof(double));
+    if (s->exact) {
+        or_deposit_dcu_f64(&s->g, s->x, s->y, s->ux, s->uy, s->uz, s->w, s->n, s->qm, gb, dd);
+        for (size_t c = 0; c < 3 * (size_t)nc; ++c) s->dcu[c] = (float)dd[c];
+        for (size_t c = 0; c < 4 * (size_t)nc; ++c) dd[3 * (size_t)nc + c] = d[4 * (size_t)nc + c];
+    } else {
+        const float Sd = or_dcu_scale((float)fabs(s->qm), s->coef_max, s->ucur, emax, bmax);
+        int64_t* acc = (int64_t*)calloc(3 * (size_t)nc, sizeof(int64_t));
+        or_deposit_dcu(&s->g, s->x, s->y, s->ux, s->uy, s->uz, s->w, s->n, s->qm, gb, Sd, acc);
+        const float S3[3] = {Sd, Sd, Sd};
+        or_finalize(acc, 3, nc, S3, s->dcu);
+        free(acc);
+        for (size_t c = 0; c < 3 * (size_t)nc; ++c) dd[c] = s->dcu[c];
+        for (size_t c = 0; c < 4 * (size_t)nc; ++c) dd[3 * (size_t)nc + c] = s->amu[c];
+    }
     double* et = (double*)malloc(sizeof(double) * 3 * (size_t)nc);
     or_solve_et(&s->g, s->eps0, s->c, s->n0, dd, dd + 3 * (size_t)nc, et);
     double se2 = 0, me2 = 0, sb2 = 0;

@@ -42,6 +42,10 @@ void or_deposit_dcu(const or_geo* g, const float* x, const float* y, const float
                     const float* uz, const float* w, int64_t n, double qm, const float* gb, float S,
                     int64_t* acc);
 void or_finalize(const int64_t* acc, int nf, int32_t ncell, const float* S, float* out);
+void or_deposit_f64(const or_geo* g, const float* x, const float* y, const float* ux, const float* uy,
+                    const float* uz, const float* w, int64_t n, double qm, int set, double* acc);
+void or_deposit_dcu_f64(const or_geo* g, const float* x, const float* y, const float* ux, const float* uy,
+                        const float* uz, const float* w, int64_t n, double qm, const float* gb, double* acc);
 
 float or_scale_for_bound(float b);
 void  or_src_scales(float coef_max, const float umax[3], float cref, float S[8]);
@@ -101,6 +105,7 @@ typedef struct or_state {
     float *ex, *ey, *ez, *bx, *by, *bz, *elx, *ely, *etx, *ety, *etz;
     double ke, ee, charge, px, py, pz, eb, max_e;
     int nthreads;
+    int exact;           /* 1: FP64 deposits of the current state (the FP64 oracle) */
 } or_state;
 
 void or_init(or_state* s, int darwin);
