@@ -127,7 +127,7 @@ const char* const kPhaseNamesES[kPhasesES] = {
 const char* const kPhaseNamesDarwin[kPhasesDarwin] = {
     "finalize_src", "fft_r2c_src8", "kspace_elb", "fft_c2r_elb5", "fields_dcu", "deposit_dcu",
     "finalize_dcu", "fft_r2c_dcu3", "kspace_et", "fft_c2r_et3", "fields_push", "push_deposit_em",
-    "diag_reduce"};
+    "rms_reduce", "diag_reduce"};
 
 struct NoMark { void operator()(int) const {} };
 
@@ -621,8 +621,10 @@ int aw_init(aw_ctx* ctx) {
             aw::launch_deposit_src(c, 1);    // pending rho(x^0) for step 0
         } else {
             aw::launch_deposit_src(c, 8);
+            aw::launch_rms_reduce(c, true, false);     // source rms for the capped scales
             aw::darwin_fields_from_pending(c, true);   // t = 0 fields
             aw::launch_copy_umax(c);
+            aw::launch_promote_scales(c);              // the rms-capped scales of step 0
             aw::launch_deposit_src(c, 8);              // pending rho,J,amu for step 0
             aw::launch_rms_reduce(c, true, true);
         }

@@ -17,19 +17,27 @@
 // Structure of every kernel (one CTA = one chunk of kChunk consecutive
 // particles; no kernel sorts particles, so the ES path keeps the reference's
 // particle order):
-//   pass 1  coalesced 128-bit loads (4 consecutive particles per thread per
-//           iteration), per-particle work (gather / push / wrap), coalesced
-//           128-bit stores of the new state, and a copy of what the deposit
-//           needs into a shared-memory stage; bounding box of the cells.
-//   window  block-wide bounding box -> int32 shared window [NF][W*H].
-//   pass 2  each lane deposits 8 consecutive particles from the stage,
-//           summing same-cell runs exactly in integer registers; the lanes of a
-//           warp sit 64 particles apart (different cells), so each run's flush
-//           is a set of conflict-free int32 shared atomics.
-//   flush   window -> global int64 accumulators (red.global.add.u64).
+//   load    one thread issues a bulk copy (cp.async.bulk, the TMA engine) per
+//           SoA array of the chunk into shared memory; the chunk's bytes are all
+//           in flight at once and every thread waits on one mbarrier.
+//   pass 1  one particle per thread per iteration, read from shared memory:
+//           gather / push / wrap, coalesced stores of the new state, the
+//           deposit coefficients and their fast-range test, the cell bounding
+//           box; then, per warp and in place, the values the deposit needs are
+//           rewritten into the swizzled stage layout. A particle whose scaled
+//           coefficient leaves the fast range goes on the chunk's slow list.
+//   window  block-wide bounding box -> shared window of NF exact sums per cell,
+//           each kept as two int32 words (native 32-bit shared atomics).
+//   pass 2  each lane deposits 8 consecutive particles from the stage, summing
+//           same-cell runs exactly in integer registers; lanes of a warp sit 64
+//           particles apart (different cells), so each run's flush is a set of
+//           conflict-free shared atomics.
+//   flush   window -> global int64 accumulators (red.global.add.u64), then the
+//           slow list straight into the global accumulators (exact products).
 #include "aw_internal.h"
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 
 namespace aw {
@@ -43,18 +51,30 @@ template <> struct SetNF<SET_RHOJ> { static constexpr int NF = 4, NS = 6; };   /
 template <> struct SetNF<SET_AMU>  { static constexpr int NF = 4, NS = 6; };
 template <> struct SetNF<SET_ALL>  { static constexpr int NF = 8, NS = 6; };
 
-// Window capacity in cells for NF int64 planes (<= 56 KB per CTA, so the
-// NF = 8 push kernel keeps two CTAs per SM with its 48 KB stage).
-constexpr int wmax_cells(int nf) { return nf == 1 ? 4096 : (nf == 3 ? 2048 : (nf == 4 ? 1536 : 896)); }
-constexpr size_t smem_bytes(int nf, int ns) {
-    return static_cast<size_t>(ns) * kChunk * 4 + static_cast<size_t>(wmax_cells(nf)) * nf * 8
-           + kThreads / 32 * 4 * sizeof(int);
+// Window capacity in cells for NF split (2 x int32) planes. The NF = 8 push kernel keeps
+// two CTAs per SM with its 48 KB stage; the ES push kernel keeps three.
+constexpr int wmax_cells(int nf) { return nf == 1 ? 2048 : (nf == 3 ? 2048 : (nf == 4 ? 1536 : 896)); }
+constexpr int kRedInts = kThreads / 32 * 4;
+// stage [np][kChunk] f32 | window [2*nf][wmax] i32 | red ints | slow list u16[kChunk]
+constexpr size_t win_offset(int np) { return static_cast<size_t>(np) * kChunk * 4; }
+constexpr size_t smem_bytes(int nf, int np) {
+    return win_offset(np) + static_cast<size_t>(wmax_cells(nf)) * nf * 8 + kRedInts * sizeof(int)
+           + kChunk * sizeof(unsigned short);
 }
 
-__device__ __forceinline__ void ref_cell(const Parts& p, long long c0, const Geo& g, int& ir, int& jr) {
-    const float x = __ldg(p.x + c0), y = __ldg(p.y + c0);
-    ir = (x >= 0.0f && x < g.nxf) ? static_cast<int>(x) : 0;
-    jr = (y >= 0.0f && y < g.nyf) ? static_cast<int>(y) : 0;
+struct Smem {
+    float* stage;
+    int* win;          // split window: 2 * NF int32 planes
+    int* red;
+    unsigned short* slow;
+};
+__device__ __forceinline__ Smem carve(unsigned char* smem, int np, int nf, int wmaxc) {
+    Smem m;
+    m.stage = reinterpret_cast<float*>(smem);
+    m.win = reinterpret_cast<int*>(smem + win_offset(np));
+    m.red = m.win + static_cast<size_t>(wmaxc) * nf * 2;
+    m.slow = reinterpret_cast<unsigned short*>(m.red + kRedInts);
+    return m;
 }
 
 // Owning cell (i, j) of a wrapped position — include/pic/particles.hpp:310-313.
@@ -67,6 +87,11 @@ __device__ __forceinline__ void cell_ij(float x, float y, const Geo& g, int& ci,
 
 __device__ __forceinline__ bool in_grid(float x, float y, const Geo& g) {
     return x >= 0.0f && x < g.nxf && y >= 0.0f && y < g.nyf;
+}
+
+__device__ __forceinline__ void ref_of(float x0, float y0, const Geo& g, int& ir, int& jr) {
+    ir = (x0 >= 0.0f && x0 < g.nxf) ? static_cast<int>(x0) : 0;
+    jr = (y0 >= 0.0f && y0 < g.nyf) ? static_cast<int>(y0) : 0;
 }
 
 // Per-particle source coefficients (unscaled), in the deposit's field order.
@@ -94,6 +119,19 @@ __device__ __forceinline__ void src_coefs(float coef, float ux, float uy, float 
         cf[6] = __fmul_rn(__fmul_rn(coef, uz), ux);
         cf[7] = __fmul_rn(__fmul_rn(coef, uz), uy);
     }
+}
+
+// Scaled coefficients cs = fl(cf * S) and whether every one is inside the fast
+// range (|cs| < 2^22; the CIC weights are <= 1, so every product is too).
+template <int NF>
+__device__ __forceinline__ bool scale_fast(const float (&cf)[NF], const float (&S)[NF], float (&cs)[NF]) {
+    bool fast = true;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        cs[f] = __fmul_rn(cf[f], S[f]);
+        fast = fast && (fabsf(cs[f]) < kFastLim);
+    }
+    return fast;
 }
 
 // Block-wide fixed-order sum of 4 doubles into part[blockIdx.x*5 + 0..3].
@@ -145,34 +183,6 @@ __device__ void block_sumsq(float (&sq)[NF], float cnt, float* __restrict__ part
     }
 }
 
-// 4 consecutive floats at a[i..i+3] (vectorised when aligned and in range).
-__device__ __forceinline__ float4 ld4(const float* __restrict__ a, long long i, long long n, bool vec) {
-    if (vec && i + 4 <= n) return __ldg(reinterpret_cast<const float4*>(a + i));
-    float4 v;
-    v.x = (i + 0 < n) ? a[i + 0] : 0.0f;
-    v.y = (i + 1 < n) ? a[i + 1] : 0.0f;
-    v.z = (i + 2 < n) ? a[i + 2] : 0.0f;
-    v.w = (i + 3 < n) ? a[i + 3] : 0.0f;
-    return v;
-}
-__device__ __forceinline__ void st4(float* __restrict__ a, long long i, long long n, bool vec, float4 v) {
-    if (vec && i + 4 <= n) { *reinterpret_cast<float4*>(a + i) = v; return; }
-    if (i + 0 < n) a[i + 0] = v.x;
-    if (i + 1 < n) a[i + 1] = v.y;
-    if (i + 2 < n) a[i + 2] = v.z;
-    if (i + 3 < n) a[i + 3] = v.w;
-}
-__device__ __forceinline__ void st4i(int* __restrict__ a, long long i, long long n, bool vec, int4 v) {
-    if (vec && i + 4 <= n) { *reinterpret_cast<int4*>(a + i) = v; return; }
-    if (i + 0 < n) a[i + 0] = v.x;
-    if (i + 1 < n) a[i + 1] = v.y;
-    if (i + 2 < n) a[i + 2] = v.z;
-    if (i + 3 < n) a[i + 3] = v.w;
-}
-__device__ __forceinline__ float& comp(float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
-__device__ __forceinline__ float compc(const float4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
-__device__ __forceinline__ int& compi(int4& v, int e) { return e == 0 ? v.x : e == 1 ? v.y : e == 2 ? v.z : v.w; }
-
 // Running bounding box of wrapped cell offsets.
 struct BBox {
     int lo_i = 1 << 30, lo_j = 1 << 30, hi_i = -(1 << 30), hi_j = -(1 << 30);
@@ -183,46 +193,33 @@ struct BBox {
     }
 };
 
-// Stage plane f, quad q (4 consecutive particles), stored swizzled.
-__device__ __forceinline__ float4& stq(float* st, int f, int q) {
-    return reinterpret_cast<float4*>(st + f * kChunk)[stage_quad(q)];
+// Append chunk slot s to the slow list.
+__device__ __forceinline__ void list_slow(unsigned short* list, int* nlist, int s) {
+    list[atomicAdd(nlist, 1)] = static_cast<unsigned short>(s);
 }
 
-// Pass 2: lane l of warp w deposits quads 16l + 2w + {0,1}, i.e. the 8
-// consecutive particles 64l + 8w .. 64l + 8w + 7, accumulating same-cell runs
-// in registers; lanes sit 64 particles apart, so their flushes rarely collide.
-// coef(v, e, cs) fills the scaled coefficients of element e of the quad planes v.
+// Window set-up (syncs), zero, sync.
+template <int NF>
+__device__ __forceinline__ Win open_window(const BBox& bb, int ir, int jr, int wmaxc, const Smem& m) {
+    Win wn;
+    win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, m.red);
+    win_zero<NF>(m.win, wn);
+    __syncthreads();
+    return wn;
+}
+
+// Block tail shared by every kernel: window flush, slow list, counters.
 template <int NF, int NS, class CoefFn>
-__device__ __forceinline__ void pass2(float* stage, long long* win, const Win& wn,
-                                      unsigned long long* __restrict__ gacc, const Geo& g,
-                                      DevState* st, unsigned& nslow, CoefFn coef) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    Run<NF> run;
-    run.cw = -1;
-    run.cnt = 0;
-#pragma unroll 1
-    for (int jq = 0; jq < 2; ++jq) {
-        const int q = 16 * lane + 2 * warp + jq;
-        float4 v[NS];
-#pragma unroll
-        for (int f = 0; f < NS; ++f) v[f] = stq(stage, f, q);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const float x = compc(v[0], e), y = compc(v[1], e);
-            if (!(x >= 0.0f)) continue;
-            const Cic c = cic(x, y);
-            float cs[NF];
-            coef(v, e, cs);
-            float wv[4];
-            wv[0] = c.w0; wv[1] = c.w1; wv[2] = c.w2; wv[3] = c.w3;
-            run_deposit<NF>(run, win, wn, c.i0, c.j0, wv, cs, gacc, g, nslow, st);
-        }
+__device__ __forceinline__ void close_window(const Smem& m, const Win& wn, int nlist,
+                                             unsigned long long* __restrict__ acc, const Geo& g, DevState* st,
+                                             CoefFn coef) {
+    __syncthreads();
+    win_flush<NF>(m.win, wn, acc, g);
+    slow_pass<NF, NS>(m.stage, m.slow, nlist, !wn.use, acc, g, st, coef);
+    if (threadIdx.x == 0) {
+        atomicAdd(&st->chunks, 1ull);
+        if (!wn.use) atomicAdd(&st->overflow, 1ull);
     }
-    run.flush(win, wn);
-}
-
-__device__ __forceinline__ void weights(const Cic& s, float (&wv)[4]) {
-    wv[0] = s.w0; wv[1] = s.w1; wv[2] = s.w2; wv[3] = s.w3;
 }
 
 // ---------------------------------------------------------------------------
@@ -233,82 +230,69 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st, float* __restrict__ psq) {
     constexpr int NF = SetNF<SET>::NF, NS = SetNF<SET>::NS;
     extern __shared__ __align__(16) unsigned char smem[];
-    float* stage = reinterpret_cast<float*>(smem);
-    long long* win = reinterpret_cast<long long*>(smem + static_cast<size_t>(NS) * kChunk * 4);
-    int* red = reinterpret_cast<int*>(win + static_cast<size_t>(wmaxc) * NF);
+    const Smem m = carve(smem, NS, NF, wmaxc);
+    __shared__ unsigned long long bar;
+    __shared__ int nlist;
+    __shared__ float ssq[(NF + 1) * (kThreads / 32)];
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
-    const bool vec = p.vec_ok != 0;
+    const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
+    if (threadIdx.x == 0) nlist = 0;
+    const ChunkSrc src{{p.x, p.y, p.w, p.ux, p.uy, p.uz}};
+    float x0, y0;
+    if (!load_chunk(m.stage, src, NS, c0, cnt, p.vec_ok != 0, &bar, st, &x0, &y0)) return;
     int ir, jr;
-    ref_cell(p, c0, g, ir, jr);
-    BBox bb;
-    float sq[NF] = {};
-    float cnt = 0.f;
-    // pass 1: load into the stage (x, y, w[, ux, uy, uz]); an invalid slot has x = -1
-#pragma unroll 1
-    for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
-        const int s0 = it * 4 * kThreads + 4 * threadIdx.x;
-        const long long i = c0 + s0;
-        float4 x = ld4(p.x, i, p.n, vec), y = ld4(p.y, i, p.n, vec), w = ld4(p.w, i, p.n, vec);
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            float& xe = comp(x, e);
-            const float ye = compc(y, e);
-            if (i + e < p.n && in_grid(xe, ye, g)) {
-                bb.add(static_cast<int>(xe), static_cast<int>(ye), ir, jr, g);
-            } else {
-                if (i + e < p.n) set_err(st, AW_DEV_OUT_OF_GRID);
-                xe = -1.0f;
-            }
-        }
-        stq(stage, 0, s0 >> 2) = x; stq(stage, 1, s0 >> 2) = y; stq(stage, 2, s0 >> 2) = w;
-        if constexpr (NS == 6) {
-            const float4 ux = ld4(p.ux, i, p.n, vec), uy = ld4(p.uy, i, p.n, vec), uz = ld4(p.uz, i, p.n, vec);
-            stq(stage, 3, s0 >> 2) = ux;
-            stq(stage, 4, s0 >> 2) = uy;
-            stq(stage, 5, s0 >> 2) = uz;
-            if (psq) {
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    if (!(compc(x, e) >= 0.0f)) continue;
-                    float cf[NF];
-                    src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(compc(w, e))), compc(ux, e),
-                                   compc(uy, e), compc(uz, e), cf);
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
-                    cnt += 1.0f;
-                }
-            }
-        }
-    }
-    Win wn;
-    win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, red);   // syncs
-    win_zero<NF>(win, wn);
-    __syncthreads();
-
+    ref_of(x0, y0, g, ir, jr);
     float S[NF];
     const int foff = (SET == SET_AMU) ? 4 : 0;
 #pragma unroll
     for (int f = 0; f < NF; ++f) S[f] = Sdev[foff + f];
-    unsigned nslow = 0;
-    pass2<NF, NS>(stage, win, wn, acc, g, st, nslow, [&](const float4 (&v)[NS], int e, float (&cs)[NF]) {
-        const float coef = __double2float_rn(qoa * static_cast<double>(compc(v[2], e)));
-        if constexpr (NS == 6) src_coefs<SET>(coef, compc(v[3], e), compc(v[4], e), compc(v[5], e), cs);
-        else src_coefs<SET>(coef, 0.f, 0.f, 0.f, cs);
+
+    BBox bb;
+    float sq[NF] = {};
+    float nval = 0.f;
+#pragma unroll 1
+    for (int it = 0; it < kPPT; ++it) {
+        const int s = it * kThreads + threadIdx.x;
+        float a[NS];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cs[f], S[f]);
-    });
-    __syncthreads();
-    win_flush<NF>(win, wn, acc, g);
-    if (psq) {
-        __shared__ float ssq[(NF + 1) * (kThreads / 32)];
-        block_sumsq<NF>(sq, cnt, psq, ssq);
+        for (int f = 0; f < NS; ++f) a[f] = m.stage[f * kChunk + s];
+        float xs = -1.0f;
+        if (s < cnt) {
+            if (in_grid(a[0], a[1], g)) {
+                bb.add(static_cast<int>(a[0]), static_cast<int>(a[1]), ir, jr, g);
+                float cf[NF], cs[NF];
+                if constexpr (NS == 6) src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), a[3], a[4], a[5], cf);
+                else src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), 0.f, 0.f, 0.f, cf);
+                const bool fast = scale_fast<NF>(cf, S, cs);
+                if (psq) {
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
+                    nval += 1.0f;
+                }
+                xs = __fadd_rn(a[0], 0.0f);
+                if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
+            } else {
+                set_err(st, AW_DEV_OUT_OF_GRID);
+            }
+        }
+        __syncwarp();
+        const int d = stage_slot(s);
+        m.stage[d] = xs;
+#pragma unroll
+        for (int f = 1; f < NS; ++f) m.stage[f * kChunk + d] = a[f];
     }
-    if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
-    if (threadIdx.x == 0) {
-        atomicAdd(&st->chunks, 1ull);
-        if (!wn.use) atomicAdd(&st->overflow, 1ull);
-    }
+    const Win wn = open_window<NF>(bb, ir, jr, wmaxc, m);
+    auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
+        float cf[NF];
+        if constexpr (NS == 6) src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), a[3], a[4], a[5], cf);
+        else src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), 0.f, 0.f, 0.f, cf);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cf[f], S[f]);
+    };
+    window_pass<NF, NS>(m.stage, m.win, wn, g, coef);
+    close_window<NF, NS>(m, wn, nlist, acc, g, st, coef);
+    if (psq) block_sumsq<NF>(sq, nval, psq, ssq);
 }
 
 // ---------------------------------------------------------------------------
@@ -349,84 +333,74 @@ __device__ __forceinline__ void dcu_scales(const DevState* st, float abs_qm, boo
     }
 }
 
-// dcu deposit: stage = x, y, ax, ay, az (the three scaled coefficients).
+// dcu deposit: input x y w ux uy uz; stage = x, y, ax, ay, az (scaled coefficients).
 __global__ void __launch_bounds__(kThreads, 2)
 k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restrict__ gb,
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st, int use_rms,
               float* __restrict__ psq) {
-    constexpr int NF = 3, NS = 5;
+    constexpr int NF = 3, NS = 5, NIN = 6;
     extern __shared__ __align__(16) unsigned char smem[];
-    float* stage = reinterpret_cast<float*>(smem);
-    long long* win = reinterpret_cast<long long*>(smem + static_cast<size_t>(NS) * kChunk * 4);
-    int* red = reinterpret_cast<int*>(win + static_cast<size_t>(wmaxc) * NF);
+    const Smem m = carve(smem, NIN, NF, wmaxc);
+    __shared__ unsigned long long bar;
+    __shared__ int nlist;
+    __shared__ float ssq[(NF + 1) * (kThreads / 32)];
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
-    const bool vec = p.vec_ok != 0;
+    const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
     float S[3];
     dcu_scales(st, abs_qm, use_rms != 0, S);
     if (blockIdx.x == 0 && threadIdx.x == 0) { st->S_dcu[0] = S[0]; st->S_dcu[1] = S[1]; st->S_dcu[2] = S[2]; }
+    if (threadIdx.x == 0) nlist = 0;
+    const ChunkSrc src{{p.x, p.y, p.w, p.ux, p.uy, p.uz}};
+    float x0, y0;
+    if (!load_chunk(m.stage, src, NIN, c0, cnt, p.vec_ok != 0, &bar, st, &x0, &y0)) return;
     int ir, jr;
-    ref_cell(p, c0, g, ir, jr);
+    ref_of(x0, y0, g, ir, jr);
+
     BBox bb;
     float sq[NF] = {};
-    float cnt = 0.f;
-#pragma unroll 1
-    for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
-        const int s0 = it * 4 * kThreads + 4 * threadIdx.x;
-        const long long i = c0 + s0;
-        float4 x = ld4(p.x, i, p.n, vec);
-        const float4 y = ld4(p.y, i, p.n, vec), w = ld4(p.w, i, p.n, vec);
-        const float4 ux = ld4(p.ux, i, p.n, vec), uy = ld4(p.uy, i, p.n, vec), uz = ld4(p.uz, i, p.n, vec);
-        float4 ax = make_float4(0.f, 0.f, 0.f, 0.f), ay = ax, az = ax;
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            float& xe = comp(x, e);
-            const float ye = compc(y, e);
-            if (i + e < p.n && in_grid(xe, ye, g)) {
-                const Cic s = cic(xe, ye);
-                bb.add(s.i0, s.j0, ir, jr, g);
+    float nval = 0.f;
+#pragma unroll 2
+    for (int it = 0; it < kPPT; ++it) {
+        const int s = it * kThreads + threadIdx.x;
+        const float x = m.stage[s], y = m.stage[kChunk + s], w = m.stage[2 * kChunk + s];
+        const float vx = m.stage[3 * kChunk + s], vy = m.stage[4 * kChunk + s], vz = m.stage[5 * kChunk + s];
+        float xs = -1.0f, cs[NF] = {0.f, 0.f, 0.f};
+        if (s < cnt) {
+            if (in_grid(x, y, g)) {
+                const Cic c = cic(x, y);
+                bb.add(c.i0, c.j0, ir, jr, g);
                 float ex, ey, ez, bx, by, bz;
-                gather_em(gb, s, g, ex, ey, ez, bx, by, bz);
-                const float vx = compc(ux, e), vy = compc(uy, e), vz = compc(uz, e);
-                const float coef = __double2float_rn(qm2oa * static_cast<double>(compc(w, e)));
+                gather_em(gb, c, g, ex, ey, ez, bx, by, bz);
+                const float coef = __double2float_rn(qm2oa * static_cast<double>(w));
                 const float cx = __fmaf_rn(vy, bz, -__fmul_rn(vz, by));
                 const float cy = __fmaf_rn(vz, bx, -__fmul_rn(vx, bz));
                 const float cz = __fmaf_rn(vx, by, -__fmul_rn(vy, bx));
-                const float a0 = __fmul_rn(coef, __fadd_rn(ex, cx));
-                const float a1 = __fmul_rn(coef, __fadd_rn(ey, cy));
-                const float a2 = __fmul_rn(coef, __fadd_rn(ez, cz));
-                comp(ax, e) = __fmul_rn(a0, S[0]);
-                comp(ay, e) = __fmul_rn(a1, S[1]);
-                comp(az, e) = __fmul_rn(a2, S[2]);
-                sq[0] = __fmaf_rn(a0, a0, sq[0]); sq[1] = __fmaf_rn(a1, a1, sq[1]); sq[2] = __fmaf_rn(a2, a2, sq[2]);
-                cnt += 1.0f;
+                const float cf[NF] = {__fmul_rn(coef, __fadd_rn(ex, cx)), __fmul_rn(coef, __fadd_rn(ey, cy)),
+                                      __fmul_rn(coef, __fadd_rn(ez, cz))};
+                const bool fast = scale_fast<NF>(cf, S, cs);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
+                nval += 1.0f;
+                xs = __fadd_rn(x, 0.0f);
+                if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
             } else {
-                if (i + e < p.n) set_err(st, AW_DEV_OUT_OF_GRID);
-                xe = -1.0f;
+                set_err(st, AW_DEV_OUT_OF_GRID);
             }
         }
-        stq(stage, 0, s0 >> 2) = x; stq(stage, 1, s0 >> 2) = y;
-        stq(stage, 2, s0 >> 2) = ax; stq(stage, 3, s0 >> 2) = ay; stq(stage, 4, s0 >> 2) = az;
+        __syncwarp();
+        const int d = stage_slot(s);
+        m.stage[d] = xs;
+        m.stage[kChunk + d] = y;
+        m.stage[2 * kChunk + d] = cs[0];
+        m.stage[3 * kChunk + d] = cs[1];
+        m.stage[4 * kChunk + d] = cs[2];
     }
-    Win wn;
-    win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, red);
-    win_zero<NF>(win, wn);
-    __syncthreads();
-    unsigned nslow = 0;
-    pass2<NF, NS>(stage, win, wn, acc, g, st, nslow, [&](const float4 (&v)[NS], int e, float (&cs)[NF]) {
-        cs[0] = compc(v[2], e); cs[1] = compc(v[3], e); cs[2] = compc(v[4], e);
-    });
-    __syncthreads();
-    win_flush<NF>(win, wn, acc, g);
-    if (psq) {
-        __shared__ float ssq[(NF + 1) * (kThreads / 32)];
-        block_sumsq<NF>(sq, cnt, psq, ssq);
-    }
-    if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
-    if (threadIdx.x == 0) {
-        atomicAdd(&st->chunks, 1ull);
-        if (!wn.use) atomicAdd(&st->overflow, 1ull);
-    }
+    const Win wn = open_window<NF>(bb, ir, jr, wmaxc, m);
+    auto coef = [&](const float (&a)[NS], float (&cs)[NF]) { cs[0] = a[2]; cs[1] = a[3]; cs[2] = a[4]; };
+    window_pass<NF, NS>(m.stage, m.win, wn, g, coef);
+    close_window<NF, NS>(m, wn, nlist, acc, g, st, coef);
+    if (psq) block_sumsq<NF>(sq, nval, psq, ssq);
 }
 
 // ---------------------------------------------------------------------------
@@ -435,169 +409,186 @@ struct PushP {
     int    has_b0;
     float  b0x, b0y, b0z;
     double dt;
+    double dtx, dty;      // dt/dx, dt/dy (exact when dx, dy are powers of two)
     int    write_cell;
 };
 
-// Fused ES step kernel: stage = new x, y, w.
+template <bool POW2>
+__device__ __forceinline__ void move_xy(float& x, float& y, float ux, float uy, const PushP& pp, const Geo& g) {
+    if constexpr (POW2) {
+        x = wrap_pos(move1_pow2(x, ux, pp.dtx), g.nxf);
+        y = wrap_pos(move1_pow2(y, uy, pp.dty), g.nyf);
+    } else {
+        x = wrap_pos(move1(x, ux, pp.dt, g.dx), g.nxf);
+        y = wrap_pos(move1(y, uy, pp.dt, g.dy), g.nyf);
+    }
+}
+
+// Fused ES step kernel: input x y w ux uy uz; stage = new x, y, w.
+template <bool POW2>
 __global__ void __launch_bounds__(kThreads, 3)
 k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                   double qoa, unsigned long long* __restrict__ acc, int wmaxc,
                   double* __restrict__ part, DevState* st) {
-    constexpr int NF = 1, NS = 3;
+    constexpr int NF = 1, NS = 3, NIN = 6;
     extern __shared__ __align__(16) unsigned char smem[];
-    float* stage = reinterpret_cast<float*>(smem);
-    long long* win = reinterpret_cast<long long*>(smem + static_cast<size_t>(NS) * kChunk * 4);
-    int* red = reinterpret_cast<int*>(win + static_cast<size_t>(wmaxc) * NF);
+    const Smem m = carve(smem, NIN, NF, wmaxc);
+    __shared__ unsigned long long bar;
+    __shared__ int nlist;
     __shared__ double dsh[4 * (kThreads / 32)];
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
-    const bool vec = p.vec_ok != 0;
-    const float S = st->S_next[0];
+    const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
+    const float S1[1] = {st->S_next[0]};
+    if (threadIdx.x == 0) nlist = 0;
+    const ChunkSrc src{{p.x, p.y, p.w, p.ux, p.uy, p.uz}};
+    float x0, y0;
+    if (!load_chunk(m.stage, src, NIN, c0, cnt, p.vec_ok != 0, &bar, st, &x0, &y0)) return;
     int ir, jr;
-    ref_cell(p, c0, g, ir, jr);
+    ref_of(x0, y0, g, ir, jr);
+    const float2* q = reinterpret_cast<const float2*>(gb);
+
     BBox bb;
     double ke = 0, px = 0, py = 0, pz = 0;
-    const float2* q = reinterpret_cast<const float2*>(gb);
-#pragma unroll 1
-    for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
-        const int s0 = it * 4 * kThreads + 4 * threadIdx.x;
-        const long long i = c0 + s0;
-        float4 x = ld4(p.x, i, p.n, vec), y = ld4(p.y, i, p.n, vec);
-        float4 ux = ld4(p.ux, i, p.n, vec), uy = ld4(p.uy, i, p.n, vec), uz = ld4(p.uz, i, p.n, vec);
-        const float4 w = ld4(p.w, i, p.n, vec);
-        int4 cell = make_int4(0, 0, 0, 0);
-        float4 xs = x;
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            comp(xs, e) = -1.0f;
-            if (i + e >= p.n) continue;
-            float& xe = comp(x, e);
-            float& ye = comp(y, e);
-            if (!in_grid(xe, ye, g)) { set_err(st, AW_DEV_OUT_OF_GRID); continue; }
-            const Cic s = cic(xe, ye);
-            const int i1 = wrap_once(s.i0 + 1, g.nx);
-            const int r0 = s.j0 * g.nx, r1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
-            const float2 e0 = __ldg(q + r0 + s.i0), e1 = __ldg(q + r0 + i1);
-            const float2 e2 = __ldg(q + r1 + s.i0), e3 = __ldg(q + r1 + i1);
-            const float ex = gather4(s, e0.x, e1.x, e2.x, e3.x);
-            const float ey = gather4(s, e0.y, e1.y, e2.y, e3.y);
-            float& u = comp(ux, e); float& v = comp(uy, e); float& wz = comp(uz, e);
-            boris_es(u, v, wz, ex, ey, pp.qmh, pp.has_b0 != 0, pp.b0x, pp.b0y, pp.b0z);
-            xe = wrap_pos(move1(xe, u, pp.dt, g.dx), g.nxf);
-            ye = wrap_pos(move1(ye, v, pp.dt, g.dy), g.nyf);
-            int ci, cj;
-            cell_ij(xe, ye, g, ci, cj);
-            compi(cell, e) = cj * g.nx + ci;
-            if (in_grid(xe, ye, g)) {
-                bb.add(ci, cj, ir, jr, g);
-                comp(xs, e) = xe;
+#pragma unroll 2
+    for (int it = 0; it < kPPT; ++it) {
+        const int s = it * kThreads + threadIdx.x;
+        const long long i = c0 + s;
+        float x = m.stage[s], y = m.stage[kChunk + s];
+        const float w = m.stage[2 * kChunk + s];
+        float ux = m.stage[3 * kChunk + s], uy = m.stage[4 * kChunk + s], uz = m.stage[5 * kChunk + s];
+        float xs = -1.0f;
+        if (s < cnt) {
+            if (in_grid(x, y, g)) {
+                const Cic c = cic(x, y);
+                const int i1 = wrap_once(c.i0 + 1, g.nx);
+                const int r0 = c.j0 * g.nx, r1 = wrap_once(c.j0 + 1, g.ny) * g.nx;
+                const float2 e0 = __ldg(q + r0 + c.i0), e1 = __ldg(q + r0 + i1);
+                const float2 e2 = __ldg(q + r1 + c.i0), e3 = __ldg(q + r1 + i1);
+                const float ex = gather4(c, e0.x, e1.x, e2.x, e3.x);
+                const float ey = gather4(c, e0.y, e1.y, e2.y, e3.y);
+                boris_es(ux, uy, uz, ex, ey, pp.qmh, pp.has_b0 != 0, pp.b0x, pp.b0y, pp.b0z);
+                move_xy<POW2>(x, y, ux, uy, pp, g);
+                int ci, cj;
+                cell_ij(x, y, g, ci, cj);
+                p.x[i] = x; p.y[i] = y; p.ux[i] = ux; p.uy[i] = uy; p.uz[i] = uz;
+                if (pp.write_cell && p.cell) p.cell[i] = cj * g.nx + ci;
+                if (in_grid(x, y, g)) {
+                    bb.add(ci, cj, ir, jr, g);
+                    const float cf[1] = {__double2float_rn(qoa * static_cast<double>(w))};
+                    float cs[1];
+                    const bool fast = scale_fast<1>(cf, S1, cs);
+                    xs = __fadd_rn(x, 0.0f);
+                    if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
+                } else {
+                    set_err(st, AW_DEV_OUT_OF_GRID);
+                }
+                const double dw = w, du = ux, dv = uy, dz = uz;
+                ke += dw * (du * du + dv * dv + dz * dz);
+                px += dw * du; py += dw * dv; pz += dw * dz;
+            } else {
+                set_err(st, AW_DEV_OUT_OF_GRID);
             }
-            const double dw = compc(w, e), du = u, dv = v, dz = wz;
-            ke += dw * (du * du + dv * dv + dz * dz);
-            px += dw * du; py += dw * dv; pz += dw * dz;
         }
-        st4(p.x, i, p.n, vec, x);
-        st4(p.y, i, p.n, vec, y);
-        st4(p.ux, i, p.n, vec, ux);
-        st4(p.uy, i, p.n, vec, uy);
-        st4(p.uz, i, p.n, vec, uz);
-        if (pp.write_cell && p.cell) st4i(p.cell, i, p.n, vec, cell);
-        stq(stage, 0, s0 >> 2) = xs; stq(stage, 1, s0 >> 2) = y; stq(stage, 2, s0 >> 2) = w;
+        __syncwarp();
+        const int d = stage_slot(s);
+        m.stage[d] = xs;
+        m.stage[kChunk + d] = y;
+        m.stage[2 * kChunk + d] = w;
     }
-    Win wn;
-    win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, red);
-    win_zero<NF>(win, wn);
-    __syncthreads();
-    unsigned nslow = 0;
-    pass2<NF, NS>(stage, win, wn, acc, g, st, nslow, [&](const float4 (&v)[NS], int e, float (&cs)[NF]) {
-        cs[0] = __fmul_rn(__double2float_rn(qoa * static_cast<double>(compc(v[2], e))), S);
-    });
-    __syncthreads();
-    win_flush<NF>(win, wn, acc, g);
+    const Win wn = open_window<NF>(bb, ir, jr, wmaxc, m);
+    auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
+        cs[0] = __fmul_rn(__double2float_rn(qoa * static_cast<double>(a[2])), S1[0]);
+    };
+    window_pass<NF, NS>(m.stage, m.win, wn, g, coef);
+    close_window<NF, NS>(m, wn, nlist, acc, g, st, coef);
     block_sum4(ke, px, py, pz, part, dsh);
-    if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
-    if (threadIdx.x == 0) {
-        atomicAdd(&st->chunks, 1ull);
-        if (!wn.use) atomicAdd(&st->overflow, 1ull);
-        if (blockIdx.x == 0) {
-            st->S_pend[0] = S;
-            st->step += 1;
-        }
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        st->S_pend[0] = S1[0];
+        st->step += 1;
     }
 }
 
-// Fused Darwin step kernel: stage = new x, y, w, ux, uy, uz.
+// Fused Darwin step kernel: input x y w ux uy uz; stage = new x, y, w, ux, uy, uz.
+template <bool POW2>
 __global__ void __launch_bounds__(kThreads, 2)
 k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                   double qoa, unsigned long long* __restrict__ acc, int wmaxc,
                   double* __restrict__ part, DevState* st, float* __restrict__ psq) {
     constexpr int NF = 8, NS = 6;
     extern __shared__ __align__(16) unsigned char smem[];
-    float* stage = reinterpret_cast<float*>(smem);
-    long long* win = reinterpret_cast<long long*>(smem + static_cast<size_t>(NS) * kChunk * 4);
-    int* red = reinterpret_cast<int*>(win + static_cast<size_t>(wmaxc) * NF);
+    const Smem m = carve(smem, NS, NF, wmaxc);
+    __shared__ unsigned long long bar;
+    __shared__ int nlist;
     __shared__ double dsh[4 * (kThreads / 32)];
     __shared__ unsigned umx[3][kThreads / 32];
+    __shared__ float ssq[(NF + 1) * (kThreads / 32)];
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
-    const bool vec = p.vec_ok != 0;
+    const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
+    float S[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) S[f] = st->S_next[f];
+    if (threadIdx.x == 0) nlist = 0;
+    const ChunkSrc src{{p.x, p.y, p.w, p.ux, p.uy, p.uz}};
+    float x0, y0;
+    if (!load_chunk(m.stage, src, NS, c0, cnt, p.vec_ok != 0, &bar, st, &x0, &y0)) return;
     int ir, jr;
-    ref_cell(p, c0, g, ir, jr);
+    ref_of(x0, y0, g, ir, jr);
+
     BBox bb;
     double ke = 0, px = 0, py = 0, pz = 0;
     float m0 = 0.f, m1 = 0.f, m2 = 0.f;
     float sq[NF] = {};
-    float cnt = 0.f;
-#pragma unroll 1
-    for (int it = 0; it < kChunk / (4 * kThreads); ++it) {
-        const int s0 = it * 4 * kThreads + 4 * threadIdx.x;
-        const long long i = c0 + s0;
-        float4 x = ld4(p.x, i, p.n, vec), y = ld4(p.y, i, p.n, vec);
-        float4 ux = ld4(p.ux, i, p.n, vec), uy = ld4(p.uy, i, p.n, vec), uz = ld4(p.uz, i, p.n, vec);
-        const float4 w = ld4(p.w, i, p.n, vec);
-        int4 cell = make_int4(0, 0, 0, 0);
-        float4 xs = x;
+    float nval = 0.f;
+#pragma unroll 2
+    for (int it = 0; it < kPPT; ++it) {
+        const int s = it * kThreads + threadIdx.x;
+        const long long i = c0 + s;
+        float x = m.stage[s], y = m.stage[kChunk + s];
+        const float w = m.stage[2 * kChunk + s];
+        float ux = m.stage[3 * kChunk + s], uy = m.stage[4 * kChunk + s], uz = m.stage[5 * kChunk + s];
+        float xs = -1.0f;
+        if (s < cnt) {
+            if (in_grid(x, y, g)) {
+                const Cic c = cic(x, y);
+                float ex, ey, ez, bx, by, bz;
+                gather_em(gb, c, g, ex, ey, ez, bx, by, bz);
+                boris_em(ux, uy, uz, ex, ey, ez, bx, by, bz, pp.qmh);
+                move_xy<POW2>(x, y, ux, uy, pp, g);
+                int ci, cj;
+                cell_ij(x, y, g, ci, cj);
+                p.x[i] = x; p.y[i] = y; p.ux[i] = ux; p.uy[i] = uy; p.uz[i] = uz;
+                if (pp.write_cell && p.cell) p.cell[i] = cj * g.nx + ci;
+                m0 = fmaxf(m0, fabsf(ux)); m1 = fmaxf(m1, fabsf(uy)); m2 = fmaxf(m2, fabsf(uz));
+                if (in_grid(x, y, g)) {
+                    bb.add(ci, cj, ir, jr, g);
+                    float cf[NF], cs[NF];
+                    src_coefs<SET_ALL>(__double2float_rn(qoa * static_cast<double>(w)), ux, uy, uz, cf);
+                    const bool fast = scale_fast<NF>(cf, S, cs);
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            comp(xs, e) = -1.0f;
-            if (i + e >= p.n) continue;
-            float& xe = comp(x, e);
-            float& ye = comp(y, e);
-            if (!in_grid(xe, ye, g)) { set_err(st, AW_DEV_OUT_OF_GRID); continue; }
-            const Cic s = cic(xe, ye);
-            float ex, ey, ez, bx, by, bz;
-            gather_em(gb, s, g, ex, ey, ez, bx, by, bz);
-            float& u = comp(ux, e); float& v = comp(uy, e); float& wz = comp(uz, e);
-            boris_em(u, v, wz, ex, ey, ez, bx, by, bz, pp.qmh);
-            xe = wrap_pos(move1(xe, u, pp.dt, g.dx), g.nxf);
-            ye = wrap_pos(move1(ye, v, pp.dt, g.dy), g.nyf);
-            int ci, cj;
-            cell_ij(xe, ye, g, ci, cj);
-            compi(cell, e) = cj * g.nx + ci;
-            if (in_grid(xe, ye, g)) {
-                bb.add(ci, cj, ir, jr, g);
-                comp(xs, e) = xe;
+                    for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
+                    nval += 1.0f;
+                    xs = __fadd_rn(x, 0.0f);
+                    if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
+                } else {
+                    set_err(st, AW_DEV_OUT_OF_GRID);
+                }
+                const double dw = w, du = ux, dv = uy, dz = uz;
+                ke += dw * (du * du + dv * dv + dz * dz);
+                px += dw * du; py += dw * dv; pz += dw * dz;
+            } else {
+                set_err(st, AW_DEV_OUT_OF_GRID);
             }
-            m0 = fmaxf(m0, fabsf(u)); m1 = fmaxf(m1, fabsf(v)); m2 = fmaxf(m2, fabsf(wz));
-            {
-                float cf[NF];
-                src_coefs<SET_ALL>(__double2float_rn(qoa * static_cast<double>(compc(w, e))), u, v, wz, cf);
-#pragma unroll
-                for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
-                cnt += 1.0f;
-            }
-            const double dw = compc(w, e), du = u, dv = v, dz = wz;
-            ke += dw * (du * du + dv * dv + dz * dz);
-            px += dw * du; py += dw * dv; pz += dw * dz;
         }
-        st4(p.x, i, p.n, vec, x);
-        st4(p.y, i, p.n, vec, y);
-        st4(p.ux, i, p.n, vec, ux);
-        st4(p.uy, i, p.n, vec, uy);
-        st4(p.uz, i, p.n, vec, uz);
-        if (pp.write_cell && p.cell) st4i(p.cell, i, p.n, vec, cell);
-        stq(stage, 0, s0 >> 2) = xs; stq(stage, 1, s0 >> 2) = y; stq(stage, 2, s0 >> 2) = w;
-        stq(stage, 3, s0 >> 2) = ux; stq(stage, 4, s0 >> 2) = uy; stq(stage, 5, s0 >> 2) = uz;
+        __syncwarp();
+        const int d = stage_slot(s);
+        m.stage[d] = xs;
+        m.stage[kChunk + d] = y;
+        m.stage[2 * kChunk + d] = w;
+        m.stage[3 * kChunk + d] = ux;
+        m.stage[4 * kChunk + d] = uy;
+        m.stage[5 * kChunk + d] = uz;
     }
     // |u| maxima of the new state (next step's deposit scales): one atomic per block
     m0 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m0)));
@@ -608,49 +599,26 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
         umx[1][threadIdx.x >> 5] = __float_as_uint(m1);
         umx[2][threadIdx.x >> 5] = __float_as_uint(m2);
     }
-    Win wn;
-    win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, red);   // syncs
-    win_zero<NF>(win, wn);
+    const Win wn = open_window<NF>(bb, ir, jr, wmaxc, m);
     if (threadIdx.x < 3) {
-        unsigned m = 0;
-        for (int k = 0; k < kThreads / 32; ++k) m = max(m, umx[threadIdx.x][k]);
-        atomicMax(&st->umax_bits[threadIdx.x], m);
+        unsigned mx = 0;
+        for (int k = 0; k < kThreads / 32; ++k) mx = max(mx, umx[threadIdx.x][k]);
+        atomicMax(&st->umax_bits[threadIdx.x], mx);
     }
-    __syncthreads();
-    float S[NF];
+    auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
+        float cf[NF];
+        src_coefs<SET_ALL>(__double2float_rn(qoa * static_cast<double>(a[2])), a[3], a[4], a[5], cf);
 #pragma unroll
-    for (int f = 0; f < NF; ++f) S[f] = st->S_next[f];
-    unsigned nslow = 0;
-    // two 4-field sub-passes (rho, J then amu) keep the register runs small
-    pass2<4, NS>(stage, win, wn, acc, g, st, nslow, [&](const float4 (&v)[NS], int e, float (&cs)[4]) {
-        const float coef = __double2float_rn(qoa * static_cast<double>(compc(v[2], e)));
-        src_coefs<SET_RHOJ>(coef, compc(v[3], e), compc(v[4], e), compc(v[5], e), cs);
-#pragma unroll
-        for (int f = 0; f < 4; ++f) cs[f] = __fmul_rn(cs[f], S[f]);
-    });
-    pass2<4, NS>(stage, win + 4 * wn.WH, wn, acc + static_cast<size_t>(4) * g.ncell, g, st, nslow,
-                 [&](const float4 (&v)[NS], int e, float (&cs)[4]) {
-        const float coef = __double2float_rn(qoa * static_cast<double>(compc(v[2], e)));
-        src_coefs<SET_AMU>(coef, compc(v[3], e), compc(v[4], e), compc(v[5], e), cs);
-#pragma unroll
-        for (int f = 0; f < 4; ++f) cs[f] = __fmul_rn(cs[f], S[4 + f]);
-    });
-    __syncthreads();
-    win_flush<NF>(win, wn, acc, g);
-    {
-        __shared__ float ssq[(NF + 1) * (kThreads / 32)];
-        block_sumsq<NF>(sq, cnt, psq, ssq);
-    }
+        for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cf[f], S[f]);
+    };
+    window_pass<NF, NS>(m.stage, m.win, wn, g, coef);
+    close_window<NF, NS>(m, wn, nlist, acc, g, st, coef);
+    block_sumsq<NF>(sq, nval, psq, ssq);
     block_sum4(ke, px, py, pz, part, dsh);
-    if (nslow) atomicAdd(&st->slow, static_cast<unsigned long long>(nslow));
-    if (threadIdx.x == 0) {
-        atomicAdd(&st->chunks, 1ull);
-        if (!wn.use) atomicAdd(&st->overflow, 1ull);
-        if (blockIdx.x == 0) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
 #pragma unroll
-            for (int f = 0; f < NF; ++f) st->S_pend[f] = S[f];
-            st->step += 1;
-        }
+        for (int f = 0; f < NF; ++f) st->S_pend[f] = S[f];
+        st->step += 1;
     }
 }
 
@@ -662,8 +630,8 @@ inline int nchunks(long long n) { return static_cast<int>(std::max<long long>(1,
 template <class K>
 void prep_smem(K kern, size_t bytes) {
     static std::mutex mu;
-    static const void* keys[16];
-    static size_t vals[16];
+    static const void* keys[32];
+    static size_t vals[32];
     static int nkeys = 0;
     if (bytes <= 48 * 1024) return;
     std::lock_guard<std::mutex> lock(mu);
@@ -673,7 +641,7 @@ void prep_smem(K kern, size_t bytes) {
     AW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
     for (int i = 0; i < nkeys; ++i)
         if (keys[i] == key) { vals[i] = bytes; return; }
-    if (nkeys < 16) { keys[nkeys] = key; vals[nkeys] = bytes; ++nkeys; }
+    if (nkeys < 32) { keys[nkeys] = key; vals[nkeys] = bytes; ++nkeys; }
 }
 
 template <int SET>
@@ -686,6 +654,23 @@ void launch_src(Ctx& c, unsigned long long* acc) {
                                                                         wmax_cells(NF), c.st,
                                                                         SET == SET_ALL ? c.part_c : nullptr);
     AW_LAUNCH();
+}
+
+bool is_pow2(double d) {
+    int e;
+    return d > 0.0 && std::frexp(d, &e) == 0.5;
+}
+
+PushP push_params(const Ctx& c) {
+    PushP pp{};
+    pp.qmh = static_cast<float>(c.prm.qm) * 0.5f * static_cast<float>(c.prm.dt);
+    pp.has_b0 = c.prm.has_b0;
+    pp.b0x = c.prm.B0[0]; pp.b0y = c.prm.B0[1]; pp.b0z = c.prm.B0[2];
+    pp.dt = c.prm.dt;
+    pp.dtx = c.prm.dt / c.geo.dx;
+    pp.dty = c.prm.dt / c.geo.dy;
+    pp.write_cell = c.write_cell;
+    return pp;
 }
 
 }  // namespace
@@ -705,7 +690,7 @@ void launch_deposit_src(Ctx& c, int which) {
 void launch_deposit_dcu(Ctx& c, const float* gb, bool fused) {
     if (c.parts.n == 0) return;
     const double qm2oa = c.prm.qm * c.prm.qm / (c.geo.dx * c.geo.dy);
-    const size_t sh = smem_bytes(3, 5);
+    const size_t sh = smem_bytes(3, 6);
     prep_smem(k_deposit_dcu, sh);
     k_deposit_dcu<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(
         c.parts, c.geo, qm2oa, static_cast<float>(std::fabs(c.prm.qm)), gb, c.acc_dcu, wmax_cells(3), c.st,
@@ -715,31 +700,27 @@ void launch_deposit_dcu(Ctx& c, const float* gb, bool fused) {
 
 void launch_push_deposit_es(Ctx& c) {
     if (c.parts.n == 0) return;
-    PushP pp{};
-    pp.qmh = static_cast<float>(c.prm.qm) * 0.5f * static_cast<float>(c.prm.dt);
-    pp.has_b0 = c.prm.has_b0;
-    pp.b0x = c.prm.B0[0]; pp.b0y = c.prm.B0[1]; pp.b0z = c.prm.B0[2];
-    pp.dt = c.prm.dt;
-    pp.write_cell = c.write_cell;
+    const PushP pp = push_params(c);
     const double qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
-    const size_t sh = smem_bytes(1, 3);
-    prep_smem(k_push_deposit_es, sh);
-    k_push_deposit_es<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(
-        c.parts, c.geo, pp, c.gb_es, qoa, c.acc_src, wmax_cells(1), c.part_p, c.st);
+    const size_t sh = smem_bytes(1, 6);
+    const bool p2 = is_pow2(c.geo.dx) && is_pow2(c.geo.dy);
+    auto kern = p2 ? k_push_deposit_es<true> : k_push_deposit_es<false>;
+    prep_smem(kern, sh);
+    kern<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(c.parts, c.geo, pp, c.gb_es, qoa, c.acc_src,
+                                                         wmax_cells(1), c.part_p, c.st);
     AW_LAUNCH();
 }
 
 void launch_push_deposit_em(Ctx& c) {
     if (c.parts.n == 0) return;
-    PushP pp{};
-    pp.qmh = static_cast<float>(c.prm.qm) * 0.5f * static_cast<float>(c.prm.dt);
-    pp.dt = c.prm.dt;
-    pp.write_cell = c.write_cell;
+    const PushP pp = push_params(c);
     const double qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
     const size_t sh = smem_bytes(8, 6);
-    prep_smem(k_push_deposit_em, sh);
-    k_push_deposit_em<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(
-        c.parts, c.geo, pp, c.gb_push, qoa, c.acc_src, wmax_cells(8), c.part_p, c.st, c.part_c);
+    const bool p2 = is_pow2(c.geo.dx) && is_pow2(c.geo.dy);
+    auto kern = p2 ? k_push_deposit_em<true> : k_push_deposit_em<false>;
+    prep_smem(kern, sh);
+    kern<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(c.parts, c.geo, pp, c.gb_push, qoa, c.acc_src,
+                                                         wmax_cells(8), c.part_p, c.st, c.part_c);
     AW_LAUNCH();
 }
 

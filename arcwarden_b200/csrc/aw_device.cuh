@@ -35,7 +35,7 @@
 namespace aw {
 
 constexpr int kThreads = 256;          // CTA size of every particle kernel
-constexpr int kPPT     = 8;            // consecutive particles per thread
+constexpr int kPPT     = 8;            // particles per thread per chunk
 constexpr int kChunk   = kThreads * kPPT;   // particles per CTA chunk (2048)
 
 // Fast-path range of one quantised contribution: |v*S| < 2^22 rounds exactly
@@ -178,9 +178,19 @@ __device__ __forceinline__ void boris_em(float& ux, float& uy, float& uz,
 __device__ __forceinline__ float move1(float x, float u, double dt, double d) {
     return __fadd_rn(x, __double2float_rn(__ddiv_rn(__dmul_rn(static_cast<double>(u), dt), d)));
 }
-// Periodic wrap of a position — particles.hpp:301-306.
+// The same move when d is a power of two, with dtd = dt / d (exact): dividing
+// the rounded product by 2^k is exact, so RN(u*dt)/d == RN(u*dtd) bit for bit.
+__device__ __forceinline__ float move1_pow2(float x, float u, double dtd) {
+    return __fadd_rn(x, __double2float_rn(__dmul_rn(static_cast<double>(u), dtd)));
+}
+// Periodic wrap of a position — particles.hpp:301-306: x = fmodf(x, n);
+// x < 0 -> x + n; x >= n -> 0. The three common cases are answered exactly
+// without fmodf: fmodf(x, n) is x for |x| < n, and x - n (exact) for
+// n <= x < 2n.
 __device__ __forceinline__ float wrap_pos(float x, float n) {
-    x = fmodf(x, n);
+    if (x >= 0.0f && x < n) return x;
+    if (x >= n && x < __fmul_rn(2.0f, n)) return __fsub_rn(x, n);
+    if (!(x < 0.0f && x > -n)) x = fmodf(x, n);
     if (x < 0.0f) x = __fadd_rn(x, n);
     if (x >= n) x = 0.0f;
     return x;
@@ -209,41 +219,6 @@ struct Parts {
     long long n;
     int   vec_ok;     // all arrays 16-byte aligned
 };
-
-// Load / store kPPT consecutive floats starting at `base` (vectorised when the
-// whole run is in range and aligned; scalar and bounds-checked otherwise).
-__device__ __forceinline__ void load8(const float* __restrict__ a, long long base, long long n,
-                                      bool vec, float (&v)[kPPT]) {
-    if (vec && base + kPPT <= n) {
-        const float4 p = __ldg(reinterpret_cast<const float4*>(a + base));
-        const float4 q = __ldg(reinterpret_cast<const float4*>(a + base + 4));
-        v[0] = p.x; v[1] = p.y; v[2] = p.z; v[3] = p.w;
-        v[4] = q.x; v[5] = q.y; v[6] = q.z; v[7] = q.w;
-    } else {
-#pragma unroll
-        for (int k = 0; k < kPPT; ++k) v[k] = (base + k < n) ? a[base + k] : 0.0f;
-    }
-}
-__device__ __forceinline__ void store8(float* __restrict__ a, long long base, long long n,
-                                       bool vec, const float (&v)[kPPT]) {
-    if (vec && base + kPPT <= n) {
-        reinterpret_cast<float4*>(a + base)[0] = make_float4(v[0], v[1], v[2], v[3]);
-        reinterpret_cast<float4*>(a + base)[1] = make_float4(v[4], v[5], v[6], v[7]);
-    } else {
-#pragma unroll
-        for (int k = 0; k < kPPT; ++k) if (base + k < n) a[base + k] = v[k];
-    }
-}
-__device__ __forceinline__ void store8i(int* __restrict__ a, long long base, long long n,
-                                        bool vec, const int (&v)[kPPT]) {
-    if (vec && base + kPPT <= n) {
-        reinterpret_cast<int4*>(a + base)[0] = make_int4(v[0], v[1], v[2], v[3]);
-        reinterpret_cast<int4*>(a + base)[1] = make_int4(v[4], v[5], v[6], v[7]);
-    } else {
-#pragma unroll
-        for (int k = 0; k < kPPT; ++k) if (base + k < n) a[base + k] = v[k];
-    }
-}
 
 // ---------------------------------------------------------------------------
 // Window deposit engine.
@@ -290,24 +265,33 @@ __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, 
     w.WH = w.use ? w.W * w.H : 0;
 }
 
+// The window holds each (field, cell) sum as two int32 words written with
+// native 32-bit shared atomics: lo accumulates the low 16 bits of every added
+// value (unsigned) and hi its arithmetic high part (v >> 16), so
+// sum = hi * 2^16 + lo exactly. A chunk adds at most kChunk values of
+// magnitude < 2^25 to one entry: lo < 2^27 and |hi| < 2^20, no overflow.
+// Layout: plane 2f = lo of field f, plane 2f + 1 = hi, each W*H cells.
+
 // Zero NF window planes; the caller syncs afterwards.
 template <int NF>
-__device__ __forceinline__ void win_zero(long long* __restrict__ s, const Win& w) {
-    const int m = NF * w.WH;
+__device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
+    const int m = 2 * NF * w.WH;
     for (int i = threadIdx.x; i < m; i += kThreads) s[i] = 0;
 }
 
 // Flush the window into the global int64 accumulators acc[f*ncell + cell].
 // The caller syncs before calling.
 template <int NF>
-__device__ __forceinline__ void win_flush(const long long* __restrict__ s, const Win& w,
+__device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& w,
                                           unsigned long long* __restrict__ acc, const Geo& g) {
     for (int c = threadIdx.x; c < w.WH; c += kThreads) {
         const int wi = c % w.W, wj = c / w.W;
         const int gc = wrap_far(w.jr + w.mj + wj, g.ny) * g.nx + wrap_far(w.ir + w.mi + wi, g.nx);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            const long long v = s[f * w.WH + c];
+            const unsigned lo = static_cast<unsigned>(s[2 * f * w.WH + c]);
+            const int hi = s[(2 * f + 1) * w.WH + c];
+            const long long v = static_cast<long long>(hi) * 65536 + static_cast<long long>(lo);
             if (v != 0)
                 atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gc, static_cast<unsigned long long>(v));
         }
@@ -322,9 +306,12 @@ __device__ __forceinline__ int win_off(int c, int r, int n) { return wrap_signed
 // quads 16l + c, i.e. lanes 64 particles apart) are both conflict-free when
 // quad q is stored at quad position q ^ ((q >> 4) & 7).
 __device__ __forceinline__ int stage_quad(int q) { return q ^ ((q >> 4) & 7); }
+__device__ __forceinline__ float4 stq_c(const float* st, int f, int q) {
+    return reinterpret_cast<const float4*>(st + f * kChunk)[stage_quad(q)];
+}
 
 // Exact quantisation of the product a*b: rint(a*b) via one FFMA against
-// 1.5*2^23 (|a*b| < 2^20); the raw bits are summed and the magic removed later.
+// 1.5*2^23 (|a*b| < 2^22); the raw bits are summed and the magic removed later.
 __device__ __forceinline__ unsigned qbits(float a, float b) {
     return __float_as_uint(__fmaf_rn(a, b, kMagic));
 }
@@ -351,8 +338,8 @@ struct Run {
             for (int k = 0; k < 4; ++k) a[f][k] += qbits(cs[f], wv[k]);
         ++cnt;
     }
-    // Add the run into the window planes s[f*WH + cell].
-    __device__ __forceinline__ void flush(long long* __restrict__ s, const Win& w) {
+    // Add the run into the split window planes (lo, hi) of each field.
+    __device__ __forceinline__ void flush(int* __restrict__ s, const Win& w) {
         if (cw < 0) return;
         const unsigned m = cnt * kMagicU;
         const int offs[4] = {0, 1, w.W, w.W + 1};
@@ -361,9 +348,12 @@ struct Run {
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int v = static_cast<int>(a[f][k] - m);
-                if (v != 0)
-                    atomicAdd(reinterpret_cast<unsigned long long*>(s + f * w.WH + cw + offs[k]),
-                              static_cast<unsigned long long>(static_cast<long long>(v)));
+                if (v != 0) {
+                    int* e = s + 2 * f * w.WH + cw + offs[k];
+                    const int lo = v & 0xFFFF, hi = v >> 16;
+                    if (lo != 0) atomicAdd(e, lo);
+                    if (hi != 0) atomicAdd(e + w.WH, hi);
+                }
             }
     }
 };
@@ -385,30 +375,165 @@ __device__ __forceinline__ void deposit_global(int ci, int cj, const float (&wv)
         }
 }
 
-// Deposit one particle into the lane's run (flushing the previous run when the
-// base cell changes), or through the exact slow path when the window is unused
-// or a coefficient is outside the fast range.
-template <int NF>
-__device__ __forceinline__ void run_deposit(Run<NF>& run, long long* __restrict__ s, const Win& w,
-                                            int ci, int cj, const float (&wv)[4], const float (&cs)[NF],
-                                            unsigned long long* __restrict__ gacc, const Geo& g,
-                                            unsigned& nslow, DevState* st) {
-    bool fast = w.use;
+// Element e (0..3, run-time) of a float4: a select chain, no local memory.
+__device__ __forceinline__ float sel(const float4& v, int e) {
+    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
+}
+// Stage position of chunk slot s (quads swizzled, see stage_quad).
+__device__ __forceinline__ int stage_slot(int s) { return (stage_quad(s >> 2) << 2) | (s & 3); }
+
+// ---------------------------------------------------------------------------
+// Chunk loads with the bulk-copy engine (TMA, cp.async.bulk, no multicast): one
+// thread issues one global->shared copy per SoA array of the chunk and every
+// thread waits on an mbarrier, so the whole chunk (up to 48 KB) is in flight at
+// once. Waits are bounded: a copy that never completes sets AW_DEV_WAIT_LIMIT
+// and the block returns without touching the data.
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+constexpr int kWaitLimit = 1 << 22;    // try_wait rounds before a wait gives up
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (int k = 0; k < kWaitLimit; ++k)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// Source arrays of a chunk load, in stage-plane order.
+struct ChunkSrc {
+    const float* a[6];
+    // plane k with a select chain (a run-time index into a[] would live in local memory)
+    __device__ __forceinline__ const float* at(int k) const {
+        return k == 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : k == 3 ? a[3] : k == 4 ? a[4] : a[5];
+    }
+};
+
+// Load planes [0, np) of the chunk [c0, c0 + cnt) into stage[k * kChunk + s]
+// (linear layout). Bulk copies need 16-byte aligned addresses and sizes: the
+// arrays are 16-byte aligned when `vec`, chunk starts are multiples of 8 KB, and
+// the ragged tail (< 4 particles) and unaligned arrays use plain loads. Returns
+// false (block-uniformly) when the bounded wait gave up. Ends with a barrier;
+// *x0, *y0 receive the first particle's position (read before any overwrite).
+__device__ __forceinline__ bool load_chunk(float* stage, const ChunkSrc& src, int np, long long c0, int cnt, bool vec,
+                           unsigned long long* bar, DevState* st, float* x0, float* y0) {
+    const int nbulk = vec ? (cnt & ~3) : 0;
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_arrive_expect_tx(bar, static_cast<unsigned>(np * nbulk) * 4u);
+        if (nbulk > 0)
+            for (int k = 0; k < np; ++k)
+                bulk_load(stage + k * kChunk, src.at(k) + c0, static_cast<unsigned>(nbulk) * 4u, bar);
+    }
+    const int rem = cnt - nbulk;
+    if (rem > 0)
+        for (int idx = threadIdx.x; idx < rem * np; idx += kThreads) {
+            const int k = idx / rem, s = nbulk + idx % rem;
+            stage[k * kChunk + s] = __ldg(src.at(k) + c0 + s);
+        }
+    __syncthreads();                        // barrier initialised; plain loads visible
+    bool ok = mbar_wait_bounded(bar, 0u);
+    *x0 = stage[0];
+    *y0 = stage[kChunk];
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) set_err(st, 4u);     // AW_DEV_WAIT_LIMIT
+        mbar_wait_bounded(bar, 0u);                // let copies in flight land
+        return false;
+    }
+    return true;
+}
+
+// Exact slow path after the window pass: the particles pass 1 listed (a
+// coefficient outside the fast range or non-finite; their staged x carries a
+// flipped sign) and, when the window did not fit, every valid particle. Each
+// contribution is rounded exactly from the double product and added to the
+// global int64 planes. coef(a, cs) maps the staged values a[0..NS) of one
+// particle (a[0] = x, a[1] = y) to its NF scaled coefficients.
+template <int NF, int NS, class CoefFn>
+__device__ __forceinline__ void slow_pass(const float* __restrict__ stage, const unsigned short* __restrict__ list,
+                                          int nlist, bool all_slots, unsigned long long* __restrict__ gacc,
+                                          const Geo& g, DevState* st, CoefFn coef) {
+    const int total = nlist + (all_slots ? kChunk : 0);
+    unsigned n = 0;
+    for (int k = threadIdx.x; k < total; k += kThreads) {
+        const bool listed = k < nlist;
+        const int d = stage_slot(listed ? static_cast<int>(list[k]) : k - nlist);
+        float a[NS];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) fast = fast && (fabsf(cs[f]) < kFastLim);
-    if (!fast) {
-        for (int f = 0; f < NF; ++f)
-            if (!isfinite(cs[f])) { set_err(st, 1u); return; }   // AW_DEV_NONFINITE
-        deposit_global<NF>(ci, cj, wv, cs, gacc, g);
-        ++nslow;
-        return;
+        for (int f = 0; f < NS; ++f) a[f] = stage[f * kChunk + d];
+        if (listed) a[0] = -a[0];
+        else if (__float_as_int(a[0]) < 0) continue;     // invalid, or listed
+        float cs[NF];
+        coef(a, cs);
+        bool finite = true;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) finite = finite && isfinite(cs[f]);
+        if (!finite) { set_err(st, 1u); continue; }      // AW_DEV_NONFINITE
+        const Cic c = cic(a[0], a[1]);
+        const float wv[4] = {c.w0, c.w1, c.w2, c.w3};
+        deposit_global<NF>(c.i0, c.j0, wv, cs, gacc, g);
+        ++n;
     }
-    const int cw = (win_off(cj, w.jr, g.ny) - w.mj) * w.W + (win_off(ci, w.ir, g.nx) - w.mi);
-    if (cw != run.cw) {
-        run.flush(s, w);
-        run.start(cw);
+    if (n) atomicAdd(&st->slow, static_cast<unsigned long long>(n));
+}
+
+// Window pass: lane l of warp w deposits the 8 consecutive particles
+// 64l + 8w .. 64l + 8w + 7 (quads 16l + 2w + {0,1}), summing same-cell runs in
+// registers; lanes sit 64 particles apart, so their run flushes rarely meet in
+// one shared-atomic instruction. Particles whose staged x has its sign bit set
+// (invalid or listed for the slow pass) are skipped.
+template <int NF, int NS, class CoefFn>
+__device__ __forceinline__ void window_pass(const float* __restrict__ stage, int* __restrict__ win,
+                                            const Win& wn, const Geo& g, CoefFn coef) {
+    if (!wn.use) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    Run<NF> run;
+    run.cw = -1;
+    run.cnt = 0;
+    float4 v[NS];
+#pragma unroll 1
+    for (int k = 0; k < 8; ++k) {
+        if ((k & 3) == 0) {
+            const int q = 16 * lane + 2 * warp + (k >> 2);
+#pragma unroll
+            for (int f = 0; f < NS; ++f) v[f] = stq_c(stage, f, q);
+        }
+        const int e = k & 3;
+        float a[NS];
+#pragma unroll
+        for (int f = 0; f < NS; ++f) a[f] = sel(v[f], e);
+        if (__float_as_int(a[0]) < 0) continue;
+        const Cic c = cic(a[0], a[1]);
+        float cs[NF];
+        coef(a, cs);
+        const float wv[4] = {c.w0, c.w1, c.w2, c.w3};
+        const int cw = (win_off(c.j0, wn.jr, g.ny) - wn.mj) * wn.W + (win_off(c.i0, wn.ir, g.nx) - wn.mi);
+        if (cw != run.cw) {
+            run.flush(win, wn);
+            run.start(cw);
+        }
+        run.add(cs, wv);
     }
-    run.add(cs, wv);
+    run.flush(win, wn);
 }
 
 }  // namespace aw

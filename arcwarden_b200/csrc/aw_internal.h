@@ -155,6 +155,7 @@ void launch_pack_em(Ctx& c);
 void launch_grid_diag(Ctx& c);
 void launch_set_step(Ctx& c, long long n);
 void launch_copy_umax(Ctx& c);
+void launch_promote_scales(Ctx& c);                // S_pend = S_next
 void launch_rms_reduce(Ctx& c, bool src, bool dcu);
 
 }  // namespace aw

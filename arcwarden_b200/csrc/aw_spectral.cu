@@ -499,41 +499,61 @@ __global__ void k_grid_diag(const float* ex, const float* ey, const float* bx, c
 }
 
 // RMS of the (unscaled) deposit coefficients from the fixed-order block
-// partials of sum coef^2 and the particle count: rms_f = sqrt(sum / n).
-__global__ void __launch_bounds__(256)
+// partials of sum coef^2 and the particle count: rms_f = sqrt(sum / n). One
+// block of 1024 threads; a fixed assignment and tree, so the result is a pure
+// function of the partials.
+constexpr int kRmsThreads = 1024;
+__global__ void __launch_bounds__(kRmsThreads)
 k_rms_reduce(const float* __restrict__ pc, int nbc, const float* __restrict__ pd, int nbd, DevState* st) {
-    __shared__ double sh[12][256];
+    constexpr int NA = 13;                   // 8 src sums, src count, 3 dcu sums, dcu count
+    constexpr int NW = kRmsThreads / 32;
+    __shared__ double sh[NA][NW];
     const int t = threadIdx.x;
-    double a[12] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};   // 8 src + count, 3 dcu... (see below)
-    if (pc) for (int b = t; b < nbc; b += 256) for (int k = 0; k < 9; ++k) a[k] += pc[b * 9 + k];
-    double ad[4] = {0, 0, 0, 0};
-    if (pd) for (int b = t; b < nbd; b += 256) for (int k = 0; k < 4; ++k) ad[k] += pd[b * 4 + k];
-    for (int k = 0; k < 9; ++k) sh[k][t] = a[k];
-    for (int k = 0; k < 3; ++k) sh[9 + k][t] = ad[k];
-    __shared__ double shn[256];
-    shn[t] = ad[3];
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-        if (t < s) {
-            for (int k = 0; k < 12; ++k) sh[k][t] += sh[k][t + s];
-            shn[t] += shn[t + s];
-        }
-        __syncthreads();
+    double a[NA];
+#pragma unroll
+    for (int k = 0; k < NA; ++k) a[k] = 0.0;
+    if (pc) {
+#pragma unroll 4
+        for (int b = t; b < nbc; b += kRmsThreads)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) a[k] += pc[b * 9 + k];
     }
-    if (t == 0) {
-        if (pc && sh[8][0] > 0.0) {
-            for (int f = 0; f < 8; ++f)
-                st->rms_src[f] = static_cast<float>(sqrt(sh[f][0] / sh[8][0]));
+    if (pd) {
+#pragma unroll 4
+        for (int b = t; b < nbd; b += kRmsThreads)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a[9 + k] += pd[b * 4 + k];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < NA; ++k) a[k] += __shfl_down_sync(0xffffffffu, a[k], o);
+    if ((t & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < NA; ++k) sh[k][t >> 5] = a[k];
+    __syncthreads();
+    if (t < 32) {
+#pragma unroll
+        for (int k = 0; k < NA; ++k) a[k] = sh[k][t];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int k = 0; k < NA; ++k) a[k] += __shfl_down_sync(0xffffffffu, a[k], o);
+        if (t == 0) {
+            if (pc && a[8] > 0.0)
+                for (int f = 0; f < 8; ++f) st->rms_src[f] = static_cast<float>(sqrt(a[f] / a[8]));
+            if (pd && a[12] > 0.0)
+                for (int k = 0; k < 3; ++k) st->rms_dcu[k] = static_cast<float>(sqrt(a[9 + k] / a[12]));
+            st->have_rms = 1;
         }
-        if (pd && shn[0] > 0.0) {
-            for (int k = 0; k < 3; ++k)
-                st->rms_dcu[k] = static_cast<float>(sqrt(sh[9 + k][0] / shn[0]));
-        }
-        st->have_rms = 1;
     }
 }
 
 __global__ void k_set_step(DevState* st, long long n) { st->step = n; }
+// The scales a step-begin finalise chose become the pending deposit's scales.
+__global__ void k_promote_scales(DevState* st) {
+    for (int f = 0; f < 8; ++f) st->S_pend[f] = st->S_next[f];
+}
 __global__ void k_copy_umax(DevState* st) {
     for (int d = 0; d < 3; ++d) st->umax_bits[d] = st->ucur_bits[d];
 }
@@ -670,8 +690,12 @@ void launch_set_step(Ctx& c, long long n) {
     AW_LAUNCH();
 }
 void launch_rms_reduce(Ctx& c, bool src, bool dcu) {
-    k_rms_reduce<<<1, 256, 0, c.stream>>>(src ? c.part_c : nullptr, c.npart_p, dcu ? c.part_d : nullptr,
-                                          c.npart_p, c.st);
+    k_rms_reduce<<<1, kRmsThreads, 0, c.stream>>>(src ? c.part_c : nullptr, c.npart_p,
+                                                  dcu ? c.part_d : nullptr, c.npart_p, c.st);
+    AW_LAUNCH();
+}
+void launch_promote_scales(Ctx& c) {
+    k_promote_scales<<<1, 1, 0, c.stream>>>(c.st);
     AW_LAUNCH();
 }
 void launch_copy_umax(Ctx& c) {

@@ -1,0 +1,182 @@
+"""The fused CUDA-graph step (aw_init / aw_step / aw_run) against the oracle's
+restatement of Simulation<Cfg>::{init, step} (include/pic/simulation.hpp:56-119),
+plus the size-independent properties at the full workload sizes.
+
+Tolerances: the first step's sources are bit-exact (exact fixed-point deposit of
+the same loaded particles). The fields come from the FP32 cuFFT solve while the
+oracle solves in FP64, so fields are held to the reference's max-relative metric
+(tools/deposit_bench.cu:56-65) at 1e-5, and particles pushed by those fields to
+an absolute 1e-5.
+"""
+import numpy as np
+import pytest
+
+from conftest import relerr
+from gpu_helpers import C0_SPECIES, C1_SPECIES, PARTICLE_KEYS, TWO_STREAM, WEIBEL, Setup, n_particles
+
+pytestmark = pytest.mark.gpu
+
+FIELD_TO_ORACLE = {"rho": "rho", "Jx": "jx", "Jy": "jy", "Jz": "jz", "Ex": "ex", "Ey": "ey", "Ez": "ez",
+                   "Bx": "bx", "By": "by", "Bz": "bz", "ETx": "etx", "ETy": "ety", "ETz": "etz"}
+ES_FIELDS = ("rho", "Ex", "Ey")
+DARWIN_FIELDS = tuple(FIELD_TO_ORACLE)
+
+
+@pytest.fixture()
+def setup(torch_cuda, aw):
+    made = []
+
+    def make(nx, ny, Lx, Ly, n, model, **kw):
+        s = Setup(torch_cuda, aw, nx, ny, Lx, Ly, n, model, **kw)
+        made.append(s)
+        return s
+
+    yield make
+    for s in made:
+        s.close()
+
+
+def _pair(setup, aw, oracle, model, nx, ny, Lx, Ly, sp, dt, exact=False, **kw):
+    s = setup(nx, ny, Lx, Ly, n_particles(sp, nx, ny), model, dt=dt, **kw)
+    s.ctx.load_species(sp, seed=0, noisy=True)
+    p0 = s.parts()
+    st = oracle.State(oracle.geo(nx, ny, Lx, Ly), {k: p0[k] for k in PARTICLE_KEYS}, dt=dt,
+                      darwin=(model == aw.AW_MODEL_DARWIN), exact=exact, **kw)
+    s.ctx.init()
+    st.init()
+    return s, st
+
+
+def test_es_step_matches_oracle(setup, aw, oracle):
+    """ES two-stream: fields to 1e-5, diagnostics, particle state."""
+    s, st = _pair(setup, aw, oracle, aw.AW_MODEL_ES, 64, 64, 64.0, 64.0, TWO_STREAM, 0.1)
+    for n in range(4):
+        s.ctx.step(n)
+        st.step()
+        for k in ES_FIELDS:
+            assert relerr(s.grid(k), st.field(FIELD_TO_ORACLE[k])) < 1e-5, (n, k)
+        d, od = s.ctx.step_diag(), st.diag()
+        assert abs(d["charge"] - od["charge"]) <= 1e-9 * abs(od["charge"])
+        assert abs(d["ke"] - od["ke"]) <= 1e-6 * od["ke"]
+        assert abs(d["ee"] - od["ee"]) <= 1e-4 * od["ee"]
+    p = s.parts()
+    for k in ("x", "y", "ux", "uy", "uz"):
+        assert np.abs(p[k].astype(np.float64) - st.p[k]).max() < 1e-5, k
+    assert s.ctx.error_word() == 0
+
+
+def test_es_first_step_sources_bit_exact(setup, aw, oracle):
+    """The deposit of the initial particles (the first step's rho) is bit-exact."""
+    s, st = _pair(setup, aw, oracle, aw.AW_MODEL_ES, 64, 32, 64.0, 32.0, TWO_STREAM, 0.1)
+    s.ctx.step(0)
+    st.step()
+    assert np.array_equal(s.grid("rho"), st.field("rho"))
+
+
+@pytest.mark.parametrize("magnetized", [False, True])
+def test_darwin_step_matches_oracle(setup, aw, oracle, magnetized):
+    """Darwin Weibel (and a magnetized run with a pump): every field to 1e-5 of
+    the oracle with FP64 deposits."""
+    kw = {}
+    if magnetized:
+        kw = dict(B0=(0.43, 0.25, 0.0),
+                  pump=dict(ex=1e-3, ey=2e-3, ez=-1e-3, k0=2 * np.pi * 2 / 64.0, w0=0.1, trmp=1.0, toff=100.0))
+    s, st = _pair(setup, aw, oracle, aw.AW_MODEL_DARWIN, 64, 32, 64.0, 32.0, WEIBEL, 0.05, exact=True, **kw)
+    for n in range(3):
+        s.ctx.step(n)
+        st.step()
+        for k in DARWIN_FIELDS:
+            assert relerr(s.grid(k), st.field(FIELD_TO_ORACLE[k])) < 1e-5, (n, k)
+    assert s.ctx.error_word() == 0
+
+
+def test_darwin_fields_vs_fp64_oracle(setup, aw, oracle):
+    """Per-field error against the FP64 host oracle (deposits summed in double,
+    FP64 spectral solve): rho, J, E, B, E_T within 1e-5 max-relative."""
+    s, st = _pair(setup, aw, oracle, aw.AW_MODEL_DARWIN, 128, 128, 64.0, 64.0, WEIBEL, 0.05, exact=True,
+                  B0=(0.0, 0.0, 0.3))
+    worst = {}
+    for n in range(3):
+        s.ctx.step(n)
+        st.step()
+        for k in DARWIN_FIELDS:
+            worst[k] = max(worst.get(k, 0.0), relerr(s.grid(k), st.field(FIELD_TO_ORACLE[k])))
+    print("max-relative error vs FP64 oracle:", {k: f"{v:.2e}" for k, v in worst.items()})
+    assert all(v < 1e-5 for v in worst.values()), worst
+
+
+@pytest.mark.parametrize("model", [0, 1])
+def test_graph_replay_equals_stepwise_and_is_deterministic(setup, aw, model):
+    """aw_run with a captured graph reproduces aw_step bit for bit, and two runs
+    from the same load are identical (order-independent fixed-point sums)."""
+    sp = TWO_STREAM if model == aw.AW_MODEL_ES else WEIBEL
+    out = []
+    for graph in (False, True, True):
+        s = setup(128, 128, 128.0, 128.0, n_particles(sp, 128, 128), model, dt=0.05)
+        s.ctx.load_species(sp, seed=1)
+        s.ctx.init()
+        s.ctx.run(0, 6, graph=graph)
+        p = s.parts()
+        p["rho"], p["Ex"] = s.grid("rho"), s.grid("Ex")
+        out.append(p)
+    for k in out[0]:
+        assert np.array_equal(out[0][k], out[1][k]), k
+        assert np.array_equal(out[1][k], out[2][k]), k
+
+
+def test_run_diag_matches_device_diagnostics(setup, aw, oracle):
+    """aw_run_diag streams the per-step FP64 diagnostics to the host; the last row
+    equals aw_step_diag of the same step and the charge is the oracle's."""
+    s, st = _pair(setup, aw, oracle, aw.AW_MODEL_DARWIN, 64, 64, 32.0, 32.0, WEIBEL, 0.05)
+    rows = np.zeros((5, 8), np.float64)
+    s.ctx.run_diag(0, 5, rows.ctypes.data)
+    s.torch.cuda.synchronize()
+    d = s.ctx.step_diag()
+    assert np.array_equal(rows[-1], np.array([d[k] for k in ("ke", "ee", "charge", "max_e", "px", "py", "pz", "eb")]))
+    for _ in range(5):
+        st.step()
+    assert abs(rows[-1][2] - st.diag()["charge"]) <= 1e-9 * abs(st.diag()["charge"])
+
+
+def test_step_profile_names_every_phase(setup, aw):
+    s = setup(64, 64, 32.0, 32.0, n_particles(WEIBEL, 64, 64), aw.AW_MODEL_DARWIN, dt=0.05)
+    s.ctx.load_species(WEIBEL, seed=0)
+    s.ctx.init()
+    prof = s.ctx.step_profile(0)
+    assert len(prof) == 14 and "push_deposit_em" in prof and "rms_reduce" in prof
+    assert all(v >= 0.0 for v in prof.values())
+
+
+# ---- full sizes: properties that need no oracle ------------------------------------
+def _full(setup, aw, model, steps):
+    if model == aw.AW_MODEL_ES:
+        nx, L, sp, dt = 256, 256.0, C0_SPECIES, 0.1
+    else:
+        nx, L, sp, dt = 512, 256.0, C1_SPECIES, 0.05
+    s = setup(nx, nx, L, L, n_particles(sp, nx, nx), model, dt=dt)
+    s.ctx.load_species(sp, seed=0)
+    s.ctx.init()
+    s.ctx.run(0, steps, graph=True)
+    return s
+
+
+@pytest.mark.parametrize("model", [0, 1])
+def test_full_size_charge_conservation_and_determinism(setup, aw, model):
+    """At the 256^2 x 64 ppc (ES) and 512^2 x 64 ppc (Darwin) workloads: the total
+    deposited charge equals q * n0 * Lx * Ly to FP64 rounding of the fixed-point
+    sums, nothing leaves the grid or turns non-finite, and a second run is
+    bit-identical."""
+    a = _full(setup, aw, model, 10)
+    pa = a.parts()
+    rho = a.grid("rho").astype(np.float64)
+    dxdy = (a.Lx / a.nx) * (a.Ly / a.ny)
+    total = -1.0 * a.Lx * a.Ly
+    assert abs(rho.sum() * dxdy - total) < 1e-6 * abs(total)
+    assert abs(a.ctx.step_diag()["charge"] - total) < 1e-6 * abs(total)
+    assert a.ctx.error_word() == 0
+    a.close()
+    b = _full(setup, aw, model, 10)
+    pb = b.parts()
+    for k in PARTICLE_KEYS:
+        assert np.array_equal(pa[k], pb[k]), k
+    assert np.array_equal(rho, b.grid("rho").astype(np.float64))
