@@ -26,8 +26,9 @@
 //           box; then, per warp and in place, the values the deposit needs are
 //           rewritten into the swizzled stage layout. A particle whose scaled
 //           coefficient leaves the fast range goes on the chunk's slow list.
-//   window  block-wide bounding box -> shared window of NF exact sums per cell,
-//           each kept as two int32 words (native 32-bit shared atomics).
+//   window  block-wide bounding box -> shared window of NF exact sums per cell
+//           in int32 words (native 32-bit shared atomics; wrap-tracked where
+//           a chunk's sum could leave the int32 range).
 //   pass 2  each lane deposits 8 consecutive particles from the stage, summing
 //           same-cell runs exactly in integer registers; lanes of a warp sit 64
 //           particles apart (different cells), so each run's flush is a set of
@@ -51,10 +52,10 @@ template <> struct SetNF<SET_RHOJ> { static constexpr int NF = 4, NS = 6; };   /
 template <> struct SetNF<SET_AMU>  { static constexpr int NF = 4, NS = 6; };
 template <> struct SetNF<SET_ALL>  { static constexpr int NF = 8, NS = 6; };
 
-// Window capacity in cells for NF split (2 x int32) planes. The NF = 8 push kernel keeps
+// Window capacity in cells for NF fields (2 int32 planes each). The NF = 8 push kernel keeps
 // two CTAs per SM with its 48 KB stage; the ES push kernel keeps three.
 constexpr int wmax_cells(int nf) { return nf == 1 ? 2048 : (nf == 3 ? 2048 : (nf == 4 ? 1536 : 896)); }
-constexpr int kRedInts = kThreads / 32 * 4;
+constexpr int kRedInts = kThreads / 32 * (4 + 8);
 // stage [np][kChunk] f32 | window [2*nf][wmax] i32 | red ints | slow list u16[kChunk]
 constexpr size_t win_offset(int np) { return static_cast<size_t>(np) * kChunk * 4; }
 constexpr size_t smem_bytes(int nf, int np) {
@@ -64,7 +65,7 @@ constexpr size_t smem_bytes(int nf, int np) {
 
 struct Smem {
     float* stage;
-    int* win;          // split window: 2 * NF int32 planes
+    int* win;          // window: 2 * NF int32 planes
     int* red;
     unsigned short* slow;
 };
@@ -122,14 +123,20 @@ __device__ __forceinline__ void src_coefs(float coef, float ux, float uy, float 
 }
 
 // Scaled coefficients cs = fl(cf * S) and whether every one is inside the fast
-// range (|cs| < 2^22; the CIC weights are <= 1, so every product is too).
+// range (|cs| < 2^22; the CIC weights are <= 1, so every product is too). A
+// fast particle's |cs| are added to the thread's window bounds l1.
 template <int NF>
-__device__ __forceinline__ bool scale_fast(const float (&cf)[NF], const float (&S)[NF], float (&cs)[NF]) {
+__device__ __forceinline__ bool scale_fast(const float (&cf)[NF], const float (&S)[NF], float (&cs)[NF],
+                                           float (&l1)[NF]) {
     bool fast = true;
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
         cs[f] = __fmul_rn(cf[f], S[f]);
         fast = fast && (fabsf(cs[f]) < kFastLim);
+    }
+    if (fast) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) l1[f] = __fadd_rn(l1[f], fabsf(cs[f]));
     }
     return fast;
 }
@@ -199,22 +206,23 @@ __device__ __forceinline__ void list_slow(unsigned short* list, int* nlist, int 
 }
 
 // Window set-up (syncs), zero, sync.
-template <int NF>
-__device__ __forceinline__ Win open_window(const BBox& bb, int ir, int jr, int wmaxc, const Smem& m) {
+template <int NF, bool T0>
+__device__ __forceinline__ Win open_window(const BBox& bb, int ir, int jr, int wmaxc, const Smem& m,
+                                           const float (&l1)[NF]) {
     Win wn;
-    win_setup(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, m.red);
+    win_setup<NF, T0>(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, m.red, l1);
     win_zero<NF>(m.win, wn);
     __syncthreads();
     return wn;
 }
 
 // Block tail shared by every kernel: window flush, slow list, counters.
-template <int NF, int NS, class CoefFn>
+template <int NF, int NS, bool T0, class CoefFn>
 __device__ __forceinline__ void close_window(const Smem& m, const Win& wn, int nlist,
                                              unsigned long long* __restrict__ acc, const Geo& g, DevState* st,
                                              CoefFn coef) {
     __syncthreads();
-    win_flush<NF>(m.win, wn, acc, g);
+    win_flush<NF, T0>(m.win, wn, acc, g);
     slow_pass<NF, NS>(m.stage, m.slow, nlist, !wn.use, acc, g, st, coef);
     if (threadIdx.x == 0) {
         atomicAdd(&st->chunks, 1ull);
@@ -229,6 +237,7 @@ __global__ void __launch_bounds__(kThreads)
 k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st, float* __restrict__ psq) {
     constexpr int NF = SetNF<SET>::NF, NS = SetNF<SET>::NS;
+    constexpr bool T0 = SET != SET_AMU;      // field 0 is rho
     extern __shared__ __align__(16) unsigned char smem[];
     const Smem m = carve(smem, NS, NF, wmaxc);
     __shared__ unsigned long long bar;
@@ -249,6 +258,7 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
     for (int f = 0; f < NF; ++f) S[f] = Sdev[foff + f];
 
     BBox bb;
+    float l1[NF] = {};
     float sq[NF] = {};
     float nval = 0.f;
 #pragma unroll 1
@@ -264,7 +274,7 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
                 float cf[NF], cs[NF];
                 if constexpr (NS == 6) src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), a[3], a[4], a[5], cf);
                 else src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), 0.f, 0.f, 0.f, cf);
-                const bool fast = scale_fast<NF>(cf, S, cs);
+                const bool fast = scale_fast<NF>(cf, S, cs, l1);
                 if (psq) {
 #pragma unroll
                     for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
@@ -282,7 +292,7 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
 #pragma unroll
         for (int f = 1; f < NS; ++f) m.stage[f * kChunk + d] = a[f];
     }
-    const Win wn = open_window<NF>(bb, ir, jr, wmaxc, m);
+    const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
         float cf[NF];
         if constexpr (NS == 6) src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), a[3], a[4], a[5], cf);
@@ -290,8 +300,8 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
 #pragma unroll
         for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cf[f], S[f]);
     };
-    window_pass<NF, NS>(m.stage, m.win, wn, g, coef);
-    close_window<NF, NS>(m, wn, nlist, acc, g, st, coef);
+    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
+    close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
     if (psq) block_sumsq<NF>(sq, nval, psq, ssq);
 }
 
@@ -339,6 +349,7 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st, int use_rms,
               float* __restrict__ psq) {
     constexpr int NF = 3, NS = 5, NIN = 6;
+    constexpr bool T0 = false;
     extern __shared__ __align__(16) unsigned char smem[];
     const Smem m = carve(smem, NIN, NF, wmaxc);
     __shared__ unsigned long long bar;
@@ -358,6 +369,7 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
     ref_of(x0, y0, g, ir, jr);
 
     BBox bb;
+    float l1[NF] = {};
     float sq[NF] = {};
     float nval = 0.f;
 #pragma unroll 2
@@ -378,7 +390,7 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
                 const float cz = __fmaf_rn(vx, by, -__fmul_rn(vy, bx));
                 const float cf[NF] = {__fmul_rn(coef, __fadd_rn(ex, cx)), __fmul_rn(coef, __fadd_rn(ey, cy)),
                                       __fmul_rn(coef, __fadd_rn(ez, cz))};
-                const bool fast = scale_fast<NF>(cf, S, cs);
+                const bool fast = scale_fast<NF>(cf, S, cs, l1);
 #pragma unroll
                 for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
                 nval += 1.0f;
@@ -396,10 +408,10 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
         m.stage[3 * kChunk + d] = cs[1];
         m.stage[4 * kChunk + d] = cs[2];
     }
-    const Win wn = open_window<NF>(bb, ir, jr, wmaxc, m);
+    const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) { cs[0] = a[2]; cs[1] = a[3]; cs[2] = a[4]; };
-    window_pass<NF, NS>(m.stage, m.win, wn, g, coef);
-    close_window<NF, NS>(m, wn, nlist, acc, g, st, coef);
+    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
+    close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
     if (psq) block_sumsq<NF>(sq, nval, psq, ssq);
 }
 
@@ -431,6 +443,7 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                   double qoa, unsigned long long* __restrict__ acc, int wmaxc,
                   double* __restrict__ part, DevState* st) {
     constexpr int NF = 1, NS = 3, NIN = 6;
+    constexpr bool T0 = true;
     extern __shared__ __align__(16) unsigned char smem[];
     const Smem m = carve(smem, NIN, NF, wmaxc);
     __shared__ unsigned long long bar;
@@ -449,6 +462,7 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     const float2* q = reinterpret_cast<const float2*>(gb);
 
     BBox bb;
+    float l1[NF] = {};
     double ke = 0, px = 0, py = 0, pz = 0;
 #pragma unroll 2
     for (int it = 0; it < kPPT; ++it) {
@@ -477,7 +491,7 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                     bb.add(ci, cj, ir, jr, g);
                     const float cf[1] = {__double2float_rn(qoa * static_cast<double>(w))};
                     float cs[1];
-                    const bool fast = scale_fast<1>(cf, S1, cs);
+                    const bool fast = scale_fast<1>(cf, S1, cs, l1);
                     xs = __fadd_rn(x, 0.0f);
                     if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
                 } else {
@@ -496,12 +510,12 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
         m.stage[kChunk + d] = y;
         m.stage[2 * kChunk + d] = w;
     }
-    const Win wn = open_window<NF>(bb, ir, jr, wmaxc, m);
+    const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
         cs[0] = __fmul_rn(__double2float_rn(qoa * static_cast<double>(a[2])), S1[0]);
     };
-    window_pass<NF, NS>(m.stage, m.win, wn, g, coef);
-    close_window<NF, NS>(m, wn, nlist, acc, g, st, coef);
+    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
+    close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
     block_sum4(ke, px, py, pz, part, dsh);
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         st->S_pend[0] = S1[0];
@@ -516,6 +530,7 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                   double qoa, unsigned long long* __restrict__ acc, int wmaxc,
                   double* __restrict__ part, DevState* st, float* __restrict__ psq) {
     constexpr int NF = 8, NS = 6;
+    constexpr bool T0 = true;
     extern __shared__ __align__(16) unsigned char smem[];
     const Smem m = carve(smem, NS, NF, wmaxc);
     __shared__ unsigned long long bar;
@@ -537,6 +552,7 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     ref_of(x0, y0, g, ir, jr);
 
     BBox bb;
+    float l1[NF] = {};
     double ke = 0, px = 0, py = 0, pz = 0;
     float m0 = 0.f, m1 = 0.f, m2 = 0.f;
     float sq[NF] = {};
@@ -565,7 +581,7 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                     bb.add(ci, cj, ir, jr, g);
                     float cf[NF], cs[NF];
                     src_coefs<SET_ALL>(__double2float_rn(qoa * static_cast<double>(w)), ux, uy, uz, cf);
-                    const bool fast = scale_fast<NF>(cf, S, cs);
+                    const bool fast = scale_fast<NF>(cf, S, cs, l1);
 #pragma unroll
                     for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
                     nval += 1.0f;
@@ -599,7 +615,7 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
         umx[1][threadIdx.x >> 5] = __float_as_uint(m1);
         umx[2][threadIdx.x >> 5] = __float_as_uint(m2);
     }
-    const Win wn = open_window<NF>(bb, ir, jr, wmaxc, m);
+    const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
     if (threadIdx.x < 3) {
         unsigned mx = 0;
         for (int k = 0; k < kThreads / 32; ++k) mx = max(mx, umx[threadIdx.x][k]);
@@ -611,8 +627,8 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
 #pragma unroll
         for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cf[f], S[f]);
     };
-    window_pass<NF, NS>(m.stage, m.win, wn, g, coef);
-    close_window<NF, NS>(m, wn, nlist, acc, g, st, coef);
+    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
+    close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
     block_sumsq<NF>(sq, nval, psq, ssq);
     block_sum4(ke, px, py, pz, part, dsh);
     if (threadIdx.x == 0 && blockIdx.x == 0) {

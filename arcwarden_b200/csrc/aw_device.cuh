@@ -100,18 +100,17 @@ __device__ __forceinline__ void set_err(DevState* st, unsigned bits) {
     atomicOr(&st->err, bits);
 }
 
-// Power-of-two scale S such that bound * S < 2^22 (the fast path), from a
-// positive bound. Deterministic: a pure function of the bound.
-__host__ __device__ inline float scale_for_bound(float bound) {
+// Power-of-two scale S such that bound * S < 2^top (the fast path uses
+// top = 22), from a positive bound. Deterministic: a pure function of the bound.
+__host__ __device__ inline float scale_for_bound(float bound, int top = 22) {
     if (!(bound > 0.0f) || !(bound < 3.0e38f)) return 1.0f;
     int e;
     frexpf(bound, &e);            // bound in [2^(e-1), 2^e)
-    int k = 22 - e;               // bound * 2^k < 2^22
+    int k = top - e;              // bound * 2^k < 2^top
     if (k > 120) k = 120;
     if (k < -120) k = -120;
     return ldexpf(1.0f, k);
 }
-
 // ---------------------------------------------------------------------------
 // CIC stencil — include/pic/grid.hpp:135-155. Positions are in cell units and
 // already inside [0,nx)x[0,ny), so the int conversion is the floor.
@@ -234,27 +233,56 @@ struct Win {
     int W, H;        // extent in cells (incl. the +1 corner)
     int WH;
     bool use;        // fits the shared window capacity
+    bool track_all;  // some field's chunk sums may leave int32: track every field
 };
 
-// Block-wide min/max of the offsets, then the window geometry. `red` is
-// kThreads/32*4 ints of shared scratch. Every thread of the block calls it.
+// Block-wide min/max of the offsets and sums of the per-field magnitude bounds,
+// then the window geometry. `l1[f]` is this thread's sum of |scaled coefficient|
+// of field f over its fast-path particles; `red` is (4 + NF) * warps ints of
+// shared scratch. Every thread of the block calls it.
+//
+// Window mode: a window entry receives at most one rounded contribution per
+// particle, |q| <= |cs| + 1/2, so sum_p (|cs_p| + 1) bounds it. Field 0 is
+// always wrap-tracked when T0 (the charge density: its chunk sums are large by
+// design); every other field is added with plain int32 atomics when that bound
+// is < 2^31 for all of them, else the chunk tracks every field (see below).
+// The thread bound is ceil(l1 (1 + 2^-20)) + kPPT (FP32 rounding of at most
+// kPPT additions, plus the +1 per particle).
+template <int NF, bool T0>
 __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, int hi_j, int ir, int jr,
-                                          int wmaxc, int* red) {
+                                          int wmaxc, int* red, const float (&l1)[NF]) {
+    constexpr int NW = kThreads / 32;
     lo_i = __reduce_min_sync(0xffffffffu, lo_i);
     lo_j = __reduce_min_sync(0xffffffffu, lo_j);
     hi_i = __reduce_max_sync(0xffffffffu, hi_i);
     hi_j = __reduce_max_sync(0xffffffffu, hi_j);
+    unsigned wsum[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        const float b = fminf(ceilf(__fmul_rn(l1[f], 1.00000095367431640625f)), 33554432.0f);   // <= 2^25
+        wsum[f] = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(b) + static_cast<unsigned>(kPPT));
+    }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (lane == 0) {
         red[warp * 4 + 0] = lo_i; red[warp * 4 + 1] = lo_j;
         red[warp * 4 + 2] = hi_i; red[warp * 4 + 3] = hi_j;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) red[NW * 4 + f * NW + warp] = static_cast<int>(wsum[f]);
     }
     __syncthreads();
     lo_i = red[0]; lo_j = red[1]; hi_i = red[2]; hi_j = red[3];
 #pragma unroll
-    for (int k = 1; k < kThreads / 32; ++k) {
+    for (int k = 1; k < NW; ++k) {
         lo_i = min(lo_i, red[k * 4 + 0]); lo_j = min(lo_j, red[k * 4 + 1]);
         hi_i = max(hi_i, red[k * 4 + 2]); hi_j = max(hi_j, red[k * 4 + 3]);
+    }
+    bool track_all = false;
+#pragma unroll
+    for (int f = T0 ? 1 : 0; f < NF; ++f) {
+        unsigned long long t = 0;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) t += static_cast<unsigned>(red[NW * 4 + f * NW + k]);
+        track_all = track_all || (t >= 2147483648ull);
     }
     if (hi_i < lo_i) { lo_i = hi_i = 0; lo_j = hi_j = 0; }   // no valid particle
     w.ir = ir; w.jr = jr;
@@ -263,16 +291,25 @@ __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, 
     w.H = hi_j - lo_j + 2;
     w.use = static_cast<long long>(w.W) * w.H <= wmaxc;
     w.WH = w.use ? w.W * w.H : 0;
+    w.track_all = track_all;
 }
 
-// The window holds each (field, cell) sum as two int32 words written with
-// native 32-bit shared atomics: lo accumulates the low 16 bits of every added
-// value (unsigned) and hi its arithmetic high part (v >> 16), so
-// sum = hi * 2^16 + lo exactly. A chunk adds at most kChunk values of
-// magnitude < 2^25 to one entry: lo < 2^27 and |hi| < 2^20, no overflow.
-// Layout: plane 2f = lo of field f, plane 2f + 1 = hi, each W*H cells.
+// Window storage: field f owns planes 2f and 2f + 1 (W*H int32 words each).
+// Plain field (its chunk sums provably fit int32): plane 2f holds the sums,
+// added with plain 32-bit shared atomics. Tracked field: plane 2f holds the sum
+// modulo 2^32 and plane 2f + 1 the net number of times it wrapped past the
+// int32 range; each add reads the old value back (the atomic's return), so a
+// crossing is seen by exactly the add that made it (|v| < 2^25 crosses at most
+// once), and sum = (int32) plane_2f + 2^32 * plane_2f+1 exactly.
+template <bool T0>
+__device__ __forceinline__ bool tracked(const Win& w, int f) { return w.track_all || (T0 && f == 0); }
+__device__ __forceinline__ void add_tracked(int* e, int WH, int v) {
+    const int old = atomicAdd(e, v);
+    const int nw = static_cast<int>(static_cast<unsigned>(old) + static_cast<unsigned>(v));
+    if (((old ^ nw) & (v ^ nw)) < 0) atomicAdd(e + WH, v > 0 ? 1 : -1);
+}
 
-// Zero NF window planes; the caller syncs afterwards.
+// Zero the window; the caller syncs afterwards.
 template <int NF>
 __device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
     const int m = 2 * NF * w.WH;
@@ -281,7 +318,7 @@ __device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
 
 // Flush the window into the global int64 accumulators acc[f*ncell + cell].
 // The caller syncs before calling.
-template <int NF>
+template <int NF, bool T0>
 __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& w,
                                           unsigned long long* __restrict__ acc, const Geo& g) {
     for (int c = threadIdx.x; c < w.WH; c += kThreads) {
@@ -289,9 +326,8 @@ __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& 
         const int gc = wrap_far(w.jr + w.mj + wj, g.ny) * g.nx + wrap_far(w.ir + w.mi + wi, g.nx);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            const unsigned lo = static_cast<unsigned>(s[2 * f * w.WH + c]);
-            const int hi = s[(2 * f + 1) * w.WH + c];
-            const long long v = static_cast<long long>(hi) * 65536 + static_cast<long long>(lo);
+            long long v = s[2 * f * w.WH + c];
+            if (tracked<T0>(w, f)) v += static_cast<long long>(s[(2 * f + 1) * w.WH + c]) * 4294967296ll;
             if (v != 0)
                 atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gc, static_cast<unsigned long long>(v));
         }
@@ -319,7 +355,7 @@ __device__ __forceinline__ unsigned qbits(float a, float b) {
 // Per-lane run accumulator: contributions of consecutive particles that share
 // a base window cell, as sums of qbits (mod 2^32). A run holds at most 8
 // particles, so the exact sum fits in int32 after removing cnt * magic.
-template <int NF>
+template <int NF, bool T0>
 struct Run {
     int cw;                 // window cell of the run's base corner (-1 = empty)
     unsigned cnt;
@@ -338,23 +374,31 @@ struct Run {
             for (int k = 0; k < 4; ++k) a[f][k] += qbits(cs[f], wv[k]);
         ++cnt;
     }
-    // Add the run into the split window planes (lo, hi) of each field.
+    // Add the run into the window: field 0 wrap-tracked when T0, the others
+    // plain; every field tracked in a chunk that needs it.
     __device__ __forceinline__ void flush(int* __restrict__ s, const Win& w) {
         if (cw < 0) return;
         const unsigned m = cnt * kMagicU;
         const int offs[4] = {0, 1, w.W, w.W + 1};
+        if (!w.track_all) {
 #pragma unroll
-        for (int f = 0; f < NF; ++f)
+            for (int f = 0; f < NF; ++f) {
+                int* e = s + 2 * f * w.WH + cw;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int v = static_cast<int>(a[f][k] - m);
-                if (v != 0) {
-                    int* e = s + 2 * f * w.WH + cw + offs[k];
-                    const int lo = v & 0xFFFF, hi = v >> 16;
-                    if (lo != 0) atomicAdd(e, lo);
-                    if (hi != 0) atomicAdd(e + w.WH, hi);
+                for (int k = 0; k < 4; ++k) {
+                    const int v = static_cast<int>(a[f][k] - m);
+                    if (T0 && f == 0) add_tracked(e + offs[k], w.WH, v);
+                    else if (v != 0) atomicAdd(e + offs[k], v);
                 }
             }
+        } else {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                int* e = s + 2 * f * w.WH + cw;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) add_tracked(e + offs[k], w.WH, static_cast<int>(a[f][k] - m));
+            }
+        }
     }
 };
 
@@ -501,12 +545,12 @@ __device__ __forceinline__ void slow_pass(const float* __restrict__ stage, const
 // registers; lanes sit 64 particles apart, so their run flushes rarely meet in
 // one shared-atomic instruction. Particles whose staged x has its sign bit set
 // (invalid or listed for the slow pass) are skipped.
-template <int NF, int NS, class CoefFn>
+template <int NF, int NS, bool T0, class CoefFn>
 __device__ __forceinline__ void window_pass(const float* __restrict__ stage, int* __restrict__ win,
                                             const Win& wn, const Geo& g, CoefFn coef) {
     if (!wn.use) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    Run<NF> run;
+    Run<NF, T0> run;
     run.cw = -1;
     run.cnt = 0;
     float4 v[NS];

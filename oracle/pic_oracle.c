@@ -260,20 +260,22 @@ void or_finalize(const int64_t* acc, int nf, int32_t ncell, const float* S, floa
 }
 
 /* ---- deposit scales (same float arithmetic as the CUDA make_src_scales) ------- */
-float or_scale_for_bound(float b) {
+static float scale_top(float b, int top) {
     if (!(b > 0.0f) || !(b < 3.0e38f)) return 1.0f;
     int e;
     frexpf(b, &e);
-    int k = 22 - e;
+    int k = top - e;
     if (k > 120) k = 120;
     if (k < -120) k = -120;
     return ldexpf(1.0f, k);
 }
 
+float or_scale_for_bound(float b) { return scale_top(b, 22); }
+
 void or_src_scales(float cm, const float umax[3], float cref, float S[8]) {
     float U[3];
     for (int d = 0; d < 3; ++d) U[d] = fmaxf(1.25f * umax[d], 0.01f * cref);
-    S[0] = or_scale_for_bound(cm);
+    S[0] = scale_top(cm, 22);
     S[1] = or_scale_for_bound(cm * U[0]);
     S[2] = or_scale_for_bound(cm * U[1]);
     S[3] = or_scale_for_bound(cm * U[2]);
