@@ -29,10 +29,12 @@
 //   window  block-wide bounding box -> shared window of NF exact sums per cell
 //           in int32 words (native 32-bit shared atomics; wrap-tracked where
 //           a chunk's sum could leave the int32 range).
-//   pass 2  each lane deposits 8 consecutive particles from the stage, summing
-//           same-cell runs exactly in integer registers; lanes of a warp sit 64
-//           particles apart (different cells), so each run's flush is a set of
-//           conflict-free shared atomics.
+//   pass 2  each lane deposits 8 particles from the stage, every rounded
+//           contribution one native 32-bit shared atomic; lanes of a warp sit
+//           64 particles apart (different cells), so a warp's atomics rarely
+//           meet on one address. (Same-cell register runs were tried: particle
+//           order decays within a few steps and the divergent run flushes cost
+//           more than they save.)
 //   flush   window -> global int64 accumulators (red.global.add.u64), then the
 //           slow list straight into the global accumulators (exact products).
 #include "aw_internal.h"

@@ -15,11 +15,12 @@
 //                             thread mapping or atomics scheduling.
 //   * window deposit engine — one CTA owns a chunk of kChunk consecutive
 //                             particles, reduces the bounding box of their cells,
-//                             privatises that window of cells in shared memory as
-//                             int64 accumulators ([NF][W*H]), sums each lane's
-//                             same-cell runs exactly in int32 registers, adds the
-//                             runs with shared atomics and flushes the window into
-//                             the global int64 accumulators (red.global.add.u64).
+//                             privatises that window of cells in shared memory,
+//                             adds every rounded contribution with a native
+//                             32-bit shared atomic (exact: the per-chunk sums
+//                             provably fit, or the adds are wrap-tracked) and
+//                             flushes the window into the global int64
+//                             accumulators (red.global.add.u64).
 //
 // Reference arithmetic being mirrored (paths relative to the ArcWarden tree):
 //   CIC weights           include/pic/grid.hpp:135-155, depositor.hpp:136-146
@@ -299,7 +300,7 @@ __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, 
 // added with plain 32-bit shared atomics. Tracked field: plane 2f holds the sum
 // modulo 2^32 and plane 2f + 1 the net number of times it wrapped past the
 // int32 range; each add reads the old value back (the atomic's return), so a
-// crossing is seen by exactly the add that made it (|v| < 2^25 crosses at most
+// crossing is seen by exactly the add that made it (|v| < 2^22 crosses at most
 // once), and sum = (int32) plane_2f + 2^32 * plane_2f+1 exactly.
 template <bool T0>
 __device__ __forceinline__ bool tracked(const Win& w, int f) { return w.track_all || (T0 && f == 0); }
@@ -337,70 +338,18 @@ __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& 
 // Wrapped offset of a cell from the window's reference cell.
 __device__ __forceinline__ int win_off(int c, int r, int n) { return wrap_signed(c - r, n); }
 
-// Stage layout. The pass-1 writes (one float4 = 4 consecutive particles per
-// thread, consecutive quads across lanes) and the pass-2 reads (lane l reads
-// quads 16l + c, i.e. lanes 64 particles apart) are both conflict-free when
-// quad q is stored at quad position q ^ ((q >> 4) & 7).
-__device__ __forceinline__ int stage_quad(int q) { return q ^ ((q >> 4) & 7); }
-__device__ __forceinline__ float4 stq_c(const float* st, int f, int q) {
-    return reinterpret_cast<const float4*>(st + f * kChunk)[stage_quad(q)];
-}
+// Stage layout: chunk slot s is stored at s ^ ((s >> 6) & 31). Pass 1 writes
+// 32 consecutive slots per warp instruction (one aligned group of 32, permuted
+// within itself: conflict-free, and a warp only ever touches its own groups, so
+// the rewrite can be done in place); pass 2 reads slot 64 l + c in lane l, which
+// lands in bank (c ^ l) mod 32: conflict-free as well.
+__device__ __forceinline__ int stage_slot(int s) { return s ^ ((s >> 6) & 31); }
 
-// Exact quantisation of the product a*b: rint(a*b) via one FFMA against
-// 1.5*2^23 (|a*b| < 2^22); the raw bits are summed and the magic removed later.
-__device__ __forceinline__ unsigned qbits(float a, float b) {
-    return __float_as_uint(__fmaf_rn(a, b, kMagic));
+// Exact quantisation of a contribution: rint(a*b) with one FFMA against
+// 1.5*2^23 (exact for |a*b| < 2^22), read back as an integer.
+__device__ __forceinline__ int quant(float a, float b) {
+    return __float_as_int(__fmaf_rn(a, b, kMagic)) - kMagicBits;
 }
-
-// Per-lane run accumulator: contributions of consecutive particles that share
-// a base window cell, as sums of qbits (mod 2^32). A run holds at most 8
-// particles, so the exact sum fits in int32 after removing cnt * magic.
-template <int NF, bool T0>
-struct Run {
-    int cw;                 // window cell of the run's base corner (-1 = empty)
-    unsigned cnt;
-    unsigned a[NF][4];
-    __device__ __forceinline__ void start(int c) {
-        cw = c; cnt = 0;
-#pragma unroll
-        for (int f = 0; f < NF; ++f)
-#pragma unroll
-            for (int k = 0; k < 4; ++k) a[f][k] = 0u;
-    }
-    __device__ __forceinline__ void add(const float (&cs)[NF], const float (&wv)[4]) {
-#pragma unroll
-        for (int f = 0; f < NF; ++f)
-#pragma unroll
-            for (int k = 0; k < 4; ++k) a[f][k] += qbits(cs[f], wv[k]);
-        ++cnt;
-    }
-    // Add the run into the window: field 0 wrap-tracked when T0, the others
-    // plain; every field tracked in a chunk that needs it.
-    __device__ __forceinline__ void flush(int* __restrict__ s, const Win& w) {
-        if (cw < 0) return;
-        const unsigned m = cnt * kMagicU;
-        const int offs[4] = {0, 1, w.W, w.W + 1};
-        if (!w.track_all) {
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                int* e = s + 2 * f * w.WH + cw;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int v = static_cast<int>(a[f][k] - m);
-                    if (T0 && f == 0) add_tracked(e + offs[k], w.WH, v);
-                    else if (v != 0) atomicAdd(e + offs[k], v);
-                }
-            }
-        } else {
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                int* e = s + 2 * f * w.WH + cw;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) add_tracked(e + offs[k], w.WH, static_cast<int>(a[f][k] - m));
-            }
-        }
-    }
-};
 
 // Exact slow path: every contribution straight into the global int64 planes.
 template <int NF>
@@ -419,12 +368,6 @@ __device__ __forceinline__ void deposit_global(int ci, int cj, const float (&wv)
         }
 }
 
-// Element e (0..3, run-time) of a float4: a select chain, no local memory.
-__device__ __forceinline__ float sel(const float4& v, int e) {
-    return e == 0 ? v.x : (e == 1 ? v.y : (e == 2 ? v.z : v.w));
-}
-// Stage position of chunk slot s (quads swizzled, see stage_quad).
-__device__ __forceinline__ int stage_slot(int s) { return (stage_quad(s >> 2) << 2) | (s & 3); }
 
 // ---------------------------------------------------------------------------
 // Chunk loads with the bulk-copy engine (TMA, cp.async.bulk, no multicast): one
@@ -540,44 +483,48 @@ __device__ __forceinline__ void slow_pass(const float* __restrict__ stage, const
     if (n) atomicAdd(&st->slow, static_cast<unsigned long long>(n));
 }
 
-// Window pass: lane l of warp w deposits the 8 consecutive particles
-// 64l + 8w .. 64l + 8w + 7 (quads 16l + 2w + {0,1}), summing same-cell runs in
-// registers; lanes sit 64 particles apart, so their run flushes rarely meet in
-// one shared-atomic instruction. Particles whose staged x has its sign bit set
-// (invalid or listed for the slow pass) are skipped.
-template <int NF, int NS, bool T0, class CoefFn>
-__device__ __forceinline__ void window_pass(const float* __restrict__ stage, int* __restrict__ win,
-                                            const Win& wn, const Geo& g, CoefFn coef) {
-    if (!wn.use) return;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    Run<NF, T0> run;
-    run.cw = -1;
-    run.cnt = 0;
-    float4 v[NS];
+// Window pass: lane l of warp w deposits the chunk slots 64 l + 8 w + k,
+// k = 0..7, one particle at a time: each of its NF x 4 rounded contributions is
+// one native 32-bit shared atomic into the window (field 0 wrap-tracked when
+// T0; every field when the chunk needs it). Lanes sit 64 particles apart, so a
+// warp's atomics fall on different cells. Particles whose staged x has its sign
+// bit set (invalid, or listed for the slow pass) are skipped.
+template <int NF, int NS, bool T0, bool TRACK_ALL, class CoefFn>
+__device__ __forceinline__ void window_particles(const float* __restrict__ stage, int* __restrict__ win,
+                                                 const Win& wn, const Geo& g, CoefFn coef) {
+    const int base = 64 * (threadIdx.x & 31) + 8 * (threadIdx.x >> 5);
+    const int offs[4] = {0, 1, wn.W, wn.W + 1};
 #pragma unroll 1
-    for (int k = 0; k < 8; ++k) {
-        if ((k & 3) == 0) {
-            const int q = 16 * lane + 2 * warp + (k >> 2);
-#pragma unroll
-            for (int f = 0; f < NS; ++f) v[f] = stq_c(stage, f, q);
-        }
-        const int e = k & 3;
+    for (int k = 0; k < kPPT; ++k) {
+        const int d = stage_slot(base + k);
         float a[NS];
 #pragma unroll
-        for (int f = 0; f < NS; ++f) a[f] = sel(v[f], e);
+        for (int f = 0; f < NS; ++f) a[f] = stage[f * kChunk + d];
         if (__float_as_int(a[0]) < 0) continue;
         const Cic c = cic(a[0], a[1]);
         float cs[NF];
         coef(a, cs);
         const float wv[4] = {c.w0, c.w1, c.w2, c.w3};
         const int cw = (win_off(c.j0, wn.jr, g.ny) - wn.mj) * wn.W + (win_off(c.i0, wn.ir, g.nx) - wn.mi);
-        if (cw != run.cw) {
-            run.flush(win, wn);
-            run.start(cw);
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            int* e = win + 2 * f * wn.WH + cw;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int v = quant(cs[f], wv[q]);
+                if (TRACK_ALL || (T0 && f == 0)) add_tracked(e + offs[q], wn.WH, v);
+                else atomicAdd(e + offs[q], v);
+            }
         }
-        run.add(cs, wv);
     }
-    run.flush(win, wn);
+}
+
+template <int NF, int NS, bool T0, class CoefFn>
+__device__ __forceinline__ void window_pass(const float* __restrict__ stage, int* __restrict__ win,
+                                            const Win& wn, const Geo& g, CoefFn coef) {
+    if (!wn.use) return;
+    if (wn.track_all) window_particles<NF, NS, T0, true>(stage, win, wn, g, coef);
+    else window_particles<NF, NS, T0, false>(stage, win, wn, g, coef);
 }
 
 }  // namespace aw

@@ -278,7 +278,8 @@ def run_ours(args, wl, rank, world, dist):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "fp32 (deposits: int64 fixed point; diagnostics: fp64)",
+        "dtype": "f32",
+        "numerics": "f32 push/gather/solve; deposits exact int64 fixed point; diagnostics f64",
         "data": "synthetic: reference seeded loader streams (noisy load, seed 0)",
         "config": {"workload": wl["desc"], "field_model": "darwin" if wl["model"] else "electrostatic",
                    "grid": [wl["nx"], wl["ny"]], "particles_per_gpu": n, "graph": True,
