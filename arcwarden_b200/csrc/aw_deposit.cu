@@ -54,9 +54,11 @@ template <> struct SetNF<SET_RHOJ> { static constexpr int NF = 4, NS = 6; };   /
 template <> struct SetNF<SET_AMU>  { static constexpr int NF = 4, NS = 6; };
 template <> struct SetNF<SET_ALL>  { static constexpr int NF = 8, NS = 6; };
 
-// Window capacity in cells for NF fields (2 int32 planes each). The NF = 8 push kernel keeps
-// two CTAs per SM with its 48 KB stage; the ES push kernel keeps three.
-constexpr int wmax_cells(int nf) { return nf == 1 ? 2048 : (nf == 3 ? 2048 : (nf == 4 ? 1536 : 896)); }
+// Window capacity in cells for NF fields (2 int32 planes each), sized so the
+// push and dcu kernels keep three CTAs per SM next to their 48 KB stage. A
+// chunk of 2048 particles covers ~30-250 cells at 64 per cell; a chunk whose
+// window does not fit takes the exact slow path.
+constexpr int wmax_cells(int nf) { return nf == 1 ? 2048 : (nf == 3 ? 896 : (nf == 4 ? 1536 : 320)); }
 constexpr int kRedInts = kThreads / 32 * (4 + 8);
 // stage [np][kChunk] f32 | window [2*nf][wmax] i32 | red ints | slow list u16[kChunk]
 constexpr size_t win_offset(int np) { return static_cast<size_t>(np) * kChunk * 4; }
@@ -346,7 +348,7 @@ __device__ __forceinline__ void dcu_scales(const DevState* st, float abs_qm, boo
 }
 
 // dcu deposit: input x y w ux uy uz; stage = x, y, ax, ay, az (scaled coefficients).
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 3)
 k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restrict__ gb,
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st, int use_rms,
               float* __restrict__ psq) {
@@ -527,7 +529,7 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
 
 // Fused Darwin step kernel: input x y w ux uy uz; stage = new x, y, w, ux, uy, uz.
 template <bool POW2>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 3)
 k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                   double qoa, unsigned long long* __restrict__ acc, int wmaxc,
                   double* __restrict__ part, DevState* st, float* __restrict__ psq) {
