@@ -78,6 +78,7 @@ SIGNATURES = {
     "aw_sources_bind": [_P, C.POINTER(SourcePtrs)],
     "aw_fields_bind": [_P, C.POINTER(FieldPtrs)],
     "aw_load_species": [_P, C.POINTER(Species), _I32, _U64, _I32],
+    "aw_deposit_rho_noalloc": [C.POINTER(Grid), _D, _P, _P, _P, _P, _P, _P, _I64, _P, _P],
     "aw_deposit_rho": [_P], "aw_deposit_rho_j": [_P], "aw_deposit_amu": [_P], "aw_deposit_dcu": [_P],
     "aw_push_es": [_P], "aw_push_em": [_P], "aw_half_step_back": [_P], "aw_migrate": [_P],
     "aw_sort_tiles": [_P, _I32, _I32, _I32],

@@ -194,6 +194,23 @@ int aw_add_pump(aw_ctx* ctx, double t);
 int aw_fft_r2c(aw_ctx* ctx, const float* in, void* kspace);
 int aw_fft_c2r(aw_ctx* ctx, void* kspace, float* out);
 
+/* Charge deposit with no context and no device allocation. No counterpart in
+ * the reference: it serves callers that cannot call cudaMalloc (a framework or
+ * memory pool that owns every device allocation, or a run that must not grow
+ * its device footprint). Same result as aw_deposit_rho: rho[ny][nx] += the
+ * fixed-point deposit of the n particles (all six SoA arrays are read; the
+ * scales come from their maxima). Work is enqueued on `stream` (a
+ * cudaStream_t, NULL = legacy default stream).
+ * Scratch is one static device array in the library (about 3 MiB, held by
+ * every GPU that loads the library until exit), so grids are limited to
+ * 262144 cells (AW_ERR_ARG beyond); each call clears the part it uses first,
+ * and calls that overlap on the GPU race on it. The first call on a device
+ * looks up the array's address (cudaGetSymbolAddress, with that device
+ * current) and should come before any stream capture. */
+int aw_deposit_rho_noalloc(const aw_grid* g, double qm, const float* x, const float* y,
+                           const float* ux, const float* uy, const float* uz, const float* w,
+                           int64_t n, float* rho, void* stream);
+
 /* ---- the fused, graph-capturable step (the product hot path) -------------
  * Simulation<Cfg>::init, include/pic/simulation.hpp:56-77: ES deposits, solves
  * and rolls u back half a step; Darwin computes the t = 0 fields. Synchronises. */
