@@ -78,6 +78,7 @@ SIGNATURES = {
     "aw_sources_bind": [_P, C.POINTER(SourcePtrs)],
     "aw_fields_bind": [_P, C.POINTER(FieldPtrs)],
     "aw_load_species": [_P, C.POINTER(Species), _I32, _U64, _I32],
+    "aw_resort": [_P], "aw_set_resort": [_P, _I32],
     "aw_deposit_rho_noalloc": [C.POINTER(Grid), _D, _P, _P, _P, _P, _P, _P, _I64, _P, _P],
     "aw_deposit_rho": [_P], "aw_deposit_rho_j": [_P], "aw_deposit_amu": [_P], "aw_deposit_dcu": [_P],
     "aw_push_es": [_P], "aw_push_em": [_P], "aw_half_step_back": [_P], "aw_migrate": [_P],
@@ -206,6 +207,14 @@ class Context:
 
     def sort_tiles(self, tx=16, ty=16, physical=False):
         _check(self.lib.aw_sort_tiles(self.h, tx, ty, int(bool(physical))))
+
+    def resort(self):
+        """Stable spatial re-sort of the bound particles (permutes them in place)."""
+        _check(self.lib.aw_resort(self.h))
+
+    def set_resort(self, every: int):
+        """Re-sort inside run() before every step n with n % every == 0 (0 = never)."""
+        _check(self.lib.aw_set_resort(self.h, int(every)))
 
     def tile_bins(self):
         off, idx, nt, ntx = C.c_void_p(), C.c_void_p(), C.c_int32(), C.c_int32()

@@ -89,7 +89,8 @@ void free_all(Ctx& c) {
     for (cufftHandle* h : plans) if (*h) cufftDestroy(*h);
     void* bufs[] = {c.st, c.acc_src, c.acc_dcu, c.r_src, c.r_out, c.r_dcu, c.r_et, c.k_src, c.k_out,
                     c.k_dcu, c.k_et, c.gb_es, c.gb_dcu, c.gb_push, c.part_p, c.part_c, c.part_d, c.part_g, c.diag,
-                    c.bin_count, c.bin_off, c.bin_cursor, c.bin_idx, c.sort_tmp, c.fft_work};
+                    c.bin_count, c.bin_off, c.bin_cursor, c.bin_idx, c.sort_tmp, c.fft_work, c.rs_buf,
+                    c.rs_temp};
     for (void* b : bufs) if (b) cudaFree(b);
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
 }
@@ -216,6 +217,7 @@ int aw_ctx_create(const aw_grid* g, const aw_params* p, int32_t model, void* str
         c.grid = *g;
         c.prm = *p;
         c.model = model;
+        c.resort_every = (model == AW_MODEL_DARWIN) ? 50 : 0;
         c.geo.nx = g->nx; c.geo.ny = g->ny;
         c.geo.nxf = static_cast<float>(g->nx); c.geo.nyf = static_cast<float>(g->ny);
         c.geo.dx = g->Lx / g->nx; c.geo.dy = g->Ly / g->ny;
@@ -654,8 +656,13 @@ int aw_run(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph) {
         aw::require_parts(c);
         aw::ensure_pending(c);
         aw::launch_set_step(c, n0);
+        // periodic re-sort (between steps, never inside the captured step)
+        auto resort_before = [&](int64_t i) {
+            const int64_t s = n0 + i;
+            if (c.resort_every > 0 && s > 0 && s % c.resort_every == 0) aw::launch_resort(c);
+        };
         if (!use_graph) {
-            for (int64_t i = 0; i < nsteps; ++i) aw::step_body(c);
+            for (int64_t i = 0; i < nsteps; ++i) { resort_before(i); aw::step_body(c); }
             return;
         }
         if (!c.gexec) {
@@ -671,7 +678,26 @@ int aw_run(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph) {
             AW_CUDA(cudaStreamEndCapture(c.stream, &c.graph));
             AW_CUDA(cudaGraphInstantiate(&c.gexec, c.graph, 0));
         }
-        for (int64_t i = 0; i < nsteps; ++i) AW_CUDA(cudaGraphLaunch(c.gexec, c.stream));
+        for (int64_t i = 0; i < nsteps; ++i) {
+            resort_before(i);
+            AW_CUDA(cudaGraphLaunch(c.gexec, c.stream));
+        }
+    });
+}
+
+int aw_set_resort(aw_ctx* ctx, int32_t every) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::need(every >= 0, AW_ERR_ARG, "set_resort: negative interval");
+        ctx->c.resort_every = every;
+    });
+}
+
+int aw_resort(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::require_parts(ctx->c);
+        aw::launch_resort(ctx->c);
     });
 }
 

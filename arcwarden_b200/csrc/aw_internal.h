@@ -91,6 +91,10 @@ struct Ctx {
     int  bin_ntiles = 0, bin_ntx = 0, bin_tx = 0, bin_ty = 0, bin_cap = 0;
     bool bin_physical = false;
     float* sort_tmp = nullptr; long long sort_tmp_n = 0;   // 7 arrays of n
+    // periodic re-sort (aw_resort.cu): keys/values in and out, radix-sort scratch
+    int* rs_buf = nullptr; long long rs_n = 0;
+    void* rs_temp = nullptr; size_t rs_temp_bytes = 0;
+    int resort_every = 0;             // aw_run re-sorts before every step n with n % resort_every == 0
     // scales for unfused deposits
     bool have_static_scales = false;
 
@@ -125,6 +129,7 @@ void launch_push_es_from(Ctx& c, const float* ex, const float* ey, float dt_scal
 void launch_push_em_plain(Ctx& c, const float* unused);
 void launch_particle_max(Ctx& c);                  // ucur_bits, coef_max
 void launch_sort_tiles(Ctx& c, int tx, int ty, bool physical);
+void launch_resort(Ctx& c);                        // stable spatial re-sort of the SoA (aw_resort.cu)
 void launch_particle_diag(Ctx& c);                 // KE, P partials -> part_p
 
 // ---- launchers (aw_deposit.cu) --------------------------------------------

@@ -301,6 +301,29 @@ def run_ours(args, wl, rank, world, dist):
     return res
 
 
+def profile_case(wl, steps):
+    """The workload's fused step launched step by step (for ncu captures)."""
+    import torch
+    import arcwarden_b200 as aw
+    dev = torch.device("cuda", 0)
+    n = nparticles(wl)
+    ctx = aw.Context(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], dt=wl["dt"], c=wl["c"], n0=wl["n0"], B0=wl["B0"],
+                     model=wl["model"], stream=torch.cuda.current_stream(dev).cuda_stream, pump=wl["pump"])
+    P = {k: torch.empty(n, dtype=torch.float32, device=dev) for k in ("x", "y", "ux", "uy", "uz", "w")}
+    cell = torch.empty(n, dtype=torch.int32, device=dev)
+    ctx.bind_particles(P["x"], P["y"], P["ux"], P["uy"], P["uz"], P["w"], cell)
+    ctx.load_species(wl["species"], seed=0, noisy=True)
+    ctx.init()
+    for s in range(steps):
+        ctx.step(s)
+    torch.cuda.synchronize(dev)
+    err = ctx.error_word()
+    ctx.close()
+    if err:
+        raise SystemExit(f"device error word {err:#x}")
+    print(f"profile case {wl['name']}: {steps} steps of {n} particles", flush=True)
+
+
 def run_reference(args, wl, rank, world):
     """The reference's own implementation of the step: its CUDA Simulation built
     from its headers (oracle/_ref) when present, else the oracle port on CPU."""
@@ -344,6 +367,9 @@ def main():
     ap.add_argument("--workload", default="weibel512")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-case", type=int, default=0, metavar="K",
+                    help="profiling case for ncu: load, aw_init and K single aw_step launches (no graph, no "
+                         "timing, no JSON line)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -358,6 +384,9 @@ def main():
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
+    if args.profile_case:
+        profile_case(wl, args.profile_case)
+        return
     try:
         if args.impl == "reference":
             res = run_reference(args, wl, rank, world)

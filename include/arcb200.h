@@ -169,6 +169,17 @@ int aw_migrate(aw_ctx* ctx);
  * include/pic/particles.hpp:632-726: keys tile = (j/ty)*ntx + i/tx from cell.
  * The permutation (physical == 0) or the tile offsets are kept in the context. */
 int aw_sort_tiles(aw_ctx* ctx, int32_t tx, int32_t ty, int32_t physical);
+/* Stable spatial re-sort of the bound particle SoA (x, y, ux, uy, uz, w and
+ * cell are permuted together, in place) by tiles of about 1024 particles.
+ * Keeps the fused kernels' per-chunk cell windows compact as particles mix;
+ * results do not depend on particle order. The reference reorders its Darwin
+ * particles by tile every step (Particles::sort_by_tile,
+ * include/pic/particles.hpp:678-726); this sort is deterministic. */
+int aw_resort(aw_ctx* ctx);
+/* aw_run re-sorts before every step n > 0 with n % every == 0 (0 = never).
+ * Default: 50 for the Darwin model, 0 for the electrostatic model, whose
+ * reference path keeps the particle order. */
+int aw_set_resort(aw_ctx* ctx, int32_t every);
 /* Device pointers to the last tile binning: off[ntiles+1], idx[n] (idx is NULL
  * after a physical sort), and the tile geometry (BinViews, particles.hpp:63-69). */
 int aw_tile_bins(aw_ctx* ctx, const int32_t** off, const int32_t** idx,
