@@ -321,12 +321,12 @@ __device__ __forceinline__ void gather_em(const float* __restrict__ gb, const Ci
     const float4 a1 = __ldg(q + 2 * (r0 + i1)), b1 = __ldg(q + 2 * (r0 + i1) + 1);
     const float4 a2 = __ldg(q + 2 * (r1 + i0)), b2 = __ldg(q + 2 * (r1 + i0) + 1);
     const float4 a3 = __ldg(q + 2 * (r1 + i1)), b3 = __ldg(q + 2 * (r1 + i1) + 1);
-    ex = gather4(s, a0.x, a1.x, a2.x, a3.x);
-    ey = gather4(s, a0.y, a1.y, a2.y, a3.y);
-    ez = gather4(s, a0.z, a1.z, a2.z, a3.z);
-    bx = gather4(s, a0.w, a1.w, a2.w, a3.w);
-    by = gather4(s, b0.x, b1.x, b2.x, b3.x);
-    bz = gather4(s, b0.y, b1.y, b2.y, b3.y);
+    ex = gather4_tile(s, a0.x, a1.x, a2.x, a3.x);
+    ey = gather4_tile(s, a0.y, a1.y, a2.y, a3.y);
+    ez = gather4_tile(s, a0.z, a1.z, a2.z, a3.z);
+    bx = gather4_tile(s, a0.w, a1.w, a2.w, a3.w);
+    by = gather4_tile(s, b0.x, b1.x, b2.x, b3.x);
+    bz = gather4_tile(s, b0.y, b1.y, b2.y, b3.y);
 }
 
 // dcu scales: |coef_dcu (E + v x B)| <= |qm| coef_max (Emax + 2 Umax Bmax); in

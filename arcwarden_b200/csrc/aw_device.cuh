@@ -133,10 +133,22 @@ __device__ __forceinline__ Cic cic(float x, float y) {
     s.w3 = __fmul_rn(fx, fy);
     return s;
 }
-// four-term gather in the reference order: ((w0 a + w1 b) + w2 c) + w3 d
+// four-term gather in the reference order: ((w0 a + w1 b) + w2 c) + w3 d.
+// gather4: the ES gather, accumulated from zero term by term
+// (include/pic/pusher.hpp:35-43), so w0 a is rounded and each later term fused.
 __device__ __forceinline__ float gather4(const Cic& s, float a, float b, float c, float d) {
     float r = __fmul_rn(s.w0, a);
     r = __fmaf_rn(s.w1, b, r);
+    r = __fmaf_rn(s.w2, c, r);
+    r = __fmaf_rn(s.w3, d, r);
+    return r;
+}
+// gather4_tile: the shared-tile gathers of the EM push and the dcu deposit, one
+// expression w0*a + w1*b + w2*c + w3*d (pusher.hpp:244-246, depositor.hpp:300-302),
+// whose compiled form fuses w0 a and rounds w1 b in the first pair; checked bit
+// for bit against that code's outputs.
+__device__ __forceinline__ float gather4_tile(const Cic& s, float a, float b, float c, float d) {
+    float r = __fmaf_rn(s.w0, a, __fmul_rn(s.w1, b));
     r = __fmaf_rn(s.w2, c, r);
     r = __fmaf_rn(s.w3, d, r);
     return r;

@@ -128,7 +128,7 @@ __global__ void k_push_em_plain(Parts p, Geo g, EMF f, float qmh, double dt) {
     const int i0 = wrap_once(s.i0, g.nx), i1 = wrap_once(s.i0 + 1, g.nx);
     const int j0 = wrap_once(s.j0, g.ny) * g.nx, j1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
     const int c0 = j0 + i0, c1 = j0 + i1, c2 = j1 + i0, c3 = j1 + i1;
-#define AWG(a) gather4(s, __ldg(a + c0), __ldg(a + c1), __ldg(a + c2), __ldg(a + c3))
+#define AWG(a) gather4_tile(s, __ldg(a + c0), __ldg(a + c1), __ldg(a + c2), __ldg(a + c3))
     const float Ex = AWG(f.ex), Ey = AWG(f.ey), Ez = AWG(f.ez);
     const float Bx = AWG(f.bx), By = AWG(f.by), Bz = AWG(f.bz);
 #undef AWG

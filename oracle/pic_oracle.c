@@ -36,10 +36,20 @@ static inline void corners(const cic_t* s, int nx, int ny, int c[4]) {
     const int r0 = s->j0 * nx, r1 = wrap_once(s->j0 + 1, ny) * nx;
     c[0] = r0 + s->i0; c[1] = r0 + i1; c[2] = r1 + s->i0; c[3] = r1 + i1;
 }
-/* ((w0 a + w1 b) + w2 c) + w3 d with fused multiply-adds, pusher.hpp:35-43 */
+/* ((w0 a + w1 b) + w2 c) + w3 d with fused multiply-adds. ES gather,
+ * pusher.hpp:35-43 (accumulated from zero): w0 a rounded, later terms fused. */
 static inline float gather4(const cic_t* s, float a, float b, float c, float d) {
     float r = s->w[0] * a;
     r = fmaf(s->w[1], b, r);
+    r = fmaf(s->w[2], c, r);
+    r = fmaf(s->w[3], d, r);
+    return r;
+}
+/* Shared-tile gathers of the EM push and the dcu deposit (pusher.hpp:244-246,
+ * depositor.hpp:300-302): w0 a fused with the rounded w1 b first. Pinned bit for
+ * bit against the reference's EM push (tests/golden/ref_push.npz). */
+static inline float gather4_tile(const cic_t* s, float a, float b, float c, float d) {
+    float r = fmaf(s->w[0], a, s->w[1] * b);
     r = fmaf(s->w[2], c, r);
     r = fmaf(s->w[3], d, r);
     return r;
@@ -176,7 +186,7 @@ void or_deposit_dcu(const or_geo* g, const float* x, const float* y, const float
             float v[6];
             for (int q = 0; q < 6; ++q) {
                 const int o = (q < 4) ? q : q;   /* gb layout: Ex Ey Ez Bx By Bz */
-                v[q] = gather4(&s, gb[(size_t)c[0] * 8 + o], gb[(size_t)c[1] * 8 + o],
+                v[q] = gather4_tile(&s, gb[(size_t)c[0] * 8 + o], gb[(size_t)c[1] * 8 + o],
                                gb[(size_t)c[2] * 8 + o], gb[(size_t)c[3] * 8 + o]);
             }
             const float ex = v[0], ey = v[1], ez = v[2], bx = v[3], by = v[4], bz = v[5];
@@ -239,7 +249,7 @@ void or_deposit_dcu_f64(const or_geo* g, const float* x, const float* y, const f
         corners(&s, nx, ny, c);
         float v[6];
         for (int q = 0; q < 6; ++q)
-            v[q] = gather4(&s, gb[(size_t)c[0] * 8 + q], gb[(size_t)c[1] * 8 + q], gb[(size_t)c[2] * 8 + q],
+            v[q] = gather4_tile(&s, gb[(size_t)c[0] * 8 + q], gb[(size_t)c[1] * 8 + q], gb[(size_t)c[2] * 8 + q],
                            gb[(size_t)c[3] * 8 + q]);
         const float vx = ux[p], vy = uy[p], vz = uz[p];
         const float coef = (float)(qm2oa * (double)w[p]);
@@ -341,8 +351,8 @@ void or_push_em(const or_geo* g, float* x, float* y, float* ux, float* uy, float
         corners(&s, nx, ny, c);
         float v[6];
         for (int q = 0; q < 6; ++q)
-            v[q] = gather4(&s, gb[(size_t)c[0] * 8 + q], gb[(size_t)c[1] * 8 + q],
-                           gb[(size_t)c[2] * 8 + q], gb[(size_t)c[3] * 8 + q]);
+            v[q] = gather4_tile(&s, gb[(size_t)c[0] * 8 + q], gb[(size_t)c[1] * 8 + q],
+                                gb[(size_t)c[2] * 8 + q], gb[(size_t)c[3] * 8 + q]);
         float u = ux[p], vv = uy[p], wz = uz[p];
         u = fmaf(qmh, v[0], u); vv = fmaf(qmh, v[1], vv); wz = fmaf(qmh, v[2], wz);
         boris_rotate(&u, &vv, &wz, v[3], v[4], v[5], qmh);
