@@ -179,6 +179,21 @@ def cpu_baseline(wl, budget_s=15.0, max_steps=None):
 
 
 # ---------------------------------------------------------------------------
+def max_over_ranks(x: float, dist, device) -> float:
+    """The slowest rank's time: every rank takes the same all-reduce (MAX)."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_result(res: dict | None, rank: int) -> str | None:
+    """The JSON line only rank 0 prints (None on the other ranks)."""
+    return json.dumps(res) if rank == 0 and res is not None else None
+
+
 def run_ours(args, wl, rank, world, dist):
     import ctypes
     import torch
@@ -223,10 +238,7 @@ def run_ours(args, wl, rank, world, dist):
     err = ctx.error_word()
     if err:
         raise SystemExit(f"device error word {err:#x} after the timed steps")
-    if dist is not None:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, dev)
 
     # roofline of the dominant kernel: per-phase CUDA events on the step's stream
     phases = [ctx.step_profile(n0 + args.steps + i) for i in range(5)]
@@ -259,10 +271,7 @@ def run_ours(args, wl, rank, world, dist):
             out_host[k].copy_(P[k], non_blocking=True)
     stream.synchronize()
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist, dev)
     diag_last = diag_host[(K - 1) * 8:(K - 1) * 8 + 8].tolist()
     if not all(math.isfinite(v) for v in diag_last):
         raise SystemExit("non-finite diagnostics in the end-to-end run")
@@ -394,8 +403,9 @@ def main():
             res = run_ours(args, wl, rank, world, dist)
             if rank == 0 and not args.no_cpu_baseline:
                 res["cpu_baseline"] = cpu_baseline(wl)
-        if rank == 0 and res is not None:
-            print(json.dumps(res), flush=True)
+        line = rank_result(res, rank)
+        if line is not None:
+            print(line, flush=True)
     finally:
         if dist is not None:
             dist.destroy_process_group()
