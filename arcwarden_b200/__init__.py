@@ -47,6 +47,13 @@ SOURCE_NAMES = ("rho", "Jx", "Jy", "Jz", "dcux", "dcuy", "dcuz", "amu0", "amu1",
 FIELD_NAMES = ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "ELx", "ELy", "ETx", "ETy", "ETz")
 
 
+class LegacyLoad(C.Structure):
+    _fields_ = [("ppc", C.c_int32), ("weight", C.c_double), ("vth", C.c_double), ("vd", C.c_double),
+                ("two_stream", C.c_int32), ("bump_on_tail", C.c_int32), ("beam_frac", C.c_double),
+                ("beam_vd", C.c_double), ("beam_vth", C.c_double), ("perturb_amp", C.c_double),
+                ("perturb_kx", C.c_int32), ("noisy", C.c_int32), ("seed", C.c_uint64)]
+
+
 class SourcePtrs(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in SOURCE_NAMES]
 
@@ -79,6 +86,7 @@ SIGNATURES = {
     "aw_fields_bind": [_P, C.POINTER(FieldPtrs)],
     "aw_load_species": [_P, C.POINTER(Species), _I32, _U64, _I32],
     "aw_resort": [_P], "aw_set_resort": [_P, _I32],
+    "aw_load_legacy": [_P, C.POINTER(LegacyLoad)],
     "aw_deposit_rho_noalloc": [C.POINTER(Grid), _D, _P, _P, _P, _P, _P, _P, _I64, _P, _P],
     "aw_deposit_rho": [_P], "aw_deposit_rho_j": [_P], "aw_deposit_amu": [_P], "aw_deposit_dcu": [_P],
     "aw_push_es": [_P], "aw_push_em": [_P], "aw_half_step_back": [_P], "aw_migrate": [_P],
@@ -207,6 +215,14 @@ class Context:
 
     def sort_tiles(self, tx=16, ty=16, physical=False):
         _check(self.lib.aw_sort_tiles(self.h, tx, ty, int(bool(physical))))
+
+    def load_legacy(self, ppc, weight, vth=0.0, vd=0.0, two_stream=False, bump_on_tail=False, beam_frac=0.0,
+                    beam_vd=0.0, beam_vth=0.0, perturb_amp=0.0, perturb_kx=1, noisy=False, seed=0):
+        """Single-species RunParams load (Particles::initialize(rp, g, s))."""
+        L = LegacyLoad(int(ppc), float(weight), float(vth), float(vd), int(bool(two_stream)),
+                       int(bool(bump_on_tail)), float(beam_frac), float(beam_vd), float(beam_vth),
+                       float(perturb_amp), int(perturb_kx), int(bool(noisy)), int(seed))
+        _check(self.lib.aw_load_legacy(self.h, C.byref(L)))
 
     def resort(self):
         """Stable spatial re-sort of the bound particles (permutes them in place)."""

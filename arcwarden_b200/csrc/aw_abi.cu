@@ -376,6 +376,21 @@ int aw_load_species(aw_ctx* ctx, const aw_species* sp, int32_t nspecies, uint64_
     });
 }
 
+int aw_load_legacy(aw_ctx* ctx, const aw_legacy_load* L) {
+    return guarded([&] {
+        aw::need(ctx && L, AW_ERR_ARG, "null argument");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        aw::need(L->ppc > 0, AW_ERR_ARG, "load_legacy: ppc must be positive");
+        aw::need(static_cast<long long>(L->ppc) * c.geo.ncell == c.parts.n, AW_ERR_ARG,
+                 "load_legacy: bound n != ppc*nx*ny");
+        aw::need(c.parts.n <= 0x7fffffffLL, AW_ERR_ARG, "load_legacy: more than 2^31-1 particles");
+        aw::launch_load_legacy(c, *L);
+        c.pending_valid = false;
+        c.inited = false;
+    });
+}
+
 // ---- unfused operators ---------------------------------------------------------
 
 int aw_deposit_rho(aw_ctx* ctx) {

@@ -122,6 +122,7 @@ struct Ctx {
 // ---- launchers (aw_particles.cu) -------------------------------------------
 void launch_load_species(Ctx& c, const aw_species& sp, int index, long long base,
                          uint64_t seed, int noisy);
+void launch_load_legacy(Ctx& c, const aw_legacy_load& L);
 void launch_migrate(Ctx& c);
 // Gathers from the caller's Ex/Ey; dt_scale = 1 (push) or -0.5 (half-step back).
 void launch_push_es_plain(Ctx& c, const float* unused, float dt_scale, bool move);

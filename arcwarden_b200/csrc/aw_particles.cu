@@ -86,6 +86,69 @@ __global__ void k_load_species(Parts p, Geo g, LoadArgs a) {
     p.uz[t] = static_cast<float>(a.ufl[2] + r2 * a.uth[2] * erfinv(2.0 * qz - 1.0));
 }
 
+// Single-species load of RunParams (Particles::initialize(rp, g, s),
+// particle_init_kernel, include/pic/particles.hpp:211-289): particle t sits in
+// cell t / ppc; quiet or hashed sub-cell offsets; an optional single-k density
+// seed displaces x; ux is a drifting Maxwellian, two counter-streaming beams
+// (by within-cell parity) or bump-on-tail (the first beam_frac of each cell);
+// uy, uz use the bulk width.
+struct LegacyArgs {
+    int ppc;
+    float weight;
+    double vth, vd;
+    int two_stream, bump_on_tail;
+    double beam_frac, beam_vd, beam_vth;
+    double perturb_amp;
+    int perturb_kx;
+    int noisy;
+    unsigned long seed;
+};
+
+__global__ void k_load_legacy(Parts p, Geo g, LegacyArgs a) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= p.n) return;
+    const int c = t / a.ppc, s = t % a.ppc;
+    const int i = c % g.nx, j = c / g.nx;
+    const float fx = a.noisy ? static_cast<float>(uniform_open(t, 0, a.seed))
+                             : static_cast<float>(radical_inverse_d(s + 1, 2));
+    const float fy = a.noisy ? static_cast<float>(uniform_open(t, 1, a.seed))
+                             : static_cast<float>(radical_inverse_d(s + 1, 3));
+    float x = static_cast<float>(i) + fx;
+    const float y = static_cast<float>(j) + fy;
+    if (a.perturb_amp != 0.0) {
+        const float kx = 6.28318530717958648f * a.perturb_kx / static_cast<float>(g.nx);
+        x = __fmaf_rn(static_cast<float>(a.perturb_amp), sinf(kx * x), x);
+        x = fmodf(x, static_cast<float>(g.nx));
+        if (x < 0.0f) x += static_cast<float>(g.nx);
+    }
+    int ci = static_cast<int>(x);
+    if (ci >= g.nx) ci = g.nx - 1;
+    float xw = x, yw = y;
+    if (xw >= (float)g.nx) xw = nextafterf((float)g.nx, 0.f);
+    if (yw >= (float)g.ny) yw = nextafterf((float)g.ny, 0.f);
+    p.x[t] = xw;
+    p.y[t] = yw;
+    p.w[t] = a.weight;
+    if (p.cell) p.cell[t] = j * g.nx + ci;
+    const double qx = a.noisy ? uniform_open(t, 2, a.seed) : radical_inverse_d(t + 1, 5);
+    const double qy = a.noisy ? uniform_open(t, 3, a.seed) : radical_inverse_d(t + 1, 7);
+    const double qz = a.noisy ? uniform_open(t, 4, a.seed) : radical_inverse_d(t + 1, 11);
+    double drift_x = a.vd, width_x = a.vth;
+    if (a.bump_on_tail) {
+        const int n_beam = static_cast<int>(a.beam_frac * a.ppc + 0.5);
+        const bool beam = s < n_beam;
+        drift_x = beam ? a.beam_vd : 0.0;
+        width_x = beam ? a.beam_vth : a.vth;
+    } else if (a.two_stream) {
+        drift_x = (s & 1) ? -a.vd : a.vd;
+    }
+    const double r2 = 1.41421356237309515;
+    const double s2 = r2 * a.vth;
+    p.ux[t] = static_cast<float>(drift_x + r2 * width_x * erfinv(2.0 * qx - 1.0));
+    p.uy[t] = static_cast<float>(s2 * erfinv(2.0 * qy - 1.0));
+    p.uz[t] = static_cast<float>(s2 * erfinv(2.0 * qz - 1.0));
+}
+
 // ---------------------------------------------------------------------------
 __global__ void k_migrate(Parts p, Geo g) {
     const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -310,6 +373,18 @@ void launch_load_species(Ctx& c, const aw_species& sp, int index, long long base
     a.noisy = noisy;
     a.seed = static_cast<unsigned long>(seed);
     k_load_species<<<grid_for(a.count), kThreads, 0, c.stream>>>(c.parts, c.geo, a);
+    AW_LAUNCH();
+}
+
+void launch_load_legacy(Ctx& c, const aw_legacy_load& L) {
+    LegacyArgs a{};
+    a.ppc = L.ppc; a.weight = static_cast<float>(L.weight);
+    a.vth = L.vth; a.vd = L.vd;
+    a.two_stream = L.two_stream; a.bump_on_tail = L.bump_on_tail;
+    a.beam_frac = L.beam_frac; a.beam_vd = L.beam_vd; a.beam_vth = L.beam_vth;
+    a.perturb_amp = L.perturb_amp; a.perturb_kx = L.perturb_kx;
+    a.noisy = L.noisy; a.seed = static_cast<unsigned long>(L.seed);
+    k_load_legacy<<<grid_for(c.parts.n), kThreads, 0, c.stream>>>(c.parts, c.geo, a);
     AW_LAUNCH();
 }
 

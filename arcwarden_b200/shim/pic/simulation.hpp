@@ -1,0 +1,125 @@
+// pic/simulation.hpp (B200 shim) — Simulation<Cfg> (include/pic/simulation.hpp:
+// 41-126) on libarcb200's fused step. init() loads the particles, allocates the
+// reference's Sources/Fields, creates a library context bound to them and runs
+// aw_init; every step() is one replay of the captured step graph (aw_run),
+// followed by the reference's host diagnostics when they are due.
+#ifndef ARC_PIC_SIMULATION_HPP
+#define ARC_PIC_SIMULATION_HPP
+
+#include "pic/config.hpp"
+#include "pic/cuda_utils.hpp"
+#include "pic/depositor.hpp"
+#include "pic/diagnostics.hpp"
+#include "pic/fields.hpp"
+#include "pic/grid.hpp"
+#include "pic/particles.hpp"
+#include "pic/pump.hpp"
+#include "pic/pusher.hpp"
+#include "pic/solver_darwin.hpp"
+#include "pic/solver_es.hpp"
+#include "pic/sources.hpp"
+#include "pic/species.hpp"
+#include "pic/spectral.hpp"
+
+#include "../arcb200_shim.hpp"
+
+#include <string>
+
+namespace arc {
+
+template <class Cfg = arc::Cfg>
+class Simulation {
+public:
+    Simulation(const Grid& g, const RunParams& rp, const std::string& csv = "")
+        : p_(rp), grid_(g), spectral_(g), diag_(csv) {
+        diag_.set_geometry(g.dx, g.dy);
+    }
+    Simulation(const Grid& g, const RunParams& rp, const SpeciesList& species, const std::string& csv = "")
+        : p_(rp), grid_(g), species_(species), spectral_(g), diag_(csv) {
+        diag_.set_geometry(g.dx, g.dy);
+    }
+    ~Simulation() {
+        if (ctx_) aw_ctx_destroy(ctx_);
+    }
+    Simulation(const Simulation&) = delete;
+    Simulation& operator=(const Simulation&) = delete;
+
+    static constexpr bool darwin() { return Cfg::field_model == FieldModel::Darwin; }
+
+    // Load, allocate, t = 0 fields (and, for ES, the half-step velocity rollback).
+    void init() {
+        if (!species_.empty()) particles_.initialize(species_, grid_, p_, stream_);
+        else particles_.initialize(p_, grid_, stream_);
+        sources_.allocate(grid_);
+        fields_.allocate(grid_);
+        if constexpr (darwin()) {
+            sources_.allocate_em(grid_);
+            fields_.allocate_em(grid_, stream_);
+            spectral_.enable_em();
+        }
+        if (!ctx_) {
+            const aw_grid ag = shim::grid_of(grid_);
+            const aw_params ap = shim::params(p_, Cfg::has_b0);
+            shim::check(aw_ctx_create(&ag, &ap, darwin() ? AW_MODEL_DARWIN : AW_MODEL_ES, stream_.get(), &ctx_),
+                        "ctx_create");
+        }
+        particles_.bind(ctx_);
+        shim::bind_sources(ctx_, sources_);
+        shim::bind_fields(ctx_, fields_);
+        shim::check(aw_init(ctx_), "init");
+    }
+
+    // One PIC step (the fused graph), then the diagnostics when due.
+    void step(long n) {
+        shim::check(aw_run(ctx_, n, 1, 1), "run");
+        diag_.maybe_compute(n, particles_.views(), sources_, fields_, p_, stream_);
+    }
+
+    void run() {
+        for (long n = 0; n < p_.nsteps; ++n) step(n);
+        stream_.synchronize();
+    }
+
+    // The Darwin field solve for the current particle state, from the separate
+    // operators (deposits, E_L + B, dcu, E_T, E_total + pump).
+    void darwin_fields(double t, cudaStream_t s) {
+        sources_.zero_rho_j(s);
+        sources_.zero_dcu_amu(s);
+        Depositor<Cfg>::charge_current_sorted(particles_, sources_, grid_, p_, s);
+        Depositor<Cfg>::deposit_amu(particles_, sources_, grid_, p_, s);
+        dsolver_.solve_el_b(sources_, fields_, spectral_, p_, s);
+        add_background_b0(fields_, grid_, p_, s);
+        dsolver_.form_el(fields_, s);
+        add_pump_field(fields_, grid_, p_, t, s);
+        sources_.zero_dcu(s);
+        Depositor<Cfg>::deposit_dcu(particles_, sources_, fields_, grid_, p_, s);
+        dsolver_.solve_et(sources_, fields_, spectral_, p_, s);
+        dsolver_.form_etotal(fields_, s);
+        add_pump_field(fields_, grid_, p_, t, s);
+    }
+
+    const Diagnostics& diagnostics() const { return diag_; }
+    const Fields&      fields() const { return fields_; }
+    const RunParams&   params() const { return p_; }
+    const Particles&   particles() const { return particles_; }
+    Particles&         particles() { return particles_; }
+    const Grid&        grid() const { return grid_; }
+
+private:
+    RunParams      p_;
+    Grid           grid_;
+    SpeciesList    species_;
+    Particles      particles_;
+    Sources        sources_;
+    Fields         fields_;
+    SpectralEngine spectral_;
+    ElectrostaticSpectralSolver solver_;
+    DarwinSpectralSolver        dsolver_;
+    Diagnostics    diag_;
+    CudaStream     stream_;
+    aw_ctx*        ctx_ = nullptr;
+};
+
+}  // namespace arc
+
+#endif  // ARC_PIC_SIMULATION_HPP

@@ -144,6 +144,24 @@ int aw_fields_bind(aw_ctx* ctx, const aw_field_ptrs* f);
 int aw_load_species(aw_ctx* ctx, const aw_species* sp, int32_t nspecies,
                     uint64_t seed, int32_t noisy);
 
+/* Single-species load from RunParams: Particles::initialize(rp, g, s) with
+ * particle_init_kernel, include/pic/particles.hpp:211-289 and 509-516. Fills
+ * the bound SoA (n = ppc * nx * ny): uniform weight, quiet or noisy sub-cell
+ * positions, an optional single-k density seed, and a drifting Maxwellian,
+ * two-stream or bump-on-tail ux; the same streams as the reference. */
+typedef struct aw_legacy_load {
+    int32_t  ppc;
+    double   weight;
+    double   vth, vd;
+    int32_t  two_stream, bump_on_tail;
+    double   beam_frac, beam_vd, beam_vth;
+    double   perturb_amp;
+    int32_t  perturb_kx;
+    int32_t  noisy;
+    uint64_t seed;
+} aw_legacy_load;
+int aw_load_legacy(aw_ctx* ctx, const aw_legacy_load* load);
+
 /* ---- operators (unfused; each matches one reference launch sequence) ------ */
 
 /* Depositor<Cfg>::charge, include/pic/depositor.hpp:440-496: rho += deposit. */

@@ -226,6 +226,34 @@ extern "C" int ref_load(int nx, int ny, double Lx, double Ly, const ref_species*
     });
 }
 
+// The single-species RunParams load, Particles::initialize(rp, g, s).
+// f[] = weight, vth, vd, beam_frac, beam_vd, beam_vth, perturb_amp;
+// i[] = ppc, two_stream, bump_on_tail, perturb_kx, noisy.
+extern "C" int ref_load_legacy(int nx, int ny, double Lx, double Ly, const double* f, const int* i,
+             unsigned long seed, float* x, float* y, float* ux, float* uy, float* uz, float* w, int* cell) {
+    return guard([&] {
+        Grid g(nx, ny, Lx, Ly);
+        ref_params p{};
+        p.dt = 0.1; p.qm = -1; p.eps0 = 1; p.n0 = 1; p.c = 1;
+        RunParams rp = make_rp(&p, i[4], seed);
+        rp.weight = f[0]; rp.vth = f[1]; rp.vd = f[2];
+        rp.beam_frac = f[3]; rp.beam_vd = f[4]; rp.beam_vth = f[5]; rp.perturb_amp = f[6];
+        rp.ppc = i[0]; rp.two_stream = i[1] != 0; rp.bump_on_tail = i[2] != 0; rp.perturb_kx = i[3];
+        CudaStream s;
+        Particles P;
+        P.initialize(rp, g, s);
+        s.synchronize();
+        const size_t b = P.n * 4;
+        CUDA_CHECK(cudaMemcpy(x, P.x.data(), b, cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(y, P.y.data(), b, cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(ux, P.ux.data(), b, cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(uy, P.uy.data(), b, cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(uz, P.uz.data(), b, cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(w, P.w.data(), b, cudaMemcpyDeviceToHost));
+        CUDA_CHECK(cudaMemcpy(cell, P.cell.data(), b, cudaMemcpyDeviceToHost));
+    });
+}
+
 static void upload(Particles& P, long n, const float* x, const float* y, const float* ux,
                    const float* uy, const float* uz, const float* w, const Grid& g, cudaStream_t s) {
     P.allocate_n(static_cast<size_t>(n));

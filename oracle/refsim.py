@@ -52,6 +52,7 @@ def lib():
         L.ref_get.argtypes = [P, C.c_char_p, P]
         L.ref_set_particles.argtypes = [P] + [P] * 6
         L.ref_load.argtypes = [I, I, D, D, C.POINTER(RefSpecies), I, I, C.c_ulong] + [P] * 7
+        L.ref_load_legacy.argtypes = [I, I, D, D, P, P, C.c_ulong] + [P] * 7
         L.ref_deposit.argtypes = [I, I, I, D, D, D, L_] + [P] * 8
         L.ref_push.argtypes = [I, I, I, D, D, C.POINTER(RefParams), L_] + [P] * 7 + [I]
         L.ref_solve.argtypes = [I, I, I, D, D, C.POINTER(RefParams), P, P]
@@ -152,6 +153,19 @@ def load(nx, ny, Lx, Ly, sp, noisy=True, seed=0):
     out["cell"] = np.zeros(n, np.int32)
     _chk(lib().ref_load(nx, ny, Lx, Ly, arr, ns, int(noisy), seed,
                         *[_p(out[k]) for k in ("x", "y", "ux", "uy", "uz", "w", "cell")]))
+    return out
+
+
+def load_legacy(nx, ny, Lx, Ly, ppc, weight, vth=0.0, vd=0.0, two_stream=False, bump_on_tail=False,
+                beam_frac=0.0, beam_vd=0.0, beam_vth=0.0, perturb_amp=0.0, perturb_kx=1, noisy=False, seed=0):
+    """Particles::initialize(rp, g, s): the single-species RunParams load."""
+    n = ppc * nx * ny
+    out = {k: np.zeros(n, np.float32) for k in ("x", "y", "ux", "uy", "uz", "w")}
+    out["cell"] = np.zeros(n, np.int32)
+    f = np.array([weight, vth, vd, beam_frac, beam_vd, beam_vth, perturb_amp], np.float64)
+    i = np.array([ppc, int(two_stream), int(bump_on_tail), perturb_kx, int(noisy)], np.int32)
+    _chk(lib().ref_load_legacy(nx, ny, Lx, Ly, _p(f), _p(i), seed,
+                               *[_p(out[k]) for k in ("x", "y", "ux", "uy", "uz", "w", "cell")]))
     return out
 
 

@@ -1,0 +1,29 @@
+"""The reference's own tests of this path, compiled unchanged against the C++
+shim (arcwarden_b200/shim: the reference's API on libarcb200) and run on the
+GPU. Each program prints its own checks and exits non-zero on failure.
+
+The programs are built by `make -C arcwarden_b200/shim` (part of
+__graft_entry__.build()) where the reference sources are available; a test is
+skipped when its program was not built.
+"""
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+BUILD = ROOT / "arcwarden_b200" / "shim" / "_build"
+TESTS = ["test_charge_conservation", "test_poisson_sine", "test_darwin_magnetostatic", "test_fft_roundtrip",
+         "test_single_particle", "test_magnetized_boris", "test_particle_load", "test_two_stream", "test_weibel",
+         "test_langmuir", "test_conservation_longrun", "test_diagnostics"]
+
+
+@pytest.mark.parametrize("name", TESTS)
+def test_reference_test_passes_on_the_library(torch_cuda, name):
+    exe = BUILD / name
+    if not exe.exists():
+        pytest.skip(f"{name} not built (make -C arcwarden_b200/shim)")
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
