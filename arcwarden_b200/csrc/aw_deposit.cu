@@ -237,7 +237,7 @@ __device__ __forceinline__ void close_window(const Smem& m, const Win& wn, int n
 // ---------------------------------------------------------------------------
 // Standalone source deposit at the current positions.
 template <int SET>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 3)
 k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st, float* __restrict__ psq) {
     constexpr int NF = SetNF<SET>::NF, NS = SetNF<SET>::NS;
@@ -276,8 +276,9 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
             if (in_grid(a[0], a[1], g)) {
                 bb.add(static_cast<int>(a[0]), static_cast<int>(a[1]), ir, jr, g);
                 float cf[NF], cs[NF];
-                if constexpr (NS == 6) src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), a[3], a[4], a[5], cf);
-                else src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), 0.f, 0.f, 0.f, cf);
+                a[2] = __double2float_rn(qoa * static_cast<double>(a[2]));    // staged: the coefficient
+                if constexpr (NS == 6) src_coefs<SET>(a[2], a[3], a[4], a[5], cf);
+                else src_coefs<SET>(a[2], 0.f, 0.f, 0.f, cf);
                 const bool fast = scale_fast<NF>(cf, S, cs, l1);
                 if (psq) {
 #pragma unroll
@@ -299,8 +300,8 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
     const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
         float cf[NF];
-        if constexpr (NS == 6) src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), a[3], a[4], a[5], cf);
-        else src_coefs<SET>(__double2float_rn(qoa * static_cast<double>(a[2])), 0.f, 0.f, 0.f, cf);
+        if constexpr (NS == 6) src_coefs<SET>(a[2], a[3], a[4], a[5], cf);
+        else src_coefs<SET>(a[2], 0.f, 0.f, 0.f, cf);
 #pragma unroll
         for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cf[f], S[f]);
     };
@@ -440,7 +441,7 @@ __device__ __forceinline__ void move_xy(float& x, float& y, float ux, float uy, 
     }
 }
 
-// Fused ES step kernel: input x y w ux uy uz; stage = new x, y, w.
+// Fused ES step kernel: input x y w ux uy uz; stage = new x, y, coefficient q w / (dx dy).
 template <bool POW2>
 __global__ void __launch_bounds__(kThreads, 3)
 k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
@@ -475,7 +476,7 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
         float x = m.stage[s], y = m.stage[kChunk + s];
         const float w = m.stage[2 * kChunk + s];
         float ux = m.stage[3 * kChunk + s], uy = m.stage[4 * kChunk + s], uz = m.stage[5 * kChunk + s];
-        float xs = -1.0f;
+        float xs = -1.0f, cf0 = 0.0f;
         if (s < cnt) {
             if (in_grid(x, y, g)) {
                 const Cic c = cic(x, y);
@@ -493,7 +494,8 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                 if (pp.write_cell && p.cell) p.cell[i] = cj * g.nx + ci;
                 if (in_grid(x, y, g)) {
                     bb.add(ci, cj, ir, jr, g);
-                    const float cf[1] = {__double2float_rn(qoa * static_cast<double>(w))};
+                    cf0 = __double2float_rn(qoa * static_cast<double>(w));
+                    const float cf[1] = {cf0};
                     float cs[1];
                     const bool fast = scale_fast<1>(cf, S1, cs, l1);
                     xs = __fadd_rn(x, 0.0f);
@@ -512,11 +514,11 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
         const int d = stage_slot(s);
         m.stage[d] = xs;
         m.stage[kChunk + d] = y;
-        m.stage[2 * kChunk + d] = w;
+        m.stage[2 * kChunk + d] = cf0;
     }
     const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
-        cs[0] = __fmul_rn(__double2float_rn(qoa * static_cast<double>(a[2])), S1[0]);
+        cs[0] = __fmul_rn(a[2], S1[0]);
     };
     window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
@@ -527,7 +529,7 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     }
 }
 
-// Fused Darwin step kernel: input x y w ux uy uz; stage = new x, y, w, ux, uy, uz.
+// Fused Darwin step kernel: input x y w ux uy uz; stage = new x, y, coefficient, ux, uy, uz.
 template <bool POW2>
 __global__ void __launch_bounds__(kThreads, 3)
 k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
@@ -568,7 +570,7 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
         float x = m.stage[s], y = m.stage[kChunk + s];
         const float w = m.stage[2 * kChunk + s];
         float ux = m.stage[3 * kChunk + s], uy = m.stage[4 * kChunk + s], uz = m.stage[5 * kChunk + s];
-        float xs = -1.0f;
+        float xs = -1.0f, cf0 = 0.0f;
         if (s < cnt) {
             if (in_grid(x, y, g)) {
                 const Cic c = cic(x, y);
@@ -584,7 +586,8 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                 if (in_grid(x, y, g)) {
                     bb.add(ci, cj, ir, jr, g);
                     float cf[NF], cs[NF];
-                    src_coefs<SET_ALL>(__double2float_rn(qoa * static_cast<double>(w)), ux, uy, uz, cf);
+                    cf0 = __double2float_rn(qoa * static_cast<double>(w));
+                    src_coefs<SET_ALL>(cf0, ux, uy, uz, cf);
                     const bool fast = scale_fast<NF>(cf, S, cs, l1);
 #pragma unroll
                     for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
@@ -605,7 +608,7 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
         const int d = stage_slot(s);
         m.stage[d] = xs;
         m.stage[kChunk + d] = y;
-        m.stage[2 * kChunk + d] = w;
+        m.stage[2 * kChunk + d] = cf0;
         m.stage[3 * kChunk + d] = ux;
         m.stage[4 * kChunk + d] = uy;
         m.stage[5 * kChunk + d] = uz;
@@ -627,7 +630,7 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     }
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
         float cf[NF];
-        src_coefs<SET_ALL>(__double2float_rn(qoa * static_cast<double>(a[2])), a[3], a[4], a[5], cf);
+        src_coefs<SET_ALL>(a[2], a[3], a[4], a[5], cf);
 #pragma unroll
         for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cf[f], S[f]);
     };

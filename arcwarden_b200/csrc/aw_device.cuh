@@ -83,11 +83,6 @@ __device__ __forceinline__ int wrap_once(int i, int n) {
     if (i < 0) i += n;
     return i;
 }
-__device__ __forceinline__ int wrap_far(int i, int n) {
-    i %= n;
-    if (i < 0) i += n;
-    return i;
-}
 // signed offset in [-n/2, n/2) for |d| < n
 __device__ __forceinline__ int wrap_signed(int d, int n) {
     if (d >= (n >> 1)) d -= n;
@@ -334,15 +329,26 @@ __device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
 template <int NF, bool T0>
 __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& w,
                                           unsigned long long* __restrict__ acc, const Geo& g) {
-    for (int c = threadIdx.x; c < w.WH; c += kThreads) {
-        const int wi = c % w.W, wj = c / w.W;
-        const int gc = wrap_far(w.jr + w.mj + wj, g.ny) * g.nx + wrap_far(w.ir + w.mi + wi, g.nx);
+    if (!w.use) return;            // the window was not used (its words are not zeroed)
+    // warp per window row, lanes along the row: no divide per cell, and the
+    // window offsets are < nx, so one conditional add/subtract wraps them
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int wj = warp; wj < w.H; wj += kThreads / 32) {
+        int gj = w.jr + w.mj + wj;
+        if (gj < 0) gj += g.ny;
+        if (gj >= g.ny) gj -= g.ny;
+        for (int wi = lane; wi < w.W; wi += 32) {
+            int gi = w.ir + w.mi + wi;
+            if (gi < 0) gi += g.nx;
+            if (gi >= g.nx) gi -= g.nx;
+            const int c = wj * w.W + wi, gc = gj * g.nx + gi;
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            long long v = s[2 * f * w.WH + c];
-            if (tracked<T0>(w, f)) v += static_cast<long long>(s[(2 * f + 1) * w.WH + c]) * 4294967296ll;
-            if (v != 0)
-                atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gc, static_cast<unsigned long long>(v));
+            for (int f = 0; f < NF; ++f) {
+                long long v = s[2 * f * w.WH + c];
+                if (tracked<T0>(w, f)) v += static_cast<long long>(s[(2 * f + 1) * w.WH + c]) * 4294967296ll;
+                if (v != 0)
+                    atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gc, static_cast<unsigned long long>(v));
+            }
         }
     }
 }

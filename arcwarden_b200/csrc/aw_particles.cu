@@ -11,6 +11,7 @@
 #include "aw_internal.h"
 
 #include <algorithm>
+#include <cmath>
 #include <vector>
 
 namespace aw {
@@ -161,9 +162,10 @@ __global__ void k_migrate(Parts p, Geo g) {
 }
 
 // Unfused ES push / half-step rollback, gathering from [ny][nx] Ex, Ey arrays.
+template <bool POW2>
 __global__ void k_push_es_plain(Parts p, Geo g, const float* __restrict__ ex,
                                 const float* __restrict__ ey, float qmh, int has_b0,
-                                float b0x, float b0y, float b0z, double dt, int move) {
+                                float b0x, float b0y, float b0z, double dt, double dtx, double dty, int move) {
     const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= p.n) return;
     const float x = p.x[t], y = p.y[t];
@@ -176,32 +178,45 @@ __global__ void k_push_es_plain(Parts p, Geo g, const float* __restrict__ ex,
     boris_es(ux, uy, uz, Ex, Ey, qmh, has_b0 != 0, b0x, b0y, b0z);
     p.ux[t] = ux; p.uy[t] = uy; p.uz[t] = uz;
     if (move) {
-        p.x[t] = move1(x, ux, dt, g.dx);
-        p.y[t] = move1(y, uy, dt, g.dy);
+        if constexpr (POW2) {
+            p.x[t] = move1_pow2(x, ux, dtx);
+            p.y[t] = move1_pow2(y, uy, dty);
+        } else {
+            p.x[t] = move1(x, ux, dt, g.dx);
+            p.y[t] = move1(y, uy, dt, g.dy);
+        }
     }
 }
-
-// Unfused EM push (gathered E and B), [ny][nx] arrays.
-struct EMF { const float *ex, *ey, *ez, *bx, *by, *bz; };
-__global__ void k_push_em_plain(Parts p, Geo g, EMF f, float qmh, double dt) {
+// EM push from the packed field buffer gb[ncell][8] = Ex Ey Ez Bx | By Bz . .
+// (two 16-byte loads per CIC corner).
+template <bool POW2>
+__global__ void k_push_em_plain(Parts p, Geo g, const float* __restrict__ gb, float qmh, double dt, double dtx,
+                                double dty) {
     const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= p.n) return;
     const float x = p.x[t], y = p.y[t];
     const Cic s = cic(x, y);
     const int i0 = wrap_once(s.i0, g.nx), i1 = wrap_once(s.i0 + 1, g.nx);
     const int j0 = wrap_once(s.j0, g.ny) * g.nx, j1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
-    const int c0 = j0 + i0, c1 = j0 + i1, c2 = j1 + i0, c3 = j1 + i1;
-#define AWG(a) gather4_tile(s, __ldg(a + c0), __ldg(a + c1), __ldg(a + c2), __ldg(a + c3))
-    const float Ex = AWG(f.ex), Ey = AWG(f.ey), Ez = AWG(f.ez);
-    const float Bx = AWG(f.bx), By = AWG(f.by), Bz = AWG(f.bz);
-#undef AWG
+    const float4* q = reinterpret_cast<const float4*>(gb);
+    const float4 a0 = __ldg(q + 2 * (j0 + i0)), b0 = __ldg(q + 2 * (j0 + i0) + 1);
+    const float4 a1 = __ldg(q + 2 * (j0 + i1)), b1 = __ldg(q + 2 * (j0 + i1) + 1);
+    const float4 a2 = __ldg(q + 2 * (j1 + i0)), b2 = __ldg(q + 2 * (j1 + i0) + 1);
+    const float4 a3 = __ldg(q + 2 * (j1 + i1)), b3 = __ldg(q + 2 * (j1 + i1) + 1);
+    const float Ex = gather4_tile(s, a0.x, a1.x, a2.x, a3.x), Ey = gather4_tile(s, a0.y, a1.y, a2.y, a3.y);
+    const float Ez = gather4_tile(s, a0.z, a1.z, a2.z, a3.z), Bx = gather4_tile(s, a0.w, a1.w, a2.w, a3.w);
+    const float By = gather4_tile(s, b0.x, b1.x, b2.x, b3.x), Bz = gather4_tile(s, b0.y, b1.y, b2.y, b3.y);
     float ux = p.ux[t], uy = p.uy[t], uz = p.uz[t];
     boris_em(ux, uy, uz, Ex, Ey, Ez, Bx, By, Bz, qmh);
     p.ux[t] = ux; p.uy[t] = uy; p.uz[t] = uz;
-    p.x[t] = move1(x, ux, dt, g.dx);
-    p.y[t] = move1(y, uy, dt, g.dy);
+    if constexpr (POW2) {
+        p.x[t] = move1_pow2(x, ux, dtx);
+        p.y[t] = move1_pow2(y, uy, dty);
+    } else {
+        p.x[t] = move1(x, ux, dt, g.dx);
+        p.y[t] = move1(y, uy, dt, g.dy);
+    }
 }
-
 // Max |u_d| and max |qm w/(dx dy)| over the particles -> DevState.
 __global__ void k_particle_max(Parts p, double qm_over_area, DevState* st) {
     float mu0 = 0.f, mu1 = 0.f, mu2 = 0.f, mc = 0.f;
@@ -394,13 +409,20 @@ void launch_migrate(Ctx& c) {
     AW_LAUNCH();
 }
 
+bool pow2_grid(const Ctx& c) {
+    int e;
+    return std::frexp(c.geo.dx, &e) == 0.5 && std::frexp(c.geo.dy, &e) == 0.5;
+}
+
 void launch_push_es_from(Ctx& c, const float* ex, const float* ey, float dt_scale, bool move) {
     if (c.parts.n == 0) return;
     const float dt_eff = dt_scale * static_cast<float>(c.prm.dt);
     const float qmh = static_cast<float>(c.prm.qm) * 0.5f * dt_eff;
-    k_push_es_plain<<<grid_for(c.parts.n), kThreads, 0, c.stream>>>(
-        c.parts, c.geo, ex, ey, qmh, c.prm.has_b0, c.prm.B0[0], c.prm.B0[1], c.prm.B0[2],
-        c.prm.dt, move ? 1 : 0);
+    const double dtx = c.prm.dt / c.geo.dx, dty = c.prm.dt / c.geo.dy;
+    auto kern = pow2_grid(c) ? k_push_es_plain<true> : k_push_es_plain<false>;
+    kern<<<grid_for(c.parts.n), kThreads, 0, c.stream>>>(c.parts, c.geo, ex, ey, qmh, c.prm.has_b0, c.prm.B0[0],
+                                                         c.prm.B0[1], c.prm.B0[2], c.prm.dt, dtx, dty,
+                                                         move ? 1 : 0);
     AW_LAUNCH();
 }
 
@@ -413,12 +435,11 @@ void launch_push_es_plain(Ctx& c, const float* unused, float dt_scale, bool move
 void launch_push_em_plain(Ctx& c, const float* gb_unused) {
     (void)gb_unused;
     if (c.parts.n == 0) return;
-    const aw_field_ptrs& f = c.fld;
-    if (!f.Ex || !f.Ey || !f.Ez || !f.Bx || !f.By || !f.Bz)
-        throw Error(AW_ERR_STATE, "push_em: fields E/B not bound");
-    EMF e{f.Ex, f.Ey, f.Ez, f.Bx, f.By, f.Bz};
+    launch_pack_em(c);          // bound E, B -> gb_dcu [ncell][8] (checks they are bound)
     const float qmh = static_cast<float>(c.prm.qm) * 0.5f * static_cast<float>(c.prm.dt);
-    k_push_em_plain<<<grid_for(c.parts.n), kThreads, 0, c.stream>>>(c.parts, c.geo, e, qmh, c.prm.dt);
+    const double dtx = c.prm.dt / c.geo.dx, dty = c.prm.dt / c.geo.dy;
+    auto kern = pow2_grid(c) ? k_push_em_plain<true> : k_push_em_plain<false>;
+    kern<<<grid_for(c.parts.n), kThreads, 0, c.stream>>>(c.parts, c.geo, c.gb_dcu, qmh, c.prm.dt, dtx, dty);
     AW_LAUNCH();
 }
 

@@ -376,3 +376,27 @@ def test_loader_and_pushes_match_reference_fixtures(setup, aw):
     rows = lambda d: (lambda a: a[np.lexsort(a.T[::-1])])(
         np.stack([np.asarray(d[k], np.float32).view(np.uint32) for k in ("x", "y", "ux", "uy", "uz")], 1))
     assert np.array_equal(rows(q), rows({k: P[f"em_{k}"] for k in ("x", "y", "ux", "uy", "uz")}))
+
+
+@pytest.mark.parametrize("op,fset,keys", [("deposit_rho", 0, ["rho"]), ("deposit_rho_j", 1, ["rho", "Jx", "Jy", "Jz"])])
+def test_deposit_bit_exact_when_windows_overflow(setup, aw, oracle, op, fset, keys):
+    """Particles in random order over a 256 x 256 grid: every chunk's cell window
+    exceeds shared memory, so every particle takes the exact slow path; the
+    result is still the same bits."""
+    nx = ny = 256
+    n = 200_000
+    s = setup(nx, ny, 256.0, 256.0, n, aw.AW_MODEL_DARWIN, dt=0.05)
+    rng = np.random.default_rng(8)
+    vals = {"x": rng.random(n) * nx, "y": rng.random(n) * ny, "ux": rng.normal(0, 0.1, n),
+            "uy": rng.normal(0, 0.1, n), "uz": rng.normal(0, 0.2, n), "w": np.full(n, 0.25)}
+    for k, v in vals.items():
+        s.put(k, v.astype(np.float32))
+    getattr(s.ctx, op)()
+    p = s.parts()
+    st = s.ctx.stats()
+    assert st["window_overflow"] > 0
+    g = oracle.geo(nx, ny, 256.0, 256.0)
+    S, _, _ = _oracle_scales(oracle, p, -1.0)
+    fin = oracle.finalize(oracle.deposit(g, *(p[k] for k in PARTICLE_KEYS[:5]), p["w"], -1.0, S, fset), S)
+    for i, k in enumerate(keys):
+        assert np.array_equal(s.grid(k), fin[i]), k
