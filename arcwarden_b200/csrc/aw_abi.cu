@@ -88,7 +88,7 @@ void free_all(Ctx& c) {
     cufftHandle* plans[] = {&c.p_r2c1, &c.p_c2r1, &c.p_r2cS, &c.p_c2rO, &c.p_r2c3, &c.p_c2r3, &c.p_r2c4};
     for (cufftHandle* h : plans) if (*h) cufftDestroy(*h);
     void* bufs[] = {c.st, c.acc_src, c.acc_dcu, c.r_src, c.r_out, c.r_dcu, c.r_et, c.k_src, c.k_out,
-                    c.k_dcu, c.k_et, c.gb_es, c.gb_dcu, c.gb_push, c.part_p, c.part_c, c.part_d, c.part_g, c.diag,
+                    c.k_dcu, c.k_et, c.gb_es, c.gb_dcu, c.gb_push, c.part_p, c.part_c, c.part_d, c.part_g, c.diag, c.red_rows,
                     c.bin_count, c.bin_off, c.bin_cursor, c.bin_idx, c.sort_tmp, c.fft_work, c.rs_buf,
                     c.rs_temp};
     for (void* b : bufs) if (b) cudaFree(b);
@@ -122,13 +122,13 @@ void reset_acc(Ctx& c, unsigned long long* acc, int nf) {
 // ---- the step body (no host syncs; capturable) --------------------------------
 // A step is a fixed list of phases; `mark(i)` runs after phase i (used by
 // aw_step_profile to record CUDA events between phases).
-constexpr int kPhasesES = 7, kPhasesDarwin = 14;
+constexpr int kPhasesES = 7, kPhasesDarwin = 13;
 const char* const kPhaseNamesES[kPhasesES] = {
-    "finalize_rho", "fft_r2c_rho", "kspace_es", "fft_c2r_e", "fields_es", "push_deposit_es", "diag_reduce"};
+    "finalize_rho", "fft_r2c_rho", "kspace_es", "fft_c2r_e", "fields_es", "push_deposit_es", "step_reduce"};
 const char* const kPhaseNamesDarwin[kPhasesDarwin] = {
     "finalize_src", "fft_r2c_src8", "kspace_elb", "fft_c2r_elb5", "fields_dcu", "deposit_dcu",
     "finalize_dcu", "fft_r2c_dcu3", "kspace_et", "fft_c2r_et3", "fields_push", "push_deposit_em",
-    "rms_reduce", "diag_reduce"};
+    "step_reduce"};
 
 struct NoMark { void operator()(int) const {} };
 
@@ -166,18 +166,17 @@ void step_body(Ctx& c, Mark mark) {
     if (c.model == AW_MODEL_ES) {
         es_fields_from_pending(c, true, mark);
         launch_push_deposit_es(c); mark(5);
-        launch_diag_reduce(c, true); mark(6);
+        launch_step_reduce(c); mark(6);
     } else {
         darwin_fields_from_pending(c, true, mark);
         launch_push_deposit_em(c); mark(11);
-        launch_rms_reduce(c, true, true); mark(12);
-        launch_diag_reduce(c, true); mark(13);
+        launch_step_reduce(c); mark(12);
     }
 }
 void step_body(Ctx& c) { step_body(c, NoMark{}); }
 
 // Kernels of this library one fused step launches (cuFFT's own not counted).
-int kernels_per_step(const Ctx& c) { return c.model == AW_MODEL_ES ? 5 : 10; }
+int kernels_per_step(const Ctx& c) { return c.model == AW_MODEL_ES ? 5 : 9; }
 
 void ensure_pending(Ctx& c) {
     if (c.pending_valid) return;
@@ -238,6 +237,7 @@ int aw_ctx_create(const aw_grid* g, const aw_params* p, int32_t model, void* str
             aw::dalloc(c.st, 1);
             AW_CUDA(cudaMemset(c.st, 0, sizeof(aw::DevState)));
             aw::dalloc(c.diag, 1);
+            aw::dalloc(c.red_rows, static_cast<size_t>(aw::kRedBlocks) * aw::kRedVals);
             AW_CUDA(cudaMemset(c.diag, 0, sizeof(aw_diag)));
             c.npart_g = aw::grid_partial_blocks();
             aw::dalloc(c.part_g, static_cast<size_t>(c.npart_g) * 5);
@@ -304,6 +304,7 @@ int aw_set_stream(aw_ctx* ctx, void* stream) {
 int aw_set_params(aw_ctx* ctx, const aw_params* p) {
     return guarded([&] {
         aw::need(ctx && p, AW_ERR_ARG, "null argument");
+        if (std::memcmp(&ctx->c.prm, p, sizeof(aw_params)) == 0) return;   // unchanged: keep the step graph
         ctx->c.prm = *p;
         aw::drop_graph(ctx->c);
     });
@@ -317,6 +318,10 @@ int aw_particles_bind(aw_ctx* ctx, float* x, float* y, float* ux, float* uy, flo
         aw::need(n == 0 || (x && y && ux && uy && uz && w), AW_ERR_ARG, "particles_bind: null array");
         aw::need(n < (1LL << 40), AW_ERR_ARG, "particles_bind: n too large");
         Ctx& c = ctx->c;
+        // binding the arrays already bound is a no-op (operator wrappers rebind before every call)
+        if (n > 0 && c.parts.n == n && c.parts.x == x && c.parts.y == y && c.parts.ux == ux && c.parts.uy == uy &&
+            c.parts.uz == uz && c.parts.w == w && c.parts.cell == cell)
+            return;
         c.parts.x = x; c.parts.y = y; c.parts.ux = ux; c.parts.uy = uy; c.parts.uz = uz;
         c.parts.w = w; c.parts.cell = cell; c.parts.n = n;
         auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
@@ -342,6 +347,7 @@ int aw_particles_bind(aw_ctx* ctx, float* x, float* y, float* ux, float* uy, flo
 int aw_sources_bind(aw_ctx* ctx, const aw_source_ptrs* s) {
     return guarded([&] {
         aw::need(ctx && s, AW_ERR_ARG, "null argument");
+        if (std::memcmp(&ctx->c.src, s, sizeof(aw_source_ptrs)) == 0) return;
         ctx->c.src = *s;
         aw::drop_graph(ctx->c);
     });
@@ -350,6 +356,7 @@ int aw_sources_bind(aw_ctx* ctx, const aw_source_ptrs* s) {
 int aw_fields_bind(aw_ctx* ctx, const aw_field_ptrs* f) {
     return guarded([&] {
         aw::need(ctx && f, AW_ERR_ARG, "null argument");
+        if (std::memcmp(&ctx->c.fld, f, sizeof(aw_field_ptrs)) == 0) return;
         ctx->c.fld = *f;
         aw::drop_graph(ctx->c);
     });
@@ -448,7 +455,7 @@ int aw_deposit_dcu(aw_ctx* ctx) {
         aw::need(c.model == AW_MODEL_DARWIN, AW_ERR_STATE, "deposit_dcu: Darwin context required");
         aw::need(c.src.dcux && c.src.dcuy && c.src.dcuz, AW_ERR_STATE, "deposit_dcu: dcu not bound");
         aw::launch_particle_max(c);
-        aw::launch_pack_em(c);
+        aw::launch_pack_em(c, true);
         aw::reset_acc(c, c.acc_dcu, 3);
         aw::launch_deposit_dcu(c, c.gb_dcu, false);
         float* api[3] = {c.src.dcux, c.src.dcuy, c.src.dcuz};

@@ -490,8 +490,9 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                 move_xy<POW2>(x, y, ux, uy, pp, g);
                 int ci, cj;
                 cell_ij(x, y, g, ci, cj);
-                p.x[i] = x; p.y[i] = y; p.ux[i] = ux; p.uy[i] = uy; p.uz[i] = uz;
-                if (pp.write_cell && p.cell) p.cell[i] = cj * g.nx + ci;
+                // streaming stores: the new state is not read again this step
+                __stcs(p.x + i, x); __stcs(p.y + i, y); __stcs(p.ux + i, ux); __stcs(p.uy + i, uy); __stcs(p.uz + i, uz);
+                if (pp.write_cell && p.cell) __stcs(p.cell + i, cj * g.nx + ci);
                 if (in_grid(x, y, g)) {
                     bb.add(ci, cj, ir, jr, g);
                     cf0 = __double2float_rn(qoa * static_cast<double>(w));
@@ -580,8 +581,9 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                 move_xy<POW2>(x, y, ux, uy, pp, g);
                 int ci, cj;
                 cell_ij(x, y, g, ci, cj);
-                p.x[i] = x; p.y[i] = y; p.ux[i] = ux; p.uy[i] = uy; p.uz[i] = uz;
-                if (pp.write_cell && p.cell) p.cell[i] = cj * g.nx + ci;
+                // streaming stores: the new state is not read again this step
+                __stcs(p.x + i, x); __stcs(p.y + i, y); __stcs(p.ux + i, ux); __stcs(p.uy + i, uy); __stcs(p.uz + i, uz);
+                if (pp.write_cell && p.cell) __stcs(p.cell + i, cj * g.nx + ci);
                 m0 = fmaxf(m0, fabsf(ux)); m1 = fmaxf(m1, fabsf(uy)); m2 = fmaxf(m2, fabsf(uz));
                 if (in_grid(x, y, g)) {
                     bb.add(ci, cj, ir, jr, g);

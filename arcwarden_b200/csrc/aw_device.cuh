@@ -40,12 +40,17 @@ constexpr int kPPT     = 8;            // particles per thread per chunk
 constexpr int kChunk   = kThreads * kPPT;   // particles per CTA chunk (2048)
 
 // Fast-path range of one quantised contribution: |v*S| < 2^22 rounds exactly
-// with one FFMA against 1.5*2^23; a register run of at most 8 particles sums to
-// < 2^25 (int32), and the shared window planes are int64.
+// with one FFMA against 1.5*2^23. The shared window words are int32: plain adds
+// when a chunk's L1 bound stays below 2^31, wrap-tracked adds with a carry word
+// otherwise.
 constexpr float kFastLim   = 4194304.0f;      // 2^22
 constexpr float kMagic     = 12582912.0f;     // 1.5 * 2^23
 constexpr int   kMagicBits = 0x4B400000;
 constexpr unsigned kMagicU  = 0x4B400000u;
+
+// End-of-step reduction (k_step_reduce): blocks and values per block row.
+constexpr int kRedBlocks = 32;
+constexpr int kRedVals   = 21;   // ke px py pz | se2 me2 q sb2 | 8 src sq + n | 3 dcu sq + n
 
 // Geometry passed by value into every kernel.
 struct Geo {
@@ -74,6 +79,7 @@ struct DevState {
     float     rms_src[8];      // rms of the source deposit coefficients (unscaled)
     float     rms_dcu[4];      // rms of the dcu coefficients (unscaled)
     unsigned long long chunks, overflow, slow;
+    unsigned  red_ticket;      // k_step_reduce blocks finished (reset by the last)
 };
 
 // ---------------------------------------------------------------------------
@@ -405,9 +411,14 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, u
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
 }
+// Bulk copy global -> shared completing on an mbarrier, with an L2 evict-first
+// hint: particle data is streamed once per kernel, and the hint keeps the
+// grids and the int64 accumulator planes resident in L2 instead.
 __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
     unsigned ok;

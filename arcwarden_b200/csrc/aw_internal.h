@@ -85,6 +85,7 @@ struct Ctx {
     double* part_g = nullptr;   // grid partials [nblk][5]
     int     npart_p = 0, npart_g = 0;
     aw_diag* diag = nullptr;    // device aw_diag
+    double* red_rows = nullptr; // k_step_reduce block rows [kRedBlocks][kRedVals]
     // tile binning scratch
     int* bin_count = nullptr; int* bin_off = nullptr; int* bin_cursor = nullptr;
     int* bin_idx = nullptr;   long long bin_idx_n = 0;
@@ -157,11 +158,12 @@ void launch_scale_copy(Ctx& c, float* dst, const float* src, int n, float s);
 void launch_form_e(Ctx& c, float et_scale);
 void launch_add_b0(Ctx& c);
 void launch_add_pump(Ctx& c, double t);
-void launch_pack_em(Ctx& c);
+void launch_pack_em(Ctx& c, bool maxima);
 void launch_grid_diag(Ctx& c);
 void launch_set_step(Ctx& c, long long n);
 void launch_copy_umax(Ctx& c);
 void launch_promote_scales(Ctx& c);                // S_pend = S_next
 void launch_rms_reduce(Ctx& c, bool src, bool dcu);
+void launch_step_reduce(Ctx& c);                   // end of a fused step: diagnostics (+ rms for Darwin)
 
 }  // namespace aw

@@ -435,7 +435,7 @@ void launch_push_es_plain(Ctx& c, const float* unused, float dt_scale, bool move
 void launch_push_em_plain(Ctx& c, const float* gb_unused) {
     (void)gb_unused;
     if (c.parts.n == 0) return;
-    launch_pack_em(c);          // bound E, B -> gb_dcu [ncell][8] (checks they are bound)
+    launch_pack_em(c, false);   // bound E, B -> gb_dcu [ncell][8] (checks they are bound)
     const float qmh = static_cast<float>(c.prm.qm) * 0.5f * static_cast<float>(c.prm.dt);
     const double dtx = c.prm.dt / c.geo.dx, dty = c.prm.dt / c.geo.dy;
     auto kern = pow2_grid(c) ? k_push_em_plain<true> : k_push_em_plain<false>;

@@ -153,6 +153,7 @@ k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
 #pragma unroll
         for (int d = 0; d < 3; ++d) { st->ucur_bits[d] = st->umax_bits[d]; st->umax_bits[d] = 0u; }
         st->emax_bits = 0u; st->bmax_bits = 0u;
+        st->red_ticket = 0u;
         if (darwin) {
             float S[8];
             make_src_scales(st, cref, S, true);
@@ -305,6 +306,20 @@ __global__ void k_fields_es(const float* __restrict__ r, float* __restrict__ gb,
     grid_partials(se2, me2, 0.0, part);
 }
 
+// Block maxima of |E| and |B| components into st (one atomic pair per block).
+__device__ void block_max_eb(float emax, float bmax, DevState* st) {
+    __shared__ unsigned sh[2][kThreads / 32];
+    const unsigned e = __reduce_max_sync(0xffffffffu, __float_as_uint(emax));
+    const unsigned b = __reduce_max_sync(0xffffffffu, __float_as_uint(bmax));
+    if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = e; sh[1][threadIdx.x >> 5] = b; }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+        unsigned m = 0u;
+        for (int w = 0; w < kThreads / 32; ++w) m = max(m, sh[threadIdx.x][w]);
+        atomicMax(threadIdx.x == 0 ? &st->emax_bits : &st->bmax_bits, m);
+    }
+}
+
 struct PumpArgs {
     int    on;
     double ex, ey, ez, k0, w0, trmp, toff;
@@ -332,30 +347,39 @@ __global__ void k_fields_dcu(const float* __restrict__ r, float* __restrict__ gb
                              DevState* st) {
     const double t = st->t;
     float emax = 0.f, bmax = 0.f;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
-        const float elx = r[c], ely = r[ncell + c];
-        const float bx = r[2 * ncell + c] + b0x;
-        const float by = r[3 * ncell + c] + b0y;
-        const float bz = r[4 * ncell + c] + b0z;
-        float ex = elx, ey = ely, ez = 0.0f;
-        pump_add(pa, c % nx, t, ex, ey, ez);
-        float4* q = reinterpret_cast<float4*>(gb) + 2 * static_cast<size_t>(c);
-        q[0] = make_float4(ex, ey, ez, bx);
-        q[1] = make_float4(by, bz, 0.f, 0.f);
-        if (api.ELx) api.ELx[c] = elx;
-        if (api.ELy) api.ELy[c] = ely;
-        if (api.Bx) api.Bx[c] = bx;
-        if (api.By) api.By[c] = by;
-        if (api.Bz) api.Bz[c] = bz;
-        emax = fmaxf(emax, fmaxf(fabsf(ex), fmaxf(fabsf(ey), fabsf(ez))));
-        bmax = fmaxf(bmax, fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
+    const int stride = gridDim.x * blockDim.x;
+    // two cells per pass, both cells' loads issued before any store
+    for (int c0 = blockIdx.x * blockDim.x + threadIdx.x; c0 < ncell; c0 += 2 * stride) {
+        float v[2][5];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int c = c0 + u * stride;
+            if (c < ncell) {
+#pragma unroll
+                for (int k = 0; k < 5; ++k) v[u][k] = r[k * ncell + c];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int c = c0 + u * stride;
+            if (c >= ncell) break;
+            const float elx = v[u][0], ely = v[u][1];
+            const float bx = v[u][2] + b0x, by = v[u][3] + b0y, bz = v[u][4] + b0z;
+            float ex = elx, ey = ely, ez = 0.0f;
+            pump_add(pa, c % nx, t, ex, ey, ez);
+            float4* q = reinterpret_cast<float4*>(gb) + 2 * static_cast<size_t>(c);
+            q[0] = make_float4(ex, ey, ez, bx);
+            q[1] = make_float4(by, bz, 0.f, 0.f);
+            if (api.ELx) api.ELx[c] = elx;
+            if (api.ELy) api.ELy[c] = ely;
+            if (api.Bx) api.Bx[c] = bx;
+            if (api.By) api.By[c] = by;
+            if (api.Bz) api.Bz[c] = bz;
+            emax = fmaxf(emax, fmaxf(fabsf(ex), fmaxf(fabsf(ey), fabsf(ez))));
+            bmax = fmaxf(bmax, fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
+        }
     }
-    emax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(emax)));
-    bmax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(bmax)));
-    if ((threadIdx.x & 31) == 0) {
-        atomicMax(&st->emax_bits, __float_as_uint(emax));
-        atomicMax(&st->bmax_bits, __float_as_uint(bmax));
-    }
+    block_max_eb(emax, bmax, st);
 }
 
 // Darwin, after the E_T solve: r_et = [ETx, ETy, ETz], r_el = [ELx, ELy, ...].
@@ -367,27 +391,47 @@ __global__ void k_fields_push(const float* __restrict__ r_et, const float* __res
                               double* __restrict__ part) {
     const double t = st->t;
     double se2 = 0, me2 = 0, sb2 = 0;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
-        const float etx = r_et[c], ety = r_et[ncell + c], etz = r_et[2 * ncell + c];
-        float ex = r_el[c] + 1.0f * etx;
-        float ey = r_el[ncell + c] + 1.0f * ety;
-        float ez = 1.0f * etz;
-        pump_add(pa, c % nx, t, ex, ey, ez);
-        const float4* qd = reinterpret_cast<const float4*>(gb_dcu) + 2 * static_cast<size_t>(c);
-        const float4 b1 = qd[0], b2 = qd[1];
-        float4* q = reinterpret_cast<float4*>(gb) + 2 * static_cast<size_t>(c);
-        q[0] = make_float4(ex, ey, ez, b1.w);
-        q[1] = make_float4(b2.x, b2.y, 0.f, 0.f);
-        if (api.Ex) api.Ex[c] = ex;
-        if (api.Ey) api.Ey[c] = ey;
-        if (api.Ez) api.Ez[c] = ez;
-        if (api.ETx) api.ETx[c] = etx;
-        if (api.ETy) api.ETy[c] = ety;
-        if (api.ETz) api.ETz[c] = etz;
-        const double e2 = double(ex) * ex + double(ey) * ey;
-        se2 += e2;
-        me2 = fmax(me2, e2);
-        sb2 += double(b1.w) * b1.w + double(b2.x) * b2.x + double(b2.y) * b2.y;
+    const int stride = gridDim.x * blockDim.x;
+    // two cells per pass, both cells' loads issued before any store
+    for (int c0 = blockIdx.x * blockDim.x + threadIdx.x; c0 < ncell; c0 += 2 * stride) {
+        float v[2][5];
+        float4 b1[2], b2[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int c = c0 + u * stride;
+            if (c < ncell) {
+#pragma unroll
+                for (int k = 0; k < 3; ++k) v[u][k] = r_et[k * ncell + c];
+                v[u][3] = r_el[c];
+                v[u][4] = r_el[ncell + c];
+                const float4* qd = reinterpret_cast<const float4*>(gb_dcu) + 2 * static_cast<size_t>(c);
+                b1[u] = qd[0];
+                b2[u] = qd[1];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int c = c0 + u * stride;
+            if (c >= ncell) break;
+            const float etx = v[u][0], ety = v[u][1], etz = v[u][2];
+            float ex = v[u][3] + 1.0f * etx;
+            float ey = v[u][4] + 1.0f * ety;
+            float ez = 1.0f * etz;
+            pump_add(pa, c % nx, t, ex, ey, ez);
+            float4* q = reinterpret_cast<float4*>(gb) + 2 * static_cast<size_t>(c);
+            q[0] = make_float4(ex, ey, ez, b1[u].w);
+            q[1] = make_float4(b2[u].x, b2[u].y, 0.f, 0.f);
+            if (api.Ex) api.Ex[c] = ex;
+            if (api.Ey) api.Ey[c] = ey;
+            if (api.Ez) api.Ez[c] = ez;
+            if (api.ETx) api.ETx[c] = etx;
+            if (api.ETy) api.ETy[c] = ety;
+            if (api.ETz) api.ETz[c] = etz;
+            const double e2 = double(ex) * ex + double(ey) * ey;
+            se2 += e2;
+            me2 = fmax(me2, e2);
+            sb2 += double(b1[u].w) * b1[u].w + double(b2[u].x) * b2[u].x + double(b2[u].y) * b2[u].y;
+        }
     }
     grid_partials(se2, me2, sb2, part);
 }
@@ -452,8 +496,9 @@ __global__ void k_add_pump(FieldAPI f, int nx, int n, PumpArgs pa, double t) {
     f.Ex[c] = ex; f.Ey[c] = ey; f.Ez[c] = ez;
 }
 
-// Pack caller E/B arrays into the [ncell][8] gather layout (unfused dcu
-// deposit) and record the field maxima its deposit scale needs.
+// Pack caller E/B arrays into the [ncell][8] gather layout (unfused EM push and
+// dcu deposit) and, with MAX, record the field maxima the dcu deposit scale needs.
+template <bool MAX>
 __global__ void k_pack_em(FieldAPI f, float* __restrict__ gb, int ncell, DevState* st) {
     float emax = 0.f, bmax = 0.f;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
@@ -465,12 +510,7 @@ __global__ void k_pack_em(FieldAPI f, float* __restrict__ gb, int ncell, DevStat
         emax = fmaxf(emax, fmaxf(fabsf(ex), fmaxf(fabsf(ey), fabsf(ez))));
         bmax = fmaxf(bmax, fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
     }
-    emax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(emax)));
-    bmax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(bmax)));
-    if ((threadIdx.x & 31) == 0) {
-        atomicMax(&st->emax_bits, __float_as_uint(emax));
-        atomicMax(&st->bmax_bits, __float_as_uint(bmax));
-    }
+    if (MAX) block_max_eb(emax, bmax, st);
 }
 
 // Energy / charge partials from caller arrays (any may be null).
@@ -546,6 +586,91 @@ k_rms_reduce(const float* __restrict__ pc, int nbc, const float* __restrict__ pd
                 for (int k = 0; k < 3; ++k) st->rms_dcu[k] = static_cast<float>(sqrt(a[9 + k] / a[12]));
             st->have_rms = 1;
         }
+    }
+}
+
+// End-of-step reduction of the fused step, in one launch of kRedBlocks blocks:
+// the diagnostics of k_diag_reduce and, for Darwin, the coefficient rms of
+// k_rms_reduce. Block b owns a fixed contiguous range of the chunk partials
+// (part_p, part_c, part_d) and of the grid partials (part_g); thread t sums
+// entries t, t + 256, ... of its block's ranges, a fixed warp/shared tree makes
+// the block row, and the last block to finish (ticket) reduces the rows in row
+// order. Every sum is a pure function of the partials, whichever block is last.
+template <bool RMS>
+__global__ void __launch_bounds__(kThreads)
+k_step_reduce(const double* __restrict__ pp, const float* __restrict__ pc, const float* __restrict__ pd,
+              int np, const double* __restrict__ pg, int ng, double* __restrict__ rows,
+              double eps0, double dxdy, aw_diag* out, DevState* st) {
+    constexpr int NV = kRedVals;
+    constexpr int NW = kThreads / 32;
+    __shared__ double sh[NV][NW];
+    __shared__ double rs[kRedBlocks][NV];
+    __shared__ int last;
+    const int t = threadIdx.x, b = blockIdx.x;
+    double a[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) a[k] = 0.0;
+    const int plo = static_cast<int>(static_cast<long long>(b) * np / kRedBlocks);
+    const int phi = static_cast<int>(static_cast<long long>(b + 1) * np / kRedBlocks);
+    for (int i = plo + t; i < phi; i += kThreads) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) a[k] += pp[i * 5 + k];
+        if (RMS) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) a[8 + k] += pc[i * 9 + k];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) a[17 + k] += pd[i * 4 + k];
+        }
+    }
+    const int glo = b * ng / kRedBlocks, ghi = (b + 1) * ng / kRedBlocks;
+    for (int i = glo + t; i < ghi; i += kThreads) {
+        a[4] += pg[i * 5 + 0]; a[5] = fmax(a[5], pg[i * 5 + 1]); a[6] += pg[i * 5 + 2]; a[7] += pg[i * 5 + 3];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            const double v = __shfl_down_sync(0xffffffffu, a[k], o);
+            a[k] = (k == 5) ? fmax(a[k], v) : a[k] + v;
+        }
+    if ((t & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < NV; ++k) sh[k][t >> 5] = a[k];
+    __syncthreads();
+    if (t < NV) {
+        double v = sh[t][0];
+        for (int w = 1; w < NW; ++w) v = (t == 5) ? fmax(v, sh[t][w]) : v + sh[t][w];
+        rows[b * NV + t] = v;
+        __threadfence();
+    }
+    __syncthreads();
+    if (t == 0) last = (atomicAdd(&st->red_ticket, 1u) == kRedBlocks - 1);
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    for (int i = t; i < kRedBlocks * NV; i += kThreads) rs[i / NV][i % NV] = __ldcg(rows + i);
+    __syncthreads();
+    if (t < NV) {
+        double v = rs[0][t];
+        for (int r = 1; r < kRedBlocks; ++r) v = (t == 5) ? fmax(v, rs[r][t]) : v + rs[r][t];
+        sh[t][0] = v;
+    }
+    __syncthreads();
+    if (t == 0) {
+        out->ke = 0.5 * sh[0][0];
+        out->px = sh[1][0]; out->py = sh[2][0]; out->pz = sh[3][0];
+        out->ee = 0.5 * eps0 * sh[4][0] * dxdy;
+        out->max_e = sqrt(sh[5][0]);
+        out->charge = sh[6][0] * dxdy;
+        out->eb = 0.5 * sh[7][0] * dxdy;
+        if (RMS) {
+            if (sh[16][0] > 0.0)
+                for (int f = 0; f < 8; ++f) st->rms_src[f] = static_cast<float>(sqrt(sh[8 + f][0] / sh[16][0]));
+            if (sh[20][0] > 0.0)
+                for (int k = 0; k < 3; ++k) st->rms_dcu[k] = static_cast<float>(sqrt(sh[17 + k][0] / sh[20][0]));
+            st->have_rms = 1;
+        }
+        st->red_ticket = 0u;
     }
 }
 
@@ -671,12 +796,16 @@ void launch_add_pump(Ctx& c, double t) {
     AW_LAUNCH();
 }
 
-void launch_pack_em(Ctx& c) {
+void launch_pack_em(Ctx& c, bool maxima) {
     const aw_field_ptrs& f = c.fld;
     if (!f.Ex || !f.Ey || !f.Ez || !f.Bx || !f.By || !f.Bz)
-        throw Error(AW_ERR_STATE, "deposit_dcu: fields E and B must be bound");
-    AW_CUDA(cudaMemsetAsync(&c.st->emax_bits, 0, 2 * sizeof(unsigned), c.stream));
-    k_pack_em<<<kGridBlocks, kThreads, 0, c.stream>>>(api_of(f), c.gb_dcu, c.geo.ncell, c.st);
+        throw Error(AW_ERR_STATE, "fields E and B must be bound");
+    if (maxima) {
+        AW_CUDA(cudaMemsetAsync(&c.st->emax_bits, 0, 2 * sizeof(unsigned), c.stream));
+        k_pack_em<true><<<kGridBlocks, kThreads, 0, c.stream>>>(api_of(f), c.gb_dcu, c.geo.ncell, c.st);
+    } else {
+        k_pack_em<false><<<kGridBlocks, kThreads, 0, c.stream>>>(api_of(f), c.gb_dcu, c.geo.ncell, c.st);
+    }
     AW_LAUNCH();
 }
 void launch_grid_diag(Ctx& c) {
@@ -692,6 +821,18 @@ void launch_set_step(Ctx& c, long long n) {
 void launch_rms_reduce(Ctx& c, bool src, bool dcu) {
     k_rms_reduce<<<1, kRmsThreads, 0, c.stream>>>(src ? c.part_c : nullptr, c.npart_p,
                                                   dcu ? c.part_d : nullptr, c.npart_p, c.st);
+    AW_LAUNCH();
+}
+void launch_step_reduce(Ctx& c) {
+    const double dxdy = c.geo.dx * c.geo.dy;
+    if (c.model == AW_MODEL_DARWIN)
+        k_step_reduce<true><<<kRedBlocks, kThreads, 0, c.stream>>>(c.part_p, c.part_c, c.part_d, c.npart_p, c.part_g,
+                                                                    kGridBlocks, c.red_rows, c.prm.eps0, dxdy,
+                                                                    c.diag, c.st);
+    else
+        k_step_reduce<false><<<kRedBlocks, kThreads, 0, c.stream>>>(c.part_p, nullptr, nullptr, c.npart_p, c.part_g,
+                                                                     kGridBlocks, c.red_rows, c.prm.eps0, dxdy,
+                                                                     c.diag, c.st);
     AW_LAUNCH();
 }
 void launch_promote_scales(Ctx& c) {

@@ -129,7 +129,10 @@ int aw_set_params(aw_ctx* ctx, const aw_params* p);
 
 /* ---- binding caller-owned device memory ----------------------------------
  * Particles: the reference Particles SoA (include/pic/particles.hpp:453-516).
- * `cell` may be NULL only if the caller never calls aw_migrate/aw_sort_tiles. */
+ * `cell` may be NULL only if the caller never calls aw_migrate/aw_sort_tiles.
+ * Binding exactly what is already bound (same pointers and n; for sources and
+ * fields, the same pointer sets; for aw_set_params, the same values) changes
+ * nothing and keeps a captured step graph. */
 int aw_particles_bind(aw_ctx* ctx, float* x, float* y, float* ux, float* uy,
                       float* uz, float* w, int32_t* cell, int64_t n);
 /* Sources (include/pic/sources.hpp:23-86) and Fields (include/pic/fields.hpp:24-73). */
@@ -260,7 +263,7 @@ int aw_run_diag(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph, aw_d
 
 /* One fused step (like aw_step) with CUDA events recorded on the context's
  * stream between its phases; ms[i] = duration of phase i, *nphase = number of
- * phases (cap >= 14). Synchronises. Phase names: aw_step_phase_name. */
+ * phases (cap >= 13). Synchronises. Phase names: aw_step_phase_name. */
 int aw_step_profile(aw_ctx* ctx, int64_t n, float* ms, int32_t cap, int32_t* nphase);
 const char* aw_step_phase_name(int32_t model, int32_t i);
 

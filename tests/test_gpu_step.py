@@ -168,7 +168,7 @@ def test_step_profile_names_every_phase(setup, aw):
     s.ctx.load_species(WEIBEL, seed=0)
     s.ctx.init()
     prof = s.ctx.step_profile(0)
-    assert len(prof) == 14 and "push_deposit_em" in prof and "rms_reduce" in prof
+    assert len(prof) == 13 and "push_deposit_em" in prof and "step_reduce" in prof
     assert all(v >= 0.0 for v in prof.values())
 
 
