@@ -86,6 +86,7 @@ SIGNATURES = {
     "aw_fields_bind": [_P, C.POINTER(FieldPtrs)],
     "aw_load_species": [_P, C.POINTER(Species), _I32, _U64, _I32],
     "aw_resort": [_P], "aw_set_resort": [_P, _I32],
+    "aw_grad_es": [_P, _I64, _I32, _P, _P, _P, C.POINTER(_D)],
     "aw_load_legacy": [_P, C.POINTER(LegacyLoad)],
     "aw_deposit_rho_noalloc": [C.POINTER(Grid), _D, _P, _P, _P, _P, _P, _P, _I64, _P, _P],
     "aw_deposit_rho": [_P], "aw_deposit_rho_j": [_P], "aw_deposit_amu": [_P], "aw_deposit_dcu": [_P],
@@ -231,6 +232,15 @@ class Context:
     def set_resort(self, every: int):
         """Re-sort inside run() before every step n with n % every == 0 (0 = never)."""
         _check(self.lib.aw_set_resort(self.h, int(every)))
+
+    def grad_es(self, nsteps: int, checkpoint_every: int, dux, duy, duz) -> float:
+        """d(final field energy)/d(initial velocities) into the device arrays
+        dux, duy, duz (the bound particles hold the initial state before and
+        after). Returns the loss."""
+        loss = C.c_double()
+        _check(self.lib.aw_grad_es(self.h, int(nsteps), int(checkpoint_every), _ptr(dux), _ptr(duy), _ptr(duz),
+                                   C.byref(loss)))
+        return loss.value
 
     def tile_bins(self):
         off, idx, nt, ntx = C.c_void_p(), C.c_void_p(), C.c_int32(), C.c_int32()

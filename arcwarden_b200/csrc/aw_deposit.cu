@@ -58,7 +58,9 @@ template <> struct SetNF<SET_ALL>  { static constexpr int NF = 8, NS = 6; };
 // push and dcu kernels keep three CTAs per SM next to their 48 KB stage. A
 // chunk of 2048 particles covers ~30-250 cells at 64 per cell; a chunk whose
 // window does not fit takes the exact slow path.
-constexpr int wmax_cells(int nf) { return nf == 1 ? 2048 : (nf == 3 ? 896 : (nf == 4 ? 1536 : 320)); }
+constexpr int wmax_cells(int nf) {
+    return (nf == 1 || nf == 2) ? 2048 : (nf == 3 ? 896 : (nf == 4 ? 1536 : 320));
+}
 constexpr int kRedInts = kThreads / 32 * (4 + 8);
 // stage [np][kChunk] f32 | window [2*nf][wmax] i32 | red ints | slow list u16[kChunk]
 constexpr size_t win_offset(int np) { return static_cast<size_t>(np) * kChunk * 4; }
@@ -421,6 +423,101 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
 }
 
 // ---------------------------------------------------------------------------
+// Backward step A of the ES adjoint (the transpose of k_push_deposit_es's push
+// at step n). Per particle, from its cotangents after the step (lx, ly, lu) and
+// its position x_n:
+//   lu3 = lu + (dt/dx lx, dt/dy ly, 0)            move transpose
+//   lu1 = R^T lu3                                   rotation transpose
+//   lE  = qmh (lu3 + lu1), x and y                  the two half kicks
+//   lx += lE . dE/dx(x_n),  ly += lE . dE/dy(x_n)   gather, position derivative
+//   lu  = lu1
+// and lE is scattered onto the grid with the CIC weights at x_n (the transpose
+// of the gather) on this window engine, 2 fields, exact fixed point. The
+// scales come from the bound max|lu3| of the previous backward step:
+// |lE_d| <= 2 |qmh| |lu3| (R is a rotation); particles beyond it take the slow
+// path. Stage = x, y, lEx*S0, lEy*S1.
+__global__ void __launch_bounds__(kThreads, 3)
+k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ E, AdjDev* ad,
+              unsigned long long* __restrict__ acc, int wmaxc, DevState* st) {
+    constexpr int NF = 2, NS = 4, NIN = 2;
+    constexpr bool T0 = false;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const Smem m = carve(smem, NS, NF, wmaxc);
+    __shared__ unsigned long long bar;
+    __shared__ int nlist;
+
+    const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
+    const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), a.n - c0));
+    const float lmax = __uint_as_float(ad->lmax_bits);
+    const float sc = scale_for_bound(__fmul_rn(__fmul_rn(2.0f * fabsf(k.qmh), lmax), 1.0001f));
+    const float S[NF] = {sc, sc};
+    if (blockIdx.x == 0 && threadIdx.x == 0) { ad->S[0] = sc; ad->S[1] = sc; }
+    if (threadIdx.x == 0) nlist = 0;
+    const ChunkSrc src{{a.xn, a.yn, nullptr, nullptr, nullptr, nullptr}};
+    float x0, y0;
+    if (!load_chunk(m.stage, src, NIN, c0, cnt, a.vec_ok != 0, &bar, st, &x0, &y0)) return;
+    int ir, jr;
+    ref_of(x0, y0, g, ir, jr);
+
+    BBox bb;
+    float l1[NF] = {};
+#pragma unroll 1
+    for (int it = 0; it < kPPT; ++it) {
+        const int s = it * kThreads + threadIdx.x;
+        const long long i = c0 + s;
+        const float x = m.stage[s], y = m.stage[kChunk + s];
+        float xs = -1.0f, cs[NF] = {0.f, 0.f};
+        if (s < cnt && in_grid(x, y, g)) {
+            float lx = a.lx[i], ly = a.ly[i];
+            const float u3x = __fmaf_rn(k.dtx, lx, a.lux[i]);
+            const float u3y = __fmaf_rn(k.dty, ly, a.luy[i]);
+            const float u3z = a.luz[i];
+            float u1x = u3x, u1y = u3y, u1z = u3z;
+            if (k.rot) {   // R^T l = l - l x s + (l x s) x t
+                const float cx = __fmaf_rn(u3y, k.sz, -__fmul_rn(u3z, k.sy));
+                const float cy = __fmaf_rn(u3z, k.sx, -__fmul_rn(u3x, k.sz));
+                const float cz = __fmaf_rn(u3x, k.sy, -__fmul_rn(u3y, k.sx));
+                u1x = __fadd_rn(__fsub_rn(u3x, cx), __fmaf_rn(cy, k.tz, -__fmul_rn(cz, k.ty)));
+                u1y = __fadd_rn(__fsub_rn(u3y, cy), __fmaf_rn(cz, k.tx, -__fmul_rn(cx, k.tz)));
+                u1z = __fadd_rn(__fsub_rn(u3z, cz), __fmaf_rn(cx, k.ty, -__fmul_rn(cy, k.tx)));
+            }
+            const float lex = __fmul_rn(k.qmh, __fadd_rn(u3x, u1x));
+            const float ley = __fmul_rn(k.qmh, __fadd_rn(u3y, u1y));
+            const Cic c = cic(x, y);
+            const float fx = __fsub_rn(x, static_cast<float>(c.i0)), fy = __fsub_rn(y, static_cast<float>(c.j0));
+            const float gx = __fsub_rn(1.0f, fx), gy = __fsub_rn(1.0f, fy);
+            const int i1 = wrap_once(c.i0 + 1, g.nx);
+            const int r0 = c.j0 * g.nx, r1 = wrap_once(c.j0 + 1, g.ny) * g.nx;
+            const float2 e00 = __ldg(E + r0 + c.i0), e10 = __ldg(E + r0 + i1);
+            const float2 e01 = __ldg(E + r1 + c.i0), e11 = __ldg(E + r1 + i1);
+            const float dxx = __fmaf_rn(gy, __fsub_rn(e10.x, e00.x), __fmul_rn(fy, __fsub_rn(e11.x, e01.x)));
+            const float dxy = __fmaf_rn(gx, __fsub_rn(e01.x, e00.x), __fmul_rn(fx, __fsub_rn(e11.x, e10.x)));
+            const float dyx = __fmaf_rn(gy, __fsub_rn(e10.y, e00.y), __fmul_rn(fy, __fsub_rn(e11.y, e01.y)));
+            const float dyy = __fmaf_rn(gx, __fsub_rn(e01.y, e00.y), __fmul_rn(fx, __fsub_rn(e11.y, e10.y)));
+            lx = __fadd_rn(lx, __fmaf_rn(lex, dxx, __fmul_rn(ley, dyx)));
+            ly = __fadd_rn(ly, __fmaf_rn(lex, dxy, __fmul_rn(ley, dyy)));
+            a.lx[i] = lx; a.ly[i] = ly;
+            a.lux[i] = u1x; a.luy[i] = u1y; a.luz[i] = u1z;
+            bb.add(c.i0, c.j0, ir, jr, g);
+            const float cf[NF] = {lex, ley};
+            const bool fast = scale_fast<NF>(cf, S, cs, l1);
+            xs = __fadd_rn(x, 0.0f);
+            if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
+        }
+        __syncwarp();
+        const int d = stage_slot(s);
+        m.stage[d] = xs;
+        m.stage[kChunk + d] = y;
+        m.stage[2 * kChunk + d] = cs[0];
+        m.stage[3 * kChunk + d] = cs[1];
+    }
+    const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
+    auto coef = [&](const float (&q)[NS], float (&c2)[NF]) { c2[0] = q[2]; c2[1] = q[3]; };
+    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
+    close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
+}
+
+// ---------------------------------------------------------------------------
 struct PushP {
     float  qmh;
     int    has_b0;
@@ -710,6 +807,16 @@ void launch_deposit_src(Ctx& c, int which) {
         case 8: launch_src<SET_ALL>(c, c.acc_src); break;
         default: throw Error(AW_ERR_ARG, "deposit_src: bad field set");
     }
+}
+
+void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* E, AdjDev* ad,
+                        unsigned long long* acc) {
+    if (a.n == 0) return;
+    const size_t sh = smem_bytes(2, 4);
+    prep_smem(k_adj_scatter, sh);
+    k_adj_scatter<<<nchunks(a.n), kThreads, sh, c.stream>>>(a, c.geo, k, reinterpret_cast<const float2*>(E), ad,
+                                                             acc, wmax_cells(2), c.st);
+    AW_LAUNCH();
 }
 
 void launch_deposit_dcu(Ctx& c, const float* gb, bool fused) {

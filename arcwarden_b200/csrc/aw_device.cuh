@@ -462,7 +462,7 @@ __device__ __forceinline__ bool load_chunk(float* stage, const ChunkSrc& src, in
     }
     const int rem = cnt - nbulk;
     if (rem > 0)
-        for (int idx = threadIdx.x; idx < rem * np; idx += kThreads) {
+        for (int idx = threadIdx.x; idx < rem * np; idx += blockDim.x) {
             const int k = idx / rem, s = nbulk + idx % rem;
             stage[k * kChunk + s] = __ldg(src.at(k) + c0 + s);
         }
@@ -476,6 +476,37 @@ __device__ __forceinline__ bool load_chunk(float* stage, const ChunkSrc& src, in
         return false;
     }
     return true;
+}
+
+// Write planes [0, np) of the stage back to the chunk [c0, c0 + cnt) of their
+// arrays: one bulk shared->global copy per plane (evict-first) for the
+// 16-byte-aligned body, plain stores for the ragged tail and unaligned arrays.
+// Every thread calls it after writing its stage slots; thread 0 waits until the
+// copies have read the stage, so the block never exits under a copy in flight.
+__device__ __forceinline__ void store_chunk(const float* stage, float* const (&dst)[6], int np, long long c0, int cnt,
+                                            bool vec) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // stage writes -> bulk-copy engine
+    __syncthreads();
+    const int nbulk = vec ? (cnt & ~3) : 0;
+    if (threadIdx.x == 0 && nbulk > 0) {
+        unsigned long long pol;
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+        for (int k = 0; k < np; ++k) {
+            float* d = k == 0 ? dst[0] : k == 1 ? dst[1] : k == 2 ? dst[2] : k == 3 ? dst[3] : k == 4 ? dst[4] : dst[5];
+            asm volatile("cp.async.bulk.global.shared::cta.bulk_group.L2::cache_hint [%0], [%1], %2, %3;"
+                         :: "l"(d + c0), "r"(smem_u32(stage + k * kChunk)), "r"(static_cast<unsigned>(nbulk) * 4u),
+                            "l"(pol) : "memory");
+        }
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+    const int rem = cnt - nbulk;
+    if (rem > 0)
+        for (int idx = threadIdx.x; idx < rem * np; idx += blockDim.x) {
+            const int k = idx / rem, s = nbulk + idx % rem;
+            float* d = k == 0 ? dst[0] : k == 1 ? dst[1] : k == 2 ? dst[2] : k == 3 ? dst[3] : k == 4 ? dst[4] : dst[5];
+            d[c0 + s] = stage[k * kChunk + s];
+        }
+    if (threadIdx.x == 0 && nbulk > 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
 
 // Exact slow path after the window pass: the particles pass 1 listed (a

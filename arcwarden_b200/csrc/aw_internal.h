@@ -116,8 +116,55 @@ struct Ctx {
     long long host_step = 0;
     int write_cell = 1;
 
+    // discrete adjoint of the ES step (aw_adjoint.cu; allocated by aw_grad_es)
+    struct AdjWS* adj = nullptr;
+
     int nsrc() const { return model == AW_MODEL_DARWIN ? 8 : 1; }
     int nout() const { return model == AW_MODEL_DARWIN ? 5 : 2; }
+};
+
+// Device constants of one ES adjoint step: the push's half-step factor, the
+// move factors dt/dx, dt/dy (cell units) and the Boris rotation about B0
+// (t = qmh B0, s = 2t / (1 + t^2), as boris_rotate computes them).
+struct AdjK {
+    float qmh, dtx, dty;
+    float tx, ty, tz, sx, sy, sz;
+    int   rot;
+};
+// Adjoint particle state (cotangents of x, y, ux, uy, uz) and the positions x_n
+// of the step being transposed.
+struct AdjP {
+    const float* xn;
+    const float* yn;
+    float *lx, *ly, *lux, *luy, *luz;
+    long long n;
+    int vec_ok;
+};
+// Device scalars of the backward sweep.
+struct AdjDev {
+    unsigned lmax_bits;   // max |lu3| (2-norm) for the next scatter's scale
+    float    S[2];        // scales of the pending field-cotangent scatter
+};
+
+// Workspace of the ES adjoint sweep (aw_grad_es): checkpoints of the forward
+// run, the trajectory of one segment, the cotangent grids.
+struct AdjWS {
+    long long n = 0, nsteps = 0;
+    int every = 0, nck = 0, ncell = 0;
+    float* lam = nullptr;                 // [5][n]  lx ly lux luy luz
+    float* init_parts = nullptr;          // [5][n]  x y ux uy uz of the initial state
+    float* ck_parts = nullptr;            // [nck][5][n]
+    unsigned long long* ck_acc = nullptr; // [nck][ncell] pending rho accumulators
+    DevState* ck_st = nullptr;            // [nck]
+    float* traj_xy = nullptr;             // [every][2][n] positions x_n of the segment
+    float* traj_E = nullptr;              // [every][ncell][2] gather fields E_n of the segment
+    unsigned long long* acc = nullptr;    // [2][ncell] field-cotangent scatter
+    float* lE = nullptr;                  // [2][ncell]
+    cufftComplex* lEk = nullptr;          // [2][nk]
+    cufftComplex* lrk = nullptr;          // [nk]
+    float* lrho = nullptr;                // [ncell] charge-density cotangent
+    AdjDev* ad = nullptr;
+    cufftHandle p_r2c2 = 0;               // batch-2 R2C
 };
 
 // ---- launchers (aw_particles.cu) -------------------------------------------
@@ -140,6 +187,11 @@ void launch_deposit_src(Ctx& c, int which);
 void launch_deposit_dcu(Ctx& c, const float* gb, bool fused);
 void launch_push_deposit_es(Ctx& c);
 void launch_push_deposit_em(Ctx& c);
+// Backward step A of the ES adjoint: Boris/move transposes, field-cotangent
+// scatter into acc [2][ncell] (scales from ad->lmax_bits, stored to ad->S) and
+// the E-gather position derivative (E = interleaved [ncell][2]).
+void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* E, AdjDev* ad,
+                        unsigned long long* acc);
 
 // ---- launchers (aw_spectral.cu) -------------------------------------------
 int  grid_partial_blocks();
@@ -158,12 +210,26 @@ void launch_scale_copy(Ctx& c, float* dst, const float* src, int n, float s);
 void launch_form_e(Ctx& c, float et_scale);
 void launch_add_b0(Ctx& c);
 void launch_add_pump(Ctx& c, double t);
-void launch_pack_em(Ctx& c, bool maxima);
+void launch_pack_em(Ctx& c);
 void launch_grid_diag(Ctx& c);
 void launch_set_step(Ctx& c, long long n);
 void launch_copy_umax(Ctx& c);
 void launch_promote_scales(Ctx& c);                // S_pend = S_next
 void launch_rms_reduce(Ctx& c, bool src, bool dcu);
 void launch_step_reduce(Ctx& c);                   // end of a fused step: diagnostics (+ rms for Darwin)
+
+// ---- the ES adjoint (aw_adjoint.cu) ----------------------------------------
+AdjK adj_constants(const Ctx& c, float dt_scale);
+void adj_prepare(Ctx& c, long long nsteps, int every);   // (re)allocates c.adj
+void free_adjoint(Ctx& c);
+// lE = acc / S (+ ext_scale * E_ext, E_ext interleaved [ncell][2], may be null);
+// acc is zeroed.
+void launch_adj_finalize(Ctx& c, const float* E_ext, float ext_scale);
+// lrho = S^T lE: the transpose of the spectral Poisson field solve.
+void adj_transpose_solve(Ctx& c);
+// Backward step B: lx += q dlrho/dx at x_n; max |lu3| of the next step A.
+void launch_adj_gather(Ctx& c, const AdjP& a, const AdjK& k);
+// Cotangent of the initial velocities through the half-step rollback.
+void launch_adj_out(Ctx& c, float* dux, float* duy, float* duz);
 
 }  // namespace aw

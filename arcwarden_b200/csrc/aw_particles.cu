@@ -161,61 +161,97 @@ __global__ void k_migrate(Parts p, Geo g) {
     if (p.cell) p.cell[t] = cell_of(x, y, g.nx, g.ny);
 }
 
-// Unfused ES push / half-step rollback, gathering from [ny][nx] Ex, Ey arrays.
-template <bool POW2>
-__global__ void k_push_es_plain(Parts p, Geo g, const float* __restrict__ ex,
-                                const float* __restrict__ ey, float qmh, int has_b0,
-                                float b0x, float b0y, float b0z, double dt, double dtx, double dty, int move) {
-    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= p.n) return;
-    const float x = p.x[t], y = p.y[t];
-    const Cic s = cic(x, y);
-    const int i0 = wrap_once(s.i0, g.nx), i1 = wrap_once(s.i0 + 1, g.nx);
-    const int j0 = wrap_once(s.j0, g.ny) * g.nx, j1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
-    const float Ex = gather4(s, __ldg(ex + j0 + i0), __ldg(ex + j0 + i1), __ldg(ex + j1 + i0), __ldg(ex + j1 + i1));
-    const float Ey = gather4(s, __ldg(ey + j0 + i0), __ldg(ey + j0 + i1), __ldg(ey + j1 + i0), __ldg(ey + j1 + i1));
-    float ux = p.ux[t], uy = p.uy[t], uz = p.uz[t];
-    boris_es(ux, uy, uz, Ex, Ey, qmh, has_b0 != 0, b0x, b0y, b0z);
-    p.ux[t] = ux; p.uy[t] = uy; p.uz[t] = uz;
-    if (move) {
-        if constexpr (POW2) {
-            p.x[t] = move1_pow2(x, ux, dtx);
-            p.y[t] = move1_pow2(y, uy, dty);
-        } else {
-            p.x[t] = move1(x, ux, dt, g.dx);
-            p.y[t] = move1(y, uy, dt, g.dy);
+// Unfused pushes on 2048-particle chunks: the chunk's x, y, ux, uy, uz arrive
+// in shared memory by bulk copy, each of the NT threads pushes 2048 / NT
+// particles (slots it * NT + tid, unrolled so their gathers overlap), and the
+// new state leaves by bulk copy.
+//
+// ES push / half-step rollback (boris_push_kernel, boris_half_back_kernel),
+// gathering from the [ny][nx] Ex, Ey arrays. With move == 0 only the velocities
+// are written back.
+template <bool POW2, int NT>
+__global__ void __launch_bounds__(NT)
+k_push_es_chunk(Parts p, Geo g, const float* __restrict__ ex, const float* __restrict__ ey, float qmh, int has_b0,
+                float b0x, float b0y, float b0z, double dt, double dtx, double dty, int move, DevState* st) {
+    extern __shared__ __align__(16) float stage[];
+    __shared__ unsigned long long bar;
+    const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
+    const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
+    const ChunkSrc src{{p.x, p.y, p.ux, p.uy, p.uz, nullptr}};
+    float x0, y0;
+    if (!load_chunk(stage, src, 5, c0, cnt, p.vec_ok != 0, &bar, st, &x0, &y0)) return;
+#pragma unroll
+    for (int it = 0; it < kChunk / NT; ++it) {
+        const int s = it * NT + threadIdx.x;
+        if (s >= cnt) break;
+        const float x = stage[s], y = stage[kChunk + s];
+        const Cic c = cic(x, y);
+        const int i0 = wrap_once(c.i0, g.nx), i1 = wrap_once(c.i0 + 1, g.nx);
+        const int j0 = wrap_once(c.j0, g.ny) * g.nx, j1 = wrap_once(c.j0 + 1, g.ny) * g.nx;
+        const float Ex = gather4(c, __ldg(ex + j0 + i0), __ldg(ex + j0 + i1), __ldg(ex + j1 + i0), __ldg(ex + j1 + i1));
+        const float Ey = gather4(c, __ldg(ey + j0 + i0), __ldg(ey + j0 + i1), __ldg(ey + j1 + i0), __ldg(ey + j1 + i1));
+        float ux = stage[2 * kChunk + s], uy = stage[3 * kChunk + s], uz = stage[4 * kChunk + s];
+        boris_es(ux, uy, uz, Ex, Ey, qmh, has_b0 != 0, b0x, b0y, b0z);
+        stage[2 * kChunk + s] = ux; stage[3 * kChunk + s] = uy; stage[4 * kChunk + s] = uz;
+        if (move) {
+            if constexpr (POW2) {
+                stage[s] = move1_pow2(x, ux, dtx);
+                stage[kChunk + s] = move1_pow2(y, uy, dty);
+            } else {
+                stage[s] = move1(x, ux, dt, g.dx);
+                stage[kChunk + s] = move1(y, uy, dt, g.dy);
+            }
         }
     }
-}
-// EM push from the packed field buffer gb[ncell][8] = Ex Ey Ez Bx | By Bz . .
-// (two 16-byte loads per CIC corner).
-template <bool POW2>
-__global__ void k_push_em_plain(Parts p, Geo g, const float* __restrict__ gb, float qmh, double dt, double dtx,
-                                double dty) {
-    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (t >= p.n) return;
-    const float x = p.x[t], y = p.y[t];
-    const Cic s = cic(x, y);
-    const int i0 = wrap_once(s.i0, g.nx), i1 = wrap_once(s.i0 + 1, g.nx);
-    const int j0 = wrap_once(s.j0, g.ny) * g.nx, j1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
-    const float4* q = reinterpret_cast<const float4*>(gb);
-    const float4 a0 = __ldg(q + 2 * (j0 + i0)), b0 = __ldg(q + 2 * (j0 + i0) + 1);
-    const float4 a1 = __ldg(q + 2 * (j0 + i1)), b1 = __ldg(q + 2 * (j0 + i1) + 1);
-    const float4 a2 = __ldg(q + 2 * (j1 + i0)), b2 = __ldg(q + 2 * (j1 + i0) + 1);
-    const float4 a3 = __ldg(q + 2 * (j1 + i1)), b3 = __ldg(q + 2 * (j1 + i1) + 1);
-    const float Ex = gather4_tile(s, a0.x, a1.x, a2.x, a3.x), Ey = gather4_tile(s, a0.y, a1.y, a2.y, a3.y);
-    const float Ez = gather4_tile(s, a0.z, a1.z, a2.z, a3.z), Bx = gather4_tile(s, a0.w, a1.w, a2.w, a3.w);
-    const float By = gather4_tile(s, b0.x, b1.x, b2.x, b3.x), Bz = gather4_tile(s, b0.y, b1.y, b2.y, b3.y);
-    float ux = p.ux[t], uy = p.uy[t], uz = p.uz[t];
-    boris_em(ux, uy, uz, Ex, Ey, Ez, Bx, By, Bz, qmh);
-    p.ux[t] = ux; p.uy[t] = uy; p.uz[t] = uz;
-    if constexpr (POW2) {
-        p.x[t] = move1_pow2(x, ux, dtx);
-        p.y[t] = move1_pow2(y, uy, dty);
+    if (move) {
+        float* const dst[6] = {p.x, p.y, p.ux, p.uy, p.uz, nullptr};
+        store_chunk(stage, dst, 5, c0, cnt, p.vec_ok != 0);
     } else {
-        p.x[t] = move1(x, ux, dt, g.dx);
-        p.y[t] = move1(y, uy, dt, g.dy);
+        float* const dst[6] = {p.ux, p.uy, p.uz, nullptr, nullptr, nullptr};
+        store_chunk(stage + 2 * kChunk, dst, 3, c0, cnt, p.vec_ok != 0);
     }
+}
+
+// EM push (em_push_tiled_kernel's arithmetic, include/pic/pusher.hpp:212-258),
+// gathering the six [ny][nx] field arrays at the four CIC corners in the
+// reference's tile-gather order.
+template <bool POW2, int NT>
+__global__ void __launch_bounds__(NT)
+k_push_em_chunk(Parts p, Geo g, const float* __restrict__ fex, const float* __restrict__ fey,
+                const float* __restrict__ fez, const float* __restrict__ fbx, const float* __restrict__ fby,
+                const float* __restrict__ fbz, float qmh, double dt, double dtx, double dty, DevState* st) {
+    extern __shared__ __align__(16) float stage[];
+    __shared__ unsigned long long bar;
+    const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
+    const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
+    const ChunkSrc src{{p.x, p.y, p.ux, p.uy, p.uz, nullptr}};
+    float x0, y0;
+    if (!load_chunk(stage, src, 5, c0, cnt, p.vec_ok != 0, &bar, st, &x0, &y0)) return;
+#pragma unroll
+    for (int it = 0; it < kChunk / NT; ++it) {
+        const int s = it * NT + threadIdx.x;
+        if (s >= cnt) break;
+        const float x = stage[s], y = stage[kChunk + s];
+        const Cic c = cic(x, y);
+        const int i0 = wrap_once(c.i0, g.nx), i1 = wrap_once(c.i0 + 1, g.nx);
+        const int j0 = wrap_once(c.j0, g.ny) * g.nx, j1 = wrap_once(c.j0 + 1, g.ny) * g.nx;
+        auto G = [&](const float* a) {
+            return gather4_tile(c, __ldg(a + j0 + i0), __ldg(a + j0 + i1), __ldg(a + j1 + i0), __ldg(a + j1 + i1));
+        };
+        const float Ex = G(fex), Ey = G(fey), Ez = G(fez), Bx = G(fbx), By = G(fby), Bz = G(fbz);
+        float ux = stage[2 * kChunk + s], uy = stage[3 * kChunk + s], uz = stage[4 * kChunk + s];
+        boris_em(ux, uy, uz, Ex, Ey, Ez, Bx, By, Bz, qmh);
+        stage[2 * kChunk + s] = ux; stage[3 * kChunk + s] = uy; stage[4 * kChunk + s] = uz;
+        if constexpr (POW2) {
+            stage[s] = move1_pow2(x, ux, dtx);
+            stage[kChunk + s] = move1_pow2(y, uy, dty);
+        } else {
+            stage[s] = move1(x, ux, dt, g.dx);
+            stage[kChunk + s] = move1(y, uy, dt, g.dy);
+        }
+    }
+    float* const dst[6] = {p.x, p.y, p.ux, p.uy, p.uz, nullptr};
+    store_chunk(stage, dst, 5, c0, cnt, p.vec_ok != 0);
 }
 // Max |u_d| and max |qm w/(dx dy)| over the particles -> DevState.
 __global__ void k_particle_max(Parts p, double qm_over_area, DevState* st) {
@@ -414,15 +450,19 @@ bool pow2_grid(const Ctx& c) {
     return std::frexp(c.geo.dx, &e) == 0.5 && std::frexp(c.geo.dy, &e) == 0.5;
 }
 
+int push_chunks(long long n) { return static_cast<int>((n + kChunk - 1) / kChunk); }
+constexpr size_t kPushSmem = sizeof(float) * 5 * kChunk;   // 40 KB
+constexpr int kPushThreads = 512;                          // 4 particles per thread
+
 void launch_push_es_from(Ctx& c, const float* ex, const float* ey, float dt_scale, bool move) {
     if (c.parts.n == 0) return;
     const float dt_eff = dt_scale * static_cast<float>(c.prm.dt);
     const float qmh = static_cast<float>(c.prm.qm) * 0.5f * dt_eff;
     const double dtx = c.prm.dt / c.geo.dx, dty = c.prm.dt / c.geo.dy;
-    auto kern = pow2_grid(c) ? k_push_es_plain<true> : k_push_es_plain<false>;
-    kern<<<grid_for(c.parts.n), kThreads, 0, c.stream>>>(c.parts, c.geo, ex, ey, qmh, c.prm.has_b0, c.prm.B0[0],
-                                                         c.prm.B0[1], c.prm.B0[2], c.prm.dt, dtx, dty,
-                                                         move ? 1 : 0);
+    auto kern = pow2_grid(c) ? k_push_es_chunk<true, kPushThreads> : k_push_es_chunk<false, kPushThreads>;
+    kern<<<push_chunks(c.parts.n), kPushThreads, kPushSmem, c.stream>>>(c.parts, c.geo, ex, ey, qmh, c.prm.has_b0,
+                                                                     c.prm.B0[0], c.prm.B0[1], c.prm.B0[2], c.prm.dt,
+                                                                     dtx, dty, move ? 1 : 0, c.st);
     AW_LAUNCH();
 }
 
@@ -434,12 +474,15 @@ void launch_push_es_plain(Ctx& c, const float* unused, float dt_scale, bool move
 
 void launch_push_em_plain(Ctx& c, const float* gb_unused) {
     (void)gb_unused;
+    const aw_field_ptrs& f = c.fld;
+    if (!f.Ex || !f.Ey || !f.Ez || !f.Bx || !f.By || !f.Bz)
+        throw Error(AW_ERR_STATE, "push_em: fields E and B must be bound");
     if (c.parts.n == 0) return;
-    launch_pack_em(c, false);   // bound E, B -> gb_dcu [ncell][8] (checks they are bound)
     const float qmh = static_cast<float>(c.prm.qm) * 0.5f * static_cast<float>(c.prm.dt);
     const double dtx = c.prm.dt / c.geo.dx, dty = c.prm.dt / c.geo.dy;
-    auto kern = pow2_grid(c) ? k_push_em_plain<true> : k_push_em_plain<false>;
-    kern<<<grid_for(c.parts.n), kThreads, 0, c.stream>>>(c.parts, c.geo, c.gb_dcu, qmh, c.prm.dt, dtx, dty);
+    auto kern = pow2_grid(c) ? k_push_em_chunk<true, kPushThreads> : k_push_em_chunk<false, kPushThreads>;
+    kern<<<push_chunks(c.parts.n), kPushThreads, kPushSmem, c.stream>>>(c.parts, c.geo, f.Ex, f.Ey, f.Ez, f.Bx, f.By,
+                                                                     f.Bz, qmh, c.prm.dt, dtx, dty, c.st);
     AW_LAUNCH();
 }
 

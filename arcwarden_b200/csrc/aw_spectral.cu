@@ -496,9 +496,8 @@ __global__ void k_add_pump(FieldAPI f, int nx, int n, PumpArgs pa, double t) {
     f.Ex[c] = ex; f.Ey[c] = ey; f.Ez[c] = ez;
 }
 
-// Pack caller E/B arrays into the [ncell][8] gather layout (unfused EM push and
-// dcu deposit) and, with MAX, record the field maxima the dcu deposit scale needs.
-template <bool MAX>
+// Pack caller E/B arrays into the [ncell][8] gather layout (unfused dcu
+// deposit) and record the field maxima its deposit scale needs.
 __global__ void k_pack_em(FieldAPI f, float* __restrict__ gb, int ncell, DevState* st) {
     float emax = 0.f, bmax = 0.f;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
@@ -510,7 +509,7 @@ __global__ void k_pack_em(FieldAPI f, float* __restrict__ gb, int ncell, DevStat
         emax = fmaxf(emax, fmaxf(fabsf(ex), fmaxf(fabsf(ey), fabsf(ez))));
         bmax = fmaxf(bmax, fmaxf(fabsf(bx), fmaxf(fabsf(by), fabsf(bz))));
     }
-    if (MAX) block_max_eb(emax, bmax, st);
+    block_max_eb(emax, bmax, st);
 }
 
 // Energy / charge partials from caller arrays (any may be null).
@@ -796,16 +795,12 @@ void launch_add_pump(Ctx& c, double t) {
     AW_LAUNCH();
 }
 
-void launch_pack_em(Ctx& c, bool maxima) {
+void launch_pack_em(Ctx& c) {
     const aw_field_ptrs& f = c.fld;
     if (!f.Ex || !f.Ey || !f.Ez || !f.Bx || !f.By || !f.Bz)
-        throw Error(AW_ERR_STATE, "fields E and B must be bound");
-    if (maxima) {
-        AW_CUDA(cudaMemsetAsync(&c.st->emax_bits, 0, 2 * sizeof(unsigned), c.stream));
-        k_pack_em<true><<<kGridBlocks, kThreads, 0, c.stream>>>(api_of(f), c.gb_dcu, c.geo.ncell, c.st);
-    } else {
-        k_pack_em<false><<<kGridBlocks, kThreads, 0, c.stream>>>(api_of(f), c.gb_dcu, c.geo.ncell, c.st);
-    }
+        throw Error(AW_ERR_STATE, "deposit_dcu: fields E and B must be bound");
+    AW_CUDA(cudaMemsetAsync(&c.st->emax_bits, 0, 2 * sizeof(unsigned), c.stream));
+    k_pack_em<<<kGridBlocks, kThreads, 0, c.stream>>>(api_of(f), c.gb_dcu, c.geo.ncell, c.st);
     AW_LAUNCH();
 }
 void launch_grid_diag(Ctx& c) {

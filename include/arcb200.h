@@ -206,6 +206,21 @@ int aw_set_resort(aw_ctx* ctx, int32_t every);
 int aw_tile_bins(aw_ctx* ctx, const int32_t** off, const int32_t** idx,
                  int32_t* ntiles, int32_t* ntx);
 
+/* ---- adjoint (no counterpart in the reference, which has no adjoint) -------
+ * Gradient of the final electrostatic field energy with respect to the initial
+ * particle velocities, for the fused ES step (Simulation<Cfg>::init + nsteps
+ * steps, ElectrostaticSpectralSolver, Boris about B0, no pump). The bound
+ * particles hold the initial state (x, u) on entry and again on return. The
+ * forward run keeps a checkpoint every `checkpoint_every` steps (particles,
+ * pending deposit, device state); the backward sweep recomputes each segment
+ * from its checkpoint and applies the transposed step (Boris and move
+ * transposes, the CIC scatter of the field cotangent on the deposit engine,
+ * the transposed spectral solve, the gather's position derivative) in reverse.
+ * loss = 0.5 eps0 dx dy sum E^2 of the last step's field (Diagnostics ee);
+ * dux/duy/duz (device, n floats each) = dloss/du0. Synchronises. */
+int aw_grad_es(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux, float* duy, float* duz,
+               double* loss);
+
 /* ElectrostaticSpectralSolver::solve, include/pic/solver_es.hpp:238-259. */
 int aw_solve_es(aw_ctx* ctx);
 /* DarwinSpectralSolver::solve_el_b, include/pic/solver_darwin.hpp:188-216. */

@@ -186,6 +186,51 @@ def test_push_bit_exact(setup, aw, oracle, which):
         assert np.array_equal(got[k], q[k]), k
 
 
+@pytest.mark.parametrize("which", ["es", "half", "em"])
+@pytest.mark.parametrize("n, offset", [(5003, 0), (5003, 1), (2048 * 3, 1), (3, 0)])
+def test_push_ragged_and_unaligned(torch_cuda, aw, oracle, which, n, offset):
+    """The chunked pushes on a ragged last chunk (n not a multiple of 2048 or 4)
+    and on arrays that are not 16-byte aligned (views one float in): bulk copies
+    for the aligned body, plain loads and stores for the rest, same bits."""
+    nx = ny = 32
+    B0 = (0.3, 0.1, 0.2)
+    rng = np.random.default_rng(n + offset)
+    dev = torch_cuda.device("cuda:0")
+    host = {"x": rng.uniform(0, nx, n), "y": rng.uniform(0, ny, n), "ux": rng.normal(0, 0.1, n),
+            "uy": rng.normal(0, 0.1, n), "uz": rng.normal(0, 0.1, n), "w": np.full(n, 0.5)}
+    host = {k: v.astype(np.float32) for k, v in host.items()}
+    store = {k: torch_cuda.zeros(n + offset, dtype=torch_cuda.float32, device=dev) for k in host}
+    P = {k: store[k][offset:] for k in host}
+    for k in host:
+        P[k].copy_(torch_cuda.from_numpy(host[k]).to(dev))
+    cell = torch_cuda.zeros(n, dtype=torch_cuda.int32, device=dev)
+    f6 = synthetic_em(nx, ny)
+    F = {k: torch_cuda.from_numpy(f6[i]).to(dev) for i, k in enumerate(("Ex", "Ey", "Ez", "Bx", "By", "Bz"))}
+    ctx = aw.Context(nx, ny, float(nx), float(ny), model=aw.AW_MODEL_DARWIN, dt=0.1, B0=B0,
+                     stream=torch_cuda.cuda.current_stream().cuda_stream)
+    try:
+        ctx.bind_particles(*(P[k] for k in PARTICLE_KEYS), cell)
+        ctx.bind_fields(**F)
+        {"es": ctx.push_es, "half": ctx.half_step_back, "em": ctx.push_em}[which]()
+        torch_cuda.cuda.synchronize()
+        got = {k: P[k].cpu().numpy() for k in PARTICLE_KEYS}
+    finally:
+        ctx.close()
+    q = {k: host[k].copy() for k in PARTICLE_KEYS}
+    g = oracle.geo(nx, ny, float(nx), float(ny))
+    b0 = np.array(B0, np.float32)
+    if which == "es":
+        oracle.push_es(g, q["x"], q["y"], q["ux"], q["uy"], q["uz"], oracle.pack_es(f6[0], f6[1]), qmh(-1.0, 0.1),
+                       1, b0, 0.1, True, False)
+    elif which == "half":
+        oracle.push_es(g, q["x"], q["y"], q["ux"], q["uy"], q["uz"], oracle.pack_es(f6[0], f6[1]),
+                       qmh(-1.0, np.float32(-0.5) * np.float32(0.1)), 1, b0, 0.1, False, False)
+    else:
+        oracle.push_em(g, q["x"], q["y"], q["ux"], q["uy"], q["uz"], oracle.pack_em(*f6), qmh(-1.0, 0.1), 0.1, False)
+    for k in ("x", "y", "ux", "uy", "uz"):
+        assert np.array_equal(got[k], q[k]), k
+
+
 def _boris():
     return json.loads((GOLDEN / "boris.json").read_text())
 
