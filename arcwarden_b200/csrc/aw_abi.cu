@@ -99,6 +99,7 @@ void free_all(Ctx& c) {
 void drop_graph(Ctx& c) {
     if (c.gexec) { cudaGraphExecDestroy(c.gexec); c.gexec = nullptr; }
     if (c.graph) { cudaGraphDestroy(c.graph); c.graph = nullptr; }
+    adj_drop_graphs(c);
 }
 
 void set_fft_stream(Ctx& c) {
@@ -194,6 +195,155 @@ using aw::Error;
 using aw::guarded;
 
 struct aw_ctx { Ctx c; };
+
+namespace aw {
+namespace {
+// Simulation<Cfg>::init: the t = 0 field solve, the ES half-step rollback and
+// the pending deposit of step 0. Synchronises.
+void init_impl(Ctx& c) {
+    aw::drop_graph(c);
+    aw::launch_set_step(c, 0);
+    AW_CUDA(cudaMemsetAsync(&c.st->have_rms, 0, sizeof(int), c.stream));
+    aw::launch_particle_max(c);
+    aw::launch_copy_umax(c);     // the step-begin copies umax -> ucur
+    aw::launch_make_scales(c);
+    aw::reset_acc(c, c.acc_src, c.nsrc());
+    if (c.model == AW_MODEL_ES) {
+        aw::launch_deposit_src(c, 1);
+        aw::es_fields_from_pending(c, false);
+        // u -> u(-dt/2), gathering E(x^0) from the solve's output
+        aw::launch_push_es_from(c, c.r_out, c.r_out + c.geo.ncell, -0.5f, false);
+        aw::launch_particle_max(c);
+        aw::launch_copy_umax(c);
+        aw::launch_deposit_src(c, 1);    // pending rho(x^0) for step 0
+    } else {
+        aw::launch_deposit_src(c, 8);
+        aw::launch_rms_reduce(c, true, false);     // source rms for the capped scales
+        aw::darwin_fields_from_pending(c, true);   // t = 0 fields
+        aw::launch_copy_umax(c);
+        aw::launch_promote_scales(c);              // the rms-capped scales of step 0
+        aw::launch_deposit_src(c, 8);              // pending rho,J,amu for step 0
+        aw::launch_rms_reduce(c, true, true);
+    }
+    c.pending_valid = true;
+    aw::launch_set_step(c, 0);
+    AW_CUDA(cudaStreamSynchronize(c.stream));
+    c.inited = true;
+}
+}  // namespace
+}  // namespace aw
+
+namespace aw {
+namespace {
+void copy_parts_to(Ctx& c, float* dst) {
+    const size_t b = sizeof(float) * static_cast<size_t>(c.parts.n);
+    const float* a[5] = {c.parts.x, c.parts.y, c.parts.ux, c.parts.uy, c.parts.uz};
+    for (int k = 0; k < 5; ++k)
+        AW_CUDA(cudaMemcpyAsync(dst + k * c.parts.n, a[k], b, cudaMemcpyDeviceToDevice, c.stream));
+}
+void copy_parts_from(Ctx& c, const float* src) {
+    const size_t b = sizeof(float) * static_cast<size_t>(c.parts.n);
+    float* a[5] = {c.parts.x, c.parts.y, c.parts.ux, c.parts.uy, c.parts.uz};
+    for (int k = 0; k < 5; ++k)
+        AW_CUDA(cudaMemcpyAsync(a[k], src + k * c.parts.n, b, cudaMemcpyDeviceToDevice, c.stream));
+}
+
+// Capture `body` on the context's stream into an instantiated graph.
+template <class F>
+cudaGraphExec_t capture_exec(Ctx& c, F body) {
+    cudaGraph_t g = nullptr;
+    AW_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        body();
+    } catch (...) {
+        cudaStreamEndCapture(c.stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    AW_CUDA(cudaStreamEndCapture(c.stream, &g));
+    cudaGraphExec_t e = nullptr;
+    const cudaError_t r = cudaGraphInstantiate(&e, g, 0);
+    cudaGraphDestroy(g);
+    AW_CUDA(r);
+    return e;
+}
+
+// Forward run with checkpoints, then the backward sweep segment by segment
+// (recompute the segment from its checkpoint, then transpose its steps in
+// reverse). A checkpoint holds the particle state, the pending rho accumulator
+// and the device state block, so the recompute repeats the forward run bit for
+// bit (the deposits are exact). The forward step, the recompute step and the
+// backward step each replay one CUDA graph; the trajectory slot they address
+// lives on the device.
+double grad_es_impl(Ctx& c, long long nsteps, int every, float* dux, float* duy, float* duz) {
+    adj_prepare(c, nsteps, every);
+    AdjWS& w = *c.adj;
+    const long long n = c.parts.n;
+    const size_t nc = static_cast<size_t>(c.geo.ncell);
+    copy_parts_to(c, w.init_parts);
+    init_impl(c);                                   // drops the step graphs, re-created below
+    prep_adj_scatter();
+    if (!c.gexec) c.gexec = capture_exec(c, [&] { step_body(c); });
+    const AdjK kf = adj_constants(c, 1.0f);
+    AdjP a{w.traj_xy, w.lam, w.lam + n, w.lam + 2 * n, w.lam + 3 * n, w.lam + 4 * n, n, (n % 4 == 0) ? 1 : 0};
+    if (!w.g_rec)
+        w.g_rec = capture_exec(c, [&] {
+            launch_traj_store_xy(c);
+            step_body(c);
+            launch_traj_store_E(c);
+            launch_slot_add(c, 1);
+        });
+    if (!w.g_bwd)
+        w.g_bwd = capture_exec(c, [&] {
+            launch_slot_add(c, -1);
+            launch_adj_scatter(c, a, kf, w.traj_E, w.ad, w.acc);
+            launch_adj_finalize(c);
+            adj_transpose_solve(c);
+            launch_adj_gather(c, a, kf);
+        });
+
+    for (long long s = 0; s < nsteps; ++s) {
+        if (s % every == 0) {
+            const int k = static_cast<int>(s / every);
+            copy_parts_to(c, w.ck_parts + static_cast<size_t>(k) * 5 * n);
+            AW_CUDA(cudaMemcpyAsync(w.ck_acc + k * nc, c.acc_src, sizeof(unsigned long long) * nc,
+                                    cudaMemcpyDeviceToDevice, c.stream));
+            AW_CUDA(cudaMemcpyAsync(w.ck_st + k, c.st, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
+        }
+        AW_CUDA(cudaGraphLaunch(c.gexec, c.stream));
+    }
+    aw_diag d{};
+    AW_CUDA(cudaMemcpyAsync(&d, c.diag, sizeof(aw_diag), cudaMemcpyDeviceToHost, c.stream));
+    AW_CUDA(cudaStreamSynchronize(c.stream));
+    const double loss = d.ee;
+
+    AW_CUDA(cudaMemsetAsync(w.lam, 0, sizeof(float) * 5 * static_cast<size_t>(n), c.stream));
+    AdjDev ad0{};
+    ad0.ext_scale = static_cast<float>(c.prm.eps0 * c.geo.dx * c.geo.dy);   // dL/dE = eps0 E dx dy
+    for (int k = w.nck - 1; k >= 0; --k) {
+        const long long s0 = static_cast<long long>(k) * every;
+        const long long s1 = std::min(nsteps, s0 + every);
+        copy_parts_from(c, w.ck_parts + static_cast<size_t>(k) * 5 * n);
+        AW_CUDA(cudaMemcpyAsync(c.acc_src, w.ck_acc + k * nc, sizeof(unsigned long long) * nc,
+                                cudaMemcpyDeviceToDevice, c.stream));
+        AW_CUDA(cudaMemcpyAsync(c.st, w.ck_st + k, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
+        if (k == w.nck - 1) {
+            AW_CUDA(cudaMemcpyAsync(w.ad, &ad0, sizeof(AdjDev), cudaMemcpyHostToDevice, c.stream));
+        } else {
+            AW_CUDA(cudaMemsetAsync(&w.ad->slot, 0, sizeof(int), c.stream));
+        }
+        for (long long s = s0; s < s1; ++s) AW_CUDA(cudaGraphLaunch(w.g_rec, c.stream));
+        for (long long s = s1 - 1; s >= s0; --s) AW_CUDA(cudaGraphLaunch(w.g_bwd, c.stream));
+    }
+    launch_adj_out(c, dux, duy, duz);
+    copy_parts_from(c, w.init_parts);
+    c.pending_valid = false;
+    c.inited = false;
+    AW_CUDA(cudaStreamSynchronize(c.stream));
+    return loss;
+}
+}  // namespace
+}  // namespace aw
 
 extern "C" {
 
@@ -624,42 +774,6 @@ int aw_add_pump(aw_ctx* ctx, double t) {
 
 // ---- the fused step -------------------------------------------------------------
 
-namespace aw {
-namespace {
-// Simulation<Cfg>::init: the t = 0 field solve, the ES half-step rollback and
-// the pending deposit of step 0. Synchronises.
-void init_impl(Ctx& c) {
-    aw::drop_graph(c);
-    aw::launch_set_step(c, 0);
-    AW_CUDA(cudaMemsetAsync(&c.st->have_rms, 0, sizeof(int), c.stream));
-    aw::launch_particle_max(c);
-    aw::launch_copy_umax(c);     // the step-begin copies umax -> ucur
-    aw::launch_make_scales(c);
-    aw::reset_acc(c, c.acc_src, c.nsrc());
-    if (c.model == AW_MODEL_ES) {
-        aw::launch_deposit_src(c, 1);
-        aw::es_fields_from_pending(c, false);
-        // u -> u(-dt/2), gathering E(x^0) from the solve's output
-        aw::launch_push_es_from(c, c.r_out, c.r_out + c.geo.ncell, -0.5f, false);
-        aw::launch_particle_max(c);
-        aw::launch_copy_umax(c);
-        aw::launch_deposit_src(c, 1);    // pending rho(x^0) for step 0
-    } else {
-        aw::launch_deposit_src(c, 8);
-        aw::launch_rms_reduce(c, true, false);     // source rms for the capped scales
-        aw::darwin_fields_from_pending(c, true);   // t = 0 fields
-        aw::launch_copy_umax(c);
-        aw::launch_promote_scales(c);              // the rms-capped scales of step 0
-        aw::launch_deposit_src(c, 8);              // pending rho,J,amu for step 0
-        aw::launch_rms_reduce(c, true, true);
-    }
-    c.pending_valid = true;
-    aw::launch_set_step(c, 0);
-    AW_CUDA(cudaStreamSynchronize(c.stream));
-    c.inited = true;
-}
-}  // namespace
-}  // namespace aw
 
 int aw_init(aw_ctx* ctx) {
     return guarded([&] {
@@ -719,91 +833,6 @@ int aw_run(aw_ctx* ctx, int64_t n0, int64_t nsteps, int32_t use_graph) {
 
 // ---- the ES adjoint -------------------------------------------------------------
 
-namespace aw {
-namespace {
-void copy_parts_to(Ctx& c, float* dst) {
-    const size_t b = sizeof(float) * static_cast<size_t>(c.parts.n);
-    const float* a[5] = {c.parts.x, c.parts.y, c.parts.ux, c.parts.uy, c.parts.uz};
-    for (int k = 0; k < 5; ++k)
-        AW_CUDA(cudaMemcpyAsync(dst + k * c.parts.n, a[k], b, cudaMemcpyDeviceToDevice, c.stream));
-}
-void copy_parts_from(Ctx& c, const float* src) {
-    const size_t b = sizeof(float) * static_cast<size_t>(c.parts.n);
-    float* a[5] = {c.parts.x, c.parts.y, c.parts.ux, c.parts.uy, c.parts.uz};
-    for (int k = 0; k < 5; ++k)
-        AW_CUDA(cudaMemcpyAsync(a[k], src + k * c.parts.n, b, cudaMemcpyDeviceToDevice, c.stream));
-}
-
-// Forward run with checkpoints, then the backward sweep segment by segment
-// (recompute the segment from its checkpoint, then transpose its steps in
-// reverse). A checkpoint holds the particle state, the pending rho accumulator
-// and the device state block, so the recompute repeats the forward run bit for
-// bit (the deposits are exact).
-double grad_es_impl(Ctx& c, long long nsteps, int every, float* dux, float* duy, float* duz) {
-    adj_prepare(c, nsteps, every);
-    AdjWS& w = *c.adj;
-    const long long n = c.parts.n;
-    const size_t nc = static_cast<size_t>(c.geo.ncell);
-    copy_parts_to(c, w.init_parts);
-    init_impl(c);
-    for (long long s = 0; s < nsteps; ++s) {
-        if (s % every == 0) {
-            const int k = static_cast<int>(s / every);
-            copy_parts_to(c, w.ck_parts + static_cast<size_t>(k) * 5 * n);
-            AW_CUDA(cudaMemcpyAsync(w.ck_acc + k * nc, c.acc_src, sizeof(unsigned long long) * nc,
-                                    cudaMemcpyDeviceToDevice, c.stream));
-            AW_CUDA(cudaMemcpyAsync(w.ck_st + k, c.st, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
-        }
-        launch_set_step(c, s);
-        step_body(c);
-    }
-    aw_diag d{};
-    AW_CUDA(cudaMemcpyAsync(&d, c.diag, sizeof(aw_diag), cudaMemcpyDeviceToHost, c.stream));
-    AW_CUDA(cudaStreamSynchronize(c.stream));
-    const double loss = d.ee;
-
-    AW_CUDA(cudaMemsetAsync(w.lam, 0, sizeof(float) * 5 * static_cast<size_t>(n), c.stream));
-    AW_CUDA(cudaMemsetAsync(w.ad, 0, sizeof(AdjDev), c.stream));
-    const AdjK kf = adj_constants(c, 1.0f);
-    const float ext = static_cast<float>(c.prm.eps0 * c.geo.dx * c.geo.dy);   // dL/dE = eps0 E dx dy
-    for (int k = w.nck - 1; k >= 0; --k) {
-        const long long s0 = static_cast<long long>(k) * every;
-        const long long s1 = std::min(nsteps, s0 + every);
-        copy_parts_from(c, w.ck_parts + static_cast<size_t>(k) * 5 * n);
-        AW_CUDA(cudaMemcpyAsync(c.acc_src, w.ck_acc + k * nc, sizeof(unsigned long long) * nc,
-                                cudaMemcpyDeviceToDevice, c.stream));
-        AW_CUDA(cudaMemcpyAsync(c.st, w.ck_st + k, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
-        c.pending_valid = true;
-        for (long long s = s0; s < s1; ++s) {
-            float* xy = w.traj_xy + static_cast<size_t>(s - s0) * 2 * n;
-            AW_CUDA(cudaMemcpyAsync(xy, c.parts.x, sizeof(float) * n, cudaMemcpyDeviceToDevice, c.stream));
-            AW_CUDA(cudaMemcpyAsync(xy + n, c.parts.y, sizeof(float) * n, cudaMemcpyDeviceToDevice, c.stream));
-            launch_set_step(c, s);
-            step_body(c);
-            AW_CUDA(cudaMemcpyAsync(w.traj_E + static_cast<size_t>(s - s0) * 2 * nc, c.gb_es,
-                                    sizeof(float) * 2 * nc, cudaMemcpyDeviceToDevice, c.stream));
-        }
-        for (long long s = s1 - 1; s >= s0; --s) {
-            const float* xy = w.traj_xy + static_cast<size_t>(s - s0) * 2 * n;
-            const float* E = w.traj_E + static_cast<size_t>(s - s0) * 2 * nc;
-            AdjP a{xy, xy + n, w.lam, w.lam + n, w.lam + 2 * n, w.lam + 3 * n, w.lam + 4 * n, n, 0};
-            auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
-            a.vec_ok = (al(a.xn) && al(a.yn)) ? 1 : 0;
-            launch_adj_scatter(c, a, kf, E, w.ad, w.acc);
-            launch_adj_finalize(c, s == nsteps - 1 ? E : nullptr, ext);
-            adj_transpose_solve(c);
-            launch_adj_gather(c, a, kf);
-        }
-    }
-    launch_adj_out(c, dux, duy, duz);
-    copy_parts_from(c, w.init_parts);
-    c.pending_valid = false;
-    c.inited = false;
-    AW_CUDA(cudaStreamSynchronize(c.stream));
-    return loss;
-}
-}  // namespace
-}  // namespace aw
 
 int aw_grad_es(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux, float* duy, float* duz,
                double* loss) {

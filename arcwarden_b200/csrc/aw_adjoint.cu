@@ -25,10 +25,12 @@ namespace {
 
 constexpr int kT = 256;
 
-__global__ void k_adj_finalize(unsigned long long* __restrict__ acc, const AdjDev* ad, const float2* E_ext,
-                               float ext_scale, float* __restrict__ lE, int ncell) {
+__global__ void k_adj_finalize(unsigned long long* __restrict__ acc, const AdjDev* ad, const float2* trajE,
+                               float* __restrict__ lE, int ncell) {
     const double i0 = 1.0 / static_cast<double>(ad->S[0]);
     const double i1 = 1.0 / static_cast<double>(ad->S[1]);
+    const float ext = ad->ext_scale;
+    const float2* __restrict__ E = trajE + static_cast<size_t>(ad->slot) * ncell;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
         const long long a0 = static_cast<long long>(acc[c]);
         const long long a1 = static_cast<long long>(acc[ncell + c]);
@@ -36,15 +38,32 @@ __global__ void k_adj_finalize(unsigned long long* __restrict__ acc, const AdjDe
         acc[ncell + c] = 0ull;
         float v0 = __double2float_rn(static_cast<double>(a0) * i0);
         float v1 = __double2float_rn(static_cast<double>(a1) * i1);
-        if (E_ext) {
-            const float2 e = E_ext[c];
-            v0 = __fmaf_rn(ext_scale, e.x, v0);
-            v1 = __fmaf_rn(ext_scale, e.y, v1);
+        if (ext != 0.0f) {
+            const float2 e = E[c];
+            v0 = __fmaf_rn(ext, e.x, v0);
+            v1 = __fmaf_rn(ext, e.y, v1);
         }
         lE[c] = v0;
         lE[ncell + c] = v1;
     }
 }
+
+// Trajectory stores of the recompute (slot from the device).
+__global__ void k_traj_store_xy(const float* __restrict__ x, const float* __restrict__ y, long long n,
+                                float* __restrict__ traj, const AdjDev* ad) {
+    float* d = traj + static_cast<size_t>(ad->slot) * 2 * n;
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        d[i] = x[i];
+        d[n + i] = y[i];
+    }
+}
+__global__ void k_traj_store_E(const float2* __restrict__ gb, int ncell, float2* __restrict__ trajE,
+                               const AdjDev* ad) {
+    float2* d = trajE + static_cast<size_t>(ad->slot) * ncell;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) d[c] = gb[c];
+}
+__global__ void k_slot_add(AdjDev* ad, int delta) { ad->slot += delta; }
 
 // lrho_k = sum_d conj(K_d) lE_d,k with K_d = -i k_d / (eps0 k^2) (times 1/N for
 // the unnormalised C2R), zero at k = 0 and on the Nyquist lines like the
@@ -77,9 +96,10 @@ k_adj_gather(AdjP a, const float* __restrict__ w, Geo g, double qoa, const float
              AdjDev* ad) {
     __shared__ unsigned smax[kT / 32];
     const long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const float* __restrict__ xn = a.traj + static_cast<size_t>(ad->slot) * 2 * a.n;
     float m = 0.0f;
     if (i < a.n) {
-        const float x = a.xn[i], y = a.yn[i];
+        const float x = xn[i], y = xn[a.n + i];
         float lx = a.lx[i], ly = a.ly[i];
         if (x >= 0.0f && x < g.nxf && y >= 0.0f && y < g.nyf) {
             const float q = __double2float_rn(qoa * static_cast<double>(w[i]));
@@ -110,6 +130,7 @@ k_adj_gather(AdjP a, const float* __restrict__ w, Geo g, double qoa, const float
         unsigned mx = 0u;
         for (int k2 = 0; k2 < kT / 32; ++k2) mx = max(mx, smax[k2]);
         atomicMax(&ad->lmax_bits, mx);
+        if (blockIdx.x == 0) ad->ext_scale = 0.0f;   // the loss term belongs to the last step only
     }
 }
 
@@ -161,9 +182,18 @@ AdjK adj_constants(const Ctx& c, float dt_scale) {
     return k;
 }
 
+void adj_drop_graphs(Ctx& c) {
+    AdjWS* w = c.adj;
+    if (!w) return;
+    if (w->g_rec) cudaGraphExecDestroy(w->g_rec);
+    if (w->g_bwd) cudaGraphExecDestroy(w->g_bwd);
+    w->g_rec = w->g_bwd = nullptr;
+}
+
 void free_adjoint(Ctx& c) {
     AdjWS* w = c.adj;
     if (!w) return;
+    adj_drop_graphs(c);
     void* bufs[] = {w->lam, w->init_parts, w->ck_parts, w->ck_acc, w->ck_st, w->traj_xy, w->traj_E,
                     w->acc, w->lE, w->lEk, w->lrk, w->lrho, w->ad};
     for (void* b : bufs) if (b) cudaFree(b);
@@ -208,11 +238,29 @@ void adj_prepare(Ctx& c, long long nsteps, int every) {
     }
 }
 
-void launch_adj_finalize(Ctx& c, const float* E_ext, float ext_scale) {
+void launch_adj_finalize(Ctx& c) {
     AdjWS& w = *c.adj;
     const int blocks = std::min(blocks_n(c.geo.ncell), 148 * 8);
-    k_adj_finalize<<<blocks, kT, 0, c.stream>>>(w.acc, w.ad, reinterpret_cast<const float2*>(E_ext), ext_scale,
-                                                w.lE, c.geo.ncell);
+    k_adj_finalize<<<blocks, kT, 0, c.stream>>>(w.acc, w.ad, reinterpret_cast<const float2*>(w.traj_E), w.lE,
+                                                c.geo.ncell);
+    AW_LAUNCH();
+}
+
+void launch_traj_store_xy(Ctx& c) {
+    AdjWS& w = *c.adj;
+    const int blocks = static_cast<int>(std::min<long long>(blocks_n(w.n), 148 * 8));
+    k_traj_store_xy<<<blocks, kT, 0, c.stream>>>(c.parts.x, c.parts.y, w.n, w.traj_xy, w.ad);
+    AW_LAUNCH();
+}
+void launch_traj_store_E(Ctx& c) {
+    AdjWS& w = *c.adj;
+    const int blocks = std::min(blocks_n(c.geo.ncell), 148 * 8);
+    k_traj_store_E<<<blocks, kT, 0, c.stream>>>(reinterpret_cast<const float2*>(c.gb_es), c.geo.ncell,
+                                                reinterpret_cast<float2*>(w.traj_E), w.ad);
+    AW_LAUNCH();
+}
+void launch_slot_add(Ctx& c, int delta) {
+    k_slot_add<<<1, 1, 0, c.stream>>>(c.adj->ad, delta);
     AW_LAUNCH();
 }
 

@@ -437,7 +437,7 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
 // |lE_d| <= 2 |qmh| |lu3| (R is a rotation); particles beyond it take the slow
 // path. Stage = x, y, lEx*S0, lEy*S1.
 __global__ void __launch_bounds__(kThreads, 3)
-k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ E, AdjDev* ad,
+k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ trajE, AdjDev* ad,
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st) {
     constexpr int NF = 2, NS = 4, NIN = 2;
     constexpr bool T0 = false;
@@ -448,12 +448,15 @@ k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ E, AdjDev* ad,
 
     const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
     const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), a.n - c0));
+    const int slot = ad->slot;
+    const float* xn = a.traj + static_cast<size_t>(slot) * 2 * a.n;
+    const float2* __restrict__ E = trajE + static_cast<size_t>(slot) * g.ncell;
     const float lmax = __uint_as_float(ad->lmax_bits);
     const float sc = scale_for_bound(__fmul_rn(__fmul_rn(2.0f * fabsf(k.qmh), lmax), 1.0001f));
     const float S[NF] = {sc, sc};
     if (blockIdx.x == 0 && threadIdx.x == 0) { ad->S[0] = sc; ad->S[1] = sc; }
     if (threadIdx.x == 0) nlist = 0;
-    const ChunkSrc src{{a.xn, a.yn, nullptr, nullptr, nullptr, nullptr}};
+    const ChunkSrc src{{xn, xn + a.n, nullptr, nullptr, nullptr, nullptr}};
     float x0, y0;
     if (!load_chunk(m.stage, src, NIN, c0, cnt, a.vec_ok != 0, &bar, st, &x0, &y0)) return;
     int ir, jr;
@@ -809,13 +812,15 @@ void launch_deposit_src(Ctx& c, int which) {
     }
 }
 
-void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* E, AdjDev* ad,
+void prep_adj_scatter() { prep_smem(k_adj_scatter, smem_bytes(2, 4)); }
+
+void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE, AdjDev* ad,
                         unsigned long long* acc) {
     if (a.n == 0) return;
     const size_t sh = smem_bytes(2, 4);
     prep_smem(k_adj_scatter, sh);
-    k_adj_scatter<<<nchunks(a.n), kThreads, sh, c.stream>>>(a, c.geo, k, reinterpret_cast<const float2*>(E), ad,
-                                                             acc, wmax_cells(2), c.st);
+    k_adj_scatter<<<nchunks(a.n), kThreads, sh, c.stream>>>(a, c.geo, k, reinterpret_cast<const float2*>(trajE),
+                                                             ad, acc, wmax_cells(2), c.st);
     AW_LAUNCH();
 }
 

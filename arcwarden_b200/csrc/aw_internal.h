@@ -131,11 +131,12 @@ struct AdjK {
     float tx, ty, tz, sx, sy, sz;
     int   rot;
 };
-// Adjoint particle state (cotangents of x, y, ux, uy, uz) and the positions x_n
-// of the step being transposed.
+// Adjoint particle state (cotangents of x, y, ux, uy, uz) and the segment
+// trajectory: the positions of step slot k are traj[k][0][n] (x), traj[k][1][n]
+// (y), with the slot read on the device (AdjDev::slot) so that the backward
+// step is one pointer-invariant graph.
 struct AdjP {
-    const float* xn;
-    const float* yn;
+    const float* traj;
     float *lx, *ly, *lux, *luy, *luz;
     long long n;
     int vec_ok;
@@ -144,6 +145,8 @@ struct AdjP {
 struct AdjDev {
     unsigned lmax_bits;   // max |lu3| (2-norm) for the next scatter's scale
     float    S[2];        // scales of the pending field-cotangent scatter
+    int      slot;        // trajectory slot of the step being recomputed / transposed
+    float    ext_scale;   // dloss/dE = ext_scale E for the last step, 0 for the others
 };
 
 // Workspace of the ES adjoint sweep (aw_grad_es): checkpoints of the forward
@@ -165,6 +168,8 @@ struct AdjWS {
     float* lrho = nullptr;                // [ncell] charge-density cotangent
     AdjDev* ad = nullptr;
     cufftHandle p_r2c2 = 0;               // batch-2 R2C
+    cudaGraphExec_t g_rec = nullptr;      // recompute step: store x_n, step, store E_n, slot + 1
+    cudaGraphExec_t g_bwd = nullptr;      // backward step: slot - 1, A, solve^T, B
 };
 
 // ---- launchers (aw_particles.cu) -------------------------------------------
@@ -190,8 +195,9 @@ void launch_push_deposit_em(Ctx& c);
 // Backward step A of the ES adjoint: Boris/move transposes, field-cotangent
 // scatter into acc [2][ncell] (scales from ad->lmax_bits, stored to ad->S) and
 // the E-gather position derivative (E = interleaved [ncell][2]).
-void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* E, AdjDev* ad,
+void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE, AdjDev* ad,
                         unsigned long long* acc);
+void prep_adj_scatter();   // its shared-memory opt-in (before any capture)
 
 // ---- launchers (aw_spectral.cu) -------------------------------------------
 int  grid_partial_blocks();
@@ -222,9 +228,15 @@ void launch_step_reduce(Ctx& c);                   // end of a fused step: diagn
 AdjK adj_constants(const Ctx& c, float dt_scale);
 void adj_prepare(Ctx& c, long long nsteps, int every);   // (re)allocates c.adj
 void free_adjoint(Ctx& c);
-// lE = acc / S (+ ext_scale * E_ext, E_ext interleaved [ncell][2], may be null);
-// acc is zeroed.
-void launch_adj_finalize(Ctx& c, const float* E_ext, float ext_scale);
+// lE = acc / S + ad->ext_scale * E_slot (E of the slot's step, interleaved
+// [ncell][2]); acc is zeroed.
+void launch_adj_finalize(Ctx& c);
+// Trajectory stores of the recompute: x_n, y_n before the step and E_n after it,
+// at the device slot; the slot counter step.
+void launch_traj_store_xy(Ctx& c);
+void launch_traj_store_E(Ctx& c);
+void launch_slot_add(Ctx& c, int delta);
+void adj_drop_graphs(Ctx& c);
 // lrho = S^T lE: the transpose of the spectral Poisson field solve.
 void adj_transpose_solve(Ctx& c);
 // Backward step B: lx += q dlrho/dx at x_n; max |lu3| of the next step A.

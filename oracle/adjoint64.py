@@ -45,35 +45,39 @@ class Case:
 
     # ---- CIC ------------------------------------------------------------------
     def stencil(self, x, y):
+        """Flat corner indices (c00, c10, c01, c11) and fractions (fx, fy)."""
         i0 = np.floor(x).astype(np.int64)
         j0 = np.floor(y).astype(np.int64)
         fx, fy = x - i0, y - j0
         i0 %= self.nx
         j0 %= self.ny
         i1, j1 = (i0 + 1) % self.nx, (j0 + 1) % self.ny
-        return i0, j0, i1, j1, fx, fy
+        r0, r1 = j0 * self.nx, j1 * self.nx
+        return (r0 + i0, r0 + i1, r1 + i0, r1 + i1), fx, fy
 
-    def deposit(self, x, y, q):
-        i0, j0, i1, j1, fx, fy = self.stencil(x, y)
-        g = np.zeros(self.ny * self.nx)
-        nx = self.nx
-        np.add.at(g, j0 * nx + i0, q * (1 - fx) * (1 - fy))
-        np.add.at(g, j0 * nx + i1, q * fx * (1 - fy))
-        np.add.at(g, j1 * nx + i0, q * (1 - fx) * fy)
-        np.add.at(g, j1 * nx + i1, q * fx * fy)
+    def deposit(self, st, q):
+        (c00, c10, c01, c11), fx, fy = st
+        m = self.ny * self.nx
+        gx, gy = 1.0 - fx, 1.0 - fy
+        g = np.bincount(c00, q * gx * gy, minlength=m)
+        g += np.bincount(c10, q * fx * gy, minlength=m)
+        g += np.bincount(c01, q * gx * fy, minlength=m)
+        g += np.bincount(c11, q * fx * fy, minlength=m)
         return g.reshape(self.ny, self.nx)
 
-    def gather(self, G, x, y):
-        i0, j0, i1, j1, fx, fy = self.stencil(x, y)
-        return ((1 - fx) * (1 - fy) * G[j0, i0] + fx * (1 - fy) * G[j0, i1]
-                + (1 - fx) * fy * G[j1, i0] + fx * fy * G[j1, i1])
+    def gather(self, G, st):
+        (c00, c10, c01, c11), fx, fy = st
+        G = G.reshape(-1)
+        gx, gy = 1.0 - fx, 1.0 - fy
+        return gx * gy * G[c00] + fx * gy * G[c10] + gx * fy * G[c01] + fx * fy * G[c11]
 
-    def gather_grad(self, G, x, y):
+    def gather_grad(self, G, st):
         """(dG/dx, dG/dy) of the CIC interpolant at the particles (cell units)."""
-        i0, j0, i1, j1, fx, fy = self.stencil(x, y)
-        g00, g10, g01, g11 = G[j0, i0], G[j0, i1], G[j1, i0], G[j1, i1]
-        ddx = (1 - fy) * (g10 - g00) + fy * (g11 - g01)
-        ddy = (1 - fx) * (g01 - g00) + fx * (g11 - g10)
+        (c00, c10, c01, c11), fx, fy = st
+        G = G.reshape(-1)
+        g00, g10, g01, g11 = G[c00], G[c10], G[c01], G[c11]
+        ddx = (1.0 - fy) * (g10 - g00) + fy * (g11 - g01)
+        ddy = (1.0 - fx) * (g01 - g00) + fx * (g11 - g10)
         return ddx, ddy
 
     # ---- solve and its transpose ------------------------------------------------
@@ -86,43 +90,51 @@ class Case:
         s = (self.ny, self.nx)
         return np.fft.irfft2(np.conj(self.Kx) * np.fft.rfft2(lEx) + np.conj(self.Ky) * np.fft.rfft2(lEy), s=s)
 
-    # ---- Boris -------------------------------------------------------------------
+    # ---- Boris (u as three arrays) ------------------------------------------------
     def rot_ts(self, qmh):
         t = qmh * self.B0
         s = 2.0 * t / (1.0 + t @ t)
         return t, s
 
     def boris(self, u, ex, ey, qmh):
-        a = np.stack([qmh * ex, qmh * ey, np.zeros_like(ex)], axis=1)
-        u1 = u + a
-        t, s = self.rot_ts(qmh)
-        up = u1 + np.cross(u1, t)
-        u2 = u1 + np.cross(up, s)
-        return u2 + a
+        ux, uy, uz = u
+        ax, ay = qmh * ex, qmh * ey
+        ux, uy = ux + ax, uy + ay
+        if np.any(self.B0 != 0.0):
+            (tx, ty, tz), (sx, sy, sz) = self.rot_ts(qmh)
+            px, py, pz = ux + (uy * tz - uz * ty), uy + (uz * tx - ux * tz), uz + (ux * ty - uy * tx)
+            ux, uy, uz = ux + (py * sz - pz * sy), uy + (pz * sx - px * sz), uz + (px * sy - py * sx)
+        return ux + ax, uy + ay, uz
 
     def rot_T(self, lam, qmh):
-        """R^T lam for the rotation u -> u + (u + u x t) x s."""
-        t, s = self.rot_ts(qmh)
-        ls = np.cross(lam, s)
-        return lam - ls + np.cross(ls, t)
+        """R^T lam for the rotation u -> u + (u + u x t) x s (lam as three arrays)."""
+        lx, ly, lz = lam
+        if not np.any(self.B0 != 0.0):
+            return lx, ly, lz
+        (tx, ty, tz), (sx, sy, sz) = self.rot_ts(qmh)
+        cx, cy, cz = ly * sz - lz * sy, lz * sx - lx * sz, lx * sy - ly * sx      # lam x s
+        return (lx - cx + (cy * tz - cz * ty), ly - cy + (cz * tx - cx * tz), lz - cz + (cx * ty - cy * tx))
 
     # ---- forward / backward ----------------------------------------------------------
-    def forward(self, x, y, u, w, nsteps):
-        """Initial state (x, y in cell units, u [n][3], w) -> (loss, trajectory)."""
-        x, y, u = np.array(x, np.float64), np.array(y, np.float64), np.array(u, np.float64)
+    def forward(self, x, y, u, w, nsteps, keep=True):
+        """Initial state (x, y in cell units, u [n][3], w) -> (loss, trajectory, q)."""
+        x, y = np.array(x, np.float64), np.array(y, np.float64)
+        u = tuple(np.array(u[:, d], np.float64) for d in range(3))
         q = self.qm / (self.dx * self.dy) * np.asarray(w, np.float64)
         qmh = self.qm * 0.5 * self.dt
         qmh_b = self.qm * 0.5 * (-0.5 * self.dt)
-        ex, ey = self.solve(self.deposit(x, y, q))
-        u = self.boris(u, self.gather(ex, x, y), self.gather(ey, x, y), qmh_b)
+        st = self.stencil(x, y)
+        ex, ey = self.solve(self.deposit(st, q))
+        u = self.boris(u, self.gather(ex, st), self.gather(ey, st), qmh_b)
         traj = []
         for _ in range(nsteps):
-            ex, ey = self.solve(self.deposit(x, y, q))
-            traj.append((x.copy(), y.copy(), ex, ey))
-            u = self.boris(u, self.gather(ex, x, y), self.gather(ey, x, y), qmh)
-            x = np.mod(x + u[:, 0] * self.dt / self.dx, self.nx)
-            y = np.mod(y + u[:, 1] * self.dt / self.dy, self.ny)
-        ex, ey = traj[-1][2], traj[-1][3]
+            st = self.stencil(x, y)
+            ex, ey = self.solve(self.deposit(st, q))
+            if keep:
+                traj.append((x.copy(), y.copy(), ex, ey))
+            u = self.boris(u, self.gather(ex, st), self.gather(ey, st), qmh)
+            x = np.mod(x + u[0] * (self.dt / self.dx), self.nx)
+            y = np.mod(y + u[1] * (self.dt / self.dy), self.ny)
         loss = 0.5 * self.eps0 * self.dx * self.dy * float(np.sum(ex * ex + ey * ey))
         return loss, traj, q
 
@@ -133,35 +145,35 @@ class Case:
         qmh = self.qm * 0.5 * self.dt
         qmh_b = self.qm * 0.5 * (-0.5 * self.dt)
         cx, cy = self.dt / self.dx, self.dt / self.dy
-        lx, ly, lu = np.zeros(n), np.zeros(n), np.zeros((n, 3))
+        lx, ly = np.zeros(n), np.zeros(n)
+        lu = (np.zeros(n), np.zeros(n), np.zeros(n))
         ext = self.eps0 * self.dx * self.dy
         for s in range(nsteps - 1, -1, -1):
             xs, ys, ex, ey = traj[s]
-            lu3 = lu.copy()
-            lu3[:, 0] += cx * lx
-            lu3[:, 1] += cy * ly
+            st = self.stencil(xs, ys)
+            lu3 = (lu[0] + cx * lx, lu[1] + cy * ly, lu[2])
             lu1 = self.rot_T(lu3, qmh)
-            lEx = qmh * (lu3[:, 0] + lu1[:, 0])
-            lEy = qmh * (lu3[:, 1] + lu1[:, 1])
-            dxx, dxy = self.gather_grad(ex, xs, ys)
-            dyx, dyy = self.gather_grad(ey, xs, ys)
+            lEx = qmh * (lu3[0] + lu1[0])
+            lEy = qmh * (lu3[1] + lu1[1])
+            dxx, dxy = self.gather_grad(ex, st)
+            dyx, dyy = self.gather_grad(ey, st)
             lx = lx + lEx * dxx + lEy * dyx
             ly = ly + lEx * dxy + lEy * dyy
             lu = lu1
-            gEx = self.deposit(xs, ys, lEx)
-            gEy = self.deposit(xs, ys, lEy)
+            gEx = self.deposit(st, lEx)
+            gEy = self.deposit(st, lEy)
             if s == nsteps - 1:
                 gEx = gEx + ext * ex
                 gEy = gEy + ext * ey
             lrho = self.solve_T(gEx, gEy)
-            ddx, ddy = self.gather_grad(lrho, xs, ys)
+            ddx, ddy = self.gather_grad(lrho, st)
             lx = lx + q * ddx
             ly = ly + q * ddy
-        return loss, self.rot_T(lu, qmh_b)
+        return loss, np.stack(self.rot_T(lu, qmh_b), axis=1)
 
 
 def loss_at(case, x, y, u, w, nsteps):
-    return case.forward(x, y, u, w, nsteps)[0]
+    return case.forward(x, y, u, w, nsteps, keep=False)[0]
 
 
 def central_difference(case, x, y, u, w, nsteps, direction, h):
