@@ -69,6 +69,11 @@ class Diag(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class RunSpec(C.Structure):
+    _fields_ = [("model", C.c_int32), ("grid", Grid), ("params", Params), ("nspecies", C.c_int32),
+                ("species", Species * 4), ("seed", C.c_uint64), ("noisy", C.c_int32)]
+
+
 class Stats(C.Structure):
     _fields_ = [("chunks", C.c_int64), ("window_overflow", C.c_int64), ("slow_deposits", C.c_int64),
                 ("steps", C.c_int64), ("kernels_per_step", C.c_int64)]
@@ -87,6 +92,11 @@ SIGNATURES = {
     "aw_load_species": [_P, C.POINTER(Species), _I32, _U64, _I32],
     "aw_resort": [_P], "aw_set_resort": [_P, _I32],
     "aw_grad_es": [_P, _I64, _I32, _P, _P, _P, C.POINTER(_D)],
+    "aw_ensemble_create": [_I32, C.POINTER(RunSpec), _P, C.POINTER(_P)], "aw_ensemble_destroy": [_P],
+    "aw_ensemble_init": [_P], "aw_ensemble_tune": [_P, _I32],
+    "aw_ensemble_tuning": [_P, _I32, C.POINTER(_I32), C.POINTER(_I32)],
+    "aw_ensemble_run": [_P, _I64, _I32], "aw_ensemble_diag": [_P, _I32, C.POINTER(Diag)],
+    "aw_ensemble_particles": [_P, _I32] + [C.POINTER(_P)] * 6 + [C.POINTER(_I64)],
     "aw_load_legacy": [_P, C.POINTER(LegacyLoad)],
     "aw_deposit_rho_noalloc": [C.POINTER(Grid), _D, _P, _P, _P, _P, _P, _P, _I64, _P, _P],
     "aw_deposit_rho": [_P], "aw_deposit_rho_j": [_P], "aw_deposit_amu": [_P], "aw_deposit_dcu": [_P],
@@ -300,6 +310,72 @@ class Context:
         s = Stats()
         _check(self.lib.aw_stats(self.h, C.byref(s)))
         return {n: getattr(s, n) for n, _ in s._fields_}
+
+
+def run_spec(model, nx, ny, Lx, Ly, species, *, seed=0, noisy=True, **params) -> RunSpec:
+    """One run of an ensemble: grid, RunParams (make_params keywords), species
+    (dicts of ppc, density, uth, ufl) and the loader seed."""
+    r = RunSpec()
+    r.model = int(model)
+    r.grid = Grid(int(nx), int(ny), float(Lx), float(Ly))
+    r.params = make_params(**params)
+    if not 1 <= len(species) <= 4:
+        raise ValueError("1 to 4 species per run")
+    r.nspecies = len(species)
+    for i, sp in enumerate(species):
+        r.species[i] = Species(int(sp["ppc"]), float(sp["density"]), (C.c_double * 3)(*sp["uth"]),
+                               (C.c_double * 3)(*sp["ufl"]))
+    r.seed, r.noisy = int(seed), int(bool(noisy))
+    return r
+
+
+class Ensemble:
+    """Independent runs advanced together (aw_ensemble_*): one graph launch per
+    ensemble step, each run identical to the same run alone."""
+
+    def __init__(self, specs, stream=None):
+        self.lib = load_library()
+        arr = (RunSpec * len(specs))(*specs)
+        h = C.c_void_p()
+        _check(self.lib.aw_ensemble_create(len(specs), arr, stream, C.byref(h)))
+        self.h, self.n = h.value, len(specs)
+
+    def close(self):
+        if self.h:
+            self.lib.aw_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self):
+        _check(self.lib.aw_ensemble_init(self.h))
+
+    def tune(self, trial_steps=5):
+        _check(self.lib.aw_ensemble_tune(self.h, int(trial_steps)))
+
+    def tuning(self, run):
+        every, tile = C.c_int32(), C.c_int32()
+        _check(self.lib.aw_ensemble_tuning(self.h, int(run), C.byref(every), C.byref(tile)))
+        return every.value, tile.value
+
+    def run(self, nsteps, concurrent=True):
+        _check(self.lib.aw_ensemble_run(self.h, int(nsteps), int(bool(concurrent))))
+
+    def diag(self, run) -> dict:
+        d = Diag()
+        _check(self.lib.aw_ensemble_diag(self.h, int(run), C.byref(d)))
+        return d.as_dict()
+
+    def particles(self, run):
+        """Device pointers {x, y, ux, uy, uz, w} and the particle count of a run."""
+        ptrs = [C.c_void_p() for _ in range(6)]
+        n = C.c_int64()
+        _check(self.lib.aw_ensemble_particles(self.h, int(run), *[C.byref(p) for p in ptrs], C.byref(n)))
+        return {k: p.value for k, p in zip(("x", "y", "ux", "uy", "uz", "w"), ptrs)}, n.value
 
 
 _OPS = {"deposit_rho", "deposit_rho_j", "deposit_amu", "deposit_dcu", "push_es", "push_em",

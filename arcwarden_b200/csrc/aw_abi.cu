@@ -39,24 +39,9 @@ void check_cufft(cufftResult r, const char* what, const char* file, int line) {
     }
 }
 
-namespace {
+void set_last_error(const char* msg) { g_last_error = msg; }
 
-template <class F>
-int guarded(F&& f) {
-    try {
-        f();
-        return AW_OK;
-    } catch (const Error& e) {
-        g_last_error = e.what();
-        return e.code;
-    } catch (const std::exception& e) {
-        g_last_error = e.what();
-        return AW_ERR_STATE;
-    } catch (...) {
-        g_last_error = "unknown error";
-        return AW_ERR_STATE;
-    }
-}
+namespace {
 
 template <class T>
 void dalloc(T*& p, size_t n) {
@@ -64,9 +49,6 @@ void dalloc(T*& p, size_t n) {
     AW_CUDA(cudaMalloc(reinterpret_cast<void**>(&p), n * sizeof(T)));
 }
 
-void need(bool ok, int code, const char* msg) {
-    if (!ok) throw Error(code, msg);
-}
 
 void make_plan(cufftHandle& h, int ny, int nx, cufftType type, int batch, size_t& ws) {
     AW_CUFFT(cufftCreate(&h));
@@ -194,7 +176,6 @@ using aw::Ctx;
 using aw::Error;
 using aw::guarded;
 
-struct aw_ctx { Ctx c; };
 
 namespace aw {
 namespace {
@@ -343,6 +324,25 @@ double grad_es_impl(Ctx& c, long long nsteps, int every, float* dux, float* duy,
     return loss;
 }
 }  // namespace
+}  // namespace aw
+
+namespace aw {
+void prepare_step(Ctx& c) { ensure_pending(c); }
+
+cudaGraph_t capture_step_graph(Ctx& c) {
+    ensure_pending(c);
+    cudaGraph_t g = nullptr;
+    AW_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        step_body(c);
+    } catch (...) {
+        cudaStreamEndCapture(c.stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    AW_CUDA(cudaStreamEndCapture(c.stream, &g));
+    return g;
+}
 }  // namespace aw
 
 extern "C" {

@@ -26,6 +26,30 @@ void check_cufft(cufftResult r, const char* what, const char* file, int line);
 #define AW_CUFFT(x) ::aw::check_cufft((x), #x, __FILE__, __LINE__)
 #define AW_LAUNCH() ::aw::check_cuda(cudaPeekAtLastError(), "kernel launch", __FILE__, __LINE__)
 
+inline void need(bool ok, int code, const char* msg) {
+    if (!ok) throw Error(code, msg);
+}
+
+// The text aw_last_error returns (thread-local).
+void set_last_error(const char* msg);
+// Run f, mapping an exception to a status code and the last-error text.
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return AW_OK;
+    } catch (const Error& e) {
+        set_last_error(e.what());
+        return e.code;
+    } catch (const std::exception& e) {
+        set_last_error(e.what());
+        return AW_ERR_STATE;
+    } catch (...) {
+        set_last_error("unknown error");
+        return AW_ERR_STATE;
+    }
+}
+
 // Field-kernel parameters (k-space + real-space finalisers).
 struct SpecGeo {
     int    nx, ny, nkx, nk;      // nk = nkx*ny complex elements
@@ -96,6 +120,7 @@ struct Ctx {
     int* rs_buf = nullptr; long long rs_n = 0;
     void* rs_temp = nullptr; size_t rs_temp_bytes = 0;
     int resort_every = 0;             // aw_run re-sorts before every step n with n % resort_every == 0
+    int resort_tile = kChunk / 2;     // particles per re-sort tile (the ensemble autotuner sets it)
     // scales for unfused deposits
     bool have_static_scales = false;
 
@@ -224,6 +249,13 @@ void launch_promote_scales(Ctx& c);                // S_pend = S_next
 void launch_rms_reduce(Ctx& c, bool src, bool dcu);
 void launch_step_reduce(Ctx& c);                   // end of a fused step: diagnostics (+ rms for Darwin)
 
+// ---- step graph (aw_abi.cu) ------------------------------------------------
+// The fused step body captured into a graph on the context's stream (pending
+// deposit ensured first). The caller owns the graph.
+cudaGraph_t capture_step_graph(Ctx& c);
+// Make sure the deposit of the current particles is pending (before a step).
+void prepare_step(Ctx& c);
+
 // ---- the ES adjoint (aw_adjoint.cu) ----------------------------------------
 AdjK adj_constants(const Ctx& c, float dt_scale);
 void adj_prepare(Ctx& c, long long nsteps, int every);   // (re)allocates c.adj
@@ -245,3 +277,6 @@ void launch_adj_gather(Ctx& c, const AdjP& a, const AdjK& k);
 void launch_adj_out(Ctx& c, float* dux, float* duy, float* duz);
 
 }  // namespace aw
+
+// The opaque handle of the C ABI.
+struct aw_ctx { aw::Ctx c; };

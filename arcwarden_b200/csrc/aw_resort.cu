@@ -61,11 +61,12 @@ int bits_for(int v) {
 
 }  // namespace
 
-// Tile shape for a re-sort: about kChunk/2 particles per tile (two tiles per
-// chunk), roughly twice as wide as high; row-major tile order.
+// Tile shape for a re-sort: about c.resort_tile particles per tile (kChunk/2 by
+// default: two tiles per chunk), roughly twice as wide as high; row-major tile
+// order.
 void resort_tile_shape(const Ctx& c, int& tx, int& ty) {
     const double ppc = std::max(1.0, static_cast<double>(c.parts.n) / c.geo.ncell);
-    const int cpt = std::max(1, static_cast<int>(kChunk / 2 / ppc));
+    const int cpt = std::max(1, static_cast<int>(c.resort_tile / ppc));
     tx = 1;
     while (tx * tx < 2 * cpt) tx <<= 1;
     tx = std::min(tx, c.geo.nx);

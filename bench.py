@@ -1,8 +1,9 @@
 #!/usr/bin/env python3
 """Benchmark of the B200 PIC hot path: particles/s per full PIC step.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload weibel512|es256|whistler1024]
-                    [--impl ours|reference] [--no-cpu-baseline]
+    python bench.py [--gpus N] [--steps K] [--warmup W]
+                    [--workload weibel512|es256|whistler1024|adjoint256|ensemble64]
+                    [--impl ours|reference] [--no-cpu-baseline] [--dump-grad FILE]
 
 Workloads (synthetic, seeded; the reference's own seeded loader streams):
   weibel512     spectral Darwin Weibel, 512x512, dx = 0.5, 64 ppc (16,777,216
@@ -11,6 +12,14 @@ Workloads (synthetic, seeded; the reference's own seeded loader streams):
                 (4,194,304), beams +-0.2, v_th = 0.01, dt = 0.1
   whistler1024  magnetised Darwin whistler pump, 1024x128, dx = 0.25, 256 ppc
                 (33,554,432), B0 = 0.5 at 30 deg in x-y, dt = 0.05
+  ensemble64    64 independent seeded runs of uneven grids and particles per
+                cell (712 M particles in all), ES and Darwin, advanced together
+                by one graph launch per step; a bench step advances every run by
+                one PIC step
+  adjoint256    gradient of the final field energy of a 200-step electrostatic
+                two-stream run (256x256, 2 x 8 ppc = 1,048,576) with respect
+                to every initial velocity, checkpoint every 20 steps; a bench
+                step is one gradient evaluation (forward + backward sweep)
 
 `value` is the device-timed rate (K graph-launched steps bracketed by a
 barrier and a synchronize, CUDA events on the step's stream, max over ranks).
@@ -71,6 +80,18 @@ def workload(name: str) -> dict:
                     dom="push_deposit_em",
                     species=[dict(ppc=256, density=1.0, uth=(0.019,) * 3, ufl=(0.0, 0.0, 0.0))],
                     desc=f"magnetised Darwin whistler pump 1024x128 dx=0.25 ppc256 B0=0.5@30deg M={M}")
+    if name == "adjoint256":
+        return dict(name=name, model=0, nx=256, ny=256, Lx=256.0, Ly=256.0, dt=0.1, c=1.0, n0=1.0,
+                    B0=(0.0, 0.0, 0.0), pump=None, run_steps=200, every=20, dom="push_deposit_es", adjoint=True,
+                    species=[dict(ppc=8, density=0.5, uth=(0.01,) * 3, ufl=(0.2, 0.0, 0.0)),
+                             dict(ppc=8, density=0.5, uth=(0.01,) * 3, ufl=(-0.2, 0.0, 0.0))],
+                    desc="adjoint of the electrostatic two-stream 256x256 dx=1 2x8ppc v0=+-0.2 vth=0.01 dt=0.1, "
+                         "200 steps, checkpoint every 20, loss = final field energy")
+    if name == "ensemble64":
+        return dict(name=name, ensemble=True, nruns=64, run_steps=100, model=None, species=[], nx=0, ny=0,
+                    desc="64 independent runs (seeds 0-63): grid side in {64,128,256,512} (dx=1), ppc in "
+                         "{16,64,256}, vth log-uniform [0.01,0.1], beams +-vd with vd in [0,0.3], half ES "
+                         "(dt=0.1) half Darwin (dt=0.05, c=1), half magnetised (B0 along z, Wce in [0.2,1])")
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -333,6 +354,274 @@ def profile_case(wl, steps):
     print(f"profile case {wl['name']}: {steps} steps of {n} particles", flush=True)
 
 
+# bytes per particle per PIC step of one gradient evaluation: the forward step
+# (44), its recompute (44) and the trajectory store (8), the transposed step A
+# (x_n 8, cotangents 20 read + 20 written) and B (x_n 8, w 4, lx ly 8 read + 8
+# written, lu 12 read)
+ADJ_BYTES_PER_PARTICLE = 44.0 + 44.0 + 8.0 + 48.0 + 40.0
+
+
+def run_adjoint(args, wl, rank, world, dist):
+    import torch
+    import arcwarden_b200 as aw
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    n = nparticles(wl)
+    N, every = wl["run_steps"], wl["every"]
+    stream = torch.cuda.Stream(dev)
+    ctx = aw.Context(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], dt=wl["dt"], c=wl["c"], n0=wl["n0"], B0=wl["B0"],
+                     model=wl["model"], stream=stream.cuda_stream)
+    P = {k: torch.empty(n, dtype=torch.float32, device=dev) for k in ("x", "y", "ux", "uy", "uz", "w")}
+    cell = torch.empty(n, dtype=torch.int32, device=dev)
+    ctx.bind_particles(P["x"], P["y"], P["ux"], P["uy"], P["uz"], P["w"], cell)
+    ctx.load_species(wl["species"], seed=0, noisy=True)
+    p0 = {k: v.clone() for k, v in P.items()}
+    du = [torch.zeros(n, dtype=torch.float32, device=dev) for _ in range(3)]
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(fn, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        return e0.elapsed_time(e1) / reps
+
+    def forward():
+        with torch.cuda.stream(stream):
+            for k in P:
+                P[k].copy_(p0[k])
+        ctx.init()
+        ctx.run(0, N, graph=True)
+
+    loss = [0.0]
+
+    def grad():
+        loss[0] = ctx.grad_es(N, every, *du)
+
+    for _ in range(max(args.warmup, 3)):
+        forward()
+    fwd_ms = max_over_ranks(timed(forward, 3), dist, dev)
+    with torch.cuda.stream(stream):
+        for k in P:
+            P[k].copy_(p0[k])
+    for _ in range(max(args.warmup, 3)):
+        grad()
+    with ClockSampler(dev.index) as clk:
+        grad_ms = max_over_ranks(timed(grad, args.steps), dist, dev)
+    err = ctx.error_word()
+    if err:
+        raise SystemExit(f"device error word {err:#x} after the gradient runs")
+    if args.dump_grad and rank == 0:
+        import numpy as np
+        np.savez_compressed(args.dump_grad, **{k: p0[k].cpu().numpy() for k in P},
+                            g=np.stack([d.cpu().numpy() for d in du], axis=1), loss=loss[0])
+
+    # end to end: initial state from pinned host memory, the gradient back to it
+    host = {k: p0[k].cpu().pin_memory() for k in P}
+    ghost = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(3)]
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    reps = max(1, min(args.steps, 5))
+    for _ in range(reps):
+        with torch.cuda.stream(stream):
+            for k in host:
+                P[k].copy_(host[k], non_blocking=True)
+        grad()
+        with torch.cuda.stream(stream):
+            for h, d in zip(ghost, du):
+                h.copy_(d, non_blocking=True)
+        stream.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / reps, dist, dev)
+
+    peak, peak_kind = measured_peak_gbs()
+    achieved = n * N * ADJ_BYTES_PER_PARTICLE / (grad_ms * 1e-3) / 1e9
+    launches = N * (5 + 1) + N * (5 + 4) + N * 7 + 1   # forward steps, recompute steps, backward steps, output
+    res = {
+        "metric": "particles/s/step (gradient: forward + checkpointed backward)",
+        "value": world * n * N / (grad_ms * 1e-3),
+        "unit": "particles/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": grad_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32",
+        "numerics": "f32 forward and cotangents; deposits and the cotangent scatter exact int64 fixed point",
+        "data": "synthetic: reference seeded loader streams (noisy load, seed 0)",
+        "config": {"workload": wl["desc"], "field_model": "electrostatic", "grid": [wl["nx"], wl["ny"]],
+                   "particles_per_gpu": n, "pic_steps_per_gradient": N, "checkpoint_every": every,
+                   "bench_step": "one gradient evaluation", "parallelism": f"replicas x{world}",
+                   "l2": "inputs > L2 per gradient (trajectory and checkpoints, ~400 MB)"},
+        "forward": {"ms": fwd_ms, "value": world * n * N / (fwd_ms * 1e-3), "unit": "particles/s",
+                    "run": "aw_init + 200 graph-launched forward steps"},
+        "gradient_over_forward": grad_ms / fwd_ms,
+        "backward_over_forward": (grad_ms - fwd_ms) / fwd_ms,
+        "loss": loss[0],
+        "e2e": {"value": world * n * N / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": 24 * n,
+                "d2h_bytes_per_step": 12 * n,
+                "run": "H2D of the initial state from pinned memory, aw_grad_es, D2H of dL/du0"},
+        "roofline": {"bound": "hbm", "kernel": "whole gradient", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_particle_step": ADJ_BYTES_PER_PARTICLE},
+        "gpu_launches": args.steps * launches,
+        "clocks": clk.summary(),
+    }
+    ctx.close()
+    return res
+
+
+def adjoint_cpu_baseline(wl, budget_steps=8):
+    """The FP64 host reference gradient (numpy, one core) on a bounded sample:
+    budget_steps PIC steps of the same particles, forward and adjoint."""
+    import numpy as np
+    from oracle import oracle as O
+    from oracle.adjoint64 import Case
+    g = O.geo(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"])
+    p = O.load_species(g, wl["species"], seed=0, noisy=True)
+    case = Case(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], wl["dt"], B0=wl["B0"])
+    u = np.stack([p["ux"], p["uy"], p["uz"]], axis=1).astype(np.float64)
+    n = len(p["x"])
+    t0 = time.perf_counter()
+    case.gradient(p["x"].astype(np.float64), p["y"].astype(np.float64), u, p["w"].astype(np.float64), budget_steps)
+    el = time.perf_counter() - t0
+    return dict(value=n * budget_steps / el, unit="particles/s", cores=1, kind="port",
+                sample=f"FP64 numpy gradient of {budget_steps} PIC steps ({n} particles), {el:.1f} s")
+
+
+def run_ensemble(args, wl, rank, world, dist):
+    import torch
+    import arcwarden_b200 as aw
+    from arcwarden_b200.ensemble import ensemble_specs, particle_count
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+    torch.cuda.set_device(dev)
+    draws, specs = ensemble_specs(wl["nruns"])
+    ntot = particle_count(draws)
+    stream = torch.cuda.Stream(dev)
+    t_tune = time.perf_counter()
+    e = aw.Ensemble(specs, stream=stream.cuda_stream)
+    e.tune(5)
+    t_tune = time.perf_counter() - t_tune
+    tuned = [e.tuning(r) for r in range(len(specs))]
+    e.init()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(concurrent, steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        e.run(steps, concurrent=concurrent)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        barrier()
+        return e0.elapsed_time(e1) / steps
+
+    e.run(max(args.warmup, 3), concurrent=True)
+    with ClockSampler(dev.index) as clk:
+        ms = max_over_ranks(timed(True, args.steps), dist, dev)
+    seq_ms = max_over_ranks(timed(False, args.steps), dist, dev)
+    for r in range(len(specs)):
+        d = e.diag(r)
+        if not all(math.isfinite(v) for v in d.values()):
+            raise SystemExit(f"non-finite diagnostics in ensemble run {r}")
+    e.close()
+
+    # end to end through the public API: create (the seeded loads), init, one
+    # config-length run, every run's diagnostics read back
+    K = wl["run_steps"]
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    e = aw.Ensemble(specs, stream=stream.cuda_stream)
+    e.init()
+    e.run(K, concurrent=True)
+    diags = [e.diag(r) for r in range(len(specs))]
+    e2e_s = max_over_ranks(time.perf_counter() - t0, dist, dev)
+    e.close()
+    res = {
+        "metric": "particles/s/step (64-run ensemble, all runs advanced together)",
+        "value": world * ntot / (ms * 1e-3),
+        "unit": "particles/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32",
+        "numerics": "f32 push/gather/solve; deposits exact int64 fixed point; diagnostics f64",
+        "data": "synthetic: reference seeded loader streams, run r seeded r",
+        "config": {"workload": wl["desc"], "runs": len(specs), "particles_per_gpu": ntot,
+                   "es_runs": sum(1 for d in draws if d["model"] == aw.AW_MODEL_ES),
+                   "graph": "one launch per ensemble step (a child graph per run)",
+                   "autotuner": {"trial_steps": 5, "seconds": round(t_tune, 2),
+                                 "resorted_runs": sum(1 for t in tuned if t[0] > 0)},
+                   "l2": "particle state 20 GB > 126 MB L2", "parallelism": f"replicas x{world}"},
+        "sequential": {"ms_per_step": seq_ms, "value": world * ntot / (seq_ms * 1e-3),
+                       "run": "the same runs one after another (aw_run each), same GPU"},
+        "concurrent_over_sequential": seq_ms / ms,
+        "e2e": {"value": world * ntot * K / e2e_s, "unit": "particles/s",
+                "h2d_bytes_per_step": round(len(specs) * 248 / K), "d2h_bytes_per_step": round(len(specs) * 64 / K),
+                "run": f"aw_ensemble_create (device seeded loads) + init + {K} steps (default re-sort "
+                       f"settings, no tuning) + every run's diagnostics read back"},
+        "roofline": {"bound": "hbm", "kernel": "whole ensemble step",
+                     "achieved": ntot * 56.0 / (ms * 1e-3) / 1e9, "peak": measured_peak_gbs()[0], "unit": "GB/s",
+                     "frac": ntot * 56.0 / (ms * 1e-3) / 1e9 / measured_peak_gbs()[0],
+                     "peak_kind": measured_peak_gbs()[1], "traffic": None,
+                     "algorithmic_bytes_per_particle": "44 (ES) / 68 (Darwin); 56 average"},
+        "gpu_launches": args.steps * sum(5 if d["model"] == aw.AW_MODEL_ES else 9 for d in draws),
+        "clocks": clk.summary(),
+    }
+    return res
+
+
+def run_reference_ensemble(args, wl, rank):
+    """The same 64 runs one after another through the reference's Simulation
+    (oracle/_ref, headers unmodified), on this GPU."""
+    if rank != 0:
+        return None
+    from oracle import refsim as R
+    from arcwarden_b200.ensemble import ensemble_specs, particle_count
+    if not R.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref (the compiled reference) is not built"}
+    import torch
+    torch.cuda.set_device(0)
+    draws, _ = ensemble_specs(wl["nruns"])
+    total_ms = 0.0
+    for d in draws:
+        half = d["ppc"] // 2
+        sp = [dict(ppc=half, density=0.5, uth=(d["vth"],) * 3, ufl=(d["vd"], 0.0, 0.0)),
+              dict(ppc=d["ppc"] - half, density=0.5, uth=(d["vth"],) * 3, ufl=(-d["vd"], 0.0, 0.0))]
+        dt = 0.1 if d["model"] == 0 else 0.05
+        prm = R.params(dt=dt, c=1.0, n0=1.0, B0=d["B0"])
+        L = float(d["side"])
+        rs = R.RefSim(d["model"], d["side"], d["side"], L, L, prm, sp, noisy=True, seed=d["seed"])
+        rs.init()
+        rs.time_steps(0, max(args.warmup, 3))
+        total_ms += rs.time_steps(max(args.warmup, 3), args.steps)
+        rs.close()
+    ntot = particle_count(draws)
+    ms = total_ms / args.steps
+    val = ntot / (ms * 1e-3)
+    return {
+        "impl": "reference", "metric": "particles/s/step (64-run ensemble, all runs advanced together)",
+        "value": val, "unit": "particles/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "config": {"workload": wl["desc"], "runs": len(draws), "particles_per_gpu": ntot,
+                   "run": "64 reference Simulation runs one after another, each timed over the same steps"},
+        "cpu_baseline": {"value": val, "unit": "particles/s", "cores": 1, "kind": "reference", "device": "cuda",
+                         "sample": f"{args.steps} steps of each of the 64 reference runs, sequential, on this GPU"},
+        "e2e": {"value": val, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 def run_reference(args, wl, rank, world):
     """The reference's own implementation of the step: its CUDA Simulation built
     from its headers (oracle/_ref) when present, else the oracle port on CPU."""
@@ -376,6 +665,8 @@ def main():
     ap.add_argument("--workload", default="weibel512")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dump-grad", default=None, metavar="FILE",
+                    help="adjoint256: write the initial state and the gradient (.npz) for oracle/grad_check.py")
     ap.add_argument("--profile-case", type=int, default=0, metavar="K",
                     help="profiling case for ncu: load, aw_init and K single aw_step launches (no graph, no "
                          "timing, no JSON line)")
@@ -397,8 +688,19 @@ def main():
         profile_case(wl, args.profile_case)
         return
     try:
-        if args.impl == "reference":
+        if args.impl == "reference" and wl.get("ensemble"):
+            res = run_reference_ensemble(args, wl, rank)
+        elif wl.get("ensemble"):
+            res = run_ensemble(args, wl, rank, world, dist)
+        elif args.impl == "reference" and wl.get("adjoint"):
+            res = None if rank != 0 else {"impl": "reference", "unavailable": "the reference has no adjoint "
+                                          "(no backward step in ArcWarden)"}
+        elif args.impl == "reference":
             res = run_reference(args, wl, rank, world)
+        elif wl.get("adjoint"):
+            res = run_adjoint(args, wl, rank, world, dist)
+            if rank == 0 and not args.no_cpu_baseline:
+                res["cpu_baseline"] = adjoint_cpu_baseline(wl)
         else:
             res = run_ours(args, wl, rank, world, dist)
             if rank == 0 and not args.no_cpu_baseline:

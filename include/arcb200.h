@@ -221,6 +221,46 @@ int aw_tile_bins(aw_ctx* ctx, const int32_t** off, const int32_t** idx,
 int aw_grad_es(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux, float* duy, float* duz,
                double* loss);
 
+/* ---- batched ensemble (no counterpart in the reference, which runs one
+ * Simulation at a time) -------------------------------------------------------
+ * Many independent runs of uneven grids and particle counts advanced together:
+ * one context per run on the ensemble's stream, the particle SoA owned by the
+ * ensemble and loaded by the seeded loader (aw_load_species), and one CUDA
+ * graph per ensemble step whose independent branches are the runs' captured
+ * fused steps, so small runs overlap on the GPU instead of running one after
+ * another. Each run gives the same bits as the same run alone. */
+#define AW_ENSEMBLE_MAX_SPECIES 4
+typedef struct aw_run_spec {
+    int32_t    model;          /* AW_MODEL_ES or AW_MODEL_DARWIN                */
+    aw_grid    grid;
+    aw_params  params;
+    int32_t    nspecies;       /* 1 .. AW_ENSEMBLE_MAX_SPECIES                  */
+    aw_species species[AW_ENSEMBLE_MAX_SPECIES];
+    uint64_t   seed;
+    int32_t    noisy;
+} aw_run_spec;
+typedef struct aw_ensemble aw_ensemble;
+/* Create the runs and load their particles (`stream` NULL: the ensemble's own). */
+int aw_ensemble_create(int32_t nruns, const aw_run_spec* specs, void* stream, aw_ensemble** out);
+int aw_ensemble_destroy(aw_ensemble* e);
+/* Simulation<Cfg>::init for every run (synchronises). */
+int aw_ensemble_init(aw_ensemble* e);
+/* The autotuner: for each class of runs (model, grid, particles per cell) it
+ * times trial steps of a scratch copy with no spatial re-sort and with re-sort
+ * tiles of 512, 1024 and 2048 particles, and gives every run of the class the
+ * fastest choice (re-sort interval and tile size). Synchronises. */
+int aw_ensemble_tune(aw_ensemble* e, int32_t trial_steps);
+/* The tuned choice of one run: re-sort interval (0 = never) and tile size. */
+int aw_ensemble_tuning(aw_ensemble* e, int32_t run, int32_t* resort_every, int32_t* resort_tile);
+/* Advance every run by nsteps: concurrent = 1 replays the ensemble graph once
+ * per step; concurrent = 0 runs the runs one after another (aw_run each). */
+int aw_ensemble_run(aw_ensemble* e, int64_t nsteps, int32_t concurrent);
+/* Diagnostics of a run's last step (aw_step_diag; synchronises). */
+int aw_ensemble_diag(aw_ensemble* e, int32_t run, aw_diag* out);
+/* The run's particle arrays (device) and count. */
+int aw_ensemble_particles(aw_ensemble* e, int32_t run, float** x, float** y, float** ux, float** uy,
+                          float** uz, float** w, int64_t* n);
+
 /* ElectrostaticSpectralSolver::solve, include/pic/solver_es.hpp:238-259. */
 int aw_solve_es(aw_ctx* ctx);
 /* DarwinSpectralSolver::solve_el_b, include/pic/solver_darwin.hpp:188-216. */
