@@ -183,6 +183,7 @@ namespace {
 // the pending deposit of step 0. Synchronises.
 void init_impl(Ctx& c) {
     aw::drop_graph(c);
+    if (c.resort_every > 0) resort_reserve(c);
     aw::launch_set_step(c, 0);
     AW_CUDA(cudaMemsetAsync(&c.st->have_rms, 0, sizeof(int), c.stream));
     aw::launch_particle_max(c);
@@ -853,6 +854,7 @@ int aw_set_resort(aw_ctx* ctx, int32_t every) {
         aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
         aw::need(every >= 0, AW_ERR_ARG, "set_resort: negative interval");
         ctx->c.resort_every = every;
+        if (every > 0 && ctx->c.parts.x) aw::resort_reserve(ctx->c);
     });
 }
 

@@ -209,6 +209,7 @@ void launch_push_em_plain(Ctx& c, const float* unused);
 void launch_particle_max(Ctx& c);                  // ucur_bits, coef_max
 void launch_sort_tiles(Ctx& c, int tx, int ty, bool physical);
 void launch_resort(Ctx& c);                        // stable spatial re-sort of the SoA (aw_resort.cu)
+void resort_reserve(Ctx& c);                       // its scratch, allocated ahead of the steps
 void launch_particle_diag(Ctx& c);                 // KE, P partials -> part_p
 
 // ---- launchers (aw_deposit.cu) --------------------------------------------

@@ -73,15 +73,14 @@ void resort_tile_shape(const Ctx& c, int& tx, int& ty) {
     ty = std::max(1, std::min(cpt / tx, c.geo.ny));
 }
 
-void launch_resort(Ctx& c) {
+// Allocate (or grow) the re-sort scratch for the bound particles: keys and
+// values in and out, the gather copies of the seven arrays, the radix-sort
+// temporary. Done at set-up (aw_init, aw_set_resort) so the first re-sort of a
+// run does not allocate between steps.
+void resort_reserve(Ctx& c) {
     const long long n = c.parts.n;
     if (n < 2) return;
     if (n > 0x7fffffffLL) throw Error(AW_ERR_ARG, "resort: more than 2^31-1 particles");
-    int tx, ty;
-    resort_tile_shape(c, tx, ty);
-    const int ntx = (c.geo.nx + tx - 1) / tx, nty = (c.geo.ny + ty - 1) / ty;
-    const int ntiles = ntx * nty;
-    const int ni = static_cast<int>(n);
     if (c.rs_n < n) {
         if (c.rs_buf) cudaFree(c.rs_buf);
         c.rs_buf = nullptr;
@@ -94,20 +93,35 @@ void launch_resort(Ctx& c) {
         AW_CUDA(cudaMalloc(&c.sort_tmp, sizeof(float) * 7 * static_cast<size_t>(n)));
         c.sort_tmp_n = n;
     }
-    int* keys_in = c.rs_buf;
-    int* keys_out = c.rs_buf + n;
-    int* vals_in = c.rs_buf + 2 * n;
-    int* vals_out = c.rs_buf + 3 * n;
-    const int end_bit = bits_for(ntiles);
+    int tx, ty;
+    resort_tile_shape(c, tx, ty);
+    const int ntiles = ((c.geo.nx + tx - 1) / tx) * ((c.geo.ny + ty - 1) / ty);
+    int* k = c.rs_buf;
     size_t need = 0;
-    AW_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, need, keys_in, keys_out, vals_in, vals_out, ni, 0, end_bit,
-                                            c.stream));
+    AW_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, need, k, k + n, k + 2 * n, k + 3 * n, static_cast<int>(n), 0,
+                                            bits_for(ntiles), c.stream));
     if (need > c.rs_temp_bytes) {
         if (c.rs_temp) cudaFree(c.rs_temp);
         c.rs_temp = nullptr;
         AW_CUDA(cudaMalloc(&c.rs_temp, need));
         c.rs_temp_bytes = need;
     }
+}
+
+void launch_resort(Ctx& c) {
+    const long long n = c.parts.n;
+    if (n < 2) return;
+    resort_reserve(c);
+    int tx, ty;
+    resort_tile_shape(c, tx, ty);
+    const int ntx = (c.geo.nx + tx - 1) / tx, nty = (c.geo.ny + ty - 1) / ty;
+    const int ntiles = ntx * nty;
+    const int ni = static_cast<int>(n);
+    int* keys_in = c.rs_buf;
+    int* keys_out = c.rs_buf + n;
+    int* vals_in = c.rs_buf + 2 * n;
+    int* vals_out = c.rs_buf + 3 * n;
+    const int end_bit = bits_for(ntiles);
     const int blocks = static_cast<int>(std::min<long long>((n + kThreads - 1) / kThreads, 148LL * 16));
     k_resort_keys<<<blocks, kThreads, 0, c.stream>>>(c.parts.x, c.parts.y, n, c.geo, tx, ty, ntx, ntiles,
                                                       keys_in, vals_in);

@@ -460,7 +460,7 @@ def run_adjoint(args, wl, rank, world, dist):
                    "bench_step": "one gradient evaluation", "parallelism": f"replicas x{world}",
                    "l2": "inputs > L2 per gradient (trajectory and checkpoints, ~400 MB)"},
         "forward": {"ms": fwd_ms, "value": world * n * N / (fwd_ms * 1e-3), "unit": "particles/s",
-                    "run": "aw_init + 200 graph-launched forward steps"},
+                    "run": f"aw_init + {N} graph-launched forward steps"},
         "gradient_over_forward": grad_ms / fwd_ms,
         "backward_over_forward": (grad_ms - fwd_ms) / fwd_ms,
         "loss": loss[0],
@@ -665,6 +665,8 @@ def main():
     ap.add_argument("--workload", default="weibel512")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grad-steps", type=int, default=0, metavar="N",
+                    help="adjoint256: PIC steps per gradient (default 200)")
     ap.add_argument("--dump-grad", default=None, metavar="FILE",
                     help="adjoint256: write the initial state and the gradient (.npz) for oracle/grad_check.py")
     ap.add_argument("--profile-case", type=int, default=0, metavar="K",
@@ -674,6 +676,8 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     wl = workload(args.workload)
+    if args.grad_steps and wl.get("adjoint"):
+        wl["run_steps"] = args.grad_steps
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None

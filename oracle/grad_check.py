@@ -8,6 +8,7 @@ that workload: beams at ux = +-v0 with thermal spread, so dL/dv0 = sum over
 particles of sign(ux) dL/dux.
 
     python -m oracle.grad_check FILE --nx 256 --steps 200 --dt 0.1 --directions 32
+    python -m oracle.grad_check FILE --steps 25 --directions -1 --sensitivity 1e-5   (no FD)
 """
 import argparse
 import multiprocessing as mp
@@ -51,6 +52,9 @@ def main():
     ap.add_argument("--directions", type=int, default=32)
     ap.add_argument("--h", type=float, default=1e-4)
     ap.add_argument("--procs", type=int, default=8)
+    ap.add_argument("--sensitivity", type=float, default=0.0, metavar="EPS",
+                    help="also report the FP64 gradient's change when every initial position moves by "
+                         "EPS * N(0,1) cells (seed 7): the problem's own sensitivity")
     a = ap.parse_args()
     L = a.L if a.L is not None else float(a.nx)
     z = np.load(a.npz)
@@ -65,6 +69,14 @@ def main():
     print(f"gradient vs FP64 reference: |g - g64| / |g64| = {rel:.2e}")
     dv, dv64 = float(np.sum(sign * g[:, 0])), float(np.sum(sign * g64[:, 0]))
     print(f"dL/dv0: library {dv:.9g}  FP64 {dv64:.9g}  rel {abs(dv - dv64) / abs(dv64):.2e}")
+    if a.sensitivity > 0:
+        nz = np.random.default_rng(7).normal(size=(2, len(g)))
+        _, gp = _W["case"].gradient(np.mod(_W["x"] + a.sensitivity * nz[0], a.nx),
+                                    np.mod(_W["y"] + a.sensitivity * nz[1], a.nx), _W["u"], _W["w"], a.steps)
+        print(f"FP64 gradient with x0 moved by {a.sensitivity:g} cells: |g' - g64| / |g64| = "
+              f"{np.linalg.norm(gp - g64) / np.linalg.norm(g64):.2e}")
+    if a.directions < 0:
+        return
     jobs = [("v0", 0, a.h)] + [("dir", k, a.h) for k in range(a.directions)]
     t0 = time.time()
     with mp.get_context("spawn").Pool(a.procs, initializer=_init, initargs=(a.npz, a.nx, L, a.dt, a.steps)) as pool:
