@@ -398,9 +398,11 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
                 const float cf[NF] = {__fmul_rn(coef, __fadd_rn(ex, cx)), __fmul_rn(coef, __fadd_rn(ey, cy)),
                                       __fmul_rn(coef, __fadd_rn(ez, cz))};
                 const bool fast = scale_fast<NF>(cf, S, cs, l1);
+                if (((c.i0 + c.j0) & 7) == 0) {   // rms sample: the particles of one cell in 8, any order
 #pragma unroll
-                for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
-                nval += 1.0f;
+                    for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
+                    nval += 1.0f;
+                }
                 xs = __fadd_rn(x, 0.0f);
                 if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
             } else {
@@ -691,9 +693,11 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
                     cf0 = __double2float_rn(qoa * static_cast<double>(w));
                     src_coefs<SET_ALL>(cf0, ux, uy, uz, cf);
                     const bool fast = scale_fast<NF>(cf, S, cs, l1);
+                    if (((ci + cj) & 7) == 0) {   // rms sample: the particles of one cell in 8, any order
 #pragma unroll
-                    for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
-                    nval += 1.0f;
+                        for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
+                        nval += 1.0f;
+                    }
                     xs = __fadd_rn(x, 0.0f);
                     if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
                 } else {

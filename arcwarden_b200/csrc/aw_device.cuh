@@ -336,26 +336,28 @@ template <int NF, bool T0>
 __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& w,
                                           unsigned long long* __restrict__ acc, const Geo& g) {
     if (!w.use) return;            // the window was not used (its words are not zeroed)
-    // warp per window row, lanes along the row: no divide per cell, and the
-    // window offsets are < nx, so one conditional add/subtract wraps them
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int wj = warp; wj < w.H; wj += kThreads / 32) {
+    // every thread takes (field, cell) items t, t + 256, ...: all warps work even
+    // when the window is one or two rows. The item -> (field, row, column) splits
+    // use float reciprocals: (t + 0.5) / n is at least 0.5 / n away from an
+    // integer, far more than the float error for t < 2^14. Window offsets are
+    // < nx, so one conditional add/subtract wraps them.
+    const int WH = w.WH, total = NF * WH;
+    const float inv_wh = 1.0f / static_cast<float>(WH), inv_w = 1.0f / static_cast<float>(w.W);
+    for (int t = threadIdx.x; t < total; t += kThreads) {
+        const int f = static_cast<int>((static_cast<float>(t) + 0.5f) * inv_wh);
+        const int c = t - f * WH;
+        const int wj = static_cast<int>((static_cast<float>(c) + 0.5f) * inv_w);
+        const int wi = c - wj * w.W;
         int gj = w.jr + w.mj + wj;
         if (gj < 0) gj += g.ny;
         if (gj >= g.ny) gj -= g.ny;
-        for (int wi = lane; wi < w.W; wi += 32) {
-            int gi = w.ir + w.mi + wi;
-            if (gi < 0) gi += g.nx;
-            if (gi >= g.nx) gi -= g.nx;
-            const int c = wj * w.W + wi, gc = gj * g.nx + gi;
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                long long v = s[2 * f * w.WH + c];
-                if (tracked<T0>(w, f)) v += static_cast<long long>(s[(2 * f + 1) * w.WH + c]) * 4294967296ll;
-                if (v != 0)
-                    atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gc, static_cast<unsigned long long>(v));
-            }
-        }
+        int gi = w.ir + w.mi + wi;
+        if (gi < 0) gi += g.nx;
+        if (gi >= g.nx) gi -= g.nx;
+        long long v = s[2 * f * WH + c];
+        if (tracked<T0>(w, f)) v += static_cast<long long>(s[(2 * f + 1) * WH + c]) * 4294967296ll;
+        if (v != 0)
+            atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gj * g.nx + gi, static_cast<unsigned long long>(v));
     }
 }
 
