@@ -332,6 +332,97 @@ __device__ __forceinline__ void gather_em(const float* __restrict__ gb, const Ci
     bz = gather4_tile(s, b0.y, b1.y, b2.y, b3.y);
 }
 
+// ---------------------------------------------------------------------------
+// Gather tiles. Before pass 1 a chunk can copy the cells its particles gather
+// from (the bounding box of their base cells plus the +1 CIC corner) of the
+// interleaved [ncell][8] field buffer into shared memory: one bulk copy per tile
+// row, two where the row wraps at x = nx. Pass 1 then reads its four corners
+// with shared loads, without wrap arithmetic. The tile lives in the window
+// area, which the deposit only needs after pass 1.
+struct Tile {
+    int i0, j0;          // grid cell of tile (0, 0)
+    int W, H;
+    bool use;
+};
+
+// The tile of a chunk from the block-wide min/max of its particles' positions
+// (every thread passes its own extremes of valid particles; positions are
+// non-negative, so float order is integer order of the bit patterns). A chunk
+// whose particles straddle the periodic edge gets a box as wide as the grid and
+// no tile.
+__device__ __forceinline__ Tile tile_of(float xmin, float xmax, float ymin, float ymax, const Geo& g, int cap_cells,
+                                        int* red) {
+    constexpr int NW = kThreads / 32;
+    int v[4] = {__reduce_min_sync(0xffffffffu, __float_as_int(xmin)), __reduce_max_sync(0xffffffffu, __float_as_int(xmax)),
+                __reduce_min_sync(0xffffffffu, __float_as_int(ymin)), __reduce_max_sync(0xffffffffu, __float_as_int(ymax))};
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) red[warp * 4 + k] = v[k];
+    __syncthreads();
+    int lo_x = red[0], hi_x = red[1], lo_y = red[2], hi_y = red[3];
+#pragma unroll
+    for (int k = 1; k < NW; ++k) {
+        lo_x = min(lo_x, red[k * 4 + 0]); hi_x = max(hi_x, red[k * 4 + 1]);
+        lo_y = min(lo_y, red[k * 4 + 2]); hi_y = max(hi_y, red[k * 4 + 3]);
+    }
+    __syncthreads();     // red is reused by the caller
+    Tile t;
+    t.use = hi_x >= lo_x;   // some valid particle
+    t.i0 = static_cast<int>(__int_as_float(lo_x));
+    t.j0 = static_cast<int>(__int_as_float(lo_y));
+    t.W = static_cast<int>(__int_as_float(hi_x)) - t.i0 + 2;
+    t.H = static_cast<int>(__int_as_float(hi_y)) - t.j0 + 2;
+    t.use = t.use && t.W <= g.nx && t.H <= g.ny && t.W * t.H <= cap_cells;
+    return t;
+}
+
+// Copy the tile (8 floats per cell) into shared memory; false (block-uniformly)
+// when the bounded wait gave up. Ends with every thread past the wait.
+__device__ __forceinline__ bool load_tile8(float* tile, const float* __restrict__ gb, const Tile& t, const Geo& g,
+                                           unsigned long long* bar, DevState* st) {
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_arrive_expect_tx(bar, static_cast<unsigned>(t.W * t.H) * 32u);
+        for (int r = 0; r < t.H; ++r) {
+            int gj = t.j0 + r;
+            if (gj >= g.ny) gj -= g.ny;
+            const int n1 = min(t.W, g.nx - t.i0);
+            const float* row = gb + static_cast<size_t>(gj) * g.nx * 8;
+            bulk_load_keep(tile + static_cast<size_t>(r) * t.W * 8, row + static_cast<size_t>(t.i0) * 8,
+                           static_cast<unsigned>(n1) * 32u, bar);
+            if (n1 < t.W)
+                bulk_load_keep(tile + (static_cast<size_t>(r) * t.W + n1) * 8, row,
+                               static_cast<unsigned>(t.W - n1) * 32u, bar);
+        }
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(bar, 0u);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) set_err(st, 4u);     // AW_DEV_WAIT_LIMIT
+        mbar_wait_bounded(bar, 0u);
+        return false;
+    }
+    return true;
+}
+
+// The EM gather from a shared tile (same arithmetic as gather_em).
+__device__ __forceinline__ void gather_em_tile(const float* __restrict__ tile, const Cic& s, int li, int lj, int W,
+                                               float& ex, float& ey, float& ez, float& bx, float& by, float& bz) {
+    const float4* q = reinterpret_cast<const float4*>(tile);
+    const int c0 = lj * W + li, c2 = c0 + W;
+    const float4 a0 = q[2 * c0], b0 = q[2 * c0 + 1];
+    const float4 a1 = q[2 * c0 + 2], b1 = q[2 * c0 + 3];
+    const float4 a2 = q[2 * c2], b2 = q[2 * c2 + 1];
+    const float4 a3 = q[2 * c2 + 2], b3 = q[2 * c2 + 3];
+    ex = gather4_tile(s, a0.x, a1.x, a2.x, a3.x);
+    ey = gather4_tile(s, a0.y, a1.y, a2.y, a3.y);
+    ez = gather4_tile(s, a0.z, a1.z, a2.z, a3.z);
+    bx = gather4_tile(s, a0.w, a1.w, a2.w, a3.w);
+    by = gather4_tile(s, b0.x, b1.x, b2.x, b3.x);
+    bz = gather4_tile(s, b0.y, b1.y, b2.y, b3.y);
+}
+
 // dcu scales: |coef_dcu (E + v x B)| <= |qm| coef_max (Emax + 2 Umax Bmax); in
 // the fused step the bound per component is also capped at 8 x the rms the
 // previous step's dcu coefficients had.
@@ -359,7 +450,7 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
     constexpr bool T0 = false;
     extern __shared__ __align__(16) unsigned char smem[];
     const Smem m = carve(smem, NIN, NF, wmaxc);
-    __shared__ unsigned long long bar;
+    __shared__ unsigned long long bar, tbar;
     __shared__ int nlist;
     __shared__ float ssq[(NF + 1) * (kThreads / 32)];
 
@@ -374,6 +465,21 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
     if (!load_chunk(m.stage, src, NIN, c0, cnt, p.vec_ok != 0, &bar, st, &x0, &y0)) return;
     int ir, jr;
     ref_of(x0, y0, g, ir, jr);
+
+    // the field tile of the chunk's positions, in the window area
+    float xmin = 3.0e38f, xmax = -1.0f, ymin = 3.0e38f, ymax = -1.0f;
+#pragma unroll 4
+    for (int it = 0; it < kPPT; ++it) {
+        const int s = it * kThreads + threadIdx.x;
+        const float x = m.stage[s], y = m.stage[kChunk + s];
+        if (s < cnt && in_grid(x, y, g)) {
+            xmin = fminf(xmin, x); xmax = fmaxf(xmax, x);
+            ymin = fminf(ymin, y); ymax = fmaxf(ymax, y);
+        }
+    }
+    const Tile tl = tile_of(xmin, xmax, ymin, ymax, g, wmaxc * NF / 4, m.red);
+    float* const tile = reinterpret_cast<float*>(m.win);
+    if (tl.use && !load_tile8(tile, gb, tl, g, &tbar, st)) return;
 
     BBox bb;
     float l1[NF] = {};
@@ -390,7 +496,10 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
                 const Cic c = cic(x, y);
                 bb.add(c.i0, c.j0, ir, jr, g);
                 float ex, ey, ez, bx, by, bz;
-                gather_em(gb, c, g, ex, ey, ez, bx, by, bz);
+                if (tl.use)
+                    gather_em_tile(tile, c, c.i0 - tl.i0, c.j0 - tl.j0, tl.W, ex, ey, ez, bx, by, bz);
+                else
+                    gather_em(gb, c, g, ex, ey, ez, bx, by, bz);
                 const float coef = __double2float_rn(qm2oa * static_cast<double>(w));
                 const float cx = __fmaf_rn(vy, bz, -__fmul_rn(vz, by));
                 const float cy = __fmaf_rn(vz, bx, -__fmul_rn(vx, bz));
@@ -642,7 +751,7 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     constexpr bool T0 = true;
     extern __shared__ __align__(16) unsigned char smem[];
     const Smem m = carve(smem, NS, NF, wmaxc);
-    __shared__ unsigned long long bar;
+    __shared__ unsigned long long bar, tbar;
     __shared__ int nlist;
     __shared__ double dsh[4 * (kThreads / 32)];
     __shared__ unsigned umx[3][kThreads / 32];
@@ -659,6 +768,21 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     if (!load_chunk(m.stage, src, NS, c0, cnt, p.vec_ok != 0, &bar, st, &x0, &y0)) return;
     int ir, jr;
     ref_of(x0, y0, g, ir, jr);
+
+    // the field tile of the chunk's current positions, in the window area
+    float xmin = 3.0e38f, xmax = -1.0f, ymin = 3.0e38f, ymax = -1.0f;
+#pragma unroll 4
+    for (int it = 0; it < kPPT; ++it) {
+        const int s = it * kThreads + threadIdx.x;
+        const float x = m.stage[s], y = m.stage[kChunk + s];
+        if (s < cnt && in_grid(x, y, g)) {
+            xmin = fminf(xmin, x); xmax = fmaxf(xmax, x);
+            ymin = fminf(ymin, y); ymax = fmaxf(ymax, y);
+        }
+    }
+    const Tile tl = tile_of(xmin, xmax, ymin, ymax, g, wmaxc * NF / 4, m.red);
+    float* const tile = reinterpret_cast<float*>(m.win);
+    if (tl.use && !load_tile8(tile, gb, tl, g, &tbar, st)) return;
 
     BBox bb;
     float l1[NF] = {};
@@ -678,7 +802,10 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
             if (in_grid(x, y, g)) {
                 const Cic c = cic(x, y);
                 float ex, ey, ez, bx, by, bz;
-                gather_em(gb, c, g, ex, ey, ez, bx, by, bz);
+                if (tl.use)
+                    gather_em_tile(tile, c, c.i0 - tl.i0, c.j0 - tl.j0, tl.W, ex, ey, ez, bx, by, bz);
+                else
+                    gather_em(gb, c, g, ex, ey, ez, bx, by, bz);
                 boris_em(ux, uy, uz, ex, ey, ez, bx, by, bz, pp.qmh);
                 move_xy<POW2>(x, y, ux, uy, pp, g);
                 int ci, cj;
