@@ -127,21 +127,31 @@ void es_fields_from_pending(Ctx& c, bool step_begin, Mark mark) {
 }
 void es_fields_from_pending(Ctx& c, bool step_begin) { es_fields_from_pending(c, step_begin, NoMark{}); }
 
+// Darwin fields in two grid phases around the dcu deposit: A (rho, J, amu ->
+// E_L, B, the dcu gather buffer) and B (dcu -> E_T, E, the push buffer).
 template <class Mark>
-void darwin_fields_from_pending(Ctx& c, bool step_begin, Mark mark) {
+void darwin_fields_a(Ctx& c, bool step_begin, Mark mark) {
     float* api[8] = {c.src.rho, c.src.Jx, c.src.Jy, c.src.Jz, c.src.amu0, c.src.amu1, c.src.amu2, c.src.amu3};
     launch_finalize(c, c.acc_src, 0, 8, c.st->S_pend, c.r_src, api, false, true, step_begin); mark(0);
     AW_CUFFT(cufftExecR2C(c.p_r2cS, c.r_src, c.k_src)); mark(1);
     launch_kspace_elb(c, c.k_src, c.k_out); mark(2);
     AW_CUFFT(cufftExecC2R(c.p_c2rO, c.k_out, c.r_out)); mark(3);
     launch_fields_dcu(c); mark(4);
-    launch_deposit_dcu(c, c.gb_dcu, true); mark(5);
+}
+template <class Mark>
+void darwin_fields_b(Ctx& c, Mark mark) {
     float* apid[3] = {c.src.dcux, c.src.dcuy, c.src.dcuz};
     launch_finalize(c, c.acc_dcu, 0, 3, c.st->S_dcu, c.r_dcu, apid, false, false, false); mark(6);
     AW_CUFFT(cufftExecR2C(c.p_r2c3, c.r_dcu, c.k_dcu)); mark(7);
     launch_kspace_et(c, c.k_dcu, c.k_src + static_cast<size_t>(4) * c.sg.nk, c.k_et); mark(8);
     AW_CUFFT(cufftExecC2R(c.p_c2r3, c.k_et, c.r_et)); mark(9);
     launch_fields_push(c); mark(10);
+}
+template <class Mark>
+void darwin_fields_from_pending(Ctx& c, bool step_begin, Mark mark) {
+    darwin_fields_a(c, step_begin, mark);
+    launch_deposit_dcu(c, c.gb_dcu, true); mark(5);
+    darwin_fields_b(c, mark);
 }
 void darwin_fields_from_pending(Ctx& c, bool step_begin) { darwin_fields_from_pending(c, step_begin, NoMark{}); }
 
@@ -329,6 +339,18 @@ double grad_es_impl(Ctx& c, long long nsteps, int every, float* dux, float* duy,
 
 namespace aw {
 void prepare_step(Ctx& c) { ensure_pending(c); }
+
+void step_grid_phase(Ctx& c, int phase) {
+    if (phase == 0) {
+        if (c.model == AW_MODEL_ES) es_fields_from_pending(c, true, NoMark{});
+        else darwin_fields_a(c, true, NoMark{});
+    } else if (phase == 1) {
+        need(c.model == AW_MODEL_DARWIN, AW_ERR_STATE, "grid phase 1 is Darwin only");
+        darwin_fields_b(c, NoMark{});
+    } else {
+        launch_step_reduce(c);
+    }
+}
 
 cudaGraph_t capture_step_graph(Ctx& c) {
     ensure_pending(c);

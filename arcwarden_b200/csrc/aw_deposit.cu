@@ -41,7 +41,9 @@
 
 #include <algorithm>
 #include <cmath>
+#include <memory>
 #include <mutex>
+#include <vector>
 
 namespace aw {
 namespace {
@@ -147,9 +149,9 @@ __device__ __forceinline__ bool scale_fast(const float (&cf)[NF], const float (&
     return fast;
 }
 
-// Block-wide fixed-order sum of 4 doubles into part[blockIdx.x*5 + 0..3].
+// Block-wide fixed-order sum of 4 doubles into part[blk*5 + 0..3] (blk: the chunk).
 __device__ void block_sum4(double a, double b, double c, double d, double* __restrict__ part,
-                           double* sh /* 4 * warps */) {
+                           double* sh /* 4 * warps */, int blk) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         a += __shfl_down_sync(0xffffffffu, a, o);
@@ -165,16 +167,17 @@ __device__ void block_sum4(double a, double b, double c, double d, double* __res
         double s = 0;
 #pragma unroll
         for (int w = 0; w < NW; ++w) s += sh[threadIdx.x * NW + w];
-        part[blockIdx.x * 5 + threadIdx.x] = s;
+        part[blk * 5 + threadIdx.x] = s;
     }
-    if (threadIdx.x == 4) part[blockIdx.x * 5 + 4] = 0.0;
+    if (threadIdx.x == 4) part[blk * 5 + 4] = 0.0;
 }
 
 // Block-wide fixed-order sum of NF floats (plus the valid-particle count in
-// slot NF) into part[blockIdx.x * (NF + 1) + f]. Deterministic for a fixed
+// slot NF) into part[blk * (NF + 1) + f]. Deterministic for a fixed
 // launch shape.
 template <int NF>
-__device__ void block_sumsq(float (&sq)[NF], float cnt, float* __restrict__ part, float* sh /* (NF+1) * warps */) {
+__device__ void block_sumsq(float (&sq)[NF], float cnt, float* __restrict__ part, float* sh /* (NF+1) * warps */,
+                            int blk) {
     constexpr int NW = kThreads / 32;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -192,7 +195,7 @@ __device__ void block_sumsq(float (&sq)[NF], float cnt, float* __restrict__ part
     if (threadIdx.x <= NF) {
         float s = 0.f;
         for (int w = 0; w < NW; ++w) s += sh[threadIdx.x * NW + w];
-        part[blockIdx.x * (NF + 1) + threadIdx.x] = s;
+        part[blk * (NF + 1) + threadIdx.x] = s;
     }
 }
 
@@ -309,7 +312,7 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
     };
     window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
-    if (psq) block_sumsq<NF>(sq, nval, psq, ssq);
+    if (psq) block_sumsq<NF>(sq, nval, psq, ssq, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -442,10 +445,15 @@ __device__ __forceinline__ void dcu_scales(const DevState* st, float abs_qm, boo
 }
 
 // dcu deposit: input x y w ux uy uz; stage = x, y, ax, ay, az (scaled coefficients).
-__global__ void __launch_bounds__(kThreads, 3)
-k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restrict__ gb,
-              unsigned long long* __restrict__ acc, int wmaxc, DevState* st, int use_rms,
-              float* __restrict__ psq) {
+struct DcuArgs {
+    Parts p; Geo g; double qm2oa; float abs_qm; const float* gb; unsigned long long* acc; int wmaxc;
+    DevState* st; int use_rms; float* psq;
+};
+__device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int chunk) {
+    const Parts& p = A.p; const Geo& g = A.g;
+    const double qm2oa = A.qm2oa; const float abs_qm = A.abs_qm;
+    const float* __restrict__ gb = A.gb; unsigned long long* __restrict__ acc = A.acc;
+    const int wmaxc = A.wmaxc; DevState* st = A.st; const int use_rms = A.use_rms; float* __restrict__ psq = A.psq;
     constexpr int NF = 3, NS = 5, NIN = 6;
     constexpr bool T0 = false;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -454,11 +462,11 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
     __shared__ int nlist;
     __shared__ float ssq[(NF + 1) * (kThreads / 32)];
 
-    const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
+    const long long c0 = static_cast<long long>(chunk) * kChunk;
     const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
     float S[3];
     dcu_scales(st, abs_qm, use_rms != 0, S);
-    if (blockIdx.x == 0 && threadIdx.x == 0) { st->S_dcu[0] = S[0]; st->S_dcu[1] = S[1]; st->S_dcu[2] = S[2]; }
+    if (chunk == 0 && threadIdx.x == 0) { st->S_dcu[0] = S[0]; st->S_dcu[1] = S[1]; st->S_dcu[2] = S[2]; }
     if (threadIdx.x == 0) nlist = 0;
     const ChunkSrc src{{p.x, p.y, p.w, p.ux, p.uy, p.uz}};
     float x0, y0;
@@ -530,8 +538,8 @@ k_deposit_dcu(Parts p, Geo g, double qm2oa, float abs_qm, const float* __restric
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) { cs[0] = a[2]; cs[1] = a[3]; cs[2] = a[4]; };
     window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
-    if (psq) block_sumsq<NF>(sq, nval, psq, ssq);
-}
+    if (psq) block_sumsq<NF>(sq, nval, psq, ssq, chunk);}
+__global__ void __launch_bounds__(kThreads, 3) k_deposit_dcu(DcuArgs A) { deposit_dcu_chunk(A, blockIdx.x); }
 
 // ---------------------------------------------------------------------------
 // Backward step A of the ES adjoint (the transpose of k_push_deposit_es's push
@@ -653,11 +661,15 @@ __device__ __forceinline__ void move_xy(float& x, float& y, float ux, float uy, 
 }
 
 // Fused ES step kernel: input x y w ux uy uz; stage = new x, y, coefficient q w / (dx dy).
+struct EsArgs {
+    Parts p; Geo g; PushP pp; const float* gb; double qoa; unsigned long long* acc; int wmaxc;
+    double* part; DevState* st;
+};
 template <bool POW2>
-__global__ void __launch_bounds__(kThreads, 3)
-k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
-                  double qoa, unsigned long long* __restrict__ acc, int wmaxc,
-                  double* __restrict__ part, DevState* st) {
+__device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int chunk) {
+    const Parts& p = A.p; const Geo& g = A.g; const PushP& pp = A.pp;
+    const float* __restrict__ gb = A.gb; const double qoa = A.qoa; unsigned long long* __restrict__ acc = A.acc;
+    const int wmaxc = A.wmaxc; double* __restrict__ part = A.part; DevState* st = A.st;
     constexpr int NF = 1, NS = 3, NIN = 6;
     constexpr bool T0 = true;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -666,7 +678,7 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     __shared__ int nlist;
     __shared__ double dsh[4 * (kThreads / 32)];
 
-    const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
+    const long long c0 = static_cast<long long>(chunk) * kChunk;
     const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
     const float S1[1] = {st->S_next[0]};
     if (threadIdx.x == 0) nlist = 0;
@@ -734,19 +746,25 @@ k_push_deposit_es(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     };
     window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
-    block_sum4(ke, px, py, pz, part, dsh);
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
+    block_sum4(ke, px, py, pz, part, dsh, chunk);
+    if (threadIdx.x == 0 && chunk == 0) {
         st->S_pend[0] = S1[0];
         st->step += 1;
-    }
-}
+    }}
+template <bool POW2>
+__global__ void __launch_bounds__(kThreads, 3) k_push_deposit_es(EsArgs A) { push_deposit_es_chunk<POW2>(A, blockIdx.x); }
 
 // Fused Darwin step kernel: input x y w ux uy uz; stage = new x, y, coefficient, ux, uy, uz.
+struct EmArgs {
+    Parts p; Geo g; PushP pp; const float* gb; double qoa; unsigned long long* acc; int wmaxc;
+    double* part; DevState* st; float* psq;
+};
 template <bool POW2>
-__global__ void __launch_bounds__(kThreads, 3)
-k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
-                  double qoa, unsigned long long* __restrict__ acc, int wmaxc,
-                  double* __restrict__ part, DevState* st, float* __restrict__ psq) {
+__device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int chunk) {
+    const Parts& p = A.p; const Geo& g = A.g; const PushP& pp = A.pp;
+    const float* __restrict__ gb = A.gb; const double qoa = A.qoa; unsigned long long* __restrict__ acc = A.acc;
+    const int wmaxc = A.wmaxc; double* __restrict__ part = A.part; DevState* st = A.st;
+    float* __restrict__ psq = A.psq;
     constexpr int NF = 8, NS = 6;
     constexpr bool T0 = true;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -757,7 +775,7 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     __shared__ unsigned umx[3][kThreads / 32];
     __shared__ float ssq[(NF + 1) * (kThreads / 32)];
 
-    const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
+    const long long c0 = static_cast<long long>(chunk) * kChunk;
     const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
     float S[NF];
 #pragma unroll
@@ -869,13 +887,55 @@ k_push_deposit_em(Parts p, Geo g, PushP pp, const float* __restrict__ gb,
     };
     window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
-    block_sumsq<NF>(sq, nval, psq, ssq);
-    block_sum4(ke, px, py, pz, part, dsh);
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
+    block_sumsq<NF>(sq, nval, psq, ssq, chunk);
+    block_sum4(ke, px, py, pz, part, dsh, chunk);
+    if (threadIdx.x == 0 && chunk == 0) {
 #pragma unroll
         for (int f = 0; f < NF; ++f) st->S_pend[f] = S[f];
         st->step += 1;
+    }}
+template <bool POW2>
+__global__ void __launch_bounds__(kThreads, 3) k_push_deposit_em(EmArgs A) { push_deposit_em_chunk<POW2>(A, blockIdx.x); }
+
+// ---------------------------------------------------------------------------
+// Multi-run launches (batched ensembles): one grid over the chunks of several
+// runs of one kind. Block b belongs to run r with first[r] <= b < first[r + 1]
+// and handles that run's chunk b - first[r]; thread 0 copies the run's
+// arguments into shared memory.
+__device__ __forceinline__ int find_run(const int* __restrict__ first, int nruns) {
+    int lo = 0, hi = nruns - 1;
+    const int b = static_cast<int>(blockIdx.x);
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (first[mid] <= b) lo = mid; else hi = mid - 1;
     }
+    return lo;
+}
+__global__ void __launch_bounds__(kThreads, 3)
+k_deposit_dcu_multi(const DcuArgs* __restrict__ runs, const int* __restrict__ first, int nruns) {
+    __shared__ DcuArgs A;
+    __shared__ int chunk;
+    if (threadIdx.x == 0) { const int r = find_run(first, nruns); A = runs[r]; chunk = blockIdx.x - first[r]; }
+    __syncthreads();
+    deposit_dcu_chunk(A, chunk);
+}
+template <bool POW2>
+__global__ void __launch_bounds__(kThreads, 3)
+k_push_deposit_es_multi(const EsArgs* __restrict__ runs, const int* __restrict__ first, int nruns) {
+    __shared__ EsArgs A;
+    __shared__ int chunk;
+    if (threadIdx.x == 0) { const int r = find_run(first, nruns); A = runs[r]; chunk = blockIdx.x - first[r]; }
+    __syncthreads();
+    push_deposit_es_chunk<POW2>(A, chunk);
+}
+template <bool POW2>
+__global__ void __launch_bounds__(kThreads, 3)
+k_push_deposit_em_multi(const EmArgs* __restrict__ runs, const int* __restrict__ first, int nruns) {
+    __shared__ EmArgs A;
+    __shared__ int chunk;
+    if (threadIdx.x == 0) { const int r = find_run(first, nruns); A = runs[r]; chunk = blockIdx.x - first[r]; }
+    __syncthreads();
+    push_deposit_em_chunk<POW2>(A, chunk);
 }
 
 inline int nchunks(long long n) { return static_cast<int>(std::max<long long>(1, (n + kChunk - 1) / kChunk)); }
@@ -929,6 +989,31 @@ PushP push_params(const Ctx& c) {
     return pp;
 }
 
+DcuArgs dcu_args(const Ctx& c, const float* gb, bool fused) {
+    DcuArgs a{};
+    a.p = c.parts; a.g = c.geo;
+    a.qm2oa = c.prm.qm * c.prm.qm / (c.geo.dx * c.geo.dy);
+    a.abs_qm = static_cast<float>(std::fabs(c.prm.qm));
+    a.gb = gb; a.acc = c.acc_dcu; a.wmaxc = wmax_cells(3); a.st = c.st;
+    a.use_rms = fused ? 1 : 0; a.psq = fused ? c.part_d : nullptr;
+    return a;
+}
+EsArgs es_args(const Ctx& c) {
+    EsArgs a{};
+    a.p = c.parts; a.g = c.geo; a.pp = push_params(c); a.gb = c.gb_es;
+    a.qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
+    a.acc = c.acc_src; a.wmaxc = wmax_cells(1); a.part = c.part_p; a.st = c.st;
+    return a;
+}
+EmArgs em_args(const Ctx& c) {
+    EmArgs a{};
+    a.p = c.parts; a.g = c.geo; a.pp = push_params(c); a.gb = c.gb_push;
+    a.qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
+    a.acc = c.acc_src; a.wmaxc = wmax_cells(8); a.part = c.part_p; a.st = c.st; a.psq = c.part_c;
+    return a;
+}
+bool pow2_geo(const Ctx& c) { return is_pow2(c.geo.dx) && is_pow2(c.geo.dy); }
+
 }  // namespace
 
 // ===========================================================================
@@ -955,40 +1040,103 @@ void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE
     AW_LAUNCH();
 }
 
+// ---- multi-run particle phases -----------------------------------------------
+struct MultiPhase {
+    int kind = 0, nruns = 0, nblocks = 0;
+    bool pow2 = true;
+    void* d_args = nullptr;
+    int* d_first = nullptr;
+};
+
+MultiPhase* multi_create(int kind, Ctx* const* runs, int nruns) {
+    need(nruns > 0 && (kind == kMultiEsPush || kind == kMultiDcu || kind == kMultiEmPush), AW_ERR_ARG,
+         "multi-run phase: bad arguments");
+    std::unique_ptr<MultiPhase> m(new MultiPhase());
+    m->kind = kind;
+    m->nruns = nruns;
+    std::vector<int> first(nruns + 1, 0);
+    for (int r = 0; r < nruns; ++r) first[r + 1] = first[r] + (runs[r]->parts.n > 0 ? nchunks(runs[r]->parts.n) : 0);
+    m->nblocks = first[nruns];
+    m->pow2 = pow2_geo(*runs[0]);
+    for (int r = 1; r < nruns; ++r)
+        need(pow2_geo(*runs[r]) == m->pow2, AW_ERR_ARG, "multi-run phase: runs disagree on power-of-two cells");
+    size_t bytes = 0;
+    std::vector<unsigned char> host;
+    auto put = [&](const void* a, size_t sz) {
+        host.insert(host.end(), static_cast<const unsigned char*>(a), static_cast<const unsigned char*>(a) + sz);
+    };
+    for (int r = 0; r < nruns; ++r) {
+        if (kind == kMultiEsPush) { const EsArgs a = es_args(*runs[r]); put(&a, sizeof a); }
+        else if (kind == kMultiDcu) { const DcuArgs a = dcu_args(*runs[r], runs[r]->gb_dcu, true); put(&a, sizeof a); }
+        else { const EmArgs a = em_args(*runs[r]); put(&a, sizeof a); }
+    }
+    bytes = host.size();
+    try {
+        AW_CUDA(cudaMalloc(&m->d_args, bytes));
+        AW_CUDA(cudaMalloc(&m->d_first, sizeof(int) * first.size()));
+        AW_CUDA(cudaMemcpy(m->d_args, host.data(), bytes, cudaMemcpyHostToDevice));
+        AW_CUDA(cudaMemcpy(m->d_first, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
+        // the shared-memory opt-ins, before any capture
+        if (kind == kMultiDcu) prep_smem(k_deposit_dcu_multi, smem_bytes(3, 6));
+        else if (kind == kMultiEsPush) prep_smem(m->pow2 ? k_push_deposit_es_multi<true> : k_push_deposit_es_multi<false>,
+                                                 smem_bytes(1, 6));
+        else prep_smem(m->pow2 ? k_push_deposit_em_multi<true> : k_push_deposit_em_multi<false>, smem_bytes(8, 6));
+    } catch (...) {
+        multi_free(m.get());
+        m.release();
+        throw;
+    }
+    return m.release();
+}
+
+void multi_launch(MultiPhase* m, cudaStream_t s) {
+    if (m->nblocks == 0) return;
+    const auto* first = m->d_first;
+    if (m->kind == kMultiDcu) {
+        k_deposit_dcu_multi<<<m->nblocks, kThreads, smem_bytes(3, 6), s>>>(static_cast<const DcuArgs*>(m->d_args),
+                                                                             first, m->nruns);
+    } else if (m->kind == kMultiEsPush) {
+        auto kern = m->pow2 ? k_push_deposit_es_multi<true> : k_push_deposit_es_multi<false>;
+        kern<<<m->nblocks, kThreads, smem_bytes(1, 6), s>>>(static_cast<const EsArgs*>(m->d_args), first, m->nruns);
+    } else {
+        auto kern = m->pow2 ? k_push_deposit_em_multi<true> : k_push_deposit_em_multi<false>;
+        kern<<<m->nblocks, kThreads, smem_bytes(8, 6), s>>>(static_cast<const EmArgs*>(m->d_args), first, m->nruns);
+    }
+    AW_LAUNCH();
+}
+
+void multi_free(MultiPhase* m) {
+    if (!m) return;
+    if (m->d_args) cudaFree(m->d_args);
+    if (m->d_first) cudaFree(m->d_first);
+    delete m;
+}
+
 void launch_deposit_dcu(Ctx& c, const float* gb, bool fused) {
     if (c.parts.n == 0) return;
-    const double qm2oa = c.prm.qm * c.prm.qm / (c.geo.dx * c.geo.dy);
     const size_t sh = smem_bytes(3, 6);
     prep_smem(k_deposit_dcu, sh);
-    k_deposit_dcu<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(
-        c.parts, c.geo, qm2oa, static_cast<float>(std::fabs(c.prm.qm)), gb, c.acc_dcu, wmax_cells(3), c.st,
-        fused ? 1 : 0, fused ? c.part_d : nullptr);
+    k_deposit_dcu<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(dcu_args(c, gb, fused));
     AW_LAUNCH();
 }
 
 void launch_push_deposit_es(Ctx& c) {
     if (c.parts.n == 0) return;
-    const PushP pp = push_params(c);
-    const double qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
     const size_t sh = smem_bytes(1, 6);
-    const bool p2 = is_pow2(c.geo.dx) && is_pow2(c.geo.dy);
+    const bool p2 = pow2_geo(c);
     auto kern = p2 ? k_push_deposit_es<true> : k_push_deposit_es<false>;
     prep_smem(kern, sh);
-    kern<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(c.parts, c.geo, pp, c.gb_es, qoa, c.acc_src,
-                                                         wmax_cells(1), c.part_p, c.st);
+    kern<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(es_args(c));
     AW_LAUNCH();
 }
 
 void launch_push_deposit_em(Ctx& c) {
     if (c.parts.n == 0) return;
-    const PushP pp = push_params(c);
-    const double qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
     const size_t sh = smem_bytes(8, 6);
-    const bool p2 = is_pow2(c.geo.dx) && is_pow2(c.geo.dy);
+    const bool p2 = pow2_geo(c);
     auto kern = p2 ? k_push_deposit_em<true> : k_push_deposit_em<false>;
     prep_smem(kern, sh);
-    kern<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(c.parts, c.geo, pp, c.gb_push, qoa, c.acc_src,
-                                                         wmax_cells(8), c.part_p, c.st, c.part_c);
+    kern<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(em_args(c));
     AW_LAUNCH();
 }
 

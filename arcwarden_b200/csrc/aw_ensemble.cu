@@ -2,11 +2,14 @@
 // reference, which runs one Simulation at a time).
 //
 // Each run is an ordinary context on the ensemble's stream with its particle
-// SoA owned here. One ensemble step is one CUDA graph: a child-graph node per
-// run (that run's captured fused step), with no edges between them, so the
-// graph executor overlaps the runs' kernels across the GPU; small grids that
-// would leave most SMs idle when run alone share the machine. Every run
-// computes exactly what it computes alone (the same kernels on the same data).
+// SoA owned here. One ensemble step is one CUDA graph. Runs that fill the GPU
+// alone are independent child graphs (their whole fused step); the smaller
+// runs' grid phases are independent child graphs too, and each of their
+// particle phases is ONE launch over the chunks of every small run of that
+// model (k_*_multi: block -> (run, chunk) through a device table), so small
+// grids fill the machine together. The executor overlaps everything that does
+// not depend on each other. Every run computes exactly what it computes alone
+// (the same chunk code on the same data).
 //
 // The autotuner picks, per class of runs (model, grid, particles per cell), the
 // spatial re-sort interval and tile size from timed trials on a scratch copy.
@@ -32,6 +35,7 @@ struct aw_ensemble {
     cudaGraph_t parent = nullptr;
     cudaGraphExec_t pexec = nullptr;
     std::vector<cudaGraph_t> children;
+    std::vector<aw::MultiPhase*> phases;   // the multi-run particle launches of the graph
     long long step = 0;
 };
 
@@ -48,9 +52,83 @@ void drop_ensemble_graph(aw_ensemble& e) {
     if (e.pexec) cudaGraphExecDestroy(e.pexec);
     if (e.parent) cudaGraphDestroy(e.parent);
     for (cudaGraph_t g : e.children) if (g) cudaGraphDestroy(g);
+    for (MultiPhase* m : e.phases) multi_free(m);
     e.pexec = nullptr;
     e.parent = nullptr;
     e.children.clear();
+    e.phases.clear();
+}
+
+// `body` captured on the ensemble's stream into a graph the ensemble owns.
+template <class F>
+cudaGraph_t capture(aw_ensemble& e, F body) {
+    cudaGraph_t g = nullptr;
+    AW_CUDA(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        body();
+    } catch (...) {
+        cudaStreamEndCapture(e.stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    AW_CUDA(cudaStreamEndCapture(e.stream, &g));
+    e.children.push_back(g);
+    return g;
+}
+
+// Runs with at least this many chunks fill the GPU's CTA slots on their own
+// (148 SMs x 3 CTAs): they keep their whole fused step as one child graph.
+constexpr long long kOwnStepChunks = 148LL * 3;
+
+// One ensemble step as one graph. A run large enough to fill the GPU is one
+// child graph (its whole fused step), independent of the others. The smaller
+// runs share their particle phases: their grid phases are independent child
+// graphs, and each particle phase is one multi-run launch over the chunks of
+// all small runs of that model, after the grid phases it depends on.
+//   ES:     A (solve) -> [push+deposit, small ES runs] -> C (reduction)
+//   Darwin: A (E_L, B) -> [dcu deposit, small Darwin runs] -> B (E_T, E)
+//           -> [push+deposit, small Darwin runs] -> C
+// (Batching every run behind shared phase barriers measured slower: the large
+// runs then wait for all grid phases instead of overlapping them.)
+void build_ensemble_graph(aw_ensemble& e) {
+    AW_CUDA(cudaGraphCreate(&e.parent, 0));
+    auto child = [&](cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps) {
+        cudaGraphNode_t node;
+        AW_CUDA(cudaGraphAddChildGraphNode(&node, e.parent, deps.empty() ? nullptr : deps.data(), deps.size(), g));
+        return node;
+    };
+    std::vector<Ctx*> es, dw;
+    std::vector<cudaGraphNode_t> a_es, a_dw;
+    for (auto& r : e.runs) {
+        Ctx& c = r.ctx->c;
+        if ((r.n + kChunk - 1) / kChunk >= kOwnStepChunks) {
+            cudaGraph_t g = capture_step_graph(c);
+            e.children.push_back(g);
+            child(g, {});
+            continue;
+        }
+        const cudaGraphNode_t a = child(capture(e, [&] { step_grid_phase(c, 0); }), {});
+        if (c.model == AW_MODEL_ES) { es.push_back(&c); a_es.push_back(a); }
+        else { dw.push_back(&c); a_dw.push_back(a); }
+    }
+    if (!es.empty()) {
+        MultiPhase* m = multi_create(kMultiEsPush, es.data(), static_cast<int>(es.size()));
+        e.phases.push_back(m);
+        const cudaGraphNode_t p = child(capture(e, [&] { multi_launch(m, e.stream); }), a_es);
+        for (Ctx* c : es) child(capture(e, [&] { step_grid_phase(*c, 2); }), {p});
+    }
+    if (!dw.empty()) {
+        MultiPhase* md = multi_create(kMultiDcu, dw.data(), static_cast<int>(dw.size()));
+        e.phases.push_back(md);
+        const cudaGraphNode_t pd = child(capture(e, [&] { multi_launch(md, e.stream); }), a_dw);
+        std::vector<cudaGraphNode_t> b;
+        for (Ctx* c : dw) b.push_back(child(capture(e, [&] { step_grid_phase(*c, 1); }), {pd}));
+        MultiPhase* mm = multi_create(kMultiEmPush, dw.data(), static_cast<int>(dw.size()));
+        e.phases.push_back(mm);
+        const cudaGraphNode_t pm = child(capture(e, [&] { multi_launch(mm, e.stream); }), b);
+        for (Ctx* c : dw) child(capture(e, [&] { step_grid_phase(*c, 2); }), {pm});
+    }
+    AW_CUDA(cudaGraphInstantiate(&e.pexec, e.parent, 0));
 }
 
 float* arr(const aw_ensemble::Run& r, int k) { return static_cast<float*>(r.buf) + static_cast<size_t>(k) * r.n4; }
@@ -229,19 +307,17 @@ int aw_ensemble_run(aw_ensemble* e, int64_t nsteps, int32_t concurrent) {
             e->step += nsteps;
             return;
         }
-        if (!e->pexec) {
-            AW_CUDA(cudaGraphCreate(&e->parent, 0));
-            for (auto& r : e->runs) {
-                Ctx& c = r.ctx->c;
-                e->children.push_back(aw::capture_step_graph(c));
-                cudaGraphNode_t node;
-                AW_CUDA(cudaGraphAddChildGraphNode(&node, e->parent, nullptr, 0, e->children.back()));
-            }
-            AW_CUDA(cudaGraphInstantiate(&e->pexec, e->parent, 0));
-        }
         for (auto& r : e->runs) {
             aw::prepare_step(r.ctx->c);
             aw::launch_set_step(r.ctx->c, e->step);
+        }
+        if (!e->pexec) {
+            try {
+                aw::build_ensemble_graph(*e);
+            } catch (...) {
+                aw::drop_ensemble_graph(*e);
+                throw;
+            }
         }
         for (int64_t i = 0; i < nsteps; ++i) {
             const int64_t s = e->step + i;

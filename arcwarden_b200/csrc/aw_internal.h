@@ -224,6 +224,14 @@ void launch_push_deposit_em(Ctx& c);
 void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE, AdjDev* ad,
                         unsigned long long* acc);
 void prep_adj_scatter();   // its shared-memory opt-in (before any capture)
+// Multi-run particle phases (batched ensembles): one launch over the chunks of
+// several runs of one kind. The run table is built once (device copies of each
+// run's kernel arguments); the runs' buffers must stay bound while it lives.
+enum { kMultiEsPush = 0, kMultiDcu = 1, kMultiEmPush = 2 };
+struct MultiPhase;
+MultiPhase* multi_create(int kind, Ctx* const* runs, int nruns);
+void multi_launch(MultiPhase* m, cudaStream_t s);
+void multi_free(MultiPhase* m);
 
 // ---- launchers (aw_spectral.cu) -------------------------------------------
 int  grid_partial_blocks();
@@ -256,6 +264,10 @@ void launch_step_reduce(Ctx& c);                   // end of a fused step: diagn
 cudaGraph_t capture_step_graph(Ctx& c);
 // Make sure the deposit of the current particles is pending (before a step).
 void prepare_step(Ctx& c);
+// The fused step's grid work between its particle kernels: phase 0 (the
+// pending sources -> the fields the first particle kernel gathers; ES: the
+// whole solve), 1 (Darwin: dcu -> E_T, E), 2 (the end-of-step reduction).
+void step_grid_phase(Ctx& c, int phase);
 
 // ---- the ES adjoint (aw_adjoint.cu) ----------------------------------------
 AdjK adj_constants(const Ctx& c, float dt_scale);

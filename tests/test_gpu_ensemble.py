@@ -41,10 +41,13 @@ def _ens_state(torch, e, run, keys=("x", "y", "ux", "uy", "uz")):
     return {k: d2h(torch, ptrs[k], n, np.float32) for k in keys}
 
 
-@pytest.mark.parametrize("concurrent", [True, False])
-def test_ensemble_runs_equal_runs_alone(torch_cuda, aw, concurrent):
+@pytest.mark.parametrize("concurrent, sides, nruns", [
+    (True, SIDES, 8), (False, SIDES, 8),
+    (True, (32, 256), 6),          # 256^2 x 16 ppc: 512 chunks, a run with its own step graph
+])
+def test_ensemble_runs_equal_runs_alone(torch_cuda, aw, concurrent, sides, nruns):
     from arcwarden_b200.ensemble import ensemble_specs
-    draws, specs = ensemble_specs(8, SIDES, PPCS)
+    draws, specs = ensemble_specs(nruns, sides, (16,) if sides != SIDES else PPCS)
     e = aw.Ensemble(specs)
     try:
         e.init()
