@@ -8,12 +8,19 @@
 // particles by small tiles every few dozen steps keeps chunks compact. The
 // reference's Darwin path reorders its particles by 16x16 tile every step
 // (Particles::sort_by_tile, include/pic/particles.hpp:678-726); here the sort
-// is by tiles of ~kChunk/2 particles, occasional, and stable (CUB's radix sort
-// is deterministic), so runs stay bit-reproducible. Results do not depend on
-// the order: the deposits are exact sums and the push is per particle.
+// is by tiles of ~kChunk/2 particles, occasional, and stable, so runs stay
+// bit-reproducible. Results do not depend on the order: the deposits are exact
+// sums and the push is per particle.
+//
+// The sort is an LSD radix sort of (tile key, index) pairs, 8 key bits per pass.
+// Each warp owns a contiguous range of kRsItems elements. A pass counts the
+// digits of every range (warp-private shared counters), turns the counts into
+// exclusive offsets in digit-major, range-minor order (one block per digit),
+// and scatters: each warp walks its range in order, 32 elements at a time, and
+// ranks an element among the lanes holding the same digit (match.any) on top of
+// its running per-digit offset. Positions come from counts and element order
+// only, so every pass is stable and the permutation is deterministic.
 #include "aw_internal.h"
-
-#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -50,6 +57,100 @@ __global__ void k_resort_gather(Gather7 io, const int* __restrict__ perm, long l
 #pragma unroll
         for (int f = 0; f < 7; ++f)
             if (io.out[f]) io.out[f][i] = io.in[f][p];
+    }
+}
+
+// ---- radix sort ----------------------------------------------------------
+constexpr int kRsItems = 4096;               // elements per warp range
+constexpr int kRsWarps = 8;                  // warps per block (count and scatter)
+
+int rs_ranges(long long n) { return static_cast<int>((n + kRsItems - 1) / kRsItems); }
+
+// C[d][w] = number of elements of range w whose digit is d; T[d] += the same.
+__global__ void __launch_bounds__(32 * kRsWarps)
+k_rs_count(const int* __restrict__ key, long long n, int shift, int* __restrict__ C, int* __restrict__ T, int nw) {
+    __shared__ int sc[kRsWarps][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * kRsWarps + warp;
+    for (int d = lane; d < 256; d += 32) sc[warp][d] = 0;
+    __syncwarp();
+    if (w < nw) {
+        const long long lo = static_cast<long long>(w) * kRsItems;
+        const long long hi = min(n, lo + kRsItems);
+        for (long long i = lo + lane; i < hi; i += 32) atomicAdd(&sc[warp][(key[i] >> shift) & 255], 1);
+        __syncwarp();
+        for (int d = lane; d < 256; d += 32) {
+            const int c = sc[warp][d];
+            C[static_cast<size_t>(d) * nw + w] = c;
+            if (c) atomicAdd(&T[d], c);
+        }
+    }
+}
+
+// Block d: C[d][w] <- (sum of T[d'] for d' < d) + sum of C[d][w'] for w' < w.
+__global__ void __launch_bounds__(256) k_rs_offsets(int* __restrict__ C, const int* __restrict__ T, int nw) {
+    __shared__ int wsum[8];
+    __shared__ int carry;
+    const int d = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) {
+        int b = 0;
+        for (int k = 0; k < d; ++k) b += T[k];
+        carry = b;
+    }
+    __syncthreads();
+    int* row = C + static_cast<size_t>(d) * nw;
+    for (int start = 0; start < nw; start += 256) {
+        const int i = start + t;
+        const int v = i < nw ? row[i] : 0;
+        int x = v;                                    // inclusive warp scan
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        int before = carry;
+        for (int k = 0; k < warp; ++k) before += wsum[k];
+        if (i < nw) row[i] = before + x - v;          // exclusive
+        __syncthreads();
+        if (t == 0) {
+            int tot = 0;
+            for (int k = 0; k < 8; ++k) tot += wsum[k];
+            carry += tot;
+        }
+        __syncthreads();
+    }
+}
+
+// Stable scatter of one pass (vin == nullptr: the values are the indices).
+__global__ void __launch_bounds__(32 * kRsWarps)
+k_rs_scatter(const int* __restrict__ kin, const int* __restrict__ vin, int* __restrict__ kout,
+             int* __restrict__ vout, long long n, int shift, const int* __restrict__ O, int nw) {
+    __shared__ int base[kRsWarps][256];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * kRsWarps + warp;
+    if (w >= nw) return;                       // whole warps only
+    for (int d = lane; d < 256; d += 32) base[warp][d] = O[static_cast<size_t>(d) * nw + w];
+    __syncwarp();
+    const long long lo = static_cast<long long>(w) * kRsItems;
+    const long long hi = min(n, lo + kRsItems);
+    const unsigned lt = (1u << lane) - 1u;
+    for (long long i0 = lo; i0 < hi; i0 += 32) {
+        const long long i = i0 + lane;
+        const bool ok = i < hi;
+        const int k = ok ? kin[i] : 0;
+        const int d = ok ? (k >> shift) & 255 : 256 + lane;   // invalid lanes match nobody
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        int pos = 0;
+        if (ok) {
+            pos = base[warp][d] + __popc(peers & lt);
+            kout[pos] = k;
+            vout[pos] = vin ? vin[i] : static_cast<int>(i);
+        }
+        __syncwarp();
+        if (ok && lane == 31 - __clz(peers)) base[warp][d] += __popc(peers);
+        __syncwarp();
     }
 }
 
@@ -93,13 +194,8 @@ void resort_reserve(Ctx& c) {
         AW_CUDA(cudaMalloc(&c.sort_tmp, sizeof(float) * 7 * static_cast<size_t>(n)));
         c.sort_tmp_n = n;
     }
-    int tx, ty;
-    resort_tile_shape(c, tx, ty);
-    const int ntiles = ((c.geo.nx + tx - 1) / tx) * ((c.geo.ny + ty - 1) / ty);
-    int* k = c.rs_buf;
-    size_t need = 0;
-    AW_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, need, k, k + n, k + 2 * n, k + 3 * n, static_cast<int>(n), 0,
-                                            bits_for(ntiles), c.stream));
+    // radix-sort counts/offsets [256][ranges] and digit totals [256]
+    const size_t need = sizeof(int) * (static_cast<size_t>(256) * rs_ranges(n) + 256);
     if (need > c.rs_temp_bytes) {
         if (c.rs_temp) cudaFree(c.rs_temp);
         c.rs_temp = nullptr;
@@ -126,9 +222,25 @@ void launch_resort(Ctx& c) {
     k_resort_keys<<<blocks, kThreads, 0, c.stream>>>(c.parts.x, c.parts.y, n, c.geo, tx, ty, ntx, ntiles,
                                                       keys_in, vals_in);
     AW_LAUNCH();
-    size_t tb = c.rs_temp_bytes;
-    AW_CUDA(cub::DeviceRadixSort::SortPairs(c.rs_temp, tb, keys_in, keys_out, vals_in, vals_out, ni, 0, end_bit,
-                                            c.stream));
+    // LSD passes, 8 bits each; the pairs ping-pong between the two buffers
+    const int nw = rs_ranges(n);
+    int* C = static_cast<int*>(c.rs_temp);
+    int* T = C + static_cast<size_t>(256) * nw;
+    const int rs_blocks = (nw + kRsWarps - 1) / kRsWarps;
+    int *ki = keys_in, *vi = vals_in, *ko = keys_out, *vo = vals_out;
+    for (int shift = 0; shift < end_bit; shift += 8) {
+        AW_CUDA(cudaMemsetAsync(T, 0, sizeof(int) * 256, c.stream));
+        k_rs_count<<<rs_blocks, 32 * kRsWarps, 0, c.stream>>>(ki, n, shift, C, T, nw);
+        AW_LAUNCH();
+        k_rs_offsets<<<256, 256, 0, c.stream>>>(C, T, nw);
+        AW_LAUNCH();
+        k_rs_scatter<<<rs_blocks, 32 * kRsWarps, 0, c.stream>>>(ki, vi, ko, vo, n, shift, C, nw);
+        AW_LAUNCH();
+        std::swap(ki, ko);
+        std::swap(vi, vo);
+    }
+    const int* perm = vi;                      // after the last swap: the sorted values
+    (void)ni;
     float* src[7] = {c.parts.x, c.parts.y, c.parts.ux, c.parts.uy, c.parts.uz, c.parts.w,
                      reinterpret_cast<float*>(c.parts.cell)};
     Gather7 io{};
@@ -140,7 +252,7 @@ void launch_resort(Ctx& c) {
         io.in[f] = t;
         io.out[f] = src[f];
     }
-    k_resort_gather<<<blocks, kThreads, 0, c.stream>>>(io, vals_out, n);
+    k_resort_gather<<<blocks, kThreads, 0, c.stream>>>(io, perm, n);
     AW_LAUNCH();
 }
 

@@ -163,6 +163,39 @@ def test_resort_only_permutes(setup, aw, model):
     assert not np.array_equal(outs[0]["x"], outs[1]["x"])       # the re-sort did reorder
 
 
+@pytest.mark.parametrize("nx, ny, ppc", [(96, 64, 16), (512, 256, 4), (40, 24, 1)])
+def test_resort_is_the_stable_sort_by_tile(setup, aw, nx, ny, ppc):
+    """aw_resort permutes the particles into the stable order of their tile keys
+    (tiles of ~1024 particles, out-of-grid last): the hand-written LSD radix sort
+    against numpy's stable argsort, element for element. 512 x 256 x 4 needs two
+    8-bit passes."""
+    n = nx * ny * ppc
+    s = setup(nx, ny, float(nx), float(ny), n, aw.AW_MODEL_DARWIN, dt=0.05)
+    rng = np.random.default_rng(nx + ppc)
+    x = rng.uniform(0, nx, n).astype(np.float32)
+    y = rng.uniform(0, ny, n).astype(np.float32)
+    x[::97] = -1.0                                    # out of the grid: key ntiles, sorted last
+    s.put("x", x)
+    s.put("y", y)
+    s.put("w", np.arange(n, dtype=np.float32))        # tags (exact below 2^24)
+    s.ctx.resort()
+    got = s.parts()
+    cpt = max(1, int(1024 / ppc))
+    tx = 1
+    while tx * tx < 2 * cpt:
+        tx <<= 1
+    tx = min(tx, nx)
+    ty = max(1, min(cpt // tx, ny))
+    ntx, nty = (nx + tx - 1) // tx, (ny + ty - 1) // ty
+    inside = (x >= 0) & (x < nx) & (y >= 0) & (y < ny)
+    ci = np.minimum(x.astype(np.int64), nx - 1)
+    cj = np.minimum(y.astype(np.int64), ny - 1)
+    key = np.where(inside, (cj // ty) * ntx + ci // tx, ntx * nty)
+    order = np.argsort(key, kind="stable")
+    assert np.array_equal(got["w"].astype(np.int64), order)
+    assert np.array_equal(got["x"], x[order]) and np.array_equal(got["y"], y[order])
+
+
 def test_step_profile_names_every_phase(setup, aw):
     s = setup(64, 64, 32.0, 32.0, n_particles(WEIBEL, 64, 64), aw.AW_MODEL_DARWIN, dt=0.05)
     s.ctx.load_species(WEIBEL, seed=0)
