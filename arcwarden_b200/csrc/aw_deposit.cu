@@ -64,12 +64,17 @@ constexpr int wmax_cells(int nf) {
     return (nf == 1 || nf == 2) ? 2048 : (nf == 3 ? 896 : (nf == 4 ? 1536 : 320));
 }
 constexpr int kRedInts = kThreads / 32 * (4 + 8);
+// The fused ES kernel: 5 stage planes and a 1024-cell rho window keep it at 4
+// CTAs per SM (with at most 64 registers).
+constexpr int kEsWindow = 1024, kEsPlanes = 5;
 // stage [np][kChunk] f32 | window [2*nf][wmax] i32 | red ints | slow list u16[kChunk]
 constexpr size_t win_offset(int np) { return static_cast<size_t>(np) * kChunk * 4; }
-constexpr size_t smem_bytes(int nf, int np) {
-    return win_offset(np) + static_cast<size_t>(wmax_cells(nf)) * nf * 8 + kRedInts * sizeof(int)
+constexpr size_t smem_bytes_w(int nf, int np, int wmax) {
+    return win_offset(np) + static_cast<size_t>(wmax) * nf * 8 + kRedInts * sizeof(int)
            + kChunk * sizeof(unsigned short);
 }
+constexpr size_t smem_bytes(int nf, int np) { return smem_bytes_w(nf, np, wmax_cells(nf)); }
+constexpr size_t es_smem_bytes() { return smem_bytes_w(1, kEsPlanes, kEsWindow); }
 
 struct Smem {
     float* stage;
@@ -670,7 +675,7 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
     const Parts& p = A.p; const Geo& g = A.g; const PushP& pp = A.pp;
     const float* __restrict__ gb = A.gb; const double qoa = A.qoa; unsigned long long* __restrict__ acc = A.acc;
     const int wmaxc = A.wmaxc; double* __restrict__ part = A.part; DevState* st = A.st;
-    constexpr int NF = 1, NS = 3, NIN = 6;
+    constexpr int NF = 1, NS = 3, NIN = 5;          // stage in: x y ux uy uz (w read from global)
     constexpr bool T0 = true;
     extern __shared__ __align__(16) unsigned char smem[];
     const Smem m = carve(smem, NIN, NF, wmaxc);
@@ -682,7 +687,7 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
     const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
     const float S1[1] = {st->S_next[0]};
     if (threadIdx.x == 0) nlist = 0;
-    const ChunkSrc src{{p.x, p.y, p.w, p.ux, p.uy, p.uz}};
+    const ChunkSrc src{{p.x, p.y, p.ux, p.uy, p.uz, nullptr}};
     float x0, y0;
     if (!load_chunk(m.stage, src, NIN, c0, cnt, p.vec_ok != 0, &bar, st, &x0, &y0)) return;
     int ir, jr;
@@ -697,8 +702,8 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
         const int s = it * kThreads + threadIdx.x;
         const long long i = c0 + s;
         float x = m.stage[s], y = m.stage[kChunk + s];
-        const float w = m.stage[2 * kChunk + s];
-        float ux = m.stage[3 * kChunk + s], uy = m.stage[4 * kChunk + s], uz = m.stage[5 * kChunk + s];
+        float ux = m.stage[2 * kChunk + s], uy = m.stage[3 * kChunk + s], uz = m.stage[4 * kChunk + s];
+        const float w = s < cnt ? __ldcs(p.w + i) : 0.0f;
         float xs = -1.0f, cf0 = 0.0f;
         if (s < cnt) {
             if (in_grid(x, y, g)) {
@@ -752,7 +757,7 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
         st->step += 1;
     }}
 template <bool POW2>
-__global__ void __launch_bounds__(kThreads, 3) k_push_deposit_es(EsArgs A) { push_deposit_es_chunk<POW2>(A, blockIdx.x); }
+__global__ void __launch_bounds__(kThreads, 4) k_push_deposit_es(EsArgs A) { push_deposit_es_chunk<POW2>(A, blockIdx.x); }
 
 // Fused Darwin step kernel: input x y w ux uy uz; stage = new x, y, coefficient, ux, uy, uz.
 struct EmArgs {
@@ -920,7 +925,7 @@ k_deposit_dcu_multi(const DcuArgs* __restrict__ runs, const int* __restrict__ fi
     deposit_dcu_chunk(A, chunk);
 }
 template <bool POW2>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, 4)
 k_push_deposit_es_multi(const EsArgs* __restrict__ runs, const int* __restrict__ first, int nruns) {
     __shared__ EsArgs A;
     __shared__ int chunk;
@@ -1002,7 +1007,7 @@ EsArgs es_args(const Ctx& c) {
     EsArgs a{};
     a.p = c.parts; a.g = c.geo; a.pp = push_params(c); a.gb = c.gb_es;
     a.qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
-    a.acc = c.acc_src; a.wmaxc = wmax_cells(1); a.part = c.part_p; a.st = c.st;
+    a.acc = c.acc_src; a.wmaxc = kEsWindow; a.part = c.part_p; a.st = c.st;
     return a;
 }
 EmArgs em_args(const Ctx& c) {
@@ -1079,7 +1084,7 @@ MultiPhase* multi_create(int kind, Ctx* const* runs, int nruns) {
         // the shared-memory opt-ins, before any capture
         if (kind == kMultiDcu) prep_smem(k_deposit_dcu_multi, smem_bytes(3, 6));
         else if (kind == kMultiEsPush) prep_smem(m->pow2 ? k_push_deposit_es_multi<true> : k_push_deposit_es_multi<false>,
-                                                 smem_bytes(1, 6));
+                                                 es_smem_bytes());
         else prep_smem(m->pow2 ? k_push_deposit_em_multi<true> : k_push_deposit_em_multi<false>, smem_bytes(8, 6));
     } catch (...) {
         multi_free(m.get());
@@ -1097,7 +1102,7 @@ void multi_launch(MultiPhase* m, cudaStream_t s) {
                                                                              first, m->nruns);
     } else if (m->kind == kMultiEsPush) {
         auto kern = m->pow2 ? k_push_deposit_es_multi<true> : k_push_deposit_es_multi<false>;
-        kern<<<m->nblocks, kThreads, smem_bytes(1, 6), s>>>(static_cast<const EsArgs*>(m->d_args), first, m->nruns);
+        kern<<<m->nblocks, kThreads, es_smem_bytes(), s>>>(static_cast<const EsArgs*>(m->d_args), first, m->nruns);
     } else {
         auto kern = m->pow2 ? k_push_deposit_em_multi<true> : k_push_deposit_em_multi<false>;
         kern<<<m->nblocks, kThreads, smem_bytes(8, 6), s>>>(static_cast<const EmArgs*>(m->d_args), first, m->nruns);
@@ -1122,7 +1127,7 @@ void launch_deposit_dcu(Ctx& c, const float* gb, bool fused) {
 
 void launch_push_deposit_es(Ctx& c) {
     if (c.parts.n == 0) return;
-    const size_t sh = smem_bytes(1, 6);
+    const size_t sh = es_smem_bytes();
     const bool p2 = pow2_geo(c);
     auto kern = p2 ? k_push_deposit_es<true> : k_push_deposit_es<false>;
     prep_smem(kern, sh);
