@@ -64,9 +64,13 @@ constexpr int wmax_cells(int nf) {
     return (nf == 1 || nf == 2) ? 2048 : (nf == 3 ? 896 : (nf == 4 ? 1536 : 320));
 }
 constexpr int kRedInts = kThreads / 32 * (4 + 8);
-// The fused ES kernel: 5 stage planes and a 1024-cell rho window keep it at 4
-// CTAs per SM (with at most 64 registers).
-constexpr int kEsWindow = 1024, kEsPlanes = 5;
+// The fused ES kernel stages 5 planes and takes one of two rho windows. The ES
+// path keeps the particle order, so a chunk covers kChunk / ppc consecutive
+// cells of the load order plus their drift: at 32 or more particles per cell a
+// short row segment (the 1024-cell window: 4 CTAs per SM at <= 64 registers),
+// below that whole grid rows and their spread in y (3584 cells: 14 rows of 256,
+// 3 CTAs per SM).
+constexpr int kEsPlanes = 5, kEsWindowSmall = 1024, kEsWindowLarge = 3584;
 // stage [np][kChunk] f32 | window [2*nf][wmax] i32 | red ints | slow list u16[kChunk]
 constexpr size_t win_offset(int np) { return static_cast<size_t>(np) * kChunk * 4; }
 constexpr size_t smem_bytes_w(int nf, int np, int wmax) {
@@ -74,7 +78,7 @@ constexpr size_t smem_bytes_w(int nf, int np, int wmax) {
            + kChunk * sizeof(unsigned short);
 }
 constexpr size_t smem_bytes(int nf, int np) { return smem_bytes_w(nf, np, wmax_cells(nf)); }
-constexpr size_t es_smem_bytes() { return smem_bytes_w(1, kEsPlanes, kEsWindow); }
+constexpr size_t es_smem_bytes(int wmax) { return smem_bytes_w(1, kEsPlanes, wmax); }
 
 struct Smem {
     float* stage;
@@ -1003,11 +1007,14 @@ DcuArgs dcu_args(const Ctx& c, const float* gb, bool fused) {
     a.use_rms = fused ? 1 : 0; a.psq = fused ? c.part_d : nullptr;
     return a;
 }
+int es_window(const Ctx& c) {
+    return c.parts.n >= 32LL * c.geo.ncell ? kEsWindowSmall : kEsWindowLarge;
+}
 EsArgs es_args(const Ctx& c) {
     EsArgs a{};
     a.p = c.parts; a.g = c.geo; a.pp = push_params(c); a.gb = c.gb_es;
     a.qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
-    a.acc = c.acc_src; a.wmaxc = kEsWindow; a.part = c.part_p; a.st = c.st;
+    a.acc = c.acc_src; a.wmaxc = es_window(c); a.part = c.part_p; a.st = c.st;
     return a;
 }
 EmArgs em_args(const Ctx& c) {
@@ -1048,6 +1055,7 @@ void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE
 // ---- multi-run particle phases -----------------------------------------------
 struct MultiPhase {
     int kind = 0, nruns = 0, nblocks = 0;
+    size_t smem = 0;
     bool pow2 = true;
     void* d_args = nullptr;
     int* d_first = nullptr;
@@ -1070,8 +1078,13 @@ MultiPhase* multi_create(int kind, Ctx* const* runs, int nruns) {
     auto put = [&](const void* a, size_t sz) {
         host.insert(host.end(), static_cast<const unsigned char*>(a), static_cast<const unsigned char*>(a) + sz);
     };
+    m->smem = kind == kMultiDcu ? smem_bytes(3, 6) : kind == kMultiEmPush ? smem_bytes(8, 6) : 0;
     for (int r = 0; r < nruns; ++r) {
-        if (kind == kMultiEsPush) { const EsArgs a = es_args(*runs[r]); put(&a, sizeof a); }
+        if (kind == kMultiEsPush) {
+            const EsArgs a = es_args(*runs[r]);
+            put(&a, sizeof a);
+            m->smem = std::max(m->smem, es_smem_bytes(a.wmaxc));
+        }
         else if (kind == kMultiDcu) { const DcuArgs a = dcu_args(*runs[r], runs[r]->gb_dcu, true); put(&a, sizeof a); }
         else { const EmArgs a = em_args(*runs[r]); put(&a, sizeof a); }
     }
@@ -1082,10 +1095,10 @@ MultiPhase* multi_create(int kind, Ctx* const* runs, int nruns) {
         AW_CUDA(cudaMemcpy(m->d_args, host.data(), bytes, cudaMemcpyHostToDevice));
         AW_CUDA(cudaMemcpy(m->d_first, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
         // the shared-memory opt-ins, before any capture
-        if (kind == kMultiDcu) prep_smem(k_deposit_dcu_multi, smem_bytes(3, 6));
+        if (kind == kMultiDcu) prep_smem(k_deposit_dcu_multi, m->smem);
         else if (kind == kMultiEsPush) prep_smem(m->pow2 ? k_push_deposit_es_multi<true> : k_push_deposit_es_multi<false>,
-                                                 es_smem_bytes());
-        else prep_smem(m->pow2 ? k_push_deposit_em_multi<true> : k_push_deposit_em_multi<false>, smem_bytes(8, 6));
+                                                 m->smem);
+        else prep_smem(m->pow2 ? k_push_deposit_em_multi<true> : k_push_deposit_em_multi<false>, m->smem);
     } catch (...) {
         multi_free(m.get());
         m.release();
@@ -1098,14 +1111,14 @@ void multi_launch(MultiPhase* m, cudaStream_t s) {
     if (m->nblocks == 0) return;
     const auto* first = m->d_first;
     if (m->kind == kMultiDcu) {
-        k_deposit_dcu_multi<<<m->nblocks, kThreads, smem_bytes(3, 6), s>>>(static_cast<const DcuArgs*>(m->d_args),
-                                                                             first, m->nruns);
+        k_deposit_dcu_multi<<<m->nblocks, kThreads, m->smem, s>>>(static_cast<const DcuArgs*>(m->d_args), first,
+                                                                    m->nruns);
     } else if (m->kind == kMultiEsPush) {
         auto kern = m->pow2 ? k_push_deposit_es_multi<true> : k_push_deposit_es_multi<false>;
-        kern<<<m->nblocks, kThreads, es_smem_bytes(), s>>>(static_cast<const EsArgs*>(m->d_args), first, m->nruns);
+        kern<<<m->nblocks, kThreads, m->smem, s>>>(static_cast<const EsArgs*>(m->d_args), first, m->nruns);
     } else {
         auto kern = m->pow2 ? k_push_deposit_em_multi<true> : k_push_deposit_em_multi<false>;
-        kern<<<m->nblocks, kThreads, smem_bytes(8, 6), s>>>(static_cast<const EmArgs*>(m->d_args), first, m->nruns);
+        kern<<<m->nblocks, kThreads, m->smem, s>>>(static_cast<const EmArgs*>(m->d_args), first, m->nruns);
     }
     AW_LAUNCH();
 }
@@ -1127,7 +1140,7 @@ void launch_deposit_dcu(Ctx& c, const float* gb, bool fused) {
 
 void launch_push_deposit_es(Ctx& c) {
     if (c.parts.n == 0) return;
-    const size_t sh = es_smem_bytes();
+    const size_t sh = es_smem_bytes(es_window(c));
     const bool p2 = pow2_geo(c);
     auto kern = p2 ? k_push_deposit_es<true> : k_push_deposit_es<false>;
     prep_smem(kern, sh);
