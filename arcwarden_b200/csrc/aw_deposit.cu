@@ -240,11 +240,11 @@ __device__ __forceinline__ void close_window(const Smem& m, const Win& wn, int n
                                              unsigned long long* __restrict__ acc, const Geo& g, DevState* st,
                                              CoefFn coef) {
     __syncthreads();
-    win_flush<NF, T0>(m.win, wn, acc, g);
+    if (wn.nb == 1) win_flush<NF, T0>(m.win, wn, acc, g);
     slow_pass<NF, NS>(m.stage, m.slow, nlist, !wn.use, acc, g, st, coef);
     if (threadIdx.x == 0) {
         atomicAdd(&st->chunks, 1ull);
-        if (!wn.use) atomicAdd(&st->overflow, 1ull);
+        if (!wn.use || wn.nb > 1) atomicAdd(&st->overflow, 1ull);
     }
 }
 
@@ -319,7 +319,7 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
 #pragma unroll
         for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cf[f], S[f]);
     };
-    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
+    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef, acc);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
     if (psq) block_sumsq<NF>(sq, nval, psq, ssq, blockIdx.x);
 }
@@ -545,7 +545,7 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
     }
     const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) { cs[0] = a[2]; cs[1] = a[3]; cs[2] = a[4]; };
-    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
+    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef, acc);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
     if (psq) block_sumsq<NF>(sq, nval, psq, ssq, chunk);}
 __global__ void __launch_bounds__(kThreads, 3) k_deposit_dcu(DcuArgs A) { deposit_dcu_chunk(A, blockIdx.x); }
@@ -644,7 +644,7 @@ k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ trajE, AdjDev* a
     }
     const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
     auto coef = [&](const float (&q)[NS], float (&c2)[NF]) { c2[0] = q[2]; c2[1] = q[3]; };
-    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
+    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef, acc);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
 }
 
@@ -753,7 +753,7 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
         cs[0] = __fmul_rn(a[2], S1[0]);
     };
-    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
+    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef, acc);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
     block_sum4(ke, px, py, pz, part, dsh, chunk);
     if (threadIdx.x == 0 && chunk == 0) {
@@ -894,7 +894,7 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
 #pragma unroll
         for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cf[f], S[f]);
     };
-    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef);
+    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef, acc);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
     block_sumsq<NF>(sq, nval, psq, ssq, chunk);
     block_sum4(ke, px, py, pz, part, dsh, chunk);

@@ -241,12 +241,18 @@ struct Parts {
 // for the +1 CIC corner. Window cell (di, dj) maps back to grid cell
 // (wrap(ir + mi + di), wrap(jr + mj + dj)), so correctness never depends on the
 // reference cell; only the window size does.
+// A chunk's box of W x H cells is deposited in nb bands of Hb rows (nb = 1
+// when the whole box fits the shared capacity): each band is zeroed, takes the
+// corners of every particle that fall in its rows, and is flushed before the
+// next. A box that would need more than kMaxBands bands takes the slow path.
+constexpr int kMaxBands = 8;
 struct Win {
     int ir, jr;      // reference cell
     int mi, mj;      // min wrapped offsets
     int W, H;        // extent in cells (incl. the +1 corner)
-    int WH;
-    bool use;        // fits the shared window capacity
+    int Hb, nb;      // rows per band, bands
+    int WH;          // W * Hb: the words of one plane
+    bool use;        // deposited in the shared window (in one or more bands)
     bool track_all;  // some field's chunk sums may leave int32: track every field
 };
 
@@ -303,8 +309,15 @@ __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, 
     w.mi = lo_i; w.mj = lo_j;
     w.W = hi_i - lo_i + 2;
     w.H = hi_j - lo_j + 2;
-    w.use = static_cast<long long>(w.W) * w.H <= wmaxc;
-    w.WH = w.use ? w.W * w.H : 0;
+    if (static_cast<long long>(w.W) * w.H <= wmaxc) {
+        w.Hb = w.H;
+        w.nb = 1;
+    } else {
+        w.Hb = wmaxc / w.W;
+        w.nb = w.Hb > 0 ? (w.H + w.Hb - 1) / w.Hb : kMaxBands + 1;
+    }
+    w.use = w.nb <= kMaxBands;
+    w.WH = w.use ? w.W * w.Hb : 0;
     w.track_all = track_all;
 }
 
@@ -330,25 +343,25 @@ __device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
     for (int i = threadIdx.x; i < m; i += kThreads) s[i] = 0;
 }
 
-// Flush the window into the global int64 accumulators acc[f*ncell + cell].
-// The caller syncs before calling.
+// Flush band `band` of the window into the global int64 accumulators
+// acc[f*ncell + cell]. The caller syncs before calling.
 template <int NF, bool T0>
 __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& w,
-                                          unsigned long long* __restrict__ acc, const Geo& g) {
+                                          unsigned long long* __restrict__ acc, const Geo& g, int band = 0) {
     if (!w.use) return;            // the window was not used (its words are not zeroed)
     // every thread takes (field, cell) items t, t + 256, ...: all warps work even
     // when the window is one or two rows. The item -> (field, row, column) splits
     // use float reciprocals: (t + 0.5) / n is at least 0.5 / n away from an
     // integer, far more than the float error for t < 2^14. Window offsets are
     // < nx, so one conditional add/subtract wraps them.
-    const int WH = w.WH, total = NF * WH;
-    const float inv_wh = 1.0f / static_cast<float>(WH), inv_w = 1.0f / static_cast<float>(w.W);
+    const int WH = w.WH, r0 = band * w.Hb, cells = w.W * min(w.Hb, w.H - r0), total = NF * cells;
+    const float inv_c = 1.0f / static_cast<float>(cells), inv_w = 1.0f / static_cast<float>(w.W);
     for (int t = threadIdx.x; t < total; t += kThreads) {
-        const int f = static_cast<int>((static_cast<float>(t) + 0.5f) * inv_wh);
-        const int c = t - f * WH;
+        const int f = static_cast<int>((static_cast<float>(t) + 0.5f) * inv_c);
+        const int c = t - f * cells;
         const int wj = static_cast<int>((static_cast<float>(c) + 0.5f) * inv_w);
         const int wi = c - wj * w.W;
-        int gj = w.jr + w.mj + wj;
+        int gj = w.jr + w.mj + r0 + wj;
         if (gj < 0) gj += g.ny;
         if (gj >= g.ny) gj -= g.ny;
         int gi = w.ir + w.mi + wi;
@@ -587,12 +600,70 @@ __device__ __forceinline__ void window_particles(const float* __restrict__ stage
     }
 }
 
+// Banded window pass over rows [r0, r0 + Hb) of the box: a particle adds the
+// corners of its two rows that fall in the band (same contributions, same
+// integer sums per cell as one window).
+template <int NF, int NS, bool T0, bool TRACK_ALL, class CoefFn>
+__device__ __forceinline__ void window_band(const float* __restrict__ stage, int* __restrict__ win,
+                                            const Win& wn, int r0, const Geo& g, CoefFn coef) {
+    const int base = 64 * (threadIdx.x & 31) + 8 * (threadIdx.x >> 5);
+#pragma unroll 1
+    for (int k = 0; k < kPPT; ++k) {
+        const int d = stage_slot(base + k);
+        const float x = stage[d];
+        if (__float_as_int(x) < 0) continue;
+        const float y = stage[kChunk + d];
+        const int rj = win_off(static_cast<int>(y), wn.jr, g.ny) - wn.mj - r0;
+        if (rj < -1 || rj >= wn.Hb) continue;        // both rows outside the band
+        float a[NS];
+        a[0] = x; a[1] = y;
+#pragma unroll
+        for (int f = 2; f < NS; ++f) a[f] = stage[f * kChunk + d];
+        const Cic c = cic(a[0], a[1]);
+        float cs[NF];
+        coef(a, cs);
+        const float wv[4] = {c.w0, c.w1, c.w2, c.w3};
+        const int ci = win_off(c.i0, wn.ir, g.nx) - wn.mi;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int row = rj + (q >> 1);                // corners 0, 1 in row rj; 2, 3 in rj + 1
+            if (row < 0 || row >= wn.Hb) continue;
+            const int cw = row * wn.W + ci + (q & 1);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const int v = quant(cs[f], wv[q]);
+                int* t = win + 2 * f * wn.WH + cw;
+                if (TRACK_ALL || (T0 && f == 0)) add_tracked(t, wn.WH, v);
+                else atomicAdd(t, v);
+            }
+        }
+    }
+}
+
+// The window pass. With one band the caller flushes (close_window); with
+// several, each band is flushed here, and the window is zeroed for the next.
 template <int NF, int NS, bool T0, class CoefFn>
 __device__ __forceinline__ void window_pass(const float* __restrict__ stage, int* __restrict__ win,
-                                            const Win& wn, const Geo& g, CoefFn coef) {
+                                            const Win& wn, const Geo& g, CoefFn coef,
+                                            unsigned long long* __restrict__ acc) {
     if (!wn.use) return;
-    if (wn.track_all) window_particles<NF, NS, T0, true>(stage, win, wn, g, coef);
-    else window_particles<NF, NS, T0, false>(stage, win, wn, g, coef);
+    if (wn.nb == 1) {
+        if (wn.track_all) window_particles<NF, NS, T0, true>(stage, win, wn, g, coef);
+        else window_particles<NF, NS, T0, false>(stage, win, wn, g, coef);
+        return;
+    }
+#pragma unroll 1
+    for (int b = 0; b < wn.nb; ++b) {
+        if (b > 0) {
+            win_zero<NF>(win, wn);
+            __syncthreads();
+        }
+        if (wn.track_all) window_band<NF, NS, T0, true>(stage, win, wn, b * wn.Hb, g, coef);
+        else window_band<NF, NS, T0, false>(stage, win, wn, b * wn.Hb, g, coef);
+        __syncthreads();
+        win_flush<NF, T0>(win, wn, acc, g, b);
+        __syncthreads();
+    }
 }
 
 }  // namespace aw

@@ -439,7 +439,35 @@ def test_deposit_bit_exact_when_windows_overflow(setup, aw, oracle, op, fset, ke
     getattr(s.ctx, op)()
     p = s.parts()
     st = s.ctx.stats()
-    assert st["window_overflow"] > 0
+    assert st["window_overflow"] > 0 and st["slow_deposits"] > 0
+    g = oracle.geo(nx, ny, 256.0, 256.0)
+    S, _, _ = _oracle_scales(oracle, p, -1.0)
+    fin = oracle.finalize(oracle.deposit(g, *(p[k] for k in PARTICLE_KEYS[:5]), p["w"], -1.0, S, fset), S)
+    for i, k in enumerate(keys):
+        assert np.array_equal(s.grid(k), fin[i]), k
+
+
+@pytest.mark.parametrize("op,fset,keys", [("deposit_rho", 0, ["rho"]), ("deposit_rho_j", 1, ["rho", "Jx", "Jy", "Jz"])])
+@pytest.mark.parametrize("rows", [8, 20])
+def test_deposit_bit_exact_in_window_bands(setup, aw, oracle, op, fset, keys, rows):
+    """Each chunk of 2048 particles spreads over the full grid width and `rows`
+    rows: its box exceeds the shared window, which then takes the box in bands
+    of rows (2 to 5 bands here), with no particle on the slow path; the result
+    is still the same bits."""
+    nx = ny = 256
+    nchunk = 16
+    n = 2048 * nchunk
+    s = setup(nx, ny, 256.0, 256.0, n, aw.AW_MODEL_DARWIN, dt=0.05)
+    rng = np.random.default_rng(9)
+    row0 = np.repeat((np.arange(nchunk) * 37) % ny, 2048)
+    vals = {"x": rng.random(n) * nx, "y": (row0 + rng.random(n) * rows) % ny, "ux": rng.normal(0, 0.1, n),
+            "uy": rng.normal(0, 0.1, n), "uz": rng.normal(0, 0.2, n), "w": np.full(n, 0.25)}
+    for k, v in vals.items():
+        s.put(k, v.astype(np.float32))
+    getattr(s.ctx, op)()
+    p = s.parts()
+    st = s.ctx.stats()
+    assert st["window_overflow"] > 0 and st["slow_deposits"] == 0, st
     g = oracle.geo(nx, ny, 256.0, 256.0)
     S, _, _ = _oracle_scales(oracle, p, -1.0)
     fin = oracle.finalize(oracle.deposit(g, *(p[k] for k in PARTICLE_KEYS[:5]), p["w"], -1.0, S, fset), S)
