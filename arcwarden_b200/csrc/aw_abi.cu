@@ -278,53 +278,70 @@ double grad_es_impl(Ctx& c, long long nsteps, int every, float* dux, float* duy,
     if (!c.gexec) c.gexec = capture_exec(c, [&] { step_body(c); });
     const AdjK kf = adj_constants(c, 1.0f);
     AdjP a{w.traj_xy, w.lam, w.lam + n, w.lam + 2 * n, w.lam + 3 * n, w.lam + 4 * n, n, (n % 4 == 0) ? 1 : 0};
+    // The recording step: the ES step whose kernels also write x_n, y_n and E_n
+    // into the trajectory slot they advance; with the end-of-step reduction for
+    // the forward run's last segment, without it (diagnostics only) for the
+    // recompute.
+    struct Recording {
+        Ctx& c;
+        Recording(Ctx& cc, AdjWS& ws) : c(cc) { c.rec_ad = ws.ad; c.rec_xy = ws.traj_xy; c.rec_E = ws.traj_E; }
+        ~Recording() { c.rec_ad = nullptr; c.rec_xy = nullptr; c.rec_E = nullptr; }
+    };
     if (!w.g_rec)
         w.g_rec = capture_exec(c, [&] {
-            launch_traj_store_xy(c);
+            Recording r(c, w);
+            es_fields_from_pending(c, true, NoMark{});
+            launch_push_deposit_es(c);
+        });
+    if (!w.g_frec)
+        w.g_frec = capture_exec(c, [&] {
+            Recording r(c, w);
             step_body(c);
-            launch_traj_store_E(c);
-            launch_slot_add(c, 1);
         });
     if (!w.g_bwd)
         w.g_bwd = capture_exec(c, [&] {
-            launch_slot_add(c, -1);
             launch_adj_scatter(c, a, kf, w.traj_E, w.ad, w.acc);
             launch_adj_finalize(c);
             adj_transpose_solve(c);
             launch_adj_gather(c, a, kf);
         });
 
+    // Forward run: checkpoints at the starts of all segments but the last, whose
+    // trajectory the run records itself (slot -1 -> its last step).
+    const int klast = w.nck - 1;
+    const long long slast = static_cast<long long>(klast) * every;
+    AdjDev ad0{};
+    ad0.slot = -1;
+    ad0.ext_scale = static_cast<float>(c.prm.eps0 * c.geo.dx * c.geo.dy);   // dL/dE = eps0 E dx dy
     for (long long s = 0; s < nsteps; ++s) {
-        if (s % every == 0) {
+        if (s % every == 0 && s < slast) {
             const int k = static_cast<int>(s / every);
             copy_parts_to(c, w.ck_parts + static_cast<size_t>(k) * 5 * n);
             AW_CUDA(cudaMemcpyAsync(w.ck_acc + k * nc, c.acc_src, sizeof(unsigned long long) * nc,
                                     cudaMemcpyDeviceToDevice, c.stream));
             AW_CUDA(cudaMemcpyAsync(w.ck_st + k, c.st, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
         }
-        AW_CUDA(cudaGraphLaunch(c.gexec, c.stream));
+        if (s == slast) AW_CUDA(cudaMemcpyAsync(w.ad, &ad0, sizeof(AdjDev), cudaMemcpyHostToDevice, c.stream));
+        AW_CUDA(cudaGraphLaunch(s < slast ? c.gexec : w.g_frec, c.stream));
     }
     aw_diag d{};
     AW_CUDA(cudaMemcpyAsync(&d, c.diag, sizeof(aw_diag), cudaMemcpyDeviceToHost, c.stream));
     AW_CUDA(cudaStreamSynchronize(c.stream));
     const double loss = d.ee;
 
+    // Backward sweep: every backward step leaves the slot one step earlier, so a
+    // segment ends at slot -1, where the recompute of the one before starts.
     AW_CUDA(cudaMemsetAsync(w.lam, 0, sizeof(float) * 5 * static_cast<size_t>(n), c.stream));
-    AdjDev ad0{};
-    ad0.ext_scale = static_cast<float>(c.prm.eps0 * c.geo.dx * c.geo.dy);   // dL/dE = eps0 E dx dy
-    for (int k = w.nck - 1; k >= 0; --k) {
+    for (int k = klast; k >= 0; --k) {
         const long long s0 = static_cast<long long>(k) * every;
         const long long s1 = std::min(nsteps, s0 + every);
-        copy_parts_from(c, w.ck_parts + static_cast<size_t>(k) * 5 * n);
-        AW_CUDA(cudaMemcpyAsync(c.acc_src, w.ck_acc + k * nc, sizeof(unsigned long long) * nc,
-                                cudaMemcpyDeviceToDevice, c.stream));
-        AW_CUDA(cudaMemcpyAsync(c.st, w.ck_st + k, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
-        if (k == w.nck - 1) {
-            AW_CUDA(cudaMemcpyAsync(w.ad, &ad0, sizeof(AdjDev), cudaMemcpyHostToDevice, c.stream));
-        } else {
-            AW_CUDA(cudaMemsetAsync(&w.ad->slot, 0, sizeof(int), c.stream));
+        if (k < klast) {
+            copy_parts_from(c, w.ck_parts + static_cast<size_t>(k) * 5 * n);
+            AW_CUDA(cudaMemcpyAsync(c.acc_src, w.ck_acc + k * nc, sizeof(unsigned long long) * nc,
+                                    cudaMemcpyDeviceToDevice, c.stream));
+            AW_CUDA(cudaMemcpyAsync(c.st, w.ck_st + k, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
+            for (long long s = s0; s < s1; ++s) AW_CUDA(cudaGraphLaunch(w.g_rec, c.stream));
         }
-        for (long long s = s0; s < s1; ++s) AW_CUDA(cudaGraphLaunch(w.g_rec, c.stream));
         for (long long s = s1 - 1; s >= s0; --s) AW_CUDA(cudaGraphLaunch(w.g_bwd, c.stream));
     }
     launch_adj_out(c, dux, duy, duz);

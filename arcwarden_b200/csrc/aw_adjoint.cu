@@ -48,29 +48,14 @@ __global__ void k_adj_finalize(unsigned long long* __restrict__ acc, const AdjDe
     }
 }
 
-// Trajectory stores of the recompute (slot from the device).
-__global__ void k_traj_store_xy(const float* __restrict__ x, const float* __restrict__ y, long long n,
-                                float* __restrict__ traj, const AdjDev* ad) {
-    float* d = traj + static_cast<size_t>(ad->slot) * 2 * n;
-    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<long long>(gridDim.x) * blockDim.x) {
-        d[i] = x[i];
-        d[n + i] = y[i];
-    }
-}
-__global__ void k_traj_store_E(const float2* __restrict__ gb, int ncell, float2* __restrict__ trajE,
-                               const AdjDev* ad) {
-    float2* d = trajE + static_cast<size_t>(ad->slot) * ncell;
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) d[c] = gb[c];
-}
-__global__ void k_slot_add(AdjDev* ad, int delta) { ad->slot += delta; }
-
 // lrho_k = sum_d conj(K_d) lE_d,k with K_d = -i k_d / (eps0 k^2) (times 1/N for
 // the unnormalised C2R), zero at k = 0 and on the Nyquist lines like the
-// forward solve (es_k in aw_spectral.cu).
+// forward solve (es_k in aw_spectral.cu). Between the scatter (which read the
+// bound max |lu3|) and the gather (which takes it anew) it resets that bound.
 __global__ void k_adj_kspace(const cufftComplex* __restrict__ lEk, cufftComplex* __restrict__ lrk, SpecGeo g,
-                             double eps0) {
+                             double eps0, AdjDev* ad) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) ad->lmax_bits = 0u;
     if (t >= g.nk) return;
     const int i = t % g.nkx, j = t / g.nkx;
     const double kx = i * g.dkx;
@@ -90,7 +75,8 @@ __global__ void k_adj_kspace(const cufftComplex* __restrict__ lEk, cufftComplex*
     lrk[t] = r;
 }
 
-// Backward step B, one particle per thread.
+// Backward step B, one particle per thread. The last block to finish moves the
+// trajectory slot to the previous step (every block has read it by then).
 __global__ void __launch_bounds__(kT)
 k_adj_gather(AdjP a, const float* __restrict__ w, Geo g, double qoa, const float* __restrict__ lrho, AdjK k,
              AdjDev* ad) {
@@ -99,10 +85,12 @@ k_adj_gather(AdjP a, const float* __restrict__ w, Geo g, double qoa, const float
     const float* __restrict__ xn = a.traj + static_cast<size_t>(ad->slot) * 2 * a.n;
     float m = 0.0f;
     if (i < a.n) {
+        // every load of the particle first, so that they are in flight together
         const float x = xn[i], y = xn[a.n + i];
         float lx = a.lx[i], ly = a.ly[i];
+        const float lux = a.lux[i], luy = a.luy[i], luz = a.luz[i], wi = w[i];
         if (x >= 0.0f && x < g.nxf && y >= 0.0f && y < g.nyf) {
-            const float q = __double2float_rn(qoa * static_cast<double>(w[i]));
+            const float q = __double2float_rn(qoa * static_cast<double>(wi));
             const Cic c = cic(x, y);
             const float fx = __fsub_rn(x, static_cast<float>(c.i0)), fy = __fsub_rn(y, static_cast<float>(c.j0));
             const float gx = __fsub_rn(1.0f, fx), gy = __fsub_rn(1.0f, fy);
@@ -117,9 +105,9 @@ k_adj_gather(AdjP a, const float* __restrict__ w, Geo g, double qoa, const float
             a.lx[i] = lx;
             a.ly[i] = ly;
         }
-        const float u3x = __fmaf_rn(k.dtx, lx, a.lux[i]);
-        const float u3y = __fmaf_rn(k.dty, ly, a.luy[i]);
-        const float u3z = a.luz[i];
+        const float u3x = __fmaf_rn(k.dtx, lx, lux);
+        const float u3y = __fmaf_rn(k.dty, ly, luy);
+        const float u3z = luz;
         m = sqrtf(__fmaf_rn(u3x, u3x, __fmaf_rn(u3y, u3y, __fmul_rn(u3z, u3z))));
         if (!(m < 3.0e38f)) m = 0.0f;   // a non-finite cotangent is caught by the scatter's slow path
     }
@@ -131,6 +119,11 @@ k_adj_gather(AdjP a, const float* __restrict__ w, Geo g, double qoa, const float
         for (int k2 = 0; k2 < kT / 32; ++k2) mx = max(mx, smax[k2]);
         atomicMax(&ad->lmax_bits, mx);
         if (blockIdx.x == 0) ad->ext_scale = 0.0f;   // the loss term belongs to the last step only
+        __threadfence();
+        if (atomicAdd(&ad->ticket, 1u) == gridDim.x - 1) {
+            ad->ticket = 0u;
+            ad->slot -= 1;
+        }
     }
 }
 
@@ -186,8 +179,9 @@ void adj_drop_graphs(Ctx& c) {
     AdjWS* w = c.adj;
     if (!w) return;
     if (w->g_rec) cudaGraphExecDestroy(w->g_rec);
+    if (w->g_frec) cudaGraphExecDestroy(w->g_frec);
     if (w->g_bwd) cudaGraphExecDestroy(w->g_bwd);
-    w->g_rec = w->g_bwd = nullptr;
+    w->g_rec = w->g_frec = w->g_bwd = nullptr;
 }
 
 void free_adjoint(Ctx& c) {
@@ -246,29 +240,11 @@ void launch_adj_finalize(Ctx& c) {
     AW_LAUNCH();
 }
 
-void launch_traj_store_xy(Ctx& c) {
-    AdjWS& w = *c.adj;
-    const int blocks = static_cast<int>(std::min<long long>(blocks_n(w.n), 148 * 8));
-    k_traj_store_xy<<<blocks, kT, 0, c.stream>>>(c.parts.x, c.parts.y, w.n, w.traj_xy, w.ad);
-    AW_LAUNCH();
-}
-void launch_traj_store_E(Ctx& c) {
-    AdjWS& w = *c.adj;
-    const int blocks = std::min(blocks_n(c.geo.ncell), 148 * 8);
-    k_traj_store_E<<<blocks, kT, 0, c.stream>>>(reinterpret_cast<const float2*>(c.gb_es), c.geo.ncell,
-                                                reinterpret_cast<float2*>(w.traj_E), w.ad);
-    AW_LAUNCH();
-}
-void launch_slot_add(Ctx& c, int delta) {
-    k_slot_add<<<1, 1, 0, c.stream>>>(c.adj->ad, delta);
-    AW_LAUNCH();
-}
-
 void adj_transpose_solve(Ctx& c) {
     AdjWS& w = *c.adj;
     AW_CUFFT(cufftSetStream(w.p_r2c2, c.stream));
     AW_CUFFT(cufftExecR2C(w.p_r2c2, w.lE, w.lEk));
-    k_adj_kspace<<<blocks_n(c.sg.nk), kT, 0, c.stream>>>(w.lEk, w.lrk, c.sg, c.prm.eps0);
+    k_adj_kspace<<<blocks_n(c.sg.nk), kT, 0, c.stream>>>(w.lEk, w.lrk, c.sg, c.prm.eps0, w.ad);
     AW_LAUNCH();
     AW_CUFFT(cufftExecC2R(c.p_c2r1, w.lrk, w.lrho));
 }
@@ -276,7 +252,6 @@ void adj_transpose_solve(Ctx& c) {
 void launch_adj_gather(Ctx& c, const AdjP& a, const AdjK& k) {
     AdjWS& w = *c.adj;
     if (a.n == 0) return;
-    AW_CUDA(cudaMemsetAsync(&w.ad->lmax_bits, 0, sizeof(unsigned), c.stream));
     const double qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
     k_adj_gather<<<blocks_n(a.n), kT, 0, c.stream>>>(a, c.parts.w, c.geo, qoa, w.lrho, k, w.ad);
     AW_LAUNCH();

@@ -563,11 +563,16 @@ __global__ void __launch_bounds__(kThreads, 3) k_deposit_dcu(DcuArgs A) { deposi
 // of the gather) on this window engine, 2 fields, exact fixed point. The
 // scales come from the bound max|lu3| of the previous backward step:
 // |lE_d| <= 2 |qmh| |lu3| (R is a rotation); particles beyond it take the slow
-// path. Stage = x, y, lEx*S0, lEy*S1.
+// path. Stage = x, y, lEx*S0, lEy*S1. The chunk's cotangents are bulk-copied
+// in with its positions: lx, ly into stage planes 2, 3 (read, then rewritten
+// in place like x, y), lux, luy, luz into planes 4-6, which lie in the window
+// area, idle until the window opens after pass 1.
+constexpr int kAdjWindow = wmax_cells(2);
+static_assert(3 * kChunk * 4 <= kAdjWindow * 2 * 8, "the cotangent planes must fit the window area");
 __global__ void __launch_bounds__(kThreads, 3)
 k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ trajE, AdjDev* ad,
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st) {
-    constexpr int NF = 2, NS = 4, NIN = 2;
+    constexpr int NF = 2, NS = 4, NIN = 7;
     constexpr bool T0 = false;
     extern __shared__ __align__(16) unsigned char smem[];
     const Smem m = carve(smem, NS, NF, wmaxc);
@@ -584,7 +589,7 @@ k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ trajE, AdjDev* a
     const float S[NF] = {sc, sc};
     if (blockIdx.x == 0 && threadIdx.x == 0) { ad->S[0] = sc; ad->S[1] = sc; }
     if (threadIdx.x == 0) nlist = 0;
-    const ChunkSrc src{{xn, xn + a.n, nullptr, nullptr, nullptr, nullptr}};
+    const ChunkSrc src{{xn, xn + a.n, a.lx, a.ly, a.lux, a.luy, a.luz}};
     float x0, y0;
     if (!load_chunk(m.stage, src, NIN, c0, cnt, a.vec_ok != 0, &bar, st, &x0, &y0)) return;
     int ir, jr;
@@ -598,11 +603,11 @@ k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ trajE, AdjDev* a
         const long long i = c0 + s;
         const float x = m.stage[s], y = m.stage[kChunk + s];
         float xs = -1.0f, cs[NF] = {0.f, 0.f};
+        float lx = m.stage[2 * kChunk + s], ly = m.stage[3 * kChunk + s];
         if (s < cnt && in_grid(x, y, g)) {
-            float lx = a.lx[i], ly = a.ly[i];
-            const float u3x = __fmaf_rn(k.dtx, lx, a.lux[i]);
-            const float u3y = __fmaf_rn(k.dty, ly, a.luy[i]);
-            const float u3z = a.luz[i];
+            const float u3x = __fmaf_rn(k.dtx, lx, m.stage[4 * kChunk + s]);
+            const float u3y = __fmaf_rn(k.dty, ly, m.stage[5 * kChunk + s]);
+            const float u3z = m.stage[6 * kChunk + s];
             float u1x = u3x, u1y = u3y, u1z = u3z;
             if (k.rot) {   // R^T l = l - l x s + (l x s) x t
                 const float cx = __fmaf_rn(u3y, k.sz, -__fmul_rn(u3z, k.sy));
@@ -673,8 +678,9 @@ __device__ __forceinline__ void move_xy(float& x, float& y, float ux, float uy, 
 struct EsArgs {
     Parts p; Geo g; PushP pp; const float* gb; double qoa; unsigned long long* acc; int wmaxc;
     double* part; DevState* st;
+    float* traj; const AdjDev* rec;   // trajectory recording (x_n, y_n into slot rec->slot), or null
 };
-template <bool POW2>
+template <bool POW2, bool RECORD = false>
 __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int chunk) {
     const Parts& p = A.p; const Geo& g = A.g; const PushP& pp = A.pp;
     const float* __restrict__ gb = A.gb; const double qoa = A.qoa; unsigned long long* __restrict__ acc = A.acc;
@@ -697,6 +703,7 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
     int ir, jr;
     ref_of(x0, y0, g, ir, jr);
     const float2* q = reinterpret_cast<const float2*>(gb);
+    float* __restrict__ tr = RECORD ? A.traj + static_cast<size_t>(A.rec->slot) * 2 * p.n : nullptr;
 
     BBox bb;
     float l1[NF] = {};
@@ -708,6 +715,7 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
         float x = m.stage[s], y = m.stage[kChunk + s];
         float ux = m.stage[2 * kChunk + s], uy = m.stage[3 * kChunk + s], uz = m.stage[4 * kChunk + s];
         const float w = s < cnt ? __ldcs(p.w + i) : 0.0f;
+        if (RECORD && s < cnt) { tr[i] = x; tr[p.n + i] = y; }
         float xs = -1.0f, cf0 = 0.0f;
         if (s < cnt) {
             if (in_grid(x, y, g)) {
@@ -760,8 +768,10 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
         st->S_pend[0] = S1[0];
         st->step += 1;
     }}
-template <bool POW2>
-__global__ void __launch_bounds__(kThreads, 4) k_push_deposit_es(EsArgs A) { push_deposit_es_chunk<POW2>(A, blockIdx.x); }
+template <bool POW2, bool RECORD>
+__global__ void __launch_bounds__(kThreads, 4) k_push_deposit_es(EsArgs A) {
+    push_deposit_es_chunk<POW2, RECORD>(A, blockIdx.x);
+}
 
 // Fused Darwin step kernel: input x y w ux uy uz; stage = new x, y, coefficient, ux, uy, uz.
 struct EmArgs {
@@ -1015,6 +1025,7 @@ EsArgs es_args(const Ctx& c) {
     a.p = c.parts; a.g = c.geo; a.pp = push_params(c); a.gb = c.gb_es;
     a.qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
     a.acc = c.acc_src; a.wmaxc = es_window(c); a.part = c.part_p; a.st = c.st;
+    a.traj = c.rec_xy; a.rec = c.rec_ad;
     return a;
 }
 EmArgs em_args(const Ctx& c) {
@@ -1048,7 +1059,7 @@ void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE
     const size_t sh = smem_bytes(2, 4);
     prep_smem(k_adj_scatter, sh);
     k_adj_scatter<<<nchunks(a.n), kThreads, sh, c.stream>>>(a, c.geo, k, reinterpret_cast<const float2*>(trajE),
-                                                             ad, acc, wmax_cells(2), c.st);
+                                                             ad, acc, kAdjWindow, c.st);
     AW_LAUNCH();
 }
 
@@ -1142,7 +1153,9 @@ void launch_push_deposit_es(Ctx& c) {
     if (c.parts.n == 0) return;
     const size_t sh = es_smem_bytes(es_window(c));
     const bool p2 = pow2_geo(c);
-    auto kern = p2 ? k_push_deposit_es<true> : k_push_deposit_es<false>;
+    const bool rec = c.rec_xy != nullptr;
+    auto kern = p2 ? (rec ? k_push_deposit_es<true, true> : k_push_deposit_es<true, false>)
+                   : (rec ? k_push_deposit_es<false, true> : k_push_deposit_es<false, false>);
     prep_smem(kern, sh);
     kern<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(es_args(c));
     AW_LAUNCH();

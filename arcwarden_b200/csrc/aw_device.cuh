@@ -458,10 +458,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
 
 // Source arrays of a chunk load, in stage-plane order.
 struct ChunkSrc {
-    const float* a[6];
+    const float* a[7];
     // plane k with a select chain (a run-time index into a[] would live in local memory)
     __device__ __forceinline__ const float* at(int k) const {
-        return k == 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : k == 3 ? a[3] : k == 4 ? a[4] : a[5];
+        return k == 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : k == 3 ? a[3] : k == 4 ? a[4] : k == 5 ? a[5] : a[6];
     }
 };
 

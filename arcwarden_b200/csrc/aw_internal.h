@@ -143,6 +143,12 @@ struct Ctx {
 
     // discrete adjoint of the ES step (aw_adjoint.cu; allocated by aw_grad_es)
     struct AdjWS* adj = nullptr;
+    // Trajectory recording, set only while the adjoint's recording ES step is
+    // captured: the step's finalize advances rec_ad->slot, the fused push
+    // writes x_n, y_n and the field kernel E_n into that slot.
+    struct AdjDev* rec_ad = nullptr;
+    float* rec_xy = nullptr;
+    float* rec_E = nullptr;
 
     int nsrc() const { return model == AW_MODEL_DARWIN ? 8 : 1; }
     int nout() const { return model == AW_MODEL_DARWIN ? 5 : 2; }
@@ -170,8 +176,9 @@ struct AdjP {
 struct AdjDev {
     unsigned lmax_bits;   // max |lu3| (2-norm) for the next scatter's scale
     float    S[2];        // scales of the pending field-cotangent scatter
-    int      slot;        // trajectory slot of the step being recomputed / transposed
+    int      slot;        // trajectory slot of the step being recorded / transposed
     float    ext_scale;   // dloss/dE = ext_scale E for the last step, 0 for the others
+    unsigned ticket;      // blocks of the backward gather done (the last one moves the slot)
 };
 
 // Workspace of the ES adjoint sweep (aw_grad_es): checkpoints of the forward
@@ -193,8 +200,9 @@ struct AdjWS {
     float* lrho = nullptr;                // [ncell] charge-density cotangent
     AdjDev* ad = nullptr;
     cufftHandle p_r2c2 = 0;               // batch-2 R2C
-    cudaGraphExec_t g_rec = nullptr;      // recompute step: store x_n, step, store E_n, slot + 1
-    cudaGraphExec_t g_bwd = nullptr;      // backward step: slot - 1, A, solve^T, B
+    cudaGraphExec_t g_rec = nullptr;      // recompute step: slot + 1, the step recording x_n and E_n
+    cudaGraphExec_t g_frec = nullptr;     // the same with the step's reduction (the forward's last segment)
+    cudaGraphExec_t g_bwd = nullptr;      // backward step: A, solve^T, B (its last block: slot - 1)
 };
 
 // ---- launchers (aw_particles.cu) -------------------------------------------
@@ -278,9 +286,6 @@ void free_adjoint(Ctx& c);
 void launch_adj_finalize(Ctx& c);
 // Trajectory stores of the recompute: x_n, y_n before the step and E_n after it,
 // at the device slot; the slot counter step.
-void launch_traj_store_xy(Ctx& c);
-void launch_traj_store_E(Ctx& c);
-void launch_slot_add(Ctx& c, int delta);
 void adj_drop_graphs(Ctx& c);
 // lrho = S^T lE: the transpose of the spectral Poisson field solve.
 void adj_transpose_solve(Ctx& c);

@@ -91,7 +91,8 @@ template <int NF>
 __global__ void __launch_bounds__(kThreads)
 k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
            const float* __restrict__ Sdev, float* __restrict__ r, FinOut api, int accumulate,
-           double* __restrict__ part, DevState* st, int step_begin, double dt, float cref, int darwin) {
+           double* __restrict__ part, DevState* st, int step_begin, double dt, float cref, int darwin,
+           AdjDev* rec) {
     double invS[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) invS[f] = 1.0 / static_cast<double>(Sdev[first + f]);
@@ -148,6 +149,7 @@ k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
         }
     }
     if (step_begin && blockIdx.x == 0 && threadIdx.x == 0) {
+        if (rec) rec->slot += 1;     // the recorded step's trajectory slot
         st->t = static_cast<double>(st->step) * dt;
         // the particle state is the last push's output: its |u| maxima
 #pragma unroll
@@ -290,13 +292,17 @@ __device__ void grid_partials(double se2, double me2, double sb2, double* __rest
     }
 }
 
-// ES: r = [Ex, Ey] -> gather buffer [ncell][2], caller Ex/Ey, energy partials.
+// ES: r = [Ex, Ey] -> gather buffer [ncell][2], caller Ex/Ey, energy partials;
+// when recording, also the trajectory slot rec->slot of trajE.
 __global__ void k_fields_es(const float* __restrict__ r, float* __restrict__ gb, float* ex_api,
-                            float* ey_api, int ncell, double* __restrict__ part) {
+                            float* ey_api, int ncell, double* __restrict__ part, float2* trajE,
+                            const AdjDev* rec) {
     double se2 = 0, me2 = 0;
+    float2* __restrict__ te = trajE ? trajE + static_cast<size_t>(rec->slot) * ncell : nullptr;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
         const float ex = r[c], ey = r[ncell + c];
         reinterpret_cast<float2*>(gb)[c] = make_float2(ex, ey);
+        if (te) te[c] = make_float2(ex, ey);
         if (ex_api) ex_api[c] = ex;
         if (ey_api) ey_api[c] = ey;
         const double e2 = double(ex) * ex + double(ey) * ey;
@@ -718,11 +724,12 @@ void launch_finalize(Ctx& c, unsigned long long* acc, int first, int nf, const f
     const float cref = cref_of(c);
     if (charge_partials && blocks != kGridBlocks) throw Error(AW_ERR_STATE, "finalize: partials need the fixed grid");
     const int nb = charge_partials ? kGridBlocks : blocks;
+    AdjDev* rec = step_begin ? c.rec_ad : nullptr;
     switch (nf) {
-        case 1: k_finalize<1><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw); break;
-        case 3: k_finalize<3><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw); break;
-        case 4: k_finalize<4><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw); break;
-        case 8: k_finalize<8><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw); break;
+        case 1: k_finalize<1><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec); break;
+        case 3: k_finalize<3><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec); break;
+        case 4: k_finalize<4><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec); break;
+        case 8: k_finalize<8><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec); break;
         default: throw Error(AW_ERR_ARG, "finalize: unsupported field count");
     }
     AW_LAUNCH();
@@ -748,7 +755,8 @@ void launch_kspace_et(Ctx& c, const cufftComplex* dcu_k, const cufftComplex* amu
 }
 void launch_fields_es(Ctx& c) {
     k_fields_es<<<kGridBlocks, kThreads, 0, c.stream>>>(c.r_out, c.gb_es, c.fld.Ex, c.fld.Ey,
-                                                        c.geo.ncell, c.part_g);
+                                                        c.geo.ncell, c.part_g,
+                                                        reinterpret_cast<float2*>(c.rec_E), c.rec_ad);
     AW_LAUNCH();
 }
 void launch_fields_dcu(Ctx& c) {
