@@ -300,19 +300,23 @@ double grad_es_impl(Ctx& c, long long nsteps, int every, float* dux, float* duy,
         });
     if (!w.g_bwd)
         w.g_bwd = capture_exec(c, [&] {
-            launch_adj_scatter(c, a, kf, w.traj_E, w.ad, w.acc);
+            launch_adj_scatter(c, a, kf, w.traj_E, w.ad, w.acc, w.st);
             launch_adj_finalize(c);
             adj_transpose_solve(c);
             launch_adj_gather(c, a, kf);
         });
 
     // Forward run: checkpoints at the starts of all segments but the last, whose
-    // trajectory the run records itself (slot -1 -> its last step).
+    // trajectory the run records itself. Segment k records into trajectory
+    // slots [(k % 2) every, (k % 2) every + m_k): two buffers, so that the
+    // recompute of segment k - 1 runs beside the backward steps of segment k.
     const int klast = w.nck - 1;
     const long long slast = static_cast<long long>(klast) * every;
-    AdjDev ad0{};
-    ad0.slot = -1;
-    ad0.ext_scale = static_cast<float>(c.prm.eps0 * c.geo.dx * c.geo.dy);   // dL/dE = eps0 E dx dy
+    auto seg_steps = [&](int k) {
+        const long long s0 = static_cast<long long>(k) * every;
+        return static_cast<int>(std::min<long long>(nsteps, s0 + every) - s0);
+    };
+    auto base_slot = [&](int k) { return (k & 1) * every; };
     for (long long s = 0; s < nsteps; ++s) {
         if (s % every == 0 && s < slast) {
             const int k = static_cast<int>(s / every);
@@ -321,7 +325,7 @@ double grad_es_impl(Ctx& c, long long nsteps, int every, float* dux, float* duy,
                                     cudaMemcpyDeviceToDevice, c.stream));
             AW_CUDA(cudaMemcpyAsync(w.ck_st + k, c.st, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
         }
-        if (s == slast) AW_CUDA(cudaMemcpyAsync(w.ad, &ad0, sizeof(AdjDev), cudaMemcpyHostToDevice, c.stream));
+        if (s == slast) launch_adj_slot(c, c.stream, 1, base_slot(klast) - 1);
         AW_CUDA(cudaGraphLaunch(s < slast ? c.gexec : w.g_frec, c.stream));
     }
     aw_diag d{};
@@ -329,21 +333,34 @@ double grad_es_impl(Ctx& c, long long nsteps, int every, float* dux, float* duy,
     AW_CUDA(cudaStreamSynchronize(c.stream));
     const double loss = d.ee;
 
-    // Backward sweep: every backward step leaves the slot one step earlier, so a
-    // segment ends at slot -1, where the recompute of the one before starts.
+    // Backward sweep on stream sb; the recompute of each earlier segment on the
+    // context's stream, after the backward steps that last read its buffer.
+    AdjDev ad0{};
+    ad0.ext_scale = static_cast<float>(c.prm.eps0 * c.geo.dx * c.geo.dy);   // dL/dE = eps0 E dx dy
+    AW_CUDA(cudaMemcpyAsync(w.ad, &ad0, sizeof(AdjDev), cudaMemcpyHostToDevice, c.stream));
+    AW_CUDA(cudaMemsetAsync(w.st, 0, sizeof(DevState), c.stream));
     AW_CUDA(cudaMemsetAsync(w.lam, 0, sizeof(float) * 5 * static_cast<size_t>(n), c.stream));
+    AW_CUDA(cudaEventRecord(w.ev_fwd, c.stream));
+    AW_CUDA(cudaStreamWaitEvent(w.sb, w.ev_fwd, 0));
     for (int k = klast; k >= 0; --k) {
-        const long long s0 = static_cast<long long>(k) * every;
-        const long long s1 = std::min(nsteps, s0 + every);
-        if (k < klast) {
-            copy_parts_from(c, w.ck_parts + static_cast<size_t>(k) * 5 * n);
-            AW_CUDA(cudaMemcpyAsync(c.acc_src, w.ck_acc + k * nc, sizeof(unsigned long long) * nc,
+        if (k >= 1) {                                   // recompute segment k - 1
+            const int r = k - 1;
+            if (k + 1 <= klast) AW_CUDA(cudaStreamWaitEvent(c.stream, w.ev_bwd[(k + 1) & 1], 0));
+            copy_parts_from(c, w.ck_parts + static_cast<size_t>(r) * 5 * n);
+            AW_CUDA(cudaMemcpyAsync(c.acc_src, w.ck_acc + r * nc, sizeof(unsigned long long) * nc,
                                     cudaMemcpyDeviceToDevice, c.stream));
-            AW_CUDA(cudaMemcpyAsync(c.st, w.ck_st + k, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
-            for (long long s = s0; s < s1; ++s) AW_CUDA(cudaGraphLaunch(w.g_rec, c.stream));
+            AW_CUDA(cudaMemcpyAsync(c.st, w.ck_st + r, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
+            launch_adj_slot(c, c.stream, 1, base_slot(r) - 1);
+            for (int s = 0; s < seg_steps(r); ++s) AW_CUDA(cudaGraphLaunch(w.g_rec, c.stream));
+            AW_CUDA(cudaEventRecord(w.ev_rec[r & 1], c.stream));
         }
-        for (long long s = s1 - 1; s >= s0; --s) AW_CUDA(cudaGraphLaunch(w.g_bwd, c.stream));
+        if (k < klast) AW_CUDA(cudaStreamWaitEvent(w.sb, w.ev_rec[k & 1], 0));
+        launch_adj_slot(c, w.sb, 0, base_slot(k) + seg_steps(k) - 1);
+        for (int s = 0; s < seg_steps(k); ++s) AW_CUDA(cudaGraphLaunch(w.g_bwd, w.sb));
+        AW_CUDA(cudaEventRecord(w.ev_bwd[k & 1], w.sb));
     }
+    AW_CUDA(cudaStreamWaitEvent(c.stream, w.ev_bwd[0], 0));
+    launch_merge_err(c);
     launch_adj_out(c, dux, duy, duz);
     copy_parts_from(c, w.init_parts);
     c.pending_valid = false;

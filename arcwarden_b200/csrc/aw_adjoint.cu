@@ -75,6 +75,15 @@ __global__ void k_adj_kspace(const cufftComplex* __restrict__ lEk, cufftComplex*
     lrk[t] = r;
 }
 
+// Slot counters: which = 0 the backward's, 1 the recording's.
+__global__ void k_adj_slot(AdjDev* ad, int which, int v) {
+    if (which == 0) ad->slot = v;
+    else ad->rec_slot = v;
+}
+__global__ void k_merge_err(DevState* dst, const DevState* src) {
+    if (src->err) atomicOr(&dst->err, src->err);
+}
+
 // Backward step B, one particle per thread. The last block to finish moves the
 // trajectory slot to the previous step (every block has read it by then).
 __global__ void __launch_bounds__(kT)
@@ -189,9 +198,13 @@ void free_adjoint(Ctx& c) {
     if (!w) return;
     adj_drop_graphs(c);
     void* bufs[] = {w->lam, w->init_parts, w->ck_parts, w->ck_acc, w->ck_st, w->traj_xy, w->traj_E,
-                    w->acc, w->lE, w->lEk, w->lrk, w->lrho, w->ad};
+                    w->acc, w->lE, w->lEk, w->lrk, w->lrho, w->ad, w->st};
     for (void* b : bufs) if (b) cudaFree(b);
     if (w->p_r2c2) cufftDestroy(w->p_r2c2);
+    if (w->p_c2r1) cufftDestroy(w->p_c2r1);
+    cudaEvent_t evs[] = {w->ev_fwd, w->ev_rec[0], w->ev_rec[1], w->ev_bwd[0], w->ev_bwd[1]};
+    for (cudaEvent_t e : evs) if (e) cudaEventDestroy(e);
+    if (w->sb) cudaStreamDestroy(w->sb);
     delete w;
     c.adj = nullptr;
 }
@@ -212,20 +225,26 @@ void adj_prepare(Ctx& c, long long nsteps, int every) {
         alloc(w->ck_parts, static_cast<size_t>(nck) * 5 * n);
         alloc(w->ck_acc, static_cast<size_t>(nck) * nc);
         alloc(w->ck_st, static_cast<size_t>(nck));
-        alloc(w->traj_xy, static_cast<size_t>(every) * 2 * n);
-        alloc(w->traj_E, static_cast<size_t>(every) * 2 * nc);
+        alloc(w->traj_xy, static_cast<size_t>(2 * every) * 2 * n);
+        alloc(w->traj_E, static_cast<size_t>(2 * every) * 2 * nc);
         alloc(w->acc, 2 * nc);
         alloc(w->lE, 2 * nc);
         alloc(w->lEk, 2 * nk);
         alloc(w->lrk, nk);
         alloc(w->lrho, nc);
         alloc(w->ad, 1);
+        alloc(w->st, 1);
         AW_CUDA(cudaMemset(w->acc, 0, sizeof(unsigned long long) * 2 * nc));
         AW_CUFFT(cufftCreate(&w->p_r2c2));
         int dims[2] = {c.geo.ny, c.geo.nx};
         const int rdist = c.geo.ncell, cdist = c.sg.nkx * c.geo.ny;
         size_t ws = 0;
         AW_CUFFT(cufftMakePlanMany(w->p_r2c2, 2, dims, nullptr, 1, rdist, nullptr, 1, cdist, CUFFT_R2C, 2, &ws));
+        AW_CUFFT(cufftCreate(&w->p_c2r1));
+        AW_CUFFT(cufftMakePlan2d(w->p_c2r1, c.geo.ny, c.geo.nx, CUFFT_C2R, &ws));
+        AW_CUDA(cudaStreamCreateWithFlags(&w->sb, cudaStreamNonBlocking));
+        cudaEvent_t* evs[] = {&w->ev_fwd, &w->ev_rec[0], &w->ev_rec[1], &w->ev_bwd[0], &w->ev_bwd[1]};
+        for (cudaEvent_t* e : evs) AW_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     } catch (...) {
         free_adjoint(c);
         throw;
@@ -240,13 +259,23 @@ void launch_adj_finalize(Ctx& c) {
     AW_LAUNCH();
 }
 
+void launch_adj_slot(Ctx& c, cudaStream_t s, int which, int v) {
+    k_adj_slot<<<1, 1, 0, s>>>(c.adj->ad, which, v);
+    AW_LAUNCH();
+}
+void launch_merge_err(Ctx& c) {
+    k_merge_err<<<1, 1, 0, c.stream>>>(c.st, c.adj->st);
+    AW_LAUNCH();
+}
+
 void adj_transpose_solve(Ctx& c) {
     AdjWS& w = *c.adj;
     AW_CUFFT(cufftSetStream(w.p_r2c2, c.stream));
     AW_CUFFT(cufftExecR2C(w.p_r2c2, w.lE, w.lEk));
     k_adj_kspace<<<blocks_n(c.sg.nk), kT, 0, c.stream>>>(w.lEk, w.lrk, c.sg, c.prm.eps0, w.ad);
     AW_LAUNCH();
-    AW_CUFFT(cufftExecC2R(c.p_c2r1, w.lrk, w.lrho));
+    AW_CUFFT(cufftSetStream(w.p_c2r1, c.stream));
+    AW_CUFFT(cufftExecC2R(w.p_c2r1, w.lrk, w.lrho));
 }
 
 void launch_adj_gather(Ctx& c, const AdjP& a, const AdjK& k) {

@@ -678,7 +678,7 @@ __device__ __forceinline__ void move_xy(float& x, float& y, float ux, float uy, 
 struct EsArgs {
     Parts p; Geo g; PushP pp; const float* gb; double qoa; unsigned long long* acc; int wmaxc;
     double* part; DevState* st;
-    float* traj; const AdjDev* rec;   // trajectory recording (x_n, y_n into slot rec->slot), or null
+    float* traj; const AdjDev* rec;   // trajectory recording (x_n, y_n into slot rec->rec_slot), or null
 };
 template <bool POW2, bool RECORD = false>
 __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int chunk) {
@@ -703,7 +703,7 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
     int ir, jr;
     ref_of(x0, y0, g, ir, jr);
     const float2* q = reinterpret_cast<const float2*>(gb);
-    float* __restrict__ tr = RECORD ? A.traj + static_cast<size_t>(A.rec->slot) * 2 * p.n : nullptr;
+    float* __restrict__ tr = RECORD ? A.traj + static_cast<size_t>(A.rec->rec_slot) * 2 * p.n : nullptr;
 
     BBox bb;
     float l1[NF] = {};
@@ -1054,12 +1054,12 @@ void launch_deposit_src(Ctx& c, int which) {
 void prep_adj_scatter() { prep_smem(k_adj_scatter, smem_bytes(2, 4)); }
 
 void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE, AdjDev* ad,
-                        unsigned long long* acc) {
+                        unsigned long long* acc, DevState* st) {
     if (a.n == 0) return;
     const size_t sh = smem_bytes(2, 4);
     prep_smem(k_adj_scatter, sh);
     k_adj_scatter<<<nchunks(a.n), kThreads, sh, c.stream>>>(a, c.geo, k, reinterpret_cast<const float2*>(trajE),
-                                                             ad, acc, kAdjWindow, c.st);
+                                                             ad, acc, kAdjWindow, st);
     AW_LAUNCH();
 }
 

@@ -144,7 +144,7 @@ struct Ctx {
     // discrete adjoint of the ES step (aw_adjoint.cu; allocated by aw_grad_es)
     struct AdjWS* adj = nullptr;
     // Trajectory recording, set only while the adjoint's recording ES step is
-    // captured: the step's finalize advances rec_ad->slot, the fused push
+    // captured: the step's finalize advances rec_ad->rec_slot, the fused push
     // writes x_n, y_n and the field kernel E_n into that slot.
     struct AdjDev* rec_ad = nullptr;
     float* rec_xy = nullptr;
@@ -176,9 +176,10 @@ struct AdjP {
 struct AdjDev {
     unsigned lmax_bits;   // max |lu3| (2-norm) for the next scatter's scale
     float    S[2];        // scales of the pending field-cotangent scatter
-    int      slot;        // trajectory slot of the step being recorded / transposed
+    int      slot;        // trajectory slot of the step being transposed
     float    ext_scale;   // dloss/dE = ext_scale E for the last step, 0 for the others
     unsigned ticket;      // blocks of the backward gather done (the last one moves the slot)
+    int      rec_slot;    // trajectory slot of the step being recorded
 };
 
 // Workspace of the ES adjoint sweep (aw_grad_es): checkpoints of the forward
@@ -191,15 +192,19 @@ struct AdjWS {
     float* ck_parts = nullptr;            // [nck][5][n]
     unsigned long long* ck_acc = nullptr; // [nck][ncell] pending rho accumulators
     DevState* ck_st = nullptr;            // [nck]
-    float* traj_xy = nullptr;             // [every][2][n] positions x_n of the segment
-    float* traj_E = nullptr;              // [every][ncell][2] gather fields E_n of the segment
+    float* traj_xy = nullptr;             // [2 every][2][n] positions x_n, two segments (double buffer)
+    float* traj_E = nullptr;              // [2 every][ncell][2] gather fields E_n, two segments
     unsigned long long* acc = nullptr;    // [2][ncell] field-cotangent scatter
     float* lE = nullptr;                  // [2][ncell]
     cufftComplex* lEk = nullptr;          // [2][nk]
     cufftComplex* lrk = nullptr;          // [nk]
     float* lrho = nullptr;                // [ncell] charge-density cotangent
     AdjDev* ad = nullptr;
+    DevState* st = nullptr;               // the backward's error word and counters
     cufftHandle p_r2c2 = 0;               // batch-2 R2C
+    cufftHandle p_c2r1 = 0;               // C2R with its own work area (runs beside the recompute)
+    cudaStream_t sb = nullptr;            // the backward sweep's stream
+    cudaEvent_t ev_fwd = nullptr, ev_rec[2] = {nullptr, nullptr}, ev_bwd[2] = {nullptr, nullptr};
     cudaGraphExec_t g_rec = nullptr;      // recompute step: slot + 1, the step recording x_n and E_n
     cudaGraphExec_t g_frec = nullptr;     // the same with the step's reduction (the forward's last segment)
     cudaGraphExec_t g_bwd = nullptr;      // backward step: A, solve^T, B (its last block: slot - 1)
@@ -228,9 +233,10 @@ void launch_push_deposit_es(Ctx& c);
 void launch_push_deposit_em(Ctx& c);
 // Backward step A of the ES adjoint: Boris/move transposes, field-cotangent
 // scatter into acc [2][ncell] (scales from ad->lmax_bits, stored to ad->S) and
-// the E-gather position derivative (E = interleaved [ncell][2]).
+// the E-gather position derivative (E = interleaved [ncell][2]); errors and
+// counters go to st.
 void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE, AdjDev* ad,
-                        unsigned long long* acc);
+                        unsigned long long* acc, DevState* st);
 void prep_adj_scatter();   // its shared-memory opt-in (before any capture)
 // Multi-run particle phases (batched ensembles): one launch over the chunks of
 // several runs of one kind. The run table is built once (device copies of each
@@ -284,9 +290,11 @@ void free_adjoint(Ctx& c);
 // lE = acc / S + ad->ext_scale * E_slot (E of the slot's step, interleaved
 // [ncell][2]); acc is zeroed.
 void launch_adj_finalize(Ctx& c);
-// Trajectory stores of the recompute: x_n, y_n before the step and E_n after it,
-// at the device slot; the slot counter step.
 void adj_drop_graphs(Ctx& c);
+// Set the backward's (which = 0) or the recording's (1) trajectory slot on s.
+void launch_adj_slot(Ctx& c, cudaStream_t s, int which, int v);
+// OR the backward's device error word into the context's.
+void launch_merge_err(Ctx& c);
 // lrho = S^T lE: the transpose of the spectral Poisson field solve.
 void adj_transpose_solve(Ctx& c);
 // Backward step B: lx += q dlrho/dx at x_n; max |lu3| of the next step A.

@@ -149,7 +149,7 @@ k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
         }
     }
     if (step_begin && blockIdx.x == 0 && threadIdx.x == 0) {
-        if (rec) rec->slot += 1;     // the recorded step's trajectory slot
+        if (rec) rec->rec_slot += 1;     // the recorded step's trajectory slot
         st->t = static_cast<double>(st->step) * dt;
         // the particle state is the last push's output: its |u| maxima
 #pragma unroll
@@ -298,7 +298,7 @@ __global__ void k_fields_es(const float* __restrict__ r, float* __restrict__ gb,
                             float* ey_api, int ncell, double* __restrict__ part, float2* trajE,
                             const AdjDev* rec) {
     double se2 = 0, me2 = 0;
-    float2* __restrict__ te = trajE ? trajE + static_cast<size_t>(rec->slot) * ncell : nullptr;
+    float2* __restrict__ te = trajE ? trajE + static_cast<size_t>(rec->rec_slot) * ncell : nullptr;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
         const float ex = r[c], ey = r[ncell + c];
         reinterpret_cast<float2*>(gb)[c] = make_float2(ex, ey);
