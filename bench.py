@@ -343,9 +343,14 @@ def profile_case(wl, steps):
     cell = torch.empty(n, dtype=torch.int32, device=dev)
     ctx.bind_particles(P["x"], P["y"], P["ux"], P["uy"], P["uz"], P["w"], cell)
     ctx.load_species(wl["species"], seed=0, noisy=True)
-    ctx.init()
-    for s in range(steps):
-        ctx.step(s)
+    if wl.get("adjoint"):
+        # one gradient of K steps (checkpoint interval as the workload's, at most K)
+        du = [torch.zeros(n, dtype=torch.float32, device=dev) for _ in range(3)]
+        ctx.grad_es(steps, min(wl["every"], steps), *du)
+    else:
+        ctx.init()
+        for s in range(steps):
+            ctx.step(s)
     torch.cuda.synchronize(dev)
     err = ctx.error_word()
     ctx.close()
@@ -354,11 +359,23 @@ def profile_case(wl, steps):
     print(f"profile case {wl['name']}: {steps} steps of {n} particles", flush=True)
 
 
-# bytes per particle per PIC step of one gradient evaluation: the forward step
-# (44), its recompute (44) and the trajectory store (8), the transposed step A
-# (x_n 8, cotangents 20 read + 20 written) and B (x_n 8, w 4, lx ly 8 read + 8
-# written, lu 12 read)
-ADJ_BYTES_PER_PARTICLE = 44.0 + 44.0 + 8.0 + 48.0 + 40.0
+def adj_bytes_per_particle_step(nsteps, every):
+    """Algorithmic bytes per particle per PIC step of one gradient evaluation:
+    the forward step (44), its recompute (44, for every segment but the last,
+    which the forward run records itself), the trajectory store (8), the
+    transposed step A (x_n 8, cotangents 20 read + 20 written) and B (x_n 8, w 4,
+    lx ly 8 read + 8 written, lu 12 read)."""
+    last = nsteps - (math.ceil(nsteps / every) - 1) * every
+    return 44.0 + 44.0 * (nsteps - last) / nsteps + 8.0 + 48.0 + 40.0
+
+
+def adj_launches(nsteps, every):
+    """Kernels of this library one gradient launches: aw_init's 13; per forward
+    step 5; per recomputed step 4 (no reduction); per backward step 4; two slot
+    settings per segment; the output and the error merge."""
+    nseg = math.ceil(nsteps / every)
+    last = nsteps - (nseg - 1) * every
+    return 13 + 5 * nsteps + 4 * (nsteps - last) + 4 * nsteps + 2 * nseg + 2
 
 
 def run_adjoint(args, wl, rank, world, dist):
@@ -444,8 +461,9 @@ def run_adjoint(args, wl, rank, world, dist):
     e2e_s = max_over_ranks((time.perf_counter() - t0) / reps, dist, dev)
 
     peak, peak_kind = measured_peak_gbs()
-    achieved = n * N * ADJ_BYTES_PER_PARTICLE / (grad_ms * 1e-3) / 1e9
-    launches = N * (5 + 1) + N * (5 + 4) + N * 7 + 1   # forward steps, recompute steps, backward steps, output
+    bpp = adj_bytes_per_particle_step(N, every)
+    achieved = n * N * bpp / (grad_ms * 1e-3) / 1e9
+    launches = adj_launches(N, every)
     res = {
         "metric": "particles/s/step (gradient: forward + checkpointed backward)",
         "value": world * n * N / (grad_ms * 1e-3),
@@ -469,7 +487,7 @@ def run_adjoint(args, wl, rank, world, dist):
                 "run": "H2D of the initial state from pinned memory, aw_grad_es, D2H of dL/du0"},
         "roofline": {"bound": "hbm", "kernel": "whole gradient", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
-                     "algorithmic_bytes_per_particle_step": ADJ_BYTES_PER_PARTICLE},
+                     "algorithmic_bytes_per_particle_step": bpp},
         "gpu_launches": args.steps * launches,
         "clocks": clk.summary(),
     }
@@ -670,8 +688,8 @@ def main():
     ap.add_argument("--dump-grad", default=None, metavar="FILE",
                     help="adjoint256: write the initial state and the gradient (.npz) for oracle/grad_check.py")
     ap.add_argument("--profile-case", type=int, default=0, metavar="K",
-                    help="profiling case for ncu: load, aw_init and K single aw_step launches (no graph, no "
-                         "timing, no JSON line)")
+                    help="profiling case for ncu: load, aw_init and K single aw_step launches (adjoint256: one "
+                         "gradient of K steps; no timing, no JSON line)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
