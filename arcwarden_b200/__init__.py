@@ -91,6 +91,7 @@ SIGNATURES = {
     "aw_fields_bind": [_P, C.POINTER(FieldPtrs)],
     "aw_load_species": [_P, C.POINTER(Species), _I32, _U64, _I32],
     "aw_resort": [_P], "aw_set_resort": [_P, _I32],
+    "aw_set_form_factor": [_P, _D, _D, _I32, _D],
     "aw_grad_es": [_P, _I64, _I32, _P, _P, _P, C.POINTER(_D)],
     "aw_ensemble_create": [_I32, C.POINTER(RunSpec), _P, C.POINTER(_P)], "aw_ensemble_destroy": [_P],
     "aw_ensemble_init": [_P], "aw_ensemble_tune": [_P, _I32],
@@ -242,6 +243,12 @@ class Context:
     def set_resort(self, every: int):
         """Re-sort inside run() before every step n with n % every == 0 (0 = never)."""
         _check(self.lib.aw_set_resort(self.h, int(every)))
+
+    def set_form_factor(self, ax: float = 0.0, ay: float = 0.0, cic_order: int = 0, k_filter: float = 0.0):
+        """k-space form factor s(k) on every solve: exp(-((kx ax)^2 + (ky ay)^2)/2)
+        * [sinc(kx dx/2) sinc(ky dy/2)]^(2 cic_order), 0 past |k| > k_filter (> 0).
+        All zero (the default) is the reference's solve."""
+        _check(self.lib.aw_set_form_factor(self.h, float(ax), float(ay), int(cic_order), float(k_filter)))
 
     def grad_es(self, nsteps: int, checkpoint_every: int, dux, duy, duz) -> float:
         """d(final field energy)/d(initial velocities) into the device arrays

@@ -13,11 +13,13 @@
 #include "aw_internal.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <vector>
 
 namespace aw {
 
@@ -73,7 +75,7 @@ void free_all(Ctx& c) {
     void* bufs[] = {c.st, c.acc_src, c.acc_dcu, c.r_src, c.r_out, c.r_dcu, c.r_et, c.k_src, c.k_out,
                     c.k_dcu, c.k_et, c.gb_es, c.gb_dcu, c.gb_push, c.part_p, c.part_c, c.part_d, c.part_g, c.diag, c.red_rows,
                     c.bin_count, c.bin_off, c.bin_cursor, c.bin_idx, c.sort_tmp, c.fft_work, c.rs_buf,
-                    c.rs_temp};
+                    c.rs_temp, c.ffac};
     for (void* b : bufs) if (b) cudaFree(b);
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
 }
@@ -902,6 +904,43 @@ int aw_grad_es(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux
         aw::need(nsteps >= 1 && checkpoint_every >= 1, AW_ERR_ARG, "grad_es: nsteps and checkpoint_every >= 1");
         aw::need(c.prm.pump == 0, AW_ERR_ARG, "grad_es: no pump in the ES step");
         *loss = aw::grad_es_impl(c, nsteps, checkpoint_every, dux, duy, duz);
+    });
+}
+
+int aw_set_form_factor(aw_ctx* ctx, double ax, double ay, int32_t cic_order, double k_filter) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::need(std::isfinite(ax) && std::isfinite(ay) && std::isfinite(k_filter) && ax >= 0.0 && ay >= 0.0 &&
+                     k_filter >= 0.0 && cic_order >= 0 && cic_order <= 4,
+                 AW_ERR_ARG, "set_form_factor: ax, ay, k_filter >= 0 and finite, cic_order in [0, 4]");
+        Ctx& c = ctx->c;
+        aw::drop_graph(c);                       // captured solves hold the table pointer
+        if (ax == 0.0 && ay == 0.0 && cic_order == 0 && k_filter == 0.0) {
+            AW_CUDA(cudaStreamSynchronize(c.stream));
+            if (c.ffac) cudaFree(c.ffac);
+            c.ffac = nullptr;
+            c.sg.ff = nullptr;
+            return;
+        }
+        // s(k) = exp(-((kx ax)^2 + (ky ay)^2) / 2) * [sinc(kx dx/2) sinc(ky dy/2)]^(2 cic_order),
+        // 0 past |k| > k_filter when k_filter > 0; kx, ky as the solves take them
+        const int ny = c.sg.ny, nkx = c.sg.nkx;
+        std::vector<double> s(static_cast<size_t>(c.sg.nk));
+        auto sinc = [](double z) { return z == 0.0 ? 1.0 : std::sin(z) / z; };
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nkx; ++i) {
+                const double kx = i * c.sg.dkx;
+                const double ky = ((j <= ny / 2) ? j : j - ny) * c.sg.dky;
+                double v = std::exp(-0.5 * ((kx * ax) * (kx * ax) + (ky * ay) * (ky * ay)));
+                const double sc = sinc(0.5 * kx * c.geo.dx) * sinc(0.5 * ky * c.geo.dy);
+                for (int m = 0; m < cic_order; ++m) v *= sc * sc;
+                if (k_filter > 0.0 && kx * kx + ky * ky > k_filter * k_filter) v = 0.0;
+                s[static_cast<size_t>(j) * nkx + i] = v;
+            }
+        if (!c.ffac) AW_CUDA(cudaMalloc(reinterpret_cast<void**>(&c.ffac), sizeof(double) * s.size()));
+        AW_CUDA(cudaMemcpyAsync(c.ffac, s.data(), sizeof(double) * s.size(), cudaMemcpyHostToDevice, c.stream));
+        AW_CUDA(cudaStreamSynchronize(c.stream));
+        c.sg.ff = c.ffac;
     });
 }
 

@@ -67,7 +67,7 @@ __global__ void k_adj_kspace(const cufftComplex* __restrict__ lEk, cufftComplex*
     r.x = r.y = 0.0f;
     if (k2 > 0.0 && !nyq) {
         const cufftComplex ax = lEk[t], ay = lEk[g.nk + t];
-        const double gr = 1.0 / (eps0 * k2) * static_cast<double>(g.invN);
+        const double gr = 1.0 / (eps0 * k2) * static_cast<double>(g.invN) * (g.ff ? g.ff[t] : 1.0);
         const double zx = kx * ax.x + ky * ay.x, zy = kx * ax.y + ky * ay.y;   // k . lE
         r.x = static_cast<float>(-zy * gr);                                      // i z
         r.y = static_cast<float>(zx * gr);

@@ -55,6 +55,8 @@ struct SpecGeo {
     int    nx, ny, nkx, nk;      // nk = nkx*ny complex elements
     double dkx, dky;
     float  invN;                 // 1/(nx*ny), a power of two for the config grids
+    const double* ff = nullptr;  // form factor s(k) [ny][nkx] multiplying every Green's
+                                 // function, or null: s = 1 (the reference's solve)
 };
 
 // Pump parameters (RunParams pump_*; include/pic/pump.hpp:27-47).
@@ -140,6 +142,9 @@ struct Ctx {
     bool pending_valid = false;       // acc_src holds the deposit of the current state
     long long host_step = 0;
     int write_cell = 1;
+
+    // k-space form factor table (aw_set_form_factor), c.sg.ff points at it
+    double* ffac = nullptr;
 
     // discrete adjoint of the ES step (aw_adjoint.cu; allocated by aw_grad_es)
     struct AdjWS* adj = nullptr;

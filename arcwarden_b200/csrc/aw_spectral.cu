@@ -95,7 +95,7 @@ k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
            AdjDev* rec) {
     double invS[NF];
 #pragma unroll
-    for (int f = 0; f < NF; ++f) invS[f] = 1.0 / static_cast<double>(Sdev[first + f]);
+    for (int f = 0; f < NF; ++f) invS[f] = __drcp_rn(static_cast<double>(Sdev[first + f]));   // = 1.0 / S
     double qsum = 0.0;
     const int npair = (ncell + 1) >> 1;
     for (int pi = blockIdx.x * blockDim.x + threadIdx.x; pi < npair; pi += gridDim.x * blockDim.x) {
@@ -103,14 +103,21 @@ k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
         const bool two = (c + 1 < ncell);
         const bool vec = two && ((ncell & 1) == 0);   // planes 16-byte aligned
         long long v[NF][2];
+        if (vec) {
+            // every field's load first, then the zeroing stores: all loads in flight together
+            longlong2 q[NF];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            unsigned long long* a = acc + static_cast<size_t>(first + f) * ncell + c;
-            if (vec) {
-                const longlong2 q = *reinterpret_cast<const longlong2*>(a);
-                v[f][0] = q.x; v[f][1] = q.y;
-                *reinterpret_cast<longlong2*>(a) = make_longlong2(0, 0);
-            } else {
+            for (int f = 0; f < NF; ++f)
+                q[f] = *reinterpret_cast<const longlong2*>(acc + static_cast<size_t>(first + f) * ncell + c);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                *reinterpret_cast<longlong2*>(acc + static_cast<size_t>(first + f) * ncell + c) = make_longlong2(0, 0);
+                v[f][0] = q[f].x; v[f][1] = q[f].y;
+            }
+        } else {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                unsigned long long* a = acc + static_cast<size_t>(first + f) * ncell + c;
                 v[f][0] = static_cast<long long>(a[0]); a[0] = 0ull;
                 v[f][1] = 0;
                 if (two) { v[f][1] = static_cast<long long>(a[1]); a[1] = 0ull; }
@@ -166,12 +173,15 @@ k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
 }
 
 // ---- k-space -------------------------------------------------------------
+// Form factor of mode t (1 without a table).
+__device__ __forceinline__ double ffac_of(const SpecGeo& g, int t) { return g.ff ? g.ff[t] : 1.0; }
+
 __device__ __forceinline__ void es_k(cufftComplex r, int i, int j, const SpecGeo& g, double eps0,
                                      cufftComplex& ex, cufftComplex& ey) {
     const double kxi = kx_of(i, g.dkx);
     const double kyj = ky_of(j, g.ny, g.dky);
     const double k2 = kxi * kxi + kyj * kyj;
-    const double gr = (k2 > 0.0 ? 1.0 / (eps0 * k2) : 0.0) * 1.0;
+    const double gr = (k2 > 0.0 ? 1.0 / (eps0 * k2) : 0.0) * ffac_of(g, j * g.nkx + i);
     cufftComplex phi;
     phi.x = static_cast<float>(r.x * gr);
     phi.y = static_cast<float>(r.y * gr);
@@ -212,7 +222,7 @@ __global__ void k_kspace_elb(const cufftComplex* __restrict__ src_k, cufftComple
 
     const double kxi = kx_of(i, g.dkx), kyj = ky_of(j, g.ny, g.dky);
     const double k2 = kxi * kxi + kyj * kyj;
-    const double G = k2 > 0.0 ? 1.0 / (eps0 * c * c * k2) : 0.0;
+    const double G = (k2 > 0.0 ? 1.0 / (eps0 * c * c * k2) : 0.0) * ffac_of(g, t);
     cufftComplex bx, by, bz;
     if (nyquist(i, j, g.nx, g.ny) || k2 == 0.0) {
         bx.x = bx.y = by.x = by.y = bz.x = bz.y = 0.0f;
@@ -242,7 +252,7 @@ __global__ void k_kspace_et(const cufftComplex* __restrict__ dcu_k, const cufftC
     const size_t nk = g.nk;
     const double kxi = kx_of(i, g.dkx), kyj = ky_of(j, g.ny, g.dky);
     const double k2 = kxi * kxi + kyj * kyj;
-    const double G = k2 > 0.0 ? 1.0 / (eps0 * c * c * k2 + n0) : 0.0;
+    const double G = (k2 > 0.0 ? 1.0 / (eps0 * c * c * k2 + n0) : 0.0) * ffac_of(g, t);
     cufftComplex ex, ey, ez;
     if (nyquist(i, j, g.nx, g.ny) || k2 == 0.0) {
         ex.x = ex.y = ey.x = ey.y = ez.x = ez.y = 0.0f;

@@ -201,6 +201,16 @@ int aw_resort(aw_ctx* ctx);
  * Default: 50 for the Darwin model, 0 for the electrostatic model, whose
  * reference path keeps the particle order. */
 int aw_set_resort(aw_ctx* ctx, int32_t every);
+/* k-space form factor (SpectralFormFactor::smoothing, include/pic/spectral.hpp:
+ * 63-99, whose RunParams knobs ax, ay, k_filter (include/pic/config.hpp:281-283)
+ * the reference documents but never reads: its smoothing is 1). Every Green's
+ * function of the solves (Poisson E and E_L, Darwin B and E_T, and the
+ * adjoint's transposed solve) is multiplied by
+ *   s(k) = exp(-((kx ax)^2 + (ky ay)^2) / 2) * [sinc(kx dx/2) sinc(ky dy/2)]^(2 cic_order)
+ * (sinc z = sin z / z: cic_order CIC particle-shape form factors), and by 0
+ * where |k| > k_filter when k_filter > 0. ax, ay in length units. All zero
+ * (the default) is the reference's solve, bit for bit. */
+int aw_set_form_factor(aw_ctx* ctx, double ax, double ay, int32_t cic_order, double k_filter);
 /* Device pointers to the last tile binning: off[ntiles+1], idx[n] (idx is NULL
  * after a physical sort), and the tile geometry (BinViews, particles.hpp:63-69). */
 int aw_tile_bins(aw_ctx* ctx, const int32_t** off, const int32_t** idx,

@@ -22,7 +22,9 @@ import numpy as np
 
 
 class Case:
-    def __init__(self, nx, ny, Lx, Ly, dt, qm=-1.0, eps0=1.0, B0=(0.0, 0.0, 0.0)):
+    def __init__(self, nx, ny, Lx, Ly, dt, qm=-1.0, eps0=1.0, B0=(0.0, 0.0, 0.0), smooth=None):
+        """smooth: an optional k-space form factor s(k) [ny][nx/2 + 1] on the
+        Green's function (oracle/formfactor64.py; aw_set_form_factor)."""
         self.nx, self.ny, self.Lx, self.Ly = nx, ny, Lx, Ly
         self.dx, self.dy = Lx / nx, Ly / ny
         self.dt, self.qm, self.eps0 = dt, qm, eps0
@@ -40,6 +42,8 @@ class Case:
         if ny % 2 == 0:
             nyq[ny // 2, :] = True
         keep = (~nyq).astype(np.float64)
+        if smooth is not None:
+            gr = gr * smooth
         self.Kx = -1j * KX * gr * keep                   # E_d,k = K_d rho_k
         self.Ky = -1j * KY * gr * keep
 

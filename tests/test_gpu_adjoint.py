@@ -56,6 +56,29 @@ def test_grad_matches_fp64_reference(torch_cuda, aw, B0):
         s.close()
 
 
+def test_grad_with_form_factor_matches_fp64_reference(torch_cuda, aw):
+    """With a k-space form factor the forward and the transposed solve both carry
+    s(k): the gradient still matches the FP64 reference with the same s(k)."""
+    from oracle.adjoint64 import Case
+    from oracle.formfactor64 import form_factor
+    nx, nsteps = 32, 16
+    s = _setup(torch_cuda, aw, nx, (0.0, 0.0, 0.0), seed=2)
+    try:
+        s.ctx.set_form_factor(ax=0.7, ay=0.4, cic_order=1)
+        p0 = s.parts()
+        loss, g = _grad(torch_cuda, s, nsteps, 5)
+        sm = form_factor(nx, nx, float(nx), float(nx), ax=0.7, ay=0.4, cic_order=1)
+        case = Case(nx, nx, float(nx), float(nx), 0.1, smooth=sm)
+        u0 = np.stack([p0["ux"], p0["uy"], p0["uz"]], axis=1).astype(np.float64)
+        L64, g64 = case.gradient(p0["x"].astype(np.float64), p0["y"].astype(np.float64), u0,
+                                 p0["w"].astype(np.float64), nsteps)
+        assert abs(loss - L64) <= 1e-4 * abs(L64), (loss, L64)
+        rel = np.linalg.norm(g - g64) / np.linalg.norm(g64)
+        assert rel < 2e-3, rel
+    finally:
+        s.close()
+
+
 def test_grad_bit_identical_across_runs_and_checkpoint_intervals(torch_cuda, aw):
     s = _setup(torch_cuda, aw, 32, (0.0, 0.0, 0.0), seed=3)
     try:

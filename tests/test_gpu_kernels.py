@@ -355,6 +355,56 @@ def test_solves_match_fp64_oracle(setup, aw, oracle):
         assert relerr(s.grid(k), et[i]) < 1e-5, k
 
 
+@pytest.mark.parametrize("ax,ay,m,kf", [(0.3, 0.2, 1, 0.0), (0.0, 0.0, 2, 0.0), (0.1, 0.0, 0, 6.0)])
+def test_solves_with_form_factor_match_fp64(setup, aw, ax, ay, m, kf):
+    """aw_set_form_factor: every solve's Green's function times s(k), against the
+    FP64 restatement with the same s(k) (oracle/formfactor64.py)."""
+    from oracle import formfactor64 as ff
+    nx, ny, L = 64, 32, 2 * math.pi
+    s = setup(nx, ny, L, L, 16, aw.AW_MODEL_DARWIN, dt=0.1)
+    src = _grid_inputs(nx, ny, L, L)
+    for k, v in src.items():
+        s.put(k, v)
+    s.ctx.set_form_factor(ax=ax, ay=ay, cic_order=m, k_filter=kf)
+    sm = ff.form_factor(nx, ny, L, L, ax, ay, m, kf)
+    s.ctx.solve_es()
+    ex, ey = ff.solve_es(src["rho"], L, L, sm)
+    assert relerr(s.grid("Ex"), ex) < 1e-5 and relerr(s.grid("Ey"), ey) < 1e-5
+    s.ctx.solve_darwin_el_b()
+    o = ff.solve_elb(src["rho"], src["Jx"], src["Jy"], src["Jz"], L, L, sm)
+    for i, k in enumerate(("ELx", "ELy", "Bx", "By", "Bz")):
+        assert relerr(s.grid(k), o[i]) < 1e-5, k
+    s.ctx.solve_darwin_et()
+    et = ff.solve_et(np.stack([src[k] for k in ("dcux", "dcuy", "dcuz")]),
+                     np.stack([src[k] for k in ("amu0", "amu1", "amu2", "amu3")]), L, L, sm)
+    for i, k in enumerate(("ETx", "ETy", "ETz")):
+        assert relerr(s.grid(k), et[i]) < 1e-5, k
+
+
+def test_form_factor_off_is_the_reference_solve(setup, aw):
+    """Setting a form factor and clearing it (all zero) gives the same bits as
+    never setting one; bad arguments are refused."""
+    nx, ny, L = 64, 32, 2 * math.pi
+    s = setup(nx, ny, L, L, 16, aw.AW_MODEL_DARWIN, dt=0.1)
+    src = _grid_inputs(nx, ny, L, L)
+    for k, v in src.items():
+        s.put(k, v)
+    s.ctx.solve_es()
+    s.ctx.solve_darwin_el_b()
+    a = [s.grid(k) for k in ("Ex", "Ey", "Bx", "By", "Bz")]
+    s.ctx.set_form_factor(ax=0.5, cic_order=1)
+    s.ctx.solve_es()
+    assert not np.array_equal(s.grid("Ex"), a[0])
+    s.ctx.set_form_factor()
+    s.ctx.solve_es()
+    s.ctx.solve_darwin_el_b()
+    b = [s.grid(k) for k in ("Ex", "Ey", "Bx", "By", "Bz")]
+    assert all(np.array_equal(x, y) for x, y in zip(a, b))
+    for bad in (dict(ax=-1.0), dict(cic_order=5), dict(k_filter=float("nan"))):
+        with pytest.raises(aw.ArcError):
+            s.ctx.set_form_factor(**bad)
+
+
 def test_poisson_sine_kat(setup, aw):
     """tests/test_poisson_sine.cu: a sine charge density gives the analytic Ex to 1e-4."""
     d = np.load(GOLDEN / "poisson_sine.npz")
