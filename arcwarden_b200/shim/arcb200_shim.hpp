@@ -8,10 +8,11 @@
 //          -L arcwarden_b200 -larcb200 -lcufft -Xlinker -rpath,<repo>/arcwarden_b200
 //
 // The shim's pic/*.hpp replace the hot-path headers (particles, depositor,
-// pusher, spectral, solver_es, solver_darwin, pump, simulation) with classes of
+// pusher, spectral, solver_es, solver_darwin, pump, simulation) and the
+// diagnostics (reduced on the GPU, copied back asynchronously) with classes of
 // the same names and signatures that call the library; every other pic/*.hpp
-// (grid, config, device_array, cuda_utils, species, sources, fields,
-// diagnostics, deck, the Yee branch, ...) is the reference's own. Data stays in
+// (grid, config, device_array, cuda_utils, species, sources, fields, deck, the
+// Yee branch, ...) is the reference's own. Data stays in
 // the reference's containers (DeviceArray in Particles, Sources, Fields): the
 // library works on those arrays in place, bound by pointer before each call.
 //

@@ -2,7 +2,8 @@
 // 41-126) on libarcb200's fused step. init() loads the particles, allocates the
 // reference's Sources/Fields, creates a library context bound to them and runs
 // aw_init; every step() is one replay of the captured step graph (aw_run),
-// followed by the reference's host diagnostics when they are due.
+// and a dump step enqueues an asynchronous copy of the step's GPU-reduced
+// diagnostics (the shim's pic/diagnostics.hpp), with no host sync.
 #ifndef ARC_PIC_SIMULATION_HPP
 #define ARC_PIC_SIMULATION_HPP
 
@@ -67,17 +68,20 @@ public:
         shim::bind_sources(ctx_, sources_);
         shim::bind_fields(ctx_, fields_);
         shim::check(aw_init(ctx_), "init");
+        shim::check(aw_step_diag_device(ctx_, &dev_diag_), "step_diag_device");
     }
 
-    // One PIC step (the fused graph), then the diagnostics when due.
+    // One PIC step (the fused graph), then the diagnostics when due
+    // (Diagnostics::maybe_compute's cadence: dump_every <= 0 means every step).
     void step(long n) {
         shim::check(aw_run(ctx_, n, 1, 1), "run");
-        diag_.maybe_compute(n, particles_.views(), sources_, fields_, p_, stream_);
+        if (p_.dump_every <= 0 || n % p_.dump_every == 0) diag_.record_async(n, n * p_.dt, dev_diag_, stream_);
     }
 
     void run() {
         for (long n = 0; n < p_.nsteps; ++n) step(n);
         stream_.synchronize();
+        diag_.drain();
     }
 
     // The Darwin field solve for the current particle state, from the separate
@@ -118,6 +122,7 @@ private:
     Diagnostics    diag_;
     CudaStream     stream_;
     aw_ctx*        ctx_ = nullptr;
+    const aw_diag* dev_diag_ = nullptr;
 };
 
 }  // namespace arc
