@@ -74,6 +74,11 @@ class RunSpec(C.Structure):
                 ("species", Species * 4), ("seed", C.c_uint64), ("noisy", C.c_int32)]
 
 
+class CheckpointInfo(C.Structure):
+    _fields_ = [("rng_seed", C.c_uint64), ("step", C.c_int64), ("time", C.c_double), ("sd", C.c_double),
+                ("eps_l", C.c_double), ("deck", C.c_char_p), ("git_hash", C.c_char_p)]
+
+
 class Stats(C.Structure):
     _fields_ = [("chunks", C.c_int64), ("window_overflow", C.c_int64), ("slow_deposits", C.c_int64),
                 ("steps", C.c_int64), ("kernels_per_step", C.c_int64)]
@@ -92,6 +97,8 @@ SIGNATURES = {
     "aw_load_species": [_P, C.POINTER(Species), _I32, _U64, _I32],
     "aw_resort": [_P], "aw_set_resort": [_P, _I32],
     "aw_set_form_factor": [_P, _D, _D, _I32, _D],
+    "aw_checkpoint_write": [_P, C.c_char_p, C.POINTER(CheckpointInfo), _I32], "aw_checkpoint_wait": [_P],
+    "aw_checkpoint_read": [_P, C.c_char_p, C.POINTER(CheckpointInfo)],
     "aw_grad_es": [_P, _I64, _I32, _P, _P, _P, C.POINTER(_D)],
     "aw_ensemble_create": [_I32, C.POINTER(RunSpec), _P, C.POINTER(_P)], "aw_ensemble_destroy": [_P],
     "aw_ensemble_init": [_P], "aw_ensemble_tune": [_P, _I32],
@@ -249,6 +256,25 @@ class Context:
         * [sinc(kx dx/2) sinc(ky dy/2)]^(2 cic_order), 0 past |k| > k_filter (> 0).
         All zero (the default) is the reference's solve."""
         _check(self.lib.aw_set_form_factor(self.h, float(ax), float(ay), int(cic_order), float(k_filter)))
+
+    def checkpoint(self, path: str, step: int, time: float = None, deck: str = "", git_hash: str = "",
+                   rng_seed: int = 0, sd: float = 1.0, eps_l: float = 0.0, wait: bool = True):
+        """Write the run's state at `step` to `path` in the reference's checkpoint
+        format (header, manifest, array payloads). wait=False returns once the
+        device snapshot is enqueued; checkpoint_wait() joins the file write."""
+        info = CheckpointInfo(int(rng_seed), int(step), float(step * self.params.dt if time is None else time), float(sd),
+                              float(eps_l), deck.encode(), git_hash.encode())
+        _check(self.lib.aw_checkpoint_write(self.h, str(path).encode(), C.byref(info), int(bool(wait))))
+
+    def checkpoint_wait(self):
+        _check(self.lib.aw_checkpoint_wait(self.h))
+
+    def restore(self, path: str) -> dict:
+        """Read a checkpoint back into the bound arrays; aw_run from the returned
+        step continues the saved run bit for bit."""
+        info = CheckpointInfo()
+        _check(self.lib.aw_checkpoint_read(self.h, str(path).encode(), C.byref(info)))
+        return {"step": info.step, "time": info.time, "rng_seed": info.rng_seed, "sd": info.sd, "eps_l": info.eps_l}
 
     def grad_es(self, nsteps: int, checkpoint_every: int, dux, duy, duz) -> float:
         """d(final field energy)/d(initial velocities) into the device arrays

@@ -67,6 +67,7 @@ void make_plan(cufftHandle& h, int ny, int nx, cufftType type, int batch, size_t
 }
 
 void free_all(Ctx& c) {
+    free_checkpoint(c);
     free_adjoint(c);
     if (c.gexec) cudaGraphExecDestroy(c.gexec);
     if (c.graph) cudaGraphDestroy(c.graph);
@@ -941,6 +942,27 @@ int aw_set_form_factor(aw_ctx* ctx, double ax, double ay, int32_t cic_order, dou
         AW_CUDA(cudaMemcpyAsync(c.ffac, s.data(), sizeof(double) * s.size(), cudaMemcpyHostToDevice, c.stream));
         AW_CUDA(cudaStreamSynchronize(c.stream));
         c.sg.ff = c.ffac;
+    });
+}
+
+int aw_checkpoint_write(aw_ctx* ctx, const char* path, const aw_checkpoint_info* info, int32_t wait) {
+    return guarded([&] {
+        aw::need(ctx && path && info, AW_ERR_ARG, "null argument");
+        aw::checkpoint_write(ctx->c, path, *info, wait != 0);
+    });
+}
+
+int aw_checkpoint_wait(aw_ctx* ctx) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::checkpoint_wait(ctx->c);
+    });
+}
+
+int aw_checkpoint_read(aw_ctx* ctx, const char* path, aw_checkpoint_info* out) {
+    return guarded([&] {
+        aw::need(ctx && path, AW_ERR_ARG, "null argument");
+        aw::checkpoint_read(ctx->c, path, out);
     });
 }
 

@@ -146,6 +146,9 @@ struct Ctx {
     // k-space form factor table (aw_set_form_factor), c.sg.ff points at it
     double* ffac = nullptr;
 
+    // checkpoint writer (aw_checkpoint.cu): snapshot buffer, pinned chunks, thread
+    struct CkWriter* ck = nullptr;
+
     // discrete adjoint of the ES step (aw_adjoint.cu; allocated by aw_grad_es)
     struct AdjWS* adj = nullptr;
     // Trajectory recording, set only while the adjoint's recording ES step is
@@ -287,6 +290,15 @@ void prepare_step(Ctx& c);
 // pending sources -> the fields the first particle kernel gathers; ES: the
 // whole solve), 1 (Darwin: dcu -> E_T, E), 2 (the end-of-step reduction).
 void step_grid_phase(Ctx& c, int phase);
+
+// ---- checkpoint / restart (aw_checkpoint.cu) ---------------------------------
+// Write (snapshot on the context's stream, then streamed to the file by a host
+// thread; wait = join it), join a write in flight, read back (the run then
+// continues bit for bit), free the writer (joins).
+void checkpoint_write(Ctx& c, const std::string& path, const aw_checkpoint_info& info, bool wait);
+void checkpoint_wait(Ctx& c);
+void checkpoint_read(Ctx& c, const std::string& path, aw_checkpoint_info* out);
+void free_checkpoint(Ctx& c);
 
 // ---- the ES adjoint (aw_adjoint.cu) ----------------------------------------
 AdjK adj_constants(const Ctx& c, float dt_scale);

@@ -201,6 +201,38 @@ int aw_resort(aw_ctx* ctx);
  * Default: 50 for the Darwin model, 0 for the electrostatic model, whose
  * reference path keeps the particle order. */
 int aw_set_resort(aw_ctx* ctx, int32_t every);
+/* ---- checkpoint / restart (include/pic/checkpoint.hpp:1-17, 31-49) ---------
+ * The reference's checkpoint file: its header (magic "ARCW", version 1, seed,
+ * step, time, S_d, eps_L), deck and git blocks and manifest, followed by the
+ * array payloads the reference defers: x y ux uy uz w (f32) and cell (i32, when
+ * bound), acc_src (u64: the pending fixed-point deposit), devstate (u64 words:
+ * this library's device state block) and the bound caller fields Ex..Bz (f32).
+ * The reference's checkpoint_read_header reads the header and manifest.
+ *
+ * aw_checkpoint_write snapshots the arrays on the context's stream (device to
+ * device) and streams the snapshot to `path` from a host thread; wait = 0
+ * returns after enqueuing the snapshot (the run may go on), aw_checkpoint_wait
+ * joins the write and reports its errors. One write at a time per context.
+ * info: step and time as the caller counts them (the next aw_run continues from
+ * step), rng_seed, sd, eps_l, and NUL-terminated deck and git texts (or NULL).
+ *
+ * aw_checkpoint_read restores a file written for a context of the same grid,
+ * model and particle count: every array's dtype and count must match. Then
+ * aw_run(ctx, info.step, ...) continues the saved run bit for bit. `out` (may
+ * be NULL) gets seed, step, time, sd, eps_l (deck and git_hash set to NULL). */
+typedef struct aw_checkpoint_info {
+    uint64_t    rng_seed;
+    int64_t     step;
+    double      time;
+    double      sd;
+    double      eps_l;
+    const char* deck;
+    const char* git_hash;
+} aw_checkpoint_info;
+int aw_checkpoint_write(aw_ctx* ctx, const char* path, const aw_checkpoint_info* info, int32_t wait);
+int aw_checkpoint_wait(aw_ctx* ctx);
+int aw_checkpoint_read(aw_ctx* ctx, const char* path, aw_checkpoint_info* out);
+
 /* k-space form factor (SpectralFormFactor::smoothing, include/pic/spectral.hpp:
  * 63-99, whose RunParams knobs ax, ay, k_filter (include/pic/config.hpp:281-283)
  * the reference documents but never reads: its smoothing is 1). Every Green's
