@@ -8,6 +8,7 @@
 //
 // Everything here calls the reference's public C++ API unchanged:
 // Simulation<Cfg>/Simulation<CfgDarwin> (include/pic/simulation.hpp),
+// MaxwellSimulation (include/pic/simulation_maxwell.hpp: the Yee branch),
 // Particles::initialize / sort_by_tile / build_tile_bins (particles.hpp),
 // Depositor<Cfg> (depositor.hpp), Pusher<Cfg> (pusher.hpp), the spectral solvers
 // (solver_es.hpp, solver_darwin.hpp) and add_background_b0/add_pump_field (pump.hpp).
@@ -20,6 +21,7 @@
 #include "pic/pump.hpp"
 #include "pic/pusher.hpp"
 #include "pic/simulation.hpp"
+#include "pic/simulation_maxwell.hpp"
 #include "pic/solver_darwin.hpp"
 #include "pic/solver_es.hpp"
 #include "pic/sources.hpp"
@@ -405,3 +407,92 @@ extern "C" int ref_bins(int physical, int nx, int ny, double Lx, double Ly, long
     });
 }
 
+
+// ---- the Yee branch (MaxwellSimulation, include/pic/simulation_maxwell.hpp) ----
+// Particles from host arrays (cell recomputed by Particles::migrate); fields
+// start at zero as the reference's YeeFields do. tile_sort = 0: the flat
+// push + Esirkepov + migrate path; > 0: the tiled path with a physical sort
+// every tile_sort steps.
+struct RefYee {
+    Grid g;
+    RunParams rp;
+    MaxwellSimulation* sim = nullptr;
+    ~RefYee() { delete sim; }
+};
+
+extern "C" void* ref_yee_create(int nx, int ny, double Lx, double Ly, const ref_params* p, int tile_sort, long n,
+                                const float* x, const float* y, const float* ux, const float* uy, const float* uz,
+                                const float* w) {
+    RefYee* h = nullptr;
+    int rc = guard([&] {
+        h = new RefYee();
+        h->g = Grid(nx, ny, Lx, Ly);
+        h->rp = make_rp(p, 0, 0);
+        h->rp.tile_sort = tile_sort;
+        h->sim = new MaxwellSimulation(h->g, h->rp);
+        Particles& P = h->sim->particles();
+        P.allocate_n(static_cast<std::size_t>(n));
+        const size_t b = static_cast<size_t>(n) * sizeof(float);
+        CUDA_CHECK(cudaMemcpy(P.x.data(), x, b, cudaMemcpyHostToDevice));
+        CUDA_CHECK(cudaMemcpy(P.y.data(), y, b, cudaMemcpyHostToDevice));
+        CUDA_CHECK(cudaMemcpy(P.ux.data(), ux, b, cudaMemcpyHostToDevice));
+        CUDA_CHECK(cudaMemcpy(P.uy.data(), uy, b, cudaMemcpyHostToDevice));
+        CUDA_CHECK(cudaMemcpy(P.uz.data(), uz, b, cudaMemcpyHostToDevice));
+        CUDA_CHECK(cudaMemcpy(P.w.data(), w, b, cudaMemcpyHostToDevice));
+        P.migrate(h->g, h->sim->stream());
+        h->sim->stream().synchronize();
+    });
+    if (rc) { delete h; return nullptr; }
+    return h;
+}
+extern "C" void ref_yee_destroy(void* hv) { delete static_cast<RefYee*>(hv); }
+
+extern "C" int ref_yee_step(void* hv, long nsteps) {
+    return guard([&] {
+        RefYee* h = static_cast<RefYee*>(hv);
+        for (long i = 0; i < nsteps; ++i) h->sim->step();
+        h->sim->stream().synchronize();
+    });
+}
+
+extern "C" int ref_yee_time_steps(void* hv, long nsteps, float* ms) {
+    return guard([&] {
+        RefYee* h = static_cast<RefYee*>(hv);
+        h->sim->stream().synchronize();
+        CudaEvent a, b;
+        a.record(h->sim->stream());
+        for (long i = 0; i < nsteps; ++i) h->sim->step();
+        b.record(h->sim->stream());
+        b.synchronize();
+        *ms = b.elapsed_ms_since(a);
+    });
+}
+
+extern "C" int ref_yee_get(void* hv, const char* name, void* host) {
+    int out = 0;
+    int rc = guard([&] {
+        RefYee* h = static_cast<RefYee*>(hv);
+        h->sim->stream().synchronize();
+        Particles& P = h->sim->particles();
+        YeeFields& F = h->sim->fields();
+        const size_t n = P.n, nc = static_cast<size_t>(h->g.real_size());
+        const std::string s(name);
+        if (s == "x") out = copy_down(P.x.data(), host, n * 4);
+        else if (s == "y") out = copy_down(P.y.data(), host, n * 4);
+        else if (s == "ux") out = copy_down(P.ux.data(), host, n * 4);
+        else if (s == "uy") out = copy_down(P.uy.data(), host, n * 4);
+        else if (s == "uz") out = copy_down(P.uz.data(), host, n * 4);
+        else if (s == "w") out = copy_down(P.w.data(), host, n * 4);
+        else if (s == "Ex") out = copy_down(F.ex_.data(), host, nc * 4);
+        else if (s == "Ey") out = copy_down(F.ey_.data(), host, nc * 4);
+        else if (s == "Ez") out = copy_down(F.ez_.data(), host, nc * 4);
+        else if (s == "Bx") out = copy_down(F.bx_.data(), host, nc * 4);
+        else if (s == "By") out = copy_down(F.by_.data(), host, nc * 4);
+        else if (s == "Bz") out = copy_down(F.bz_.data(), host, nc * 4);
+        else if (s == "Jx") out = copy_down(F.jx_.data(), host, nc * 4);
+        else if (s == "Jy") out = copy_down(F.jy_.data(), host, nc * 4);
+        else if (s == "Jz") out = copy_down(F.jz_.data(), host, nc * 4);
+        else out = -3;
+    });
+    return rc ? rc : out;
+}

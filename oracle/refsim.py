@@ -57,6 +57,13 @@ def lib():
         L.ref_push.argtypes = [I, I, I, D, D, C.POINTER(RefParams), L_] + [P] * 7 + [I]
         L.ref_solve.argtypes = [I, I, I, D, D, C.POINTER(RefParams), P, P]
         L.ref_bins.argtypes = [I, I, I, D, D, L_, P, P, I, I, P, P]
+        L.ref_yee_create.restype = P
+        L.ref_yee_create.argtypes = [I, I, D, D, C.POINTER(RefParams), I, L_] + [P] * 6
+        L.ref_yee_destroy.argtypes = [P]
+        L.ref_yee_destroy.restype = None
+        L.ref_yee_step.argtypes = [P, L_]
+        L.ref_yee_time_steps.argtypes = [P, L_, C.POINTER(C.c_float)]
+        L.ref_yee_get.argtypes = [P, C.c_char_p, P]
         L.ref_last_error.restype = C.c_char_p
         _lib = L
     return _lib
@@ -203,3 +210,35 @@ def bins(physical, nx, ny, Lx, Ly, x, y, tx=16, ty=16):
     _chk(lib().ref_bins(int(physical), nx, ny, Lx, Ly, len(x), _p(np.ascontiguousarray(x, np.float32)),
                         _p(np.ascontiguousarray(y, np.float32)), tx, ty, _p(off), _p(out)))
     return off, out
+
+
+class RefYee:
+    """The reference's MaxwellSimulation (the Yee branch) on host-given particles."""
+
+    def __init__(self, nx, ny, Lx, Ly, prm, parts, tile_sort=0):
+        self.nx, self.ny = nx, ny
+        self.n = len(parts["x"])
+        arrs = [np.ascontiguousarray(parts[k], np.float32) for k in ("x", "y", "ux", "uy", "uz", "w")]
+        self.h = lib().ref_yee_create(nx, ny, Lx, Ly, C.byref(prm), tile_sort, self.n,
+                                      *(a.ctypes.data_as(C.c_void_p) for a in arrs))
+        if not self.h:
+            raise RuntimeError(lib().ref_last_error().decode())
+
+    def step(self, nsteps=1):
+        _chk(lib().ref_yee_step(self.h, nsteps))
+
+    def time_steps(self, nsteps) -> float:
+        ms = C.c_float()
+        _chk(lib().ref_yee_time_steps(self.h, nsteps, C.byref(ms)))
+        return ms.value
+
+    def get(self, name):
+        n = self.n if name in ("x", "y", "ux", "uy", "uz", "w") else self.nx * self.ny
+        out = np.empty(n, np.float32)
+        _chk(lib().ref_yee_get(self.h, name.encode(), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def close(self):
+        if self.h:
+            lib().ref_yee_destroy(self.h)
+            self.h = None
