@@ -17,7 +17,7 @@ _PKG = Path(__file__).resolve().parent
 LIB_PATH = _PKG / "libarcb200.so"
 
 AW_OK, AW_ERR_ARG, AW_ERR_CUDA, AW_ERR_CUFFT, AW_ERR_STATE, AW_ERR_DEVICE, AW_ERR_NOMEM = 0, -1, -2, -3, -4, -5, -6
-AW_MODEL_ES, AW_MODEL_DARWIN = 0, 1
+AW_MODEL_ES, AW_MODEL_DARWIN, AW_MODEL_YEE = 0, 1, 2
 AW_DEV_NONFINITE, AW_DEV_OUT_OF_GRID, AW_DEV_WAIT_LIMIT = 1, 2, 4
 
 

@@ -109,7 +109,9 @@ void reset_acc(Ctx& c, unsigned long long* acc, int nf) {
 // ---- the step body (no host syncs; capturable) --------------------------------
 // A step is a fixed list of phases; `mark(i)` runs after phase i (used by
 // aw_step_profile to record CUDA events between phases).
-constexpr int kPhasesES = 7, kPhasesDarwin = 13;
+constexpr int kPhasesES = 7, kPhasesDarwin = 13, kPhasesYee = 5;
+const char* const kPhaseNamesYee[kPhasesYee] = {"faraday_half", "push_esirkepov", "faraday_half2", "ampere",
+                                                "step_reduce"};
 const char* const kPhaseNamesES[kPhasesES] = {
     "finalize_rho", "fft_r2c_rho", "kspace_es", "fft_c2r_e", "fields_es", "push_deposit_es", "step_reduce"};
 const char* const kPhaseNamesDarwin[kPhasesDarwin] = {
@@ -160,6 +162,15 @@ void darwin_fields_from_pending(Ctx& c, bool step_begin) { darwin_fields_from_pe
 
 template <class Mark>
 void step_body(Ctx& c, Mark mark) {
+    if (c.model == AW_MODEL_YEE) {
+        // MaxwellSimulation::step_at (simulation_maxwell.hpp:52-110), periodic set
+        launch_yee_faraday(c, true); mark(0);
+        launch_push_esirkepov(c); mark(1);
+        launch_yee_faraday(c, false); mark(2);
+        launch_yee_ampere(c); mark(3);
+        launch_step_reduce(c); mark(4);
+        return;
+    }
     if (c.model == AW_MODEL_ES) {
         es_fields_from_pending(c, true, mark);
         launch_push_deposit_es(c); mark(5);
@@ -173,10 +184,10 @@ void step_body(Ctx& c, Mark mark) {
 void step_body(Ctx& c) { step_body(c, NoMark{}); }
 
 // Kernels of this library one fused step launches (cuFFT's own not counted).
-int kernels_per_step(const Ctx& c) { return c.model == AW_MODEL_ES ? 5 : 9; }
+int kernels_per_step(const Ctx& c) { return c.model == AW_MODEL_DARWIN ? 9 : 5; }
 
 void ensure_pending(Ctx& c) {
-    if (c.pending_valid) return;
+    if (c.pending_valid || c.model == AW_MODEL_YEE) return;    // the Yee step deposits inside itself
     // scales S_pend / S_next were set by aw_init or the last unfused deposit
     launch_deposit_src(c, c.model == AW_MODEL_ES ? 1 : 8);
     c.pending_valid = true;
@@ -203,7 +214,9 @@ void init_impl(Ctx& c) {
     aw::launch_copy_umax(c);     // the step-begin copies umax -> ucur
     aw::launch_make_scales(c);
     aw::reset_acc(c, c.acc_src, c.nsrc());
-    if (c.model == AW_MODEL_ES) {
+    if (c.model == AW_MODEL_YEE) {
+        // the Yee lattices are the caller's (the reference's YeeFields start at zero)
+    } else if (c.model == AW_MODEL_ES) {
         aw::launch_deposit_src(c, 1);
         aw::es_fields_from_pending(c, false);
         // u -> u(-dt/2), gathering E(x^0) from the solve's output
@@ -419,7 +432,8 @@ int aw_ctx_create(const aw_grid* g, const aw_params* p, int32_t model, void* str
     return guarded([&] {
         aw::need(g && p && out, AW_ERR_ARG, "ctx_create: null argument");
         aw::need(g->nx > 0 && g->ny > 0 && g->Lx > 0 && g->Ly > 0, AW_ERR_ARG, "ctx_create: bad grid");
-        aw::need(model == AW_MODEL_ES || model == AW_MODEL_DARWIN, AW_ERR_ARG, "ctx_create: bad model");
+        aw::need(model == AW_MODEL_ES || model == AW_MODEL_DARWIN || model == AW_MODEL_YEE, AW_ERR_ARG,
+                 "ctx_create: bad model");
         aw::need(static_cast<long long>(g->nx) * g->ny <= (1LL << 28), AW_ERR_ARG, "ctx_create: grid too large");
         *out = nullptr;
         std::unique_ptr<aw_ctx> h(new aw_ctx());
@@ -1000,7 +1014,8 @@ int aw_step_profile(aw_ctx* ctx, int64_t n, float* ms, int32_t cap, int32_t* nph
         aw::need(ctx && ms && nphase, AW_ERR_ARG, "null argument");
         Ctx& c = ctx->c;
         aw::require_parts(c);
-        const int np = c.model == AW_MODEL_ES ? aw::kPhasesES : aw::kPhasesDarwin;
+        const int np = c.model == AW_MODEL_ES ? aw::kPhasesES
+                       : c.model == AW_MODEL_YEE ? aw::kPhasesYee : aw::kPhasesDarwin;
         aw::need(cap >= np, AW_ERR_ARG, "step_profile: ms array too small");
         aw::ensure_pending(c);
         aw::launch_set_step(c, n);
@@ -1022,6 +1037,7 @@ int aw_step_profile(aw_ctx* ctx, int64_t n, float* ms, int32_t cap, int32_t* nph
 
 const char* aw_step_phase_name(int32_t model, int32_t i) {
     if (model == AW_MODEL_ES) return (i >= 0 && i < aw::kPhasesES) ? aw::kPhaseNamesES[i] : "";
+    if (model == AW_MODEL_YEE) return (i >= 0 && i < aw::kPhasesYee) ? aw::kPhaseNamesYee[i] : "";
     return (i >= 0 && i < aw::kPhasesDarwin) ? aw::kPhaseNamesDarwin[i] : "";
 }
 

@@ -1076,6 +1076,299 @@ void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE
     AW_LAUNCH();
 }
 
+// ---- the Yee branch: fused staggered gather + Boris + Esirkepov current -------
+// k_push_esirkepov (yee2d.hpp:141-305, 307-389, the flat path of
+// MaxwellSimulation::step_at, simulation_maxwell.hpp:52-77, with the migrate
+// fused): per particle the staggered CIC gather of E (+ pump) and B (+ B0) from
+// the Yee lattices, the Boris kick-rotate-kick, the move, and the Esirkepov
+// current over the 4 x 4 union stencil, deposited exactly in int64 fixed point
+// on this window engine (3 fields: Jx at (i+1/2, j), Jy at (i, j+1/2), Jz at
+// (i, j); every contribution one rounded integer, so J does not depend on the
+// particle order). The float operations follow the reference's order (its
+// expressions, contracted the same way), so the per-particle contributions are
+// its float values before they are scaled.
+//
+// Scales: a contribution to Jx is -q w / (dt dy) times a prefix sum of shape
+// differences, bounded by the move |x1 - x0| in cells (the CIC shape is
+// 1-Lipschitz), so |Jx contribution| <= |q w| |ux| / (dx dy): the same bound
+// as the Darwin J deposit, S_x = scale for cm U_x (S_next[1..3], set at the step
+// begin from the |u| maxima). A particle whose bound exceeds the fast range
+// (it sped up past 1.25 x the previous maximum) takes the exact slow path.
+constexpr int kYeePlanes = 7, kYeeWindow = 576;
+struct YeeArgs {
+    Parts p; Geo g;
+    const float *ex, *ey, *ez, *bx, *by, *bz;   // Yee lattices [ny][nx]
+    float qmh, qm, invdt, dxp, dyp, b0x, b0y, b0z;
+    double dt, dxd, dyd;                      // dxd, dyd: the float cell sizes, widened
+    PumpP pump;
+    unsigned long long* acc; int wmaxc; double* part; DevState* st; int write_cell;
+};
+
+// node shape over {b - 1, .., b + 2}: S = max(0, 1 - |x - p|) (yee2d.hpp:124-130)
+__device__ __forceinline__ void yee_shape4(float x, int b, float (&S)[4]) {
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        const float d = fabsf(x - (float)(b - 1 + n));
+        S[n] = d < 1.f ? 1.f - d : 0.f;
+    }
+}
+
+// Staggered CIC gather (yee2d.hpp:103-112): component lattice offset (ox, oy).
+__device__ __forceinline__ float yee_gather(const float* __restrict__ a, const Geo& g, float x, float y,
+                                            float ox, float oy) {
+    const float xs = x - ox, ys = y - oy;
+    const int i0 = (int)floorf(xs), j0 = (int)floorf(ys);
+    const float fx = xs - i0, fy = ys - j0;
+    const int ia = wrap_once(i0, g.nx), ib = wrap_once(i0 + 1, g.nx);
+    const int ja = wrap_once(j0, g.ny) * g.nx, jb = wrap_once(j0 + 1, g.ny) * g.nx;
+    return (1.f - fx) * (1.f - fy) * __ldg(a + ja + ia)
+         +        fx  * (1.f - fy) * __ldg(a + ja + ib)
+         + (1.f - fx) *        fy  * __ldg(a + jb + ia)
+         +        fx  *        fy  * __ldg(a + jb + ib);
+}
+
+// The Esirkepov node weights of one move (yee2d.hpp:307-355, its operation
+// order): emit(f, ni, nj, w) for every nonzero weight of field f (0: the Jx
+// prefix sums, 1: the Jy prefix sums, 2: Jz) at node (ib - 1 + ni, jb - 1 + nj).
+template <class Emit>
+__device__ __forceinline__ void esirkepov_weights(float x0, float y0, float x1, float y1, int ib, int jb,
+                                                  Emit&& emit) {
+    float Sx0[4], Sx1[4], Sy0[4], Sy1[4];
+    yee_shape4(x0, ib, Sx0); yee_shape4(x1, ib, Sx1);
+    yee_shape4(y0, jb, Sy0); yee_shape4(y1, jb, Sy1);
+    float DSx[4], DSy[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) { DSx[n] = Sx1[n] - Sx0[n]; DSy[n] = Sy1[n] - Sy0[n]; }
+#pragma unroll
+    for (int nj = 0; nj < 4; ++nj) {
+        const float sy = Sy0[nj] + 0.5f * DSy[nj];
+        float a = 0.f;
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+            a += DSx[ni] * sy;
+            if (a != 0.f) emit(0, ni, nj, a);
+        }
+    }
+#pragma unroll
+    for (int ni = 0; ni < 4; ++ni) {
+        const float sx = Sx0[ni] + 0.5f * DSx[ni];
+        float a = 0.f;
+#pragma unroll
+        for (int nj = 0; nj < 4; ++nj) {
+            a += DSy[nj] * sx;
+            if (a != 0.f) emit(1, ni, nj, a);
+        }
+    }
+#pragma unroll
+    for (int nj = 0; nj < 4; ++nj)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+            const float wz = Sx0[ni] * Sy0[nj] + 0.5f * (DSx[ni] * Sy0[nj] + Sx0[ni] * DSy[nj])
+                           + (1.f / 3.f) * DSx[ni] * DSy[nj];
+            if (wz != 0.f) emit(2, ni, nj, wz);
+        }
+}
+
+__device__ __forceinline__ int wrap_node(int i, int n) {
+    i %= n;
+    return i < 0 ? i + n : i;
+}
+
+// Stage planes: 0 x0 (sign set: skipped, listed for the slow pass), 1 y0, 2 x1,
+// 3 y1 (unwrapped), 4..6 the scaled coefficients ax ay az.
+__device__ __forceinline__ void yee_window_pass(const float* __restrict__ stage, int* __restrict__ win,
+                                                const Win& wn, const Geo& g) {
+    if (!wn.use) return;
+    const int base = 64 * (threadIdx.x & 31) + 8 * (threadIdx.x >> 5);
+#pragma unroll 1
+    for (int k = 0; k < kPPT; ++k) {
+        const int d = stage_slot(base + k);
+        const float x0 = stage[d];
+        if (__float_as_int(x0) < 0) continue;
+        const float y0 = stage[kChunk + d], x1 = stage[2 * kChunk + d], y1 = stage[3 * kChunk + d];
+        const float a0 = stage[4 * kChunk + d], a1 = stage[5 * kChunk + d], a2 = stage[6 * kChunk + d];
+        const int ib = (int)floorf(fminf(x0, x1)), jb = (int)floorf(fminf(y0, y1));
+        const int ci = win_off(ib - 1, wn.ir, g.nx) - wn.mi, cj = win_off(jb - 1, wn.jr, g.ny) - wn.mj;
+        esirkepov_weights(x0, y0, x1, y1, ib, jb, [&](int f, int ni, int nj, float w) {
+            const int v = quant(f == 0 ? a0 : f == 1 ? a1 : a2, w);
+            int* e = win + 2 * f * wn.WH + (cj + nj) * wn.W + (ci + ni);
+            if (wn.track_all) add_tracked(e, wn.WH, v);
+            else atomicAdd(e, v);
+        });
+    }
+}
+
+// The exact slow path: the same rounded contributions (the double product of
+// two floats is exact), straight into the global int64 planes.
+__device__ __forceinline__ void yee_slow_pass(const float* __restrict__ stage, const unsigned short* __restrict__ list,
+                                              int nlist, bool all_slots, unsigned long long* __restrict__ gacc,
+                                              const Geo& g, DevState* st) {
+    const int total = nlist + (all_slots ? kChunk : 0);
+    unsigned n = 0;
+    for (int k = threadIdx.x; k < total; k += kThreads) {
+        const bool listed = k < nlist;
+        const int d = stage_slot(listed ? static_cast<int>(list[k]) : k - nlist);
+        float x0 = stage[d];
+        if (listed) x0 = -x0;
+        else if (__float_as_int(x0) < 0) continue;
+        const float y0 = stage[kChunk + d], x1 = stage[2 * kChunk + d], y1 = stage[3 * kChunk + d];
+        const float a0 = stage[4 * kChunk + d], a1 = stage[5 * kChunk + d], a2 = stage[6 * kChunk + d];
+        if (!(isfinite(a0) && isfinite(a1) && isfinite(a2) && isfinite(x1) && isfinite(y1))) {
+            set_err(st, 1u);                       // AW_DEV_NONFINITE
+            continue;
+        }
+        const int ib = (int)floorf(fminf(x0, x1)), jb = (int)floorf(fminf(y0, y1));
+        esirkepov_weights(x0, y0, x1, y1, ib, jb, [&](int f, int ni, int nj, float w) {
+            const float af = f == 0 ? a0 : f == 1 ? a1 : a2;
+            const long long v = __double2ll_rn(__dmul_rn(static_cast<double>(af), static_cast<double>(w)));
+            if (v != 0)
+                atomicAdd(gacc + static_cast<size_t>(f) * g.ncell +
+                              wrap_node(jb - 1 + nj, g.ny) * g.nx + wrap_node(ib - 1 + ni, g.nx),
+                          static_cast<unsigned long long>(v));
+        });
+        ++n;
+    }
+    if (n) atomicAdd(&st->slow, static_cast<unsigned long long>(n));
+}
+
+__device__ __forceinline__ double yee_ramp(double t, double trmp, double toff) {
+    if (t >= toff) return 0.0;
+    if (t < trmp) return t / trmp;
+    if (t > toff - trmp) return (toff - t) / trmp;
+    return 1.0;
+}
+
+__global__ void __launch_bounds__(kThreads, 3) k_push_esirkepov(YeeArgs A) {
+    const Parts& p = A.p; const Geo& g = A.g;
+    unsigned long long* __restrict__ acc = A.acc;
+    DevState* st = A.st;
+    constexpr int NF = 3, NIN = 5;              // stage in: x y ux uy uz (w read from global)
+    extern __shared__ __align__(16) unsigned char smem[];
+    const Smem m = carve(smem, kYeePlanes, NF, A.wmaxc);
+    __shared__ unsigned long long bar;
+    __shared__ int nlist;
+    __shared__ double dsh[4 * (kThreads / 32)];
+    __shared__ unsigned umx[3][kThreads / 32];
+
+    const int chunk = blockIdx.x;
+    const long long c0 = static_cast<long long>(chunk) * kChunk;
+    const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), p.n - c0));
+    const float S[3] = {st->S_next[1], st->S_next[2], st->S_next[3]};
+    const double tnow = st->t;
+    const bool pump = A.pump.on && tnow < A.pump.toff;
+    const double ramp = pump ? yee_ramp(tnow, A.pump.trmp, A.pump.toff) : 0.0;
+    if (threadIdx.x == 0) nlist = 0;
+    const ChunkSrc src{{p.x, p.y, p.ux, p.uy, p.uz, nullptr}};
+    float xr, yr;
+    if (!load_chunk(m.stage, src, NIN, c0, cnt, p.vec_ok != 0, &bar, st, &xr, &yr)) return;
+    int ir, jr;
+    ref_of(xr, yr, g, ir, jr);
+
+    BBox bb;
+    float l1[NF] = {};
+    double ke = 0, px = 0, py = 0, pz = 0;
+    float m0 = 0.f, m1 = 0.f, m2 = 0.f;
+#pragma unroll 1
+    for (int it = 0; it < kPPT; ++it) {
+        const int s = it * kThreads + threadIdx.x;
+        const long long i = c0 + s;
+        const float x0 = m.stage[s], y0 = m.stage[kChunk + s];
+        float ux = m.stage[2 * kChunk + s], uy = m.stage[3 * kChunk + s], uz = m.stage[4 * kChunk + s];
+        const float w = s < cnt ? __ldcs(p.w + i) : 0.0f;
+        float xs = -1.0f, x1 = 0.f, y1 = 0.f, ax = 0.f, ay = 0.f, az = 0.f;
+        if (s < cnt) {
+            if (in_grid(x0, y0, g)) {
+                float ex = yee_gather(A.ex, g, x0, y0, 0.5f, 0.f);
+                float ey = yee_gather(A.ey, g, x0, y0, 0.f, 0.5f);
+                float ez = yee_gather(A.ez, g, x0, y0, 0.f, 0.f);
+                if (pump) {
+                    const double th = A.pump.k0 * static_cast<double>(x0) * A.dxd - A.pump.w0 * tnow;
+                    ex += (float)(A.pump.ex * cos(th) * ramp);
+                    ey += (float)(-A.pump.ey * sin(th) * ramp);
+                    ez += (float)(A.pump.ez * cos(th) * ramp);
+                }
+                const float bx = yee_gather(A.bx, g, x0, y0, 0.f, 0.5f) + A.b0x;
+                const float by = yee_gather(A.by, g, x0, y0, 0.5f, 0.f) + A.b0y;
+                const float bz = yee_gather(A.bz, g, x0, y0, 0.5f, 0.5f) + A.b0z;
+                boris_em(ux, uy, uz, ex, ey, ez, bx, by, bz, A.qmh);
+                x1 = move1(x0, ux, A.dt, A.dxd);
+                y1 = move1(y0, uy, A.dt, A.dyd);
+                const float xw = wrap_pos(x1, g.nxf), yw = wrap_pos(y1, g.nyf);
+                __stcs(p.x + i, xw); __stcs(p.y + i, yw); __stcs(p.ux + i, ux); __stcs(p.uy + i, uy);
+                __stcs(p.uz + i, uz);
+                if (A.write_cell && p.cell) {
+                    int ci, cj;
+                    cell_ij(xw, yw, g, ci, cj);
+                    __stcs(p.cell + i, cj * g.nx + ci);
+                }
+                m0 = fmaxf(m0, fabsf(ux)); m1 = fmaxf(m1, fabsf(uy)); m2 = fmaxf(m2, fabsf(uz));
+                // coefficients: cJx = -q w / (dt dy), cJy = -q w / (dt dx), cJz = q w vz / (dx dy)
+                const float qw = A.qm * w;
+                ax = __fmul_rn(-qw * A.invdt / A.dyp, S[0]);
+                ay = __fmul_rn(-qw * A.invdt / A.dxp, S[1]);
+                az = __fmul_rn(qw * uz / (A.dxp * A.dyp), S[2]);
+                const int ib = (int)floorf(fminf(x0, x1)), jb = (int)floorf(fminf(y0, y1));
+                bb.add(ib - 1, jb - 1, ir, jr, g);         // the stencil's base node (the box adds 4)
+                // per-node bound of each field's contributions (prefix sums <= the move)
+                const float tx = fabsf(ax) * (fabsf(x1 - x0) * 1.001f + 1e-6f);
+                const float ty = fabsf(ay) * (fabsf(y1 - y0) * 1.001f + 1e-6f);
+                const float tz = fabsf(az) * 1.001f;
+                xs = x0;
+                if (tx < 4194304.0f && ty < 4194304.0f && tz < 4194304.0f) {
+                    l1[0] += tx; l1[1] += ty; l1[2] += tz;
+                } else {
+                    xs = -x0;
+                    list_slow(m.slow, &nlist, s);
+                }
+                const double dw = w, du = ux, dv = uy, dz = uz;
+                ke += dw * (du * du + dv * dv + dz * dz);
+                px += dw * du; py += dw * dv; pz += dw * dz;
+            } else {
+                set_err(st, AW_DEV_OUT_OF_GRID);
+            }
+        }
+        __syncwarp();
+        const int d = stage_slot(s);
+        m.stage[d] = xs;
+        m.stage[kChunk + d] = y0;
+        m.stage[2 * kChunk + d] = x1;
+        m.stage[3 * kChunk + d] = y1;
+        m.stage[4 * kChunk + d] = ax;
+        m.stage[5 * kChunk + d] = ay;
+        m.stage[6 * kChunk + d] = az;
+    }
+    m0 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m0)));
+    m1 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m1)));
+    m2 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m2)));
+    if ((threadIdx.x & 31) == 0) {
+        umx[0][threadIdx.x >> 5] = __float_as_uint(m0);
+        umx[1][threadIdx.x >> 5] = __float_as_uint(m1);
+        umx[2][threadIdx.x >> 5] = __float_as_uint(m2);
+    }
+    // the window of the nodes every move touches (4 x 4 stencils)
+    // base offsets lo..hi, nodes to hi + 3: win_setup sizes W = hi - lo + 2, so pass hi + 2
+    Win wn;
+    win_setup<NF, false>(wn, bb.lo_i, bb.lo_j, bb.hi_i + 2, bb.hi_j + 2, ir, jr, A.wmaxc, m.red, l1);
+    if (wn.nb > 1) { wn.use = false; wn.WH = 0; }     // no bands on this path: the slow path takes the chunk
+    win_zero<NF>(m.win, wn);
+    if (threadIdx.x < 3) {
+        unsigned mx = 0;
+        for (int k = 0; k < kThreads / 32; ++k) mx = max(mx, umx[threadIdx.x][k]);
+        atomicMax(&st->umax_bits[threadIdx.x], mx);
+    }
+    __syncthreads();
+    yee_window_pass(m.stage, m.win, wn, g);
+    __syncthreads();
+    win_flush<NF, false>(m.win, wn, acc, g);
+    yee_slow_pass(m.stage, m.slow, nlist, !wn.use, acc, g, st);
+    if (threadIdx.x == 0) {
+        atomicAdd(&st->chunks, 1ull);
+        if (!wn.use) atomicAdd(&st->overflow, 1ull);
+    }
+    block_sum4(ke, px, py, pz, A.part, dsh, chunk);
+    if (threadIdx.x == 0 && chunk == 0) st->step += 1;
+}
+
 // ---- multi-run particle phases -----------------------------------------------
 struct MultiPhase {
     int kind = 0, nruns = 0, nblocks = 0;
@@ -1171,6 +1464,30 @@ void launch_push_deposit_es(Ctx& c) {
                    : (rec ? k_push_deposit_es<false, true> : k_push_deposit_es<false, false>);
     prep_smem(kern, sh);
     kern<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(es_args(c));
+    AW_LAUNCH();
+}
+
+void launch_push_esirkepov(Ctx& c) {
+    if (c.parts.n == 0) return;
+    need(c.fld.Ex && c.fld.Ey && c.fld.Ez && c.fld.Bx && c.fld.By && c.fld.Bz, AW_ERR_STATE,
+         "Yee step: bind the six field arrays (the Yee lattices)");
+    YeeArgs a{};
+    a.p = c.parts; a.g = c.geo;
+    a.ex = c.fld.Ex; a.ey = c.fld.Ey; a.ez = c.fld.Ez; a.bx = c.fld.Bx; a.by = c.fld.By; a.bz = c.fld.Bz;
+    a.qmh = static_cast<float>(c.prm.qm * 0.5 * c.prm.dt);
+    a.qm = static_cast<float>(c.prm.qm);
+    a.invdt = static_cast<float>(1.0 / c.prm.dt);
+    a.dxp = static_cast<float>(c.geo.dx); a.dyp = static_cast<float>(c.geo.dy);
+    a.b0x = c.prm.B0[0]; a.b0y = c.prm.B0[1]; a.b0z = c.prm.B0[2];
+    a.dt = c.prm.dt;
+    a.dxd = static_cast<double>(a.dxp); a.dyd = static_cast<double>(a.dyp);
+    a.pump.on = c.prm.pump;
+    a.pump.ex = c.prm.pump_ex; a.pump.ey = c.prm.pump_ey; a.pump.ez = c.prm.pump_ez;
+    a.pump.k0 = c.prm.pump_k0; a.pump.w0 = c.prm.pump_w0; a.pump.trmp = c.prm.pump_trmp; a.pump.toff = c.prm.pump_toff;
+    a.acc = c.acc_src; a.wmaxc = kYeeWindow; a.part = c.part_p; a.st = c.st; a.write_cell = c.write_cell;
+    const size_t sh = smem_bytes_w(3, kYeePlanes, kYeeWindow);
+    prep_smem(k_push_esirkepov, sh);
+    k_push_esirkepov<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(a);
     AW_LAUNCH();
 }
 

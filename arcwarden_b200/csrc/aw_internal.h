@@ -158,7 +158,7 @@ struct Ctx {
     float* rec_xy = nullptr;
     float* rec_E = nullptr;
 
-    int nsrc() const { return model == AW_MODEL_DARWIN ? 8 : 1; }
+    int nsrc() const { return model == AW_MODEL_DARWIN ? 8 : model == AW_MODEL_YEE ? 3 : 1; }
     int nout() const { return model == AW_MODEL_DARWIN ? 5 : 2; }
 };
 
@@ -239,6 +239,8 @@ void launch_deposit_src(Ctx& c, int which);
 void launch_deposit_dcu(Ctx& c, const float* gb, bool fused);
 void launch_push_deposit_es(Ctx& c);
 void launch_push_deposit_em(Ctx& c);
+// The Yee branch's fused particle kernel (gather, Boris, move, Esirkepov current).
+void launch_push_esirkepov(Ctx& c);
 // Backward step A of the ES adjoint: Boris/move transposes, field-cotangent
 // scatter into acc [2][ncell] (scales from ad->lmax_bits, stored to ad->S) and
 // the E-gather position derivative (E = interleaved [ncell][2]); errors and
@@ -279,6 +281,8 @@ void launch_copy_umax(Ctx& c);
 void launch_promote_scales(Ctx& c);                // S_pend = S_next
 void launch_rms_reduce(Ctx& c, bool src, bool dcu);
 void launch_step_reduce(Ctx& c);                   // end of a fused step: diagnostics (+ rms for Darwin)
+void launch_yee_faraday(Ctx& c, bool begin);       // Yee: B half step (begin: the step's device state)
+void launch_yee_ampere(Ctx& c);                    // Yee: E full step with the step's current
 
 // ---- step graph (aw_abi.cu) ------------------------------------------------
 // The fused step body captured into a graph on the context's stream (pending

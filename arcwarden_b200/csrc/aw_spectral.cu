@@ -713,6 +713,93 @@ PumpArgs pump_of(const Ctx& c) {
 }
 float cref_of(const Ctx& c) { return c.model == AW_MODEL_DARWIN ? static_cast<float>(c.prm.c) : 1.0f; }
 
+
+// ---- the Yee branch: field updates (yee2d.hpp:67-97) ------------------------------
+// Lattices [ny][nx] (yee2d.hpp:8-11): Ex(i+1/2, j), Ey(i, j+1/2), Ez(i, j),
+// Bx(i, j+1/2), By(i+1/2, j), Bz(i+1/2, j+1/2); periodic; eps0 = 1. The float
+// expressions are the reference's, in its order.
+struct YeeF {
+    float *ex, *ey, *ez, *bx, *by, *bz;
+    int nx, ny;
+    float dxp, dyp, c2, dt;
+};
+__device__ __forceinline__ int yee_idx(int i, int j, int nx, int ny) {
+    i += (i < 0) * nx - (i >= nx) * nx;
+    j += (j < 0) * ny - (j >= ny) * ny;
+    return j * nx + i;
+}
+
+// B half step B -= dt2 curl E (k_faraday). With `begin` (the first launch of
+// a step) one thread also opens the step: t = step dt; the |u| maxima the last
+// push wrote become the current state's; the current scales S_next[1..3] =
+// scale for cm U_d, U_d = max(1.25 |u_d|max, 0.01 c) (the J bound of the
+// Darwin deposit: |Jx contribution| <= |q w ux| / (dx dy)).
+__global__ void k_yee_faraday(YeeF v, float dt2, DevState* st, int begin, double dt, float cref) {
+    const int n = v.nx * v.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int i = c % v.nx, j = c / v.nx;
+        const float ez_xp = v.ez[yee_idx(i + 1, j, v.nx, v.ny)], ez_yp = v.ez[yee_idx(i, j + 1, v.nx, v.ny)];
+        const float ex_yp = v.ex[yee_idx(i, j + 1, v.nx, v.ny)];
+        const float ey_xp = v.ey[yee_idx(i + 1, j, v.nx, v.ny)];
+        v.bx[c] -= dt2 * (ez_yp - v.ez[c]) / v.dyp;
+        v.by[c] += dt2 * (ez_xp - v.ez[c]) / v.dxp;
+        v.bz[c] -= dt2 * ((ey_xp - v.ey[c]) / v.dxp - (ex_yp - v.ex[c]) / v.dyp);
+    }
+    if (begin && blockIdx.x == 0 && threadIdx.x == 0) {
+        st->t = static_cast<double>(st->step) * dt;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { st->ucur_bits[d] = st->umax_bits[d]; st->umax_bits[d] = 0u; }
+        st->red_ticket = 0u;
+        const float cm = st->coef_max;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const float U = fmaxf(__fmul_rn(1.25f, __uint_as_float(st->ucur_bits[d])), __fmul_rn(0.01f, cref));
+            st->S_next[1 + d] = scale_for_bound(__fmul_rn(cm, U));
+        }
+    }
+}
+
+// E full step E += dt (c^2 curl B - J) (k_ampere), J = the step's exact current
+// acc [3][ncell] / S_next[1..3] (the accumulator is zeroed for the next step and
+// J written to the caller's source arrays when bound); field-energy partials
+// (sum |E|^2, max |E|^2, sum |B|^2 of the wave field) for the step reduction.
+__global__ void k_yee_ampere(YeeF v, unsigned long long* __restrict__ acc, const DevState* st,
+                             float* jx_api, float* jy_api, float* jz_api, double* __restrict__ part) {
+    const int n = v.nx * v.ny;
+    const double ix = 1.0 / static_cast<double>(st->S_next[1]);
+    const double iy = 1.0 / static_cast<double>(st->S_next[2]);
+    const double iz = 1.0 / static_cast<double>(st->S_next[3]);
+    double se2 = 0.0, me2 = 0.0, sb2 = 0.0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const long long ax = static_cast<long long>(acc[c]);
+        const long long ay = static_cast<long long>(acc[n + c]);
+        const long long az = static_cast<long long>(acc[2 * n + c]);
+        acc[c] = 0ull; acc[n + c] = 0ull; acc[2 * n + c] = 0ull;
+        const float jx = __double2float_rn(static_cast<double>(ax) * ix);
+        const float jy = __double2float_rn(static_cast<double>(ay) * iy);
+        const float jz = __double2float_rn(static_cast<double>(az) * iz);
+        if (jx_api) jx_api[c] = jx;
+        if (jy_api) jy_api[c] = jy;
+        if (jz_api) jz_api[c] = jz;
+        const int i = c % v.nx, j = c / v.nx;
+        const float bz_ym = v.bz[yee_idx(i, j - 1, v.nx, v.ny)];
+        const float bz_xm = v.bz[yee_idx(i - 1, j, v.nx, v.ny)];
+        const float bx_ym = v.bx[yee_idx(i, j - 1, v.nx, v.ny)];
+        const float by_xm = v.by[yee_idx(i - 1, j, v.nx, v.ny)];
+        v.ex[c] += v.dt * ( v.c2 * (v.bz[c] - bz_ym) / v.dyp - jx);
+        v.ey[c] += v.dt * (-v.c2 * (v.bz[c] - bz_xm) / v.dxp - jy);
+        v.ez[c] += v.dt * ( v.c2 * ((v.by[c] - by_xm) / v.dxp
+                                  - (v.bx[c] - bx_ym) / v.dyp) - jz);
+        const double e2 = static_cast<double>(v.ex[c]) * v.ex[c] + static_cast<double>(v.ey[c]) * v.ey[c] +
+                          static_cast<double>(v.ez[c]) * v.ez[c];
+        se2 += e2;
+        me2 = fmax(me2, e2);
+        sb2 += static_cast<double>(v.bx[c]) * v.bx[c] + static_cast<double>(v.by[c]) * v.by[c] +
+               static_cast<double>(v.bz[c]) * v.bz[c];
+    }
+    grid_partials(se2, me2, sb2, part);
+}
+
 }  // namespace
 
 int grid_partial_blocks() { return kGridBlocks; }
@@ -773,6 +860,28 @@ void launch_fields_dcu(Ctx& c) {
     k_fields_dcu<<<kGridBlocks, kThreads, 0, c.stream>>>(c.r_out, c.gb_dcu, api_of(c.fld), c.geo.nx,
                                                          c.geo.ncell, c.prm.B0[0], c.prm.B0[1],
                                                          c.prm.B0[2], pump_of(c), c.st);
+    AW_LAUNCH();
+}
+YeeF yee_views(const Ctx& c) {
+    need(c.fld.Ex && c.fld.Ey && c.fld.Ez && c.fld.Bx && c.fld.By && c.fld.Bz, AW_ERR_STATE,
+         "Yee step: bind the six field arrays (the Yee lattices)");
+    YeeF v{};
+    v.ex = c.fld.Ex; v.ey = c.fld.Ey; v.ez = c.fld.Ez; v.bx = c.fld.Bx; v.by = c.fld.By; v.bz = c.fld.Bz;
+    v.nx = c.geo.nx; v.ny = c.geo.ny;
+    v.dxp = static_cast<float>(c.geo.dx); v.dyp = static_cast<float>(c.geo.dy);
+    v.c2 = static_cast<float>(c.prm.c * c.prm.c);
+    v.dt = static_cast<float>(c.prm.dt);
+    return v;
+}
+void launch_yee_faraday(Ctx& c, bool begin) {
+    const float dt2 = 0.5f * static_cast<float>(c.prm.dt);
+    k_yee_faraday<<<kGridBlocks, kThreads, 0, c.stream>>>(yee_views(c), dt2, c.st, begin ? 1 : 0, c.prm.dt,
+                                                          static_cast<float>(c.prm.c));
+    AW_LAUNCH();
+}
+void launch_yee_ampere(Ctx& c) {
+    k_yee_ampere<<<kGridBlocks, kThreads, 0, c.stream>>>(yee_views(c), c.acc_src, c.st, c.src.Jx, c.src.Jy,
+                                                         c.src.Jz, c.part_g);
     AW_LAUNCH();
 }
 void launch_fields_push(Ctx& c) {

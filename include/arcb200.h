@@ -52,7 +52,19 @@ enum {
 };
 
 /* Field models (include/pic/config.hpp:72, FieldModel). */
-enum { AW_MODEL_ES = 0, AW_MODEL_DARWIN = 1 };
+/* AW_MODEL_YEE: the full-Maxwell Yee branch (MaxwellSimulation,
+ * include/pic/simulation_maxwell.hpp:52-110, periodic: no delta-f, no
+ * relativistic push, uniform B0, no absorbing layers or antenna). Its E and B
+ * are the caller's six bound field arrays, on the Yee lattices (yee2d.hpp:8-11:
+ * Ex(i+1/2, j), Ey(i, j+1/2), Ez(i, j), Bx(i, j+1/2), By(i+1/2, j),
+ * Bz(i+1/2, j+1/2)), advanced in place; aw_init leaves them as they are (the
+ * reference's YeeFields start at zero). A step: B half step, the fused
+ * staggered gather + Boris + Esirkepov current deposit (exact int64 fixed
+ * point), B half step, E full step; the step's current goes to the bound
+ * sources Jx, Jy, Jz when bound. aw_diag: ee = 1/2 eps0 sum |E|^2 dx dy (all
+ * three components), eb = 1/2 sum |B|^2 dx dy (the wave field), max_e over
+ * |E|, charge 0. */
+enum { AW_MODEL_ES = 0, AW_MODEL_DARWIN = 1, AW_MODEL_YEE = 2 };
 
 /* ---- POD descriptions ---------------------------------------------------- */
 
@@ -273,7 +285,7 @@ int aw_grad_es(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux
  * another. Each run gives the same bits as the same run alone. */
 #define AW_ENSEMBLE_MAX_SPECIES 4
 typedef struct aw_run_spec {
-    int32_t    model;          /* AW_MODEL_ES or AW_MODEL_DARWIN                */
+    int32_t    model;          /* AW_MODEL_ES or AW_MODEL_DARWIN (ensembles)    */
     aw_grid    grid;
     aw_params  params;
     int32_t    nspecies;       /* 1 .. AW_ENSEMBLE_MAX_SPECIES                  */
