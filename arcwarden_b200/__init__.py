@@ -96,7 +96,7 @@ SIGNATURES = {
     "aw_fields_bind": [_P, C.POINTER(FieldPtrs)],
     "aw_load_species": [_P, C.POINTER(Species), _I32, _U64, _I32],
     "aw_resort": [_P], "aw_set_resort": [_P, _I32],
-    "aw_set_form_factor": [_P, _D, _D, _I32, _D],
+    "aw_set_form_factor": [_P, _D, _D, _I32, _D], "aw_set_current_filter": [_P, _I32],
     "aw_checkpoint_write": [_P, C.c_char_p, C.POINTER(CheckpointInfo), _I32], "aw_checkpoint_wait": [_P],
     "aw_checkpoint_read": [_P, C.c_char_p, C.POINTER(CheckpointInfo)],
     "aw_grad_es": [_P, _I64, _I32, _P, _P, _P, C.POINTER(_D)],
@@ -256,6 +256,10 @@ class Context:
         * [sinc(kx dx/2) sinc(ky dy/2)]^(2 cic_order), 0 past |k| > k_filter (> 0).
         All zero (the default) is the reference's solve."""
         _check(self.lib.aw_set_form_factor(self.h, float(ax), float(ay), int(cic_order), float(k_filter)))
+
+    def set_current_filter(self, passes: int):
+        """Yee: passes of the binomial current filter per step (RunParams::jfilter)."""
+        _check(self.lib.aw_set_current_filter(self.h, int(passes)))
 
     def checkpoint(self, path: str, step: int, time: float = None, deck: str = "", git_hash: str = "",
                    rng_seed: int = 0, sd: float = 1.0, eps_l: float = 0.0, wait: bool = True):

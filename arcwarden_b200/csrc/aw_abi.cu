@@ -76,7 +76,7 @@ void free_all(Ctx& c) {
     void* bufs[] = {c.st, c.acc_src, c.acc_dcu, c.r_src, c.r_out, c.r_dcu, c.r_et, c.k_src, c.k_out,
                     c.k_dcu, c.k_et, c.gb_es, c.gb_dcu, c.gb_push, c.part_p, c.part_c, c.part_d, c.part_g, c.diag, c.red_rows,
                     c.bin_count, c.bin_off, c.bin_cursor, c.bin_idx, c.sort_tmp, c.fft_work, c.rs_buf,
-                    c.rs_temp, c.ffac};
+                    c.rs_temp, c.ffac, c.acc_tmp};
     for (void* b : bufs) if (b) cudaFree(b);
     if (c.own_stream) cudaStreamDestroy(c.own_stream);
 }
@@ -109,9 +109,9 @@ void reset_acc(Ctx& c, unsigned long long* acc, int nf) {
 // ---- the step body (no host syncs; capturable) --------------------------------
 // A step is a fixed list of phases; `mark(i)` runs after phase i (used by
 // aw_step_profile to record CUDA events between phases).
-constexpr int kPhasesES = 7, kPhasesDarwin = 13, kPhasesYee = 5;
-const char* const kPhaseNamesYee[kPhasesYee] = {"faraday_half", "push_esirkepov", "faraday_half2", "ampere",
-                                                "step_reduce"};
+constexpr int kPhasesES = 7, kPhasesDarwin = 13, kPhasesYee = 6;
+const char* const kPhaseNamesYee[kPhasesYee] = {"faraday_half", "push_esirkepov", "current_filter",
+                                                "faraday_half2", "ampere", "step_reduce"};
 const char* const kPhaseNamesES[kPhasesES] = {
     "finalize_rho", "fft_r2c_rho", "kspace_es", "fft_c2r_e", "fields_es", "push_deposit_es", "step_reduce"};
 const char* const kPhaseNamesDarwin[kPhasesDarwin] = {
@@ -166,9 +166,10 @@ void step_body(Ctx& c, Mark mark) {
         // MaxwellSimulation::step_at (simulation_maxwell.hpp:52-110), periodic set
         launch_yee_faraday(c, true); mark(0);
         launch_push_esirkepov(c); mark(1);
-        launch_yee_faraday(c, false); mark(2);
-        launch_yee_ampere(c); mark(3);
-        launch_step_reduce(c); mark(4);
+        launch_yee_filter(c); mark(2);
+        launch_yee_faraday(c, false); mark(3);
+        launch_yee_ampere(c); mark(4);
+        launch_step_reduce(c); mark(5);
         return;
     }
     if (c.model == AW_MODEL_ES) {
@@ -184,7 +185,10 @@ void step_body(Ctx& c, Mark mark) {
 void step_body(Ctx& c) { step_body(c, NoMark{}); }
 
 // Kernels of this library one fused step launches (cuFFT's own not counted).
-int kernels_per_step(const Ctx& c) { return c.model == AW_MODEL_DARWIN ? 9 : 5; }
+int kernels_per_step(const Ctx& c) {
+    if (c.model == AW_MODEL_DARWIN) return 9;
+    return (c.model == AW_MODEL_YEE && c.yee_jfilter > 0) ? 7 : 5;
+}
 
 void ensure_pending(Ctx& c) {
     if (c.pending_valid || c.model == AW_MODEL_YEE) return;    // the Yee step deposits inside itself
@@ -441,7 +445,7 @@ int aw_ctx_create(const aw_grid* g, const aw_params* p, int32_t model, void* str
         c.grid = *g;
         c.prm = *p;
         c.model = model;
-        c.resort_every = (model == AW_MODEL_DARWIN) ? 50 : 0;
+        c.resort_every = (model == AW_MODEL_DARWIN || model == AW_MODEL_YEE) ? 50 : 0;
         c.geo.nx = g->nx; c.geo.ny = g->ny;
         c.geo.nxf = static_cast<float>(g->nx); c.geo.nyf = static_cast<float>(g->ny);
         c.geo.dx = g->Lx / g->nx; c.geo.dy = g->Ly / g->ny;
@@ -977,6 +981,18 @@ int aw_checkpoint_read(aw_ctx* ctx, const char* path, aw_checkpoint_info* out) {
     return guarded([&] {
         aw::need(ctx && path, AW_ERR_ARG, "null argument");
         aw::checkpoint_read(ctx->c, path, out);
+    });
+}
+
+int aw_set_current_filter(aw_ctx* ctx, int32_t passes) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::need(passes >= 0 && passes <= 4, AW_ERR_ARG, "set_current_filter: passes in [0, 4]");
+        Ctx& c = ctx->c;
+        aw::need(c.model == AW_MODEL_YEE, AW_ERR_STATE, "set_current_filter: Yee contexts only");
+        aw::drop_graph(c);
+        if (passes > 0 && !c.acc_tmp) aw::dalloc(c.acc_tmp, static_cast<size_t>(3) * c.geo.ncell);
+        c.yee_jfilter = passes;
     });
 }
 

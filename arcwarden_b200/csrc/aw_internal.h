@@ -149,6 +149,11 @@ struct Ctx {
     // checkpoint writer (aw_checkpoint.cu): snapshot buffer, pinned chunks, thread
     struct CkWriter* ck = nullptr;
 
+    // Yee: passes of the binomial current filter (aw_set_current_filter) and its
+    // integer scratch [3][ncell]
+    int yee_jfilter = 0;
+    unsigned long long* acc_tmp = nullptr;
+
     // discrete adjoint of the ES step (aw_adjoint.cu; allocated by aw_grad_es)
     struct AdjWS* adj = nullptr;
     // Trajectory recording, set only while the adjoint's recording ES step is
@@ -283,6 +288,7 @@ void launch_rms_reduce(Ctx& c, bool src, bool dcu);
 void launch_step_reduce(Ctx& c);                   // end of a fused step: diagnostics (+ rms for Darwin)
 void launch_yee_faraday(Ctx& c, bool begin);       // Yee: B half step (begin: the step's device state)
 void launch_yee_ampere(Ctx& c);                    // Yee: E full step with the step's current
+void launch_yee_filter(Ctx& c);                    // Yee: the binomial current filter, exact in integers
 
 // ---- step graph (aw_abi.cu) ------------------------------------------------
 // The fused step body captured into a graph on the context's stream (pending

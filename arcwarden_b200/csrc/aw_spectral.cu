@@ -759,16 +759,42 @@ __global__ void k_yee_faraday(YeeF v, float dt2, DevState* st, int begin, double
     }
 }
 
+// Binomial current filter (k_binomial3x3, yee2d.hpp:471-487, applied m times):
+// m passes of [1,2,1] x [1,2,1] / 16 are the separable order-2m binomial,
+// J'(i, j) = sum_{a, b} C(2m, a) C(2m, b) J(i + a - m, j + b - m) / 16^m. On the
+// integer accumulator the sums are exact; the 16^m goes into the finalising
+// scale. One pass along x (in -> out) or y, three fields, periodic.
+__global__ void k_yee_binomial(const unsigned long long* __restrict__ in, unsigned long long* __restrict__ out,
+                               int nx, int ny, int m, int along_y) {
+    const int n = nx * ny;
+    long long cb[9];
+    cb[0] = 1;
+    for (int k = 1; k <= 2 * m; ++k) cb[k] = cb[k - 1] * (2 * m - k + 1) / k;   // C(2m, k)
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * n; t += gridDim.x * blockDim.x) {
+        const int f = t / n, c = t - f * n;
+        const int i = c % nx, j = c / nx;
+        const unsigned long long* a = in + static_cast<size_t>(f) * n;
+        long long s = 0;
+        for (int k = 0; k <= 2 * m; ++k) {
+            int ii = i, jj = j;
+            if (along_y) { jj = (j + k - m) % ny; if (jj < 0) jj += ny; }
+            else { ii = (i + k - m) % nx; if (ii < 0) ii += nx; }
+            s += cb[k] * static_cast<long long>(a[jj * nx + ii]);
+        }
+        out[t] = static_cast<unsigned long long>(s);
+    }
+}
+
 // E full step E += dt (c^2 curl B - J) (k_ampere), J = the step's exact current
 // acc [3][ncell] / S_next[1..3] (the accumulator is zeroed for the next step and
 // J written to the caller's source arrays when bound); field-energy partials
 // (sum |E|^2, max |E|^2, sum |B|^2 of the wave field) for the step reduction.
 __global__ void k_yee_ampere(YeeF v, unsigned long long* __restrict__ acc, const DevState* st,
-                             float* jx_api, float* jy_api, float* jz_api, double* __restrict__ part) {
+                             float* jx_api, float* jy_api, float* jz_api, double* __restrict__ part, double fscale) {
     const int n = v.nx * v.ny;
-    const double ix = 1.0 / static_cast<double>(st->S_next[1]);
-    const double iy = 1.0 / static_cast<double>(st->S_next[2]);
-    const double iz = 1.0 / static_cast<double>(st->S_next[3]);
+    const double ix = fscale / static_cast<double>(st->S_next[1]);     // fscale = 16^-m of the filter
+    const double iy = fscale / static_cast<double>(st->S_next[2]);
+    const double iz = fscale / static_cast<double>(st->S_next[3]);
     double se2 = 0.0, me2 = 0.0, sb2 = 0.0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const long long ax = static_cast<long long>(acc[c]);
@@ -880,8 +906,18 @@ void launch_yee_faraday(Ctx& c, bool begin) {
     AW_LAUNCH();
 }
 void launch_yee_ampere(Ctx& c) {
+    const double fscale = std::ldexp(1.0, -4 * c.yee_jfilter);
     k_yee_ampere<<<kGridBlocks, kThreads, 0, c.stream>>>(yee_views(c), c.acc_src, c.st, c.src.Jx, c.src.Jy,
-                                                         c.src.Jz, c.part_g);
+                                                         c.src.Jz, c.part_g, fscale);
+    AW_LAUNCH();
+}
+void launch_yee_filter(Ctx& c) {
+    if (c.yee_jfilter <= 0) return;
+    const int n = c.geo.ncell;
+    const int blocks = std::min(4096, (3 * n + kThreads - 1) / kThreads);
+    k_yee_binomial<<<blocks, kThreads, 0, c.stream>>>(c.acc_src, c.acc_tmp, c.geo.nx, c.geo.ny, c.yee_jfilter, 0);
+    AW_LAUNCH();
+    k_yee_binomial<<<blocks, kThreads, 0, c.stream>>>(c.acc_tmp, c.acc_src, c.geo.nx, c.geo.ny, c.yee_jfilter, 1);
     AW_LAUNCH();
 }
 void launch_fields_push(Ctx& c) {

@@ -2,7 +2,7 @@
 """Benchmark of the B200 PIC hot path: particles/s per full PIC step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W]
-                    [--workload weibel512|es256|whistler1024|adjoint256|ensemble64]
+                    [--workload weibel512|es256|whistler1024|adjoint256|ensemble64|yee625]
                     [--impl ours|reference] [--no-cpu-baseline] [--dump-grad FILE]
 
 Workloads (synthetic, seeded; the reference's own seeded loader streams):
@@ -87,6 +87,16 @@ def workload(name: str) -> dict:
                              dict(ppc=8, density=0.5, uth=(0.01,) * 3, ufl=(-0.2, 0.0, 0.0))],
                     desc="adjoint of the electrostatic two-stream 256x256 dx=1 2x8ppc v0=+-0.2 vth=0.01 dt=0.1, "
                          "200 steps, checkpoint every 20, loss = final field energy")
+    if name == "yee625":
+        # the reference's Yee benchmark (its published case 7, decks/eaw_case7_tiled.ini): whistler anisotropy
+        # instability, 625^2 cells over 13.5 c/wpe, 400 particles per cell, wce/wpe = 0.25 along x, three
+        # binomial current-filter passes per step
+        return dict(name=name, model=2, nx=625, ny=625, Lx=13.5, Ly=13.5, dt=0.0145, c=1.0, n0=1.0,
+                    B0=(0.25, 0.0, 0.0), pump=None, run_steps=100, dom="push_esirkepov", jfilter=3, seed=20260714,
+                    tile_sort=20,
+                    species=[dict(ppc=400, density=1.0, uth=(0.01678, 0.03752, 0.03752), ufl=(0.0, 0.0, 0.0))],
+                    desc="Yee full-Maxwell whistler anisotropy (case 7): 625x625 cells over 13.5 c/wpe, ppc 400, "
+                         "uth=(0.01678,0.03752,0.03752), wce=0.25 along x, c=1, dt=0.0145, jfilter 3")
     if name == "ensemble64":
         return dict(name=name, ensemble=True, nruns=64, run_steps=100, model=None, species=[], nx=0, ny=0,
                     desc="64 independent runs (seeds 0-63): grid side in {64,128,256,512} (dx=1), ppc in "
@@ -178,8 +188,38 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+def yee_cpu_baseline(wl, budget_s=15.0):
+    """The FP64 numpy restatement of the Yee step (oracle/yee64.py) on one host
+    core, on a bounded sample of the workload: 1/16 of its cells (the same
+    spacing and density) for as many steps as fit the budget."""
+    import numpy as np
+    from oracle.yee64 import YeeCase
+    nx, ny = wl["nx"] // 4, wl["ny"] // 4
+    dx, dy = wl["Lx"] / wl["nx"], wl["Ly"] / wl["ny"]
+    sp = wl["species"][0]
+    n = nx * ny * sp["ppc"]
+    rng = np.random.default_rng(0)
+    p = {"x": rng.random(n) * nx, "y": rng.random(n) * ny, "w": np.full(n, sp["density"] * dx * dy / sp["ppc"])}
+    for d, k in enumerate(("ux", "uy", "uz")):
+        p[k] = sp["uth"][d] * rng.standard_normal(n)
+    case = YeeCase(nx, ny, nx * dx, ny * dy, wl["dt"], wl["c"], -1.0, wl["B0"], wl.get("jfilter", 0))
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        p = case.step(p)
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s:
+            break
+    return dict(value=n * steps / el, unit="particles/s", cores=1, kind="port",
+                sample=f"{steps} Yee steps of {nx}x{ny} cells, {n} particles (1/16 of the workload's cells), "
+                       f"FP64 numpy restatement on one core, {el:.1f} s")
+
+
 def cpu_baseline(wl, budget_s=15.0, max_steps=None):
     """The oracle port (OpenMP C) timed on this host's cores on the same config."""
+    if wl["model"] == 2:
+        return yee_cpu_baseline(wl, budget_s)
     from oracle import oracle as O
     g = O.geo(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"])
     p = O.load_species(g, wl["species"], seed=0, noisy=True)
@@ -233,7 +273,10 @@ def run_ours(args, wl, rank, world, dist):
     G = {k: torch.zeros(nc, dtype=torch.float32, device=dev) for k in aw.SOURCE_NAMES + aw.FIELD_NAMES}
     ctx.bind_sources(**{k: G[k] for k in ("rho", "Jx", "Jy", "Jz", "amu0", "amu1", "amu2", "amu3", "dcux", "dcuy", "dcuz")})
     ctx.bind_fields(**{k: G[k] for k in aw.FIELD_NAMES})
-    ctx.load_species(wl["species"], seed=0, noisy=True)
+    seed = wl.get("seed", 0)
+    ctx.load_species(wl["species"], seed=seed, noisy=True)
+    if wl["model"] == aw.AW_MODEL_YEE:
+        ctx.set_current_filter(wl.get("jfilter", 0))
     ctx.init()
 
     def barrier():
@@ -272,7 +315,7 @@ def run_ours(args, wl, rank, world, dist):
     # end to end through the C ABI from pinned host memory (one config-length run)
     host = {k: v.cpu().pin_memory() for k, v in P.items()}
     # reload the initial state on the host side: a fresh seeded load, copied down
-    ctx.load_species(wl["species"], seed=0, noisy=True)
+    ctx.load_species(wl["species"], seed=seed, noisy=True)
     torch.cuda.synchronize(dev)
     for k in host:
         host[k].copy_(P[k])
@@ -285,6 +328,9 @@ def run_ours(args, wl, rank, world, dist):
     with torch.cuda.stream(stream):
         for k in host:
             P[k].copy_(host[k], non_blocking=True)
+        if wl["model"] == aw.AW_MODEL_YEE:          # the Yee lattices start at zero (YeeFields)
+            for k in aw.FIELD_NAMES:
+                G[k].zero_()
     ctx.init()
     ctx.run_diag(0, K, diag_host.data_ptr(), graph=True)
     with torch.cuda.stream(stream):
@@ -310,8 +356,8 @@ def run_ours(args, wl, rank, world, dist):
         "vs_baseline": None,
         "dtype": "f32",
         "numerics": "f32 push/gather/solve; deposits exact int64 fixed point; diagnostics f64",
-        "data": "synthetic: reference seeded loader streams (noisy load, seed 0)",
-        "config": {"workload": wl["desc"], "field_model": "darwin" if wl["model"] else "electrostatic",
+        "data": f"synthetic: reference seeded loader streams (noisy load, seed {seed})",
+        "config": {"workload": wl["desc"], "field_model": ("electrostatic", "darwin", "yee")[wl["model"]],
                    "grid": [wl["nx"], wl["ny"]], "particles_per_gpu": n, "graph": True,
                    "l2": f"particle SoA {n * 28 / 1e6:.0f} MB per step > 126 MB L2 (no flush needed)",
                    "parallelism": f"replicas x{world}"},
@@ -342,7 +388,12 @@ def profile_case(wl, steps):
     P = {k: torch.empty(n, dtype=torch.float32, device=dev) for k in ("x", "y", "ux", "uy", "uz", "w")}
     cell = torch.empty(n, dtype=torch.int32, device=dev)
     ctx.bind_particles(P["x"], P["y"], P["ux"], P["uy"], P["uz"], P["w"], cell)
-    ctx.load_species(wl["species"], seed=0, noisy=True)
+    G = {}
+    if wl["model"] == aw.AW_MODEL_YEE:              # the Yee lattices are the caller's field arrays
+        G = {k: torch.zeros(wl["nx"] * wl["ny"], dtype=torch.float32, device=dev) for k in aw.FIELD_NAMES}
+        ctx.bind_fields(**G)
+        ctx.set_current_filter(wl.get("jfilter", 0))
+    ctx.load_species(wl["species"], seed=wl.get("seed", 0), noisy=True)
     if wl.get("adjoint"):
         # one gradient of K steps (checkpoint interval as the workload's, at most K)
         du = [torch.zeros(n, dtype=torch.float32, device=dev) for _ in range(3)]
@@ -651,15 +702,26 @@ def run_reference(args, wl, rank, world):
         import torch
         torch.cuda.set_device(0)
         prm = R.params(dt=wl["dt"], c=wl["c"], n0=wl["n0"], B0=wl["B0"], pump=wl["pump"])
-        rs = R.RefSim(wl["model"], wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], prm, wl["species"], noisy=True, seed=0)
-        rs.init()
-        rs.time_steps(0, max(args.warmup, 3))
-        ms = rs.time_steps(max(args.warmup, 3), args.steps) / args.steps
+        if wl["model"] == 2:
+            # MaxwellSimulation on its tiled path (physical tile sort every tile_sort steps), the
+            # reference's own loader, its jfilter
+            rs = R.RefYee(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], prm, tile_sort=wl["tile_sort"],
+                          jfilter=wl.get("jfilter", 0), species=wl["species"], noisy=True, seed=wl.get("seed", 0))
+            rs.time_steps(max(args.warmup, 3))
+            ms = rs.time_steps(args.steps) / args.steps
+            what = f"MaxwellSimulation, tile_sort {wl['tile_sort']}, jfilter {wl.get('jfilter', 0)}"
+        else:
+            rs = R.RefSim(wl["model"], wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], prm, wl["species"], noisy=True,
+                          seed=0)
+            rs.init()
+            rs.time_steps(0, max(args.warmup, 3))
+            ms = rs.time_steps(max(args.warmup, 3), args.steps) / args.steps
+            what = f"Simulation<{'CfgDarwin' if wl['model'] else 'Cfg'}>"
         rs.close()
         val = n / (ms * 1e-3)
         cb = dict(value=val, unit="particles/s", cores=1, kind="reference", device="cuda",
-                  sample=f"{args.steps} steps of the reference Simulation<{'CfgDarwin' if wl['model'] else 'Cfg'}> "
-                         f"({n} particles) on this GPU, headers unmodified")
+                  sample=f"{args.steps} steps of the reference {what} ({n} particles) on this GPU, "
+                         f"headers unmodified")
     else:
         cb = cpu_baseline(wl, budget_s=30.0)
         val = cb["value"]
@@ -668,7 +730,7 @@ def run_reference(args, wl, rank, world):
         "impl": "reference", "metric": "particles/s/step", "value": val, "unit": "particles/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "config": {"workload": wl["desc"], "field_model": "darwin" if wl["model"] else "electrostatic",
+        "config": {"workload": wl["desc"], "field_model": ("electrostatic", "darwin", "yee")[wl["model"]],
                    "grid": [wl["nx"], wl["ny"]], "particles_per_gpu": n},
         "cpu_baseline": cb,
         "e2e": {"value": val, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

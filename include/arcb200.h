@@ -210,9 +210,15 @@ int aw_sort_tiles(aw_ctx* ctx, int32_t tx, int32_t ty, int32_t physical);
  * include/pic/particles.hpp:678-726); this sort is deterministic. */
 int aw_resort(aw_ctx* ctx);
 /* aw_run re-sorts before every step n > 0 with n % every == 0 (0 = never).
- * Default: 50 for the Darwin model, 0 for the electrostatic model, whose
- * reference path keeps the particle order. */
+ * Default: 50 for the Darwin and Yee models (the reference sorts their
+ * particles by tile), 0 for the electrostatic model, whose reference path keeps
+ * the particle order. */
 int aw_set_resort(aw_ctx* ctx, int32_t every);
+/* Yee contexts: `passes` (0-4) passes of the binomial current filter
+ * [1,2,1] x [1,2,1] / 16 per step (RunParams::jfilter, k_binomial3x3,
+ * include/pic/yee2d.hpp:471-487, simulation_maxwell.hpp:78-92), applied exactly
+ * to the integer current as the separable order-2 passes binomial. Default 0. */
+int aw_set_current_filter(aw_ctx* ctx, int32_t passes);
 /* ---- checkpoint / restart (include/pic/checkpoint.hpp:1-17, 31-49) ---------
  * The reference's checkpoint file: its header (magic "ARCW", version 1, seed,
  * step, time, S_d, eps_L), deck and git blocks and manifest, followed by the

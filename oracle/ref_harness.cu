@@ -420,15 +420,16 @@ struct RefYee {
     ~RefYee() { delete sim; }
 };
 
-extern "C" void* ref_yee_create(int nx, int ny, double Lx, double Ly, const ref_params* p, int tile_sort, long n,
-                                const float* x, const float* y, const float* ux, const float* uy, const float* uz,
-                                const float* w) {
+extern "C" void* ref_yee_create(int nx, int ny, double Lx, double Ly, const ref_params* p, int tile_sort,
+                                int jfilter, long n, const float* x, const float* y, const float* ux, const float* uy,
+                                const float* uz, const float* w) {
     RefYee* h = nullptr;
     int rc = guard([&] {
         h = new RefYee();
         h->g = Grid(nx, ny, Lx, Ly);
         h->rp = make_rp(p, 0, 0);
         h->rp.tile_sort = tile_sort;
+        h->rp.jfilter = jfilter;
         h->sim = new MaxwellSimulation(h->g, h->rp);
         Particles& P = h->sim->particles();
         P.allocate_n(static_cast<std::size_t>(n));
@@ -445,6 +446,25 @@ extern "C" void* ref_yee_create(int nx, int ny, double Lx, double Ly, const ref_
     if (rc) { delete h; return nullptr; }
     return h;
 }
+// The same, with the particles from the reference's own seeded loader
+// (Particles::initialize(SpeciesList, Grid, RunParams, stream)).
+extern "C" void* ref_yee_create_species(int nx, int ny, double Lx, double Ly, const ref_params* p, int tile_sort,
+                                        int jfilter, const ref_species* sp, int nsp, int noisy, unsigned long seed) {
+    RefYee* h = nullptr;
+    int rc = guard([&] {
+        h = new RefYee();
+        h->g = Grid(nx, ny, Lx, Ly);
+        h->rp = make_rp(p, noisy, seed);
+        h->rp.tile_sort = tile_sort;
+        h->rp.jfilter = jfilter;
+        h->sim = new MaxwellSimulation(h->g, h->rp);
+        h->sim->particles().initialize(make_sp(sp, nsp), h->g, h->rp, h->sim->stream());
+        h->sim->stream().synchronize();
+    });
+    if (rc) { delete h; return nullptr; }
+    return h;
+}
+extern "C" long ref_yee_n(void* hv) { return static_cast<long>(static_cast<RefYee*>(hv)->sim->particles().n); }
 extern "C" void ref_yee_destroy(void* hv) { delete static_cast<RefYee*>(hv); }
 
 extern "C" int ref_yee_step(void* hv, long nsteps) {

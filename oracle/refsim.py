@@ -58,7 +58,12 @@ def lib():
         L.ref_solve.argtypes = [I, I, I, D, D, C.POINTER(RefParams), P, P]
         L.ref_bins.argtypes = [I, I, I, D, D, L_, P, P, I, I, P, P]
         L.ref_yee_create.restype = P
-        L.ref_yee_create.argtypes = [I, I, D, D, C.POINTER(RefParams), I, L_] + [P] * 6
+        L.ref_yee_create.argtypes = [I, I, D, D, C.POINTER(RefParams), I, I, L_] + [P] * 6
+        L.ref_yee_create_species.restype = P
+        L.ref_yee_create_species.argtypes = [I, I, D, D, C.POINTER(RefParams), I, I, C.POINTER(RefSpecies), I, I,
+                                             C.c_ulong]
+        L.ref_yee_n.argtypes = [P]
+        L.ref_yee_n.restype = L_
         L.ref_yee_destroy.argtypes = [P]
         L.ref_yee_destroy.restype = None
         L.ref_yee_step.argtypes = [P, L_]
@@ -215,12 +220,24 @@ def bins(physical, nx, ny, Lx, Ly, x, y, tx=16, ty=16):
 class RefYee:
     """The reference's MaxwellSimulation (the Yee branch) on host-given particles."""
 
-    def __init__(self, nx, ny, Lx, Ly, prm, parts, tile_sort=0):
+    def __init__(self, nx, ny, Lx, Ly, prm, parts=None, tile_sort=0, jfilter=0, species=None, noisy=True,
+                 seed=0):
+        """parts: host arrays x y ux uy uz w; or species (the reference's loader)."""
         self.nx, self.ny = nx, ny
-        self.n = len(parts["x"])
-        arrs = [np.ascontiguousarray(parts[k], np.float32) for k in ("x", "y", "ux", "uy", "uz", "w")]
-        self.h = lib().ref_yee_create(nx, ny, Lx, Ly, C.byref(prm), tile_sort, self.n,
-                                      *(a.ctypes.data_as(C.c_void_p) for a in arrs))
+        if parts is not None:
+            self.n = len(parts["x"])
+            arrs = [np.ascontiguousarray(parts[k], np.float32) for k in ("x", "y", "ux", "uy", "uz", "w")]
+            self.h = lib().ref_yee_create(nx, ny, Lx, Ly, C.byref(prm), tile_sort, jfilter, self.n,
+                                          *(a.ctypes.data_as(C.c_void_p) for a in arrs))
+        else:
+            arr = (RefSpecies * len(species))()
+            for i, sp in enumerate(species):
+                arr[i].ppc, arr[i].density = sp["ppc"], sp["density"]
+                for d in range(3):
+                    arr[i].uth[d], arr[i].ufl[d] = sp["uth"][d], sp["ufl"][d]
+            self.h = lib().ref_yee_create_species(nx, ny, Lx, Ly, C.byref(prm), tile_sort, jfilter, arr,
+                                                  len(species), int(noisy), seed)
+            self.n = lib().ref_yee_n(self.h) if self.h else 0
         if not self.h:
             raise RuntimeError(lib().ref_last_error().decode())
 

@@ -14,7 +14,8 @@ Restates, in float64 numpy, MaxwellSimulation::step_at
        Jy(i, j+1/2) = -(q w / (dt dx)) prefix_j sum DSy(j) (Sx0 + DSx/2)
        Jz(i, j)     =  (q w vz / (dx dy)) (Sx0 Sy0 + (DSx Sy0 + Sx0 DSy)/2 + DSx DSy/3)
                                                   (yee2d.hpp:17-29, 307-355)
-     then the periodic wrap of the positions (Particles::migrate)
+     then the periodic wrap of the positions (Particles::migrate), and jfilter
+     passes of the binomial current filter
   4. B half step
   5. E full step, k_ampere (yee2d.hpp:84-97): E += dt (c^2 curl B - J)  (eps0 = 1)
 
@@ -29,7 +30,11 @@ OFFSETS = {"Ex": (0.5, 0.0), "Ey": (0.0, 0.5), "Ez": (0.0, 0.0),
 
 
 class YeeCase:
-    def __init__(self, nx, ny, Lx, Ly, dt, c, qm=-1.0, B0=(0.0, 0.0, 0.0)):
+    def __init__(self, nx, ny, Lx, Ly, dt, c, qm=-1.0, B0=(0.0, 0.0, 0.0), jfilter=0):
+        """jfilter: passes of the binomial current filter [1,2,1] x [1,2,1] / 16
+        after the deposit (k_binomial3x3, yee2d.hpp:471-487;
+        simulation_maxwell.hpp:78-92)."""
+        self.jfilter = jfilter
         self.nx, self.ny = nx, ny
         self.dx, self.dy = Lx / nx, Ly / ny
         self.dt, self.c2, self.qm = dt, c * c, qm
@@ -119,10 +124,22 @@ class YeeCase:
                 J["Jz"] += np.bincount(cell, cJz * wz[ni, nj], minlength=nx * ny)
         self.J = {k: v.reshape(ny, nx) for k, v in J.items()}
 
+    @staticmethod
+    def binomial(a):
+        """One pass of [1,2,1] x [1,2,1] / 16, periodic: sum w_di w_dj a(i+di, j+dj)."""
+        w = (0.25, 0.5, 0.25)
+        r = np.zeros_like(a)
+        for dj in (-1, 0, 1):
+            for di in (-1, 0, 1):
+                r += w[di + 1] * w[dj + 1] * np.roll(np.roll(a, -dj, 0), -di, 1)
+        return r
+
     # ---- step -----------------------------------------------------------------
     def step(self, p):
         self.faraday(0.5 * self.dt)
         p = self.push_deposit(p)
+        for _ in range(self.jfilter):
+            self.J = {k: self.binomial(v) for k, v in self.J.items()}
         self.faraday(0.5 * self.dt)
         self.ampere()
         return p

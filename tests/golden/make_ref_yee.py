@@ -9,7 +9,8 @@ B0 = (0.2, 0, 0.1), 16 particles per cell at seeded uniform positions with
 thermal velocities 0.05 and a drift 0.02 sin(2 pi x / 32) in ux, weight 1/16.
 Stored: the initial particles; fields E, B, J and the particles after 1 and
 after 8 steps of the flat path (tile_sort = 0); the fields after 8 steps of the
-tiled path (tile_sort = 4, which reorders the particles).
+tiled path (tile_sort = 4, which reorders the particles); fields (with the
+filtered J) and particles after 8 steps with jfilter = 3.
 """
 from __future__ import annotations
 
@@ -63,6 +64,15 @@ def main():
         sim.step(8)
         for k in FIELDS:
             out[f"tiled_s8_{k}"] = sim.get(k).reshape(NY, NX)
+    finally:
+        sim.close()
+    sim = R.RefYee(NX, NY, LX, LY, prm, p0, tile_sort=0, jfilter=3)
+    try:
+        sim.step(8)
+        for k in FIELDS:
+            out[f"jf3_s8_{k}"] = sim.get(k).reshape(NY, NX)
+        for k in PARTS:
+            out[f"jf3_s8_{k}"] = sim.get(k)
     finally:
         sim.close()
     np.savez_compressed(HERE / "ref_yee.npz", nx=NX, ny=NY, Lx=LX, Ly=LY, c=C_LIGHT, dt=DT, qm=QM,

@@ -68,6 +68,36 @@ def test_yee_matches_the_reference(torch_cuda, aw, ref):
         s.close()
 
 
+def test_yee_current_filter_matches_the_reference(torch_cuda, aw, ref):
+    """aw_set_current_filter(3) (the reference's jfilter = 3): after 8 steps E
+    and B within 1e-5 of the reference's, the filtered J within 1e-4, positions
+    within 1e-5 cells. Filter off again: the unfiltered run's bits."""
+    s = _yee(torch_cuda, aw, ref, _p0(ref))
+    t = _yee(torch_cuda, aw, ref, _p0(ref))
+    u = _yee(torch_cuda, aw, ref, _p0(ref))
+    try:
+        s.ctx.set_current_filter(3)
+        s.ctx.run(0, 8, graph=True)
+        for k in FIELDS + CURRENTS:
+            bar = 1e-4 if k in CURRENTS else 1e-5
+            assert relerr(s.grid(k), ref[f"jf3_s8_{k}"]) < bar, (k, relerr(s.grid(k), ref[f"jf3_s8_{k}"]))
+        p = s.parts()
+        for k in ("x", "y"):
+            assert np.abs(p[k] - ref[f"jf3_s8_{k}"]).max() < 1e-5, k
+        t.ctx.set_current_filter(2)
+        t.ctx.set_current_filter(0)
+        t.ctx.run(0, 3, graph=True)
+        u.ctx.run(0, 3, graph=True)
+        for k in FIELDS + CURRENTS:
+            assert np.array_equal(t.grid(k), u.grid(k)), k
+        with pytest.raises(aw.ArcError):
+            s.ctx.set_current_filter(5)
+    finally:
+        s.close()
+        t.close()
+        u.close()
+
+
 def test_yee_vs_fp64_oracle(torch_cuda, aw, ref):
     """The FP32 step against the FP64 restatement after 8 steps: within the FP32
     Esirkepov's own error (the reference's is up to 1.2e-4 of the maxima)."""

@@ -53,9 +53,42 @@ def test_oracle_matches_the_reference_yee_branch(ref):
             assert np.abs(p[k] - ref[f"{tag}_{k}"]).max() < 1e-6, (tag, k)
 
 
+def test_oracle_with_current_filter_matches_the_reference(ref):
+    """jfilter = 3 (three binomial passes on J per step): fields, the filtered
+    J and the particles after 8 steps."""
+    case = _case(ref)
+    case.jfilter = 3
+    p = {k: ref["p0_" + k].astype(np.float64) for k in ("x", "y", "ux", "uy", "uz", "w")}
+    for _ in range(8):
+        p = case.step(p)
+    for k in FIELDS:
+        assert _rel(case.f[k], ref[f"jf3_s8_{k}"]) < 3e-4, k
+    for k in CURRENTS:
+        assert _rel(case.J[k], ref[f"jf3_s8_{k}"]) < 3e-4, k
+    for k in ("x", "y"):
+        assert np.abs(p[k] - ref[f"jf3_s8_{k}"]).max() < 2e-5, k
+
+
+def test_binomial_filter_is_three_one_dimensional_passes():
+    """Three 3x3 passes equal the separable order-6 binomial the library applies
+    on its integer current (C(6, k) / 64 along x, then along y)."""
+    from oracle.yee64 import YeeCase
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal((16, 24))
+    r = a
+    for _ in range(3):
+        r = YeeCase.binomial(r)
+    c6 = np.array([1, 6, 15, 20, 15, 6, 1]) / 64.0
+    s = sum(c6[k] * np.roll(a, -(k - 3), 1) for k in range(7))
+    s = sum(c6[k] * np.roll(s, -(k - 3), 0) for k in range(7))
+    assert np.abs(r - s).max() < 1e-14
+
+
 def test_reference_flat_and_tiled_paths_agree(ref):
+    """The reference's two deposit paths (float atomics in different orders):
+    fields to 1e-5, the FP32 Esirkepov current to 1e-4 (measured up to 1.0e-5)."""
     for k in FIELDS + CURRENTS:
-        assert _rel(ref[f"tiled_s8_{k}"], ref[f"s8_{k}"]) < 1e-5, k
+        assert _rel(ref[f"tiled_s8_{k}"], ref[f"s8_{k}"]) < (1e-4 if k in CURRENTS else 1e-5), k
 
 
 def test_oracle_discrete_continuity():
