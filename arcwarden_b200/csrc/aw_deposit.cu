@@ -1191,6 +1191,7 @@ __device__ __forceinline__ void yee_window_pass(const float* __restrict__ stage,
         const int ci = win_off(ib - 1, wn.ir, g.nx) - wn.mi, cj = win_off(jb - 1, wn.jr, g.ny) - wn.mj;
         esirkepov_weights(x0, y0, x1, y1, ib, jb, [&](int f, int ni, int nj, float w) {
             const int v = quant(f == 0 ? a0 : f == 1 ? a1 : a2, w);
+            if (v == 0) return;                    // prefix-sum residues that round to nothing
             int* e = win + 2 * f * wn.WH + (cj + nj) * wn.W + (ci + ni);
             if (wn.track_all) add_tracked(e, wn.WH, v);
             else atomicAdd(e, v);

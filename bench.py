@@ -749,6 +749,8 @@ def main():
                     help="adjoint256: PIC steps per gradient (default 200)")
     ap.add_argument("--dump-grad", default=None, metavar="FILE",
                     help="adjoint256: write the initial state and the gradient (.npz) for oracle/grad_check.py")
+    ap.add_argument("--ppc", type=int, default=0, metavar="N",
+                    help="profiling case only: particles per cell of the first species (a smaller capture)")
     ap.add_argument("--profile-case", type=int, default=0, metavar="K",
                     help="profiling case for ncu: load, aw_init and K single aw_step launches (adjoint256: one "
                          "gradient of K steps; no timing, no JSON line)")
@@ -769,6 +771,8 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
     if args.profile_case:
+        if args.ppc:
+            wl["species"][0]["ppc"] = args.ppc
         profile_case(wl, args.profile_case)
         return
     try:
