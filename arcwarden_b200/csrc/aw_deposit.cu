@@ -1104,10 +1104,14 @@ struct YeeArgs {
     unsigned long long* acc; int wmaxc; double* part; DevState* st; int write_cell;
 };
 
-// node shape over {b - 1, .., b + 2}: S = max(0, 1 - |x - p|) (yee2d.hpp:124-130)
+// node shape over {b - 1, .., b + 2}: S = max(0, 1 - |x - p|) (yee2d.hpp:124-130).
+// With b = floor(min(x0, x1)) the first node is always 0: x - (b - 1) >= 1,
+// and the float difference rounds monotonically from the exact 1 of x = b. So
+// only nodes 1..3 are computed and S[0] is the constant 0.
 __device__ __forceinline__ void yee_shape4(float x, int b, float (&S)[4]) {
+    S[0] = 0.f;
 #pragma unroll
-    for (int n = 0; n < 4; ++n) {
+    for (int n = 1; n < 4; ++n) {
         const float d = fabsf(x - (float)(b - 1 + n));
         S[n] = d < 1.f ? 1.f - d : 0.f;
     }
@@ -1130,6 +1134,9 @@ __device__ __forceinline__ float yee_gather(const float* __restrict__ a, const G
 // The Esirkepov node weights of one move (yee2d.hpp:307-355, its operation
 // order): emit(f, ni, nj, w) for every nonzero weight of field f (0: the Jx
 // prefix sums, 1: the Jy prefix sums, 2: Jz) at node (ib - 1 + ni, jb - 1 + nj).
+// The reference's 4 x 4 loops start at node 0, whose shapes are 0: its Jx and
+// Jy prefix sums stay exactly +0 there and its Jz weights are 0, all skipped.
+// Starting at node 1 emits the same float values.
 template <class Emit>
 __device__ __forceinline__ void esirkepov_weights(float x0, float y0, float x1, float y1, int ib, int jb,
                                                   Emit&& emit) {
@@ -1138,31 +1145,31 @@ __device__ __forceinline__ void esirkepov_weights(float x0, float y0, float x1, 
     yee_shape4(y0, jb, Sy0); yee_shape4(y1, jb, Sy1);
     float DSx[4], DSy[4];
 #pragma unroll
-    for (int n = 0; n < 4; ++n) { DSx[n] = Sx1[n] - Sx0[n]; DSy[n] = Sy1[n] - Sy0[n]; }
+    for (int n = 1; n < 4; ++n) { DSx[n] = Sx1[n] - Sx0[n]; DSy[n] = Sy1[n] - Sy0[n]; }
 #pragma unroll
-    for (int nj = 0; nj < 4; ++nj) {
+    for (int nj = 1; nj < 4; ++nj) {
         const float sy = Sy0[nj] + 0.5f * DSy[nj];
         float a = 0.f;
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) {
+        for (int ni = 1; ni < 4; ++ni) {
             a += DSx[ni] * sy;
             if (a != 0.f) emit(0, ni, nj, a);
         }
     }
 #pragma unroll
-    for (int ni = 0; ni < 4; ++ni) {
+    for (int ni = 1; ni < 4; ++ni) {
         const float sx = Sx0[ni] + 0.5f * DSx[ni];
         float a = 0.f;
 #pragma unroll
-        for (int nj = 0; nj < 4; ++nj) {
+        for (int nj = 1; nj < 4; ++nj) {
             a += DSy[nj] * sx;
             if (a != 0.f) emit(1, ni, nj, a);
         }
     }
 #pragma unroll
-    for (int nj = 0; nj < 4; ++nj)
+    for (int nj = 1; nj < 4; ++nj)
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) {
+        for (int ni = 1; ni < 4; ++ni) {
             const float wz = Sx0[ni] * Sy0[nj] + 0.5f * (DSx[ni] * Sy0[nj] + Sx0[ni] * DSy[nj])
                            + (1.f / 3.f) * DSx[ni] * DSy[nj];
             if (wz != 0.f) emit(2, ni, nj, wz);
@@ -1188,7 +1195,8 @@ __device__ __forceinline__ void yee_window_pass(const float* __restrict__ stage,
         const float y0 = stage[kChunk + d], x1 = stage[2 * kChunk + d], y1 = stage[3 * kChunk + d];
         const float a0 = stage[4 * kChunk + d], a1 = stage[5 * kChunk + d], a2 = stage[6 * kChunk + d];
         const int ib = (int)floorf(fminf(x0, x1)), jb = (int)floorf(fminf(y0, y1));
-        const int ci = win_off(ib - 1, wn.ir, g.nx) - wn.mi, cj = win_off(jb - 1, wn.jr, g.ny) - wn.mj;
+        // window column / row of node 1 (ib, jb): the stencil's first nonzero node
+        const int ci = win_off(ib, wn.ir, g.nx) - wn.mi - 1, cj = win_off(jb, wn.jr, g.ny) - wn.mj - 1;
         esirkepov_weights(x0, y0, x1, y1, ib, jb, [&](int f, int ni, int nj, float w) {
             const int v = quant(f == 0 ? a0 : f == 1 ? a1 : a2, w);
             if (v == 0) return;                    // prefix-sum residues that round to nothing
@@ -1309,7 +1317,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_push_esirkepov(YeeArgs A) {
                 ay = __fmul_rn(-qw * A.invdt / A.dxp, S[1]);
                 az = __fmul_rn(qw * uz / (A.dxp * A.dyp), S[2]);
                 const int ib = (int)floorf(fminf(x0, x1)), jb = (int)floorf(fminf(y0, y1));
-                bb.add(ib - 1, jb - 1, ir, jr, g);         // the stencil's base node (the box adds 4)
+                bb.add(ib, jb, ir, jr, g);                 // nodes ib..ib+2 (node ib-1 has no weight)
                 // per-node bound of each field's contributions (prefix sums <= the move)
                 const float tx = fabsf(ax) * (fabsf(x1 - x0) * 1.001f + 1e-6f);
                 const float ty = fabsf(ay) * (fabsf(y1 - y0) * 1.001f + 1e-6f);
@@ -1347,9 +1355,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_push_esirkepov(YeeArgs A) {
         umx[2][threadIdx.x >> 5] = __float_as_uint(m2);
     }
     // the window of the nodes every move touches (4 x 4 stencils)
-    // base offsets lo..hi, nodes to hi + 3: win_setup sizes W = hi - lo + 2, so pass hi + 2
+    // base offsets lo..hi, nodes to hi + 2: win_setup sizes W = hi - lo + 2, so pass hi + 1
     Win wn;
-    win_setup<NF, false>(wn, bb.lo_i, bb.lo_j, bb.hi_i + 2, bb.hi_j + 2, ir, jr, A.wmaxc, m.red, l1);
+    win_setup<NF, false>(wn, bb.lo_i, bb.lo_j, bb.hi_i + 1, bb.hi_j + 1, ir, jr, A.wmaxc, m.red, l1);
     if (wn.nb > 1) { wn.use = false; wn.WH = 0; }     // no bands on this path: the slow path takes the chunk
     win_zero<NF>(m.win, wn);
     if (threadIdx.x < 3) {
