@@ -92,7 +92,11 @@ void set_fft_stream(Ctx& c) {
     for (cufftHandle h : plans) if (h) AW_CUFFT(cufftSetStream(h, c.stream));
 }
 
-void require_parts(Ctx& c) { need(c.parts.x != nullptr, AW_ERR_STATE, "particles not bound"); }
+// A Yee context may run without particles (vacuum: the field half of the step
+// alone, as the reference's MaxwellSimulation does); the others need some.
+void require_parts(Ctx& c) {
+    need(c.parts.x != nullptr || (c.model == AW_MODEL_YEE && c.parts_bound), AW_ERR_STATE, "particles not bound");
+}
 
 // Deposit scales for unfused deposits: maxima of the current state, then scales.
 void static_scales(Ctx& c) {
@@ -553,6 +557,7 @@ int aw_particles_bind(aw_ctx* ctx, float* x, float* y, float* ux, float* uy, flo
             return;
         c.parts.x = x; c.parts.y = y; c.parts.ux = ux; c.parts.uy = uy; c.parts.uz = uz;
         c.parts.w = w; c.parts.cell = cell; c.parts.n = n;
+        c.parts_bound = true;
         auto al = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
         c.parts.vec_ok = (al(x) && al(y) && al(ux) && al(uy) && al(uz) && al(w) && (!cell || al(cell))) ? 1 : 0;
         const int nb = static_cast<int>(std::max<long long>(1, (n + aw::kChunk - 1) / aw::kChunk));

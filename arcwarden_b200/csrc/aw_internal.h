@@ -110,6 +110,7 @@ struct Ctx {
     float*  part_d = nullptr;   // dcu-coefficient sums of squares [nblk][4]
     double* part_g = nullptr;   // grid partials [nblk][5]
     int     npart_p = 0, npart_g = 0;
+    bool    parts_bound = false; // aw_particles_bind has run (n may be 0)
     aw_diag* diag = nullptr;    // device aw_diag
     double* red_rows = nullptr; // k_step_reduce block rows [kRedBlocks][kRedVals]
     // tile binning scratch

@@ -17,7 +17,9 @@ pytestmark = pytest.mark.gpu
 BUILD = ROOT / "arcwarden_b200" / "shim" / "_build"
 TESTS = ["test_charge_conservation", "test_poisson_sine", "test_darwin_magnetostatic", "test_fft_roundtrip",
          "test_single_particle", "test_magnetized_boris", "test_particle_load", "test_two_stream", "test_weibel",
-         "test_langmuir", "test_conservation_longrun", "test_diagnostics"]
+         "test_langmuir", "test_conservation_longrun", "test_diagnostics",
+         # the Yee branch (the shim's MaxwellSimulation on AW_MODEL_YEE)
+         "test_yee_langmuir", "test_yee_vacuum", "test_yee_tiled", "test_yee_vs_darwin_lowfreq"]
 
 
 @pytest.mark.parametrize("name", TESTS)
