@@ -176,3 +176,40 @@ def test_yee_is_deterministic_and_order_free(torch_cuda, aw, ref):
         a.close()
         b.close()
         c.close()
+
+
+def test_yee_vacuum_runs_without_particles(torch_cuda, aw):
+    """No particles bound (n = 0): the Yee step is the field half alone, as in
+    the reference's test_yee_vacuum.cu. A standing Ez mode (2, 3) on a 32 x 24
+    grid of non-square cells, Courant 0.4, 20 steps: the six lattices within
+    1e-5 of the FP64 leapfrog's maxima, J stays zero. An ES context without
+    particles still refuses to run."""
+    import math
+    from oracle.yee64 import YeeCase
+    nx, ny, dx, dy, c = 32, 24, 1.0, 0.8, 5.0
+    dt = 0.4 / (c * math.sqrt(1 / dx ** 2 + 1 / dy ** 2))
+    kx, ky = 2 * math.pi * 2 / (nx * dx), 2 * math.pi * 3 / (ny * dy)
+    I, J = np.meshgrid(np.arange(nx), np.arange(ny))
+    ez = np.cos(kx * I * dx + ky * J * dy)
+    s = Setup(torch_cuda, aw, nx, ny, nx * dx, ny * dy, 0, aw.AW_MODEL_YEE, dt=dt, c=c, qm=-1.0)
+    e = Setup(torch_cuda, aw, nx, ny, nx * dx, ny * dy, 0, aw.AW_MODEL_ES, dt=dt, qm=-1.0)
+    try:
+        s.put("Ez", ez.astype(np.float32))
+        s.ctx.init()
+        s.ctx.run(0, 20, graph=True)
+        case = YeeCase(nx, ny, nx * dx, ny * dy, dt, c)
+        case.f["Ez"] = ez.astype(np.float32).astype(np.float64)
+        for _ in range(20):
+            case.faraday(0.5 * dt)
+            case.faraday(0.5 * dt)
+            case.ampere()
+        for k in FIELDS:
+            assert relerr(s.grid(k), case.f[k]) < 1e-5, (k, relerr(s.grid(k), case.f[k]))
+        for k in CURRENTS:
+            assert np.abs(s.grid(k)).max() == 0.0, k
+        assert s.ctx.error_word() == 0
+        with pytest.raises(aw.ArcError):
+            e.ctx.init()
+    finally:
+        s.close()
+        e.close()
