@@ -85,17 +85,16 @@ __global__ void k_make_scales(DevState* st, float cref) {
 
 // Finalise NF fields of the accumulator block acc[f*ncell + c] (f = first..)
 // into real staging r[(f-first)*ncell + c] and optional caller arrays; two
-// cells per thread so every field's loads are in flight together.
+// cells per thread so every field's loads are in flight together. At most 64
+// registers: 4 CTAs per SM, so the fixed grid of the charge partials
+// (kGridBlocks) is one wave.
 struct FinOut { float* p[8]; };
 template <int NF>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
            const float* __restrict__ Sdev, float* __restrict__ r, FinOut api, int accumulate,
            double* __restrict__ part, DevState* st, int step_begin, double dt, float cref, int darwin,
            AdjDev* rec) {
-    double invS[NF];
-#pragma unroll
-    for (int f = 0; f < NF; ++f) invS[f] = __drcp_rn(static_cast<double>(Sdev[first + f]));   // = 1.0 / S
     double qsum = 0.0;
     const int npair = (ncell + 1) >> 1;
     for (int pi = blockIdx.x * blockDim.x + threadIdx.x; pi < npair; pi += gridDim.x * blockDim.x) {
@@ -125,8 +124,11 @@ k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
         }
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            const float a0 = __double2float_rn(static_cast<double>(v[f][0]) * invS[f]);
-            const float a1 = __double2float_rn(static_cast<double>(v[f][1]) * invS[f]);
+            // 1.0 / S, taken here rather than hoisted: a thread finalises about one
+            // cell pair, and NF hoisted doubles would cost the fourth CTA per SM
+            const double invS = __drcp_rn(static_cast<double>(__ldg(Sdev + first + f)));
+            const float a0 = __double2float_rn(static_cast<double>(v[f][0]) * invS);
+            const float a1 = __double2float_rn(static_cast<double>(v[f][1]) * invS);
             float* rf = r + static_cast<size_t>(f) * ncell + c;
             float* o = api.p[f];
             if (two) {
