@@ -106,7 +106,7 @@ SIGNATURES = {
     "aw_ensemble_run": [_P, _I64, _I32], "aw_ensemble_diag": [_P, _I32, C.POINTER(Diag)],
     "aw_ensemble_particles": [_P, _I32] + [C.POINTER(_P)] * 6 + [C.POINTER(_I64)],
     "aw_load_legacy": [_P, C.POINTER(LegacyLoad)],
-    "aw_deposit_rho_noalloc": [C.POINTER(Grid), _D, _P, _P, _P, _P, _P, _P, _I64, _P, _P],
+    "aw_deposit_rho_noalloc": [C.POINTER(Grid), _D, _P, _P, _P, _P, _P, _P, _I64, _P, _P, _P],
     "aw_deposit_rho": [_P], "aw_deposit_rho_j": [_P], "aw_deposit_amu": [_P], "aw_deposit_dcu": [_P],
     "aw_push_es": [_P], "aw_push_em": [_P], "aw_half_step_back": [_P], "aw_migrate": [_P],
     "aw_sort_tiles": [_P, _I32, _I32, _I32],

@@ -43,6 +43,22 @@ void check_cufft(cufftResult r, const char* what, const char* file, int line) {
 
 void set_last_error(const char* msg) { g_last_error = msg; }
 
+void opt_in_smem(const void* kern, size_t bytes) {
+    if (bytes <= 48 * 1024) return;
+    struct Entry { int dev; const void* kern; size_t bytes; };
+    static std::mutex mu;
+    static std::vector<Entry> done;
+    int dev = 0;
+    AW_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    for (const Entry& e : done)
+        if (e.dev == dev && e.kern == kern && e.bytes >= bytes) return;
+    AW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+    for (Entry& e : done)
+        if (e.dev == dev && e.kern == kern) { e.bytes = bytes; return; }
+    done.push_back({dev, kern, bytes});
+}
+
 namespace {
 
 template <class T>

@@ -965,24 +965,13 @@ k_push_deposit_em_multi(const EmArgs* __restrict__ runs, const int* __restrict__
 
 inline int nchunks(long long n) { return static_cast<int>(std::max<long long>(1, (n + kChunk - 1) / kChunk)); }
 
-// Opt a kernel into its dynamic shared-memory size once per process (never
-// inside a stream capture: aw_init launches every kernel before any capture).
-// Keyed by the kernel's address.
+// Opt a kernel into its dynamic shared-memory size (never inside a stream
+// capture: aw_init launches every kernel before any capture). The attribute
+// belongs to the kernel's instance on the current device, so the opt-in is
+// made once per (device, kernel): see opt_in_smem.
 template <class K>
 void prep_smem(K kern, size_t bytes) {
-    static std::mutex mu;
-    static const void* keys[32];
-    static size_t vals[32];
-    static int nkeys = 0;
-    if (bytes <= 48 * 1024) return;
-    std::lock_guard<std::mutex> lock(mu);
-    const void* key = reinterpret_cast<const void*>(kern);
-    for (int i = 0; i < nkeys; ++i)
-        if (keys[i] == key && vals[i] >= bytes) return;
-    AW_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
-    for (int i = 0; i < nkeys; ++i)
-        if (keys[i] == key) { vals[i] = bytes; return; }
-    if (nkeys < 32) { keys[nkeys] = key; vals[nkeys] = bytes; ++nkeys; }
+    opt_in_smem(reinterpret_cast<const void*>(kern), bytes);
 }
 
 template <int SET>

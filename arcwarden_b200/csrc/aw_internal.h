@@ -30,6 +30,13 @@ inline void need(bool ok, int code, const char* msg) {
     if (!ok) throw Error(code, msg);
 }
 
+// Raise a kernel's dynamic shared-memory limit to `bytes` (no-op at <= 48 KB).
+// cudaFuncSetAttribute acts on the kernel's instance on the CURRENT device, so
+// the set-up is remembered per (device ordinal, kernel): a process that drives
+// several GPUs opts in on each of them. Thread-safe; never call it inside a
+// stream capture.
+void opt_in_smem(const void* kern, size_t bytes);
+
 // The text aw_last_error returns (thread-local).
 void set_last_error(const char* msg);
 // Run f, mapping an exception to a status code and the last-error text.

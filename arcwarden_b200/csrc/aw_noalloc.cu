@@ -17,7 +17,13 @@
 //     calls whose work overlaps on the GPU race on it;
 //   * the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (with that device current) and caches it; that first
-//     call should come before any stream capture.
+//     call should come before any stream capture. The cached address belongs to
+//     the device's current context: after cudaDeviceReset on that device the
+//     library must be reloaded before the next call;
+//   * the kernels report bad input (a position outside the grid, a non-finite
+//     contribution) in the array's error word, which the next call clears. A
+//     caller that passes err_out gets that word back: the call then waits for
+//     its work on the stream and returns AW_ERR_DEVICE when a bit is set.
 #include "aw_internal.h"
 
 #include <cstring>
@@ -64,7 +70,7 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) ==
 
 extern "C" int aw_deposit_rho_noalloc(const aw_grid* g, double qm, const float* x, const float* y,
                                       const float* ux, const float* uy, const float* uz, const float* w,
-                                      int64_t n, float* rho, void* stream) {
+                                      int64_t n, float* rho, void* stream, uint32_t* err_out) {
     using namespace aw;
     try {
         if (!g || !rho || (n > 0 && (!x || !y || !ux || !uy || !uz || !w)))
@@ -108,6 +114,12 @@ extern "C" int aw_deposit_rho_noalloc(const aw_grid* g, double qm, const float* 
         launch_deposit_src(c, 1);
         float* api[1] = {rho};
         launch_finalize(c, c.acc_src, 0, 1, c.st->S_pend, c.r_src, api, true, false, false);
+        if (err_out) {
+            // the error word of this call: read back before any later call clears it
+            AW_CUDA(cudaMemcpyAsync(err_out, &c.st->err, sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream));
+            AW_CUDA(cudaStreamSynchronize(c.stream));
+            if (*err_out != 0) throw Error(AW_ERR_DEVICE, "deposit_rho_noalloc: device error word set");
+        }
         return AW_OK;
     } catch (const Error& e) {
         g_last_error = e.what();

@@ -20,7 +20,8 @@ namespace {
 // ---------------------------------------------------------------------------
 // Loader. The hashed RNG and van der Corput streams are the reference's seeded
 // load (they define "identical seeded particles"), so the integer hash, the
-// stream constants and the expression forms are kept the same; see DESIGN.md.
+// stream constants and the expression forms are kept the same: that is what
+// makes a load here bit-identical to the reference's for the same seed.
 __device__ inline double radical_inverse_d(unsigned int i, unsigned int base) {
     double inv = 1.0 / double(base), f = inv, r = 0.0;
     while (i > 0) { r += double(i % base) * f; i /= base; f *= inv; }
@@ -521,11 +522,9 @@ void launch_sort_tiles(Ctx& c, int tx, int ty, bool physical) {
     c.bin_physical = physical;
     const size_t sh = sizeof(int) * static_cast<size_t>(ntiles);
     if (sh > 200 * 1024) throw Error(AW_ERR_ARG, "sort_tiles: too many tiles for shared memory");
-    static int attr_set = 0;
-    if (sh > 48 * 1024 && !attr_set) {
-        AW_CUDA(cudaFuncSetAttribute(k_bin_hist, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        AW_CUDA(cudaFuncSetAttribute(k_bin_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr_set = 1;
+    if (sh > 48 * 1024) {
+        opt_in_smem(reinterpret_cast<const void*>(k_bin_hist), 200 * 1024);
+        opt_in_smem(reinterpret_cast<const void*>(k_bin_scatter), 200 * 1024);
     }
     AW_CUDA(cudaMemsetAsync(c.bin_count, 0, sh, c.stream));
     const int blocks = std::min(grid_for(n), 4 * 148);

@@ -7,11 +7,12 @@
 
 Workloads (synthetic, seeded; the reference's own seeded loader streams):
   weibel512     spectral Darwin Weibel, 512x512, dx = 0.5, 64 ppc (16,777,216
-                electrons), v_th = (0.05, 0.05, 0.2), c = 1, dt = 0.05 (default)
+                electrons), v_th = (0.05, 0.05, 0.2), c = 1, dt = 0.05
   es256         electrostatic two-stream, 256x256, dx = 1, 2 x 32 ppc
                 (4,194,304), beams +-0.2, v_th = 0.01, dt = 0.1
   whistler1024  magnetised Darwin whistler pump, 1024x128, dx = 0.25, 256 ppc
-                (33,554,432), B0 = 0.5 at 30 deg in x-y, dt = 0.05
+                (33,554,432), B0 = 0.5 at 30 deg in x-y, dt = 0.05 (default: the
+                largest single-run configuration)
   ensemble64    64 independent seeded runs of uneven grids and particles per
                 cell (712 M particles in all), ES and Darwin, advanced together
                 by one graph launch per step; a bench step advances every run by
@@ -48,16 +49,23 @@ WARM_S = 2.0   # seconds of device work before a timed region: the SM clock leav
 
 
 def warm_clocks(torch, dev, seconds=WARM_S):
-    """Keep the GPU busy for `seconds` on a scratch buffer (1 GiB, streamed) so
+    """Keep the GPU busy for `seconds` on a scratch buffer (streamed adds) so
     that the timed region starts at the boost clock, without advancing the
-    simulation. Both arms call it between their warm-up steps and the timed steps."""
-    a = torch.zeros(1 << 28, dtype=torch.float32, device=dev)
+    simulation. Both arms call it, on their own device, between their warm-up
+    steps and the timed steps. The scratch is at most 1 GiB and at most a tenth
+    of the free device memory, and is returned to the driver afterwards."""
+    free, _ = torch.cuda.mem_get_info(dev)
+    nel = max(1 << 20, min(1 << 28, int(free // 40)))
+    a = torch.zeros(nel, dtype=torch.float32, device=dev)
     t = time.perf_counter()
     while time.perf_counter() - t < seconds:
         for _ in range(16):
             a.add_(1.0)
         torch.cuda.synchronize(dev)
     del a
+    torch.cuda.empty_cache()
+
+
 ALGO_BYTES_PER_PARTICLE = 44.0   # fused push+deposit: read x,y,ux,uy,uz,w (24 B), write x,y,ux,uy,uz (20 B)
 
 
@@ -121,6 +129,14 @@ def workload(name: str) -> dict:
 
 def nparticles(wl) -> int:
     return sum(s["ppc"] for s in wl["species"]) * wl["nx"] * wl["ny"]
+
+
+def bench_config(wl, n, world) -> dict:
+    """The `config` object of a single-run workload, the same in both arms."""
+    return {"workload": wl["desc"], "field_model": ("electrostatic", "darwin", "yee")[wl["model"]],
+            "grid": [wl["nx"], wl["ny"]], "particles_per_gpu": n,
+            "l2": f"particle SoA {n * 28 / 1e6:.0f} MB per step > 126 MB L2 (no flush needed)",
+            "parallelism": f"replicas x{world}"}
 
 
 def measured_peak_gbs():
@@ -372,10 +388,8 @@ def run_ours(args, wl, rank, world, dist):
         "dtype": "f32",
         "numerics": "f32 push/gather/solve; deposits exact int64 fixed point; diagnostics f64",
         "data": f"synthetic: reference seeded loader streams (noisy load, seed {seed})",
-        "config": {"workload": wl["desc"], "field_model": ("electrostatic", "darwin", "yee")[wl["model"]],
-                   "grid": [wl["nx"], wl["ny"]], "particles_per_gpu": n, "graph": True,
-                   "l2": f"particle SoA {n * 28 / 1e6:.0f} MB per step > 126 MB L2 (no flush needed)",
-                   "parallelism": f"replicas x{world}"},
+        "config": bench_config(wl, n, world),
+        "step": "one fused PIC step, replayed from a captured CUDA graph",
         "e2e": {"value": world * n * K / e2e_s, "unit": "particles/s",
                 "h2d_bytes_per_step": round(24 * n / K), "d2h_bytes_per_step": round(20 * n / K + 64),
                 "run": f"{K} steps: H2D of the particle state, aw_init, aw_run_diag (per-step FP64 diagnostics to "
@@ -708,49 +722,84 @@ def run_reference_ensemble(args, wl, rank):
 
 def run_reference(args, wl, rank, world):
     """The reference's own implementation of the step: its CUDA Simulation built
-    from its headers (oracle/_ref) when present, else the oracle port on CPU."""
+    from its headers (oracle/_ref) when present, else the oracle port on CPU.
+    `value` times the same steps as our arm (after the same warm-up and clock
+    warm-up); `e2e` is one config-length run like ours: the reference's init
+    (its device loader) and run_steps steps, then the final particle state
+    read back to the host."""
     if rank != 0:
         return None
     from oracle import refsim as R
     n = nparticles(wl)
+    K = wl["run_steps"]
+    e2e = None
     if R.available():
         import torch
-        torch.cuda.set_device(0)
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
         prm = R.params(dt=wl["dt"], c=wl["c"], n0=wl["n0"], B0=wl["B0"], pump=wl["pump"])
+        n0 = max(args.warmup, 3)
         if wl["model"] == 2:
             # MaxwellSimulation on its tiled path (physical tile sort every tile_sort steps), the
             # reference's own loader, its jfilter
-            rs = R.RefYee(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], prm, tile_sort=wl["tile_sort"],
-                          jfilter=wl.get("jfilter", 0), species=wl["species"], noisy=True, seed=wl.get("seed", 0))
-            rs.time_steps(max(args.warmup, 3))
-            warm_clocks(torch, torch.device("cuda:0"))
+            def make():
+                return R.RefYee(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], prm, tile_sort=wl["tile_sort"],
+                                jfilter=wl.get("jfilter", 0), species=wl["species"], noisy=True,
+                                seed=wl.get("seed", 0))
+            rs = make()
+            rs.time_steps(n0)
+            warm_clocks(torch, dev)
             ms = rs.time_steps(args.steps) / args.steps
+            rs.close()
+            rs = make()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            rs.time_steps(K)
+            final = {k: rs.get(k) for k in ("x", "y", "ux", "uy", "uz")}
+            e2e_s = time.perf_counter() - t0
             what = f"MaxwellSimulation, tile_sort {wl['tile_sort']}, jfilter {wl.get('jfilter', 0)}"
+            e2e_run = f"{K} steps after the reference's load, then the final particle state to the host"
         else:
-            rs = R.RefSim(wl["model"], wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], prm, wl["species"], noisy=True,
-                          seed=0)
+            def make():
+                return R.RefSim(wl["model"], wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], prm, wl["species"],
+                                noisy=True, seed=wl.get("seed", 0))
+            rs = make()
             rs.init()
-            rs.time_steps(0, max(args.warmup, 3))
-            warm_clocks(torch, torch.device("cuda:0"))
-            ms = rs.time_steps(max(args.warmup, 3), args.steps) / args.steps
+            rs.time_steps(0, n0)
+            warm_clocks(torch, dev)
+            ms = rs.time_steps(n0, args.steps) / args.steps
+            rs.close()
+            rs = make()
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            rs.init()
+            rs.time_steps(0, K)
+            final = {k: rs.get(k) for k in ("x", "y", "ux", "uy", "uz")}
+            e2e_s = time.perf_counter() - t0
             what = f"Simulation<{'CfgDarwin' if wl['model'] else 'Cfg'}>"
+            e2e_run = (f"{K} steps: init (the reference's device loader and t=0 fields) + {K} steps, then the "
+                       f"final particle state to the host (no host diagnostics: dump_every disabled)")
         rs.close()
+        del final
         val = n / (ms * 1e-3)
+        e2e = {"value": n * K / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": 0,
+               "d2h_bytes_per_step": round(20 * n / K), "run": e2e_run}
         cb = dict(value=val, unit="particles/s", cores=1, kind="reference", device="cuda",
-                  sample=f"{args.steps} steps of the reference {what} ({n} particles) on this GPU, "
-                         f"headers unmodified")
+                  sample=f"steps {n0}..{n0 + args.steps - 1} of the reference {what} ({n} particles) on this "
+                         f"GPU, headers unmodified")
     else:
         cb = cpu_baseline(wl, budget_s=30.0)
         val = cb["value"]
         ms = n / val * 1e3
+    if e2e is None:
+        e2e = {"value": val, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     return {
         "impl": "reference", "metric": "particles/s/step", "value": val, "unit": "particles/s", "n_gpus": 1,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None,
-        "config": {"workload": wl["desc"], "field_model": ("electrostatic", "darwin", "yee")[wl["model"]],
-                   "grid": [wl["nx"], wl["ny"]], "particles_per_gpu": n},
+        "config": bench_config(wl, n, world),
         "cpu_baseline": cb,
-        "e2e": {"value": val, "unit": "particles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": e2e,
     }
 
 
@@ -759,7 +808,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="weibel512")
+    ap.add_argument("--workload", default="whistler1024")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grad-steps", type=int, default=0, metavar="N",

@@ -353,10 +353,16 @@ int aw_fft_c2r(aw_ctx* ctx, void* kspace, float* out);
  * 262144 cells (AW_ERR_ARG beyond); each call clears the part it uses first,
  * and calls that overlap on the GPU race on it. The first call on a device
  * looks up the array's address (cudaGetSymbolAddress, with that device
- * current) and should come before any stream capture. */
+ * current) and should come before any stream capture; that address is kept
+ * for the life of the device's context (reload the library after a
+ * cudaDeviceReset). err_out (host memory, may be NULL): when given, the call
+ * waits for its work on `stream`, stores the device error bits (AW_DEV_*:
+ * positions outside the grid, non-finite contributions) there and returns
+ * AW_ERR_DEVICE if any is set; when NULL the call returns at once and those
+ * bits are discarded by the next call. */
 int aw_deposit_rho_noalloc(const aw_grid* g, double qm, const float* x, const float* y,
                            const float* ux, const float* uy, const float* uz, const float* w,
-                           int64_t n, float* rho, void* stream);
+                           int64_t n, float* rho, void* stream, uint32_t* err_out);
 
 /* ---- the fused, graph-capturable step (the product hot path) -------------
  * Simulation<Cfg>::init, include/pic/simulation.hpp:56-77: ES deposits, solves

@@ -37,7 +37,7 @@ def lib():
     global _lib
     if _lib is None:
         if not LIB.exists():
-            raise FileNotFoundError(f"{LIB} not built (make -C oracle ref, needs the reference sources)")
+            raise FileNotFoundError(f"{LIB} not built (make -C oracle ref REF=<ArcWarden source tree>)")
         L = C.CDLL(str(LIB))
         P, I, D, L_ = C.c_void_p, C.c_int, C.c_double, C.c_long
         L.ref_create.restype = P
