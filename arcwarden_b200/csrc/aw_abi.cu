@@ -144,7 +144,7 @@ struct NoMark { void operator()(int) const {} };
 template <class Mark>
 void es_fields_from_pending(Ctx& c, bool step_begin, Mark mark) {
     float* api[1] = {c.src.rho};
-    launch_finalize(c, c.acc_src, 0, 1, c.st->S_pend, c.r_src, api, false, true, step_begin); mark(0);
+    launch_finalize(c, c.acc_src, 0, 1, c.st->S_pend, c.r_src, api, false, true, step_begin, true); mark(0);
     AW_CUFFT(cufftExecR2C(c.p_r2cS, c.r_src, c.k_src)); mark(1);
     launch_kspace_es(c, c.k_src, c.k_out); mark(2);
     AW_CUFFT(cufftExecC2R(c.p_c2rO, c.k_out, c.r_out)); mark(3);
@@ -157,7 +157,7 @@ void es_fields_from_pending(Ctx& c, bool step_begin) { es_fields_from_pending(c,
 template <class Mark>
 void darwin_fields_a(Ctx& c, bool step_begin, Mark mark) {
     float* api[8] = {c.src.rho, c.src.Jx, c.src.Jy, c.src.Jz, c.src.amu0, c.src.amu1, c.src.amu2, c.src.amu3};
-    launch_finalize(c, c.acc_src, 0, 8, c.st->S_pend, c.r_src, api, false, true, step_begin); mark(0);
+    launch_finalize(c, c.acc_src, 0, 8, c.st->S_pend, c.r_src, api, false, true, step_begin, true); mark(0);
     AW_CUFFT(cufftExecR2C(c.p_r2cS, c.r_src, c.k_src)); mark(1);
     launch_kspace_elb(c, c.k_src, c.k_out); mark(2);
     AW_CUFFT(cufftExecC2R(c.p_c2rO, c.k_out, c.r_out)); mark(3);
@@ -242,6 +242,7 @@ void init_impl(Ctx& c) {
         // the Yee lattices are the caller's (the reference's YeeFields start at zero)
     } else if (c.model == AW_MODEL_ES) {
         aw::launch_deposit_src(c, 1);
+        aw::launch_charge_ref(c);                 // the mean the fused solves take out
         aw::es_fields_from_pending(c, false);
         // u -> u(-dt/2), gathering E(x^0) from the solve's output
         aw::launch_push_es_from(c, c.r_out, c.r_out + c.geo.ncell, -0.5f, false);
@@ -250,6 +251,7 @@ void init_impl(Ctx& c) {
         aw::launch_deposit_src(c, 1);    // pending rho(x^0) for step 0
     } else {
         aw::launch_deposit_src(c, 8);
+        aw::launch_charge_ref(c);                  // the mean the fused solves take out
         aw::launch_rms_reduce(c, true, false);     // source rms for the capped scales
         aw::darwin_fields_from_pending(c, true);   // t = 0 fields
         aw::launch_copy_umax(c);

@@ -80,6 +80,9 @@ struct DevState {
     float     rms_dcu[4];      // rms of the dcu coefficients (unscaled)
     unsigned long long chunks, overflow, slow;
     unsigned  red_ticket;      // k_step_reduce blocks finished (reset by the last)
+    double    rho_ref;         // mean charge density, subtracted from the fused solve's
+                               // FFT input (the k = 0 mode is zeroed anyway): a large
+                               // mean would otherwise put FP32 roundoff into every mode
 };
 
 // ---------------------------------------------------------------------------

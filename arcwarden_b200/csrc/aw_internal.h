@@ -273,8 +273,12 @@ void multi_free(MultiPhase* m);
 // ---- launchers (aw_spectral.cu) -------------------------------------------
 int  grid_partial_blocks();
 void launch_make_scales(Ctx& c);
+// sub_ref: field 0 is the charge density; its staging gets rho - st->rho_ref.
 void launch_finalize(Ctx& c, unsigned long long* acc, int first, int nf, const float* S, float* r,
-                     float* const* api, bool accumulate, bool charge_partials, bool step_begin);
+                     float* const* api, bool accumulate, bool charge_partials, bool step_begin,
+                     bool sub_ref = false);
+// st->rho_ref from the pending charge deposit (acc_src field 0, scale S_pend[0]).
+void launch_charge_ref(Ctx& c);
 void launch_kspace_es(Ctx& c, const cufftComplex* rho_k, cufftComplex* e_k);
 void launch_es_solve_k(Ctx& c, const cufftComplex* rho_k, cufftComplex* ex_k, cufftComplex* ey_k);
 void launch_kspace_elb(Ctx& c, const cufftComplex* src_k, cufftComplex* out_k);

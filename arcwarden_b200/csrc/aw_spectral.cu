@@ -87,15 +87,22 @@ __global__ void k_make_scales(DevState* st, float cref) {
 // into real staging r[(f-first)*ncell + c] and optional caller arrays; two
 // cells per thread so every field's loads are in flight together. At most 64
 // registers: 4 CTAs per SM, so the fixed grid of the charge partials
-// (kGridBlocks) is one wave.
+// (kGridBlocks) is one wave. With sub_ref, field 0 (the charge density) goes
+// to the staging as rho - st->rho_ref (the caller's array keeps rho): the
+// staging feeds the R2C, whose k = 0 mode the solve discards, and with the
+// mean removed the FP32 transform's roundoff scales with the fluctuations
+// instead of the (about 20x larger) mean. Without it, the mean's roundoff
+// gathers in the kx = 0 column and reaches E_y at the 1e-5 level on a 512^2
+// grid.
 struct FinOut { float* p[8]; };
 template <int NF>
 __global__ void __launch_bounds__(kThreads, 4)
 k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
            const float* __restrict__ Sdev, float* __restrict__ r, FinOut api, int accumulate,
            double* __restrict__ part, DevState* st, int step_begin, double dt, float cref, int darwin,
-           AdjDev* rec) {
+           AdjDev* rec, int sub_ref) {
     double qsum = 0.0;
+    const double ref0 = (sub_ref && first == 0) ? st->rho_ref : 0.0;
     const int npair = (ncell + 1) >> 1;
     for (int pi = blockIdx.x * blockDim.x + threadIdx.x; pi < npair; pi += gridDim.x * blockDim.x) {
         const int c = 2 * pi;
@@ -127,19 +134,23 @@ k_finalize(unsigned long long* __restrict__ acc, int first, int ncell,
             // 1.0 / S, taken here rather than hoisted: a thread finalises about one
             // cell pair, and NF hoisted doubles would cost the fourth CTA per SM
             const double invS = __drcp_rn(static_cast<double>(__ldg(Sdev + first + f)));
-            const float a0 = __double2float_rn(static_cast<double>(v[f][0]) * invS);
-            const float a1 = __double2float_rn(static_cast<double>(v[f][1]) * invS);
+            const double d0 = static_cast<double>(v[f][0]) * invS, d1 = static_cast<double>(v[f][1]) * invS;
+            const float a0 = __double2float_rn(d0);
+            const float a1 = __double2float_rn(d1);
+            // the staging value (field 0 minus the mean when sub_ref)
+            const float s0 = f == 0 ? __double2float_rn(d0 - ref0) : a0;
+            const float s1 = f == 0 ? __double2float_rn(d1 - ref0) : a1;
             float* rf = r + static_cast<size_t>(f) * ncell + c;
             float* o = api.p[f];
             if (two) {
-                if (vec) *reinterpret_cast<float2*>(rf) = make_float2(a0, a1);
-                else { rf[0] = a0; rf[1] = a1; }
+                if (vec) *reinterpret_cast<float2*>(rf) = make_float2(s0, s1);
+                else { rf[0] = s0; rf[1] = s1; }
                 if (o) {
                     if (accumulate) { o[c] = __fadd_rn(o[c], a0); o[c + 1] = __fadd_rn(o[c + 1], a1); }
                     else { o[c] = a0; o[c + 1] = a1; }
                 }
             } else {
-                rf[0] = a0;
+                rf[0] = s0;
                 if (o) o[c] = accumulate ? __fadd_rn(o[c], a0) : a0;
             }
             if (first + f == 0) qsum += static_cast<double>(a0) + (two ? static_cast<double>(a1) : 0.0);
@@ -832,7 +843,31 @@ __global__ void k_yee_ampere(YeeF v, unsigned long long* __restrict__ acc, const
 
 int grid_partial_blocks() { return kGridBlocks; }
 
+// Mean charge density of the pending deposit, st->rho_ref = sum(acc[0]) / S / ncell:
+// one block, an exact int64 sum (order-free), so every run from the same
+// particles gets the same bits.
+__global__ void __launch_bounds__(1024) k_charge_ref(const unsigned long long* __restrict__ acc, int ncell,
+                                                     const float* __restrict__ S, DevState* st) {
+    long long t = 0;
+    for (int c = threadIdx.x; c < ncell; c += blockDim.x) t += static_cast<long long>(acc[c]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    __shared__ long long sh[32];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = t;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long s = 0;
+        for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) s += sh[w];
+        st->rho_ref = static_cast<double>(s) / static_cast<double>(S[0]) / static_cast<double>(ncell);
+    }
+}
+
 // ===========================================================================
+void launch_charge_ref(Ctx& c) {
+    k_charge_ref<<<1, 1024, 0, c.stream>>>(c.acc_src, c.geo.ncell, c.st->S_pend, c.st);
+    AW_LAUNCH();
+}
+
 void launch_make_scales(Ctx& c) {
     k_make_scales<<<1, 1, 0, c.stream>>>(c.st, cref_of(c));
     AW_LAUNCH();
@@ -840,7 +875,7 @@ void launch_make_scales(Ctx& c) {
 
 // Finalise acc fields [first, first+nf) with scales S into r (+ api arrays).
 void launch_finalize(Ctx& c, unsigned long long* acc, int first, int nf, const float* S, float* r,
-                     float* const* api, bool accumulate, bool charge_partials, bool step_begin) {
+                     float* const* api, bool accumulate, bool charge_partials, bool step_begin, bool sub_ref) {
     FinOut o{};
     for (int f = 0; f < nf && f < 8; ++f) o.p[f] = api ? api[f] : nullptr;
     const int blocks = std::max(kGridBlocks, std::min(4096, (c.geo.ncell / 2 + kThreads - 1) / kThreads));
@@ -850,11 +885,12 @@ void launch_finalize(Ctx& c, unsigned long long* acc, int first, int nf, const f
     if (charge_partials && blocks != kGridBlocks) throw Error(AW_ERR_STATE, "finalize: partials need the fixed grid");
     const int nb = charge_partials ? kGridBlocks : blocks;
     AdjDev* rec = step_begin ? c.rec_ad : nullptr;
+    const int sr = (sub_ref && first == 0) ? 1 : 0;
     switch (nf) {
-        case 1: k_finalize<1><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec); break;
-        case 3: k_finalize<3><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec); break;
-        case 4: k_finalize<4><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec); break;
-        case 8: k_finalize<8><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec); break;
+        case 1: k_finalize<1><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec, sr); break;
+        case 3: k_finalize<3><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec, sr); break;
+        case 4: k_finalize<4><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec, sr); break;
+        case 8: k_finalize<8><<<nb, kThreads, 0, c.stream>>>(acc, first, c.geo.ncell, S, r, o, acc_, part, c.st, sb, c.prm.dt, cref, dw, rec, sr); break;
         default: throw Error(AW_ERR_ARG, "finalize: unsupported field count");
     }
     AW_LAUNCH();
