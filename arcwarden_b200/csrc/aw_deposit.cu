@@ -139,6 +139,39 @@ __device__ __forceinline__ void src_coefs(float coef, float ux, float uy, float 
     }
 }
 
+// The eight Darwin source coefficients of src_coefs<SET_ALL> as pairs
+// (rho, Jx), (Jy, Jz), (amu0, amu1), (amu2, amu3): the same products, two per
+// packed multiply (amu1 = (coef ux) uy and amu2,3 = (coef uz) ux,y reuse the J
+// products, which src_coefs rounds identically).
+__device__ __forceinline__ void src_coefs8(float coef, float ux, float uy, float uz, float2 (&cp)[4]) {
+    const float2 uxy = make_float2(ux, uy);
+    const float2 jxy = __fmul2_rn(bc2(coef), uxy);
+    const float jz = __fmul_rn(coef, uz);
+    const float2 sq = __fmul2_rn(uxy, uxy);
+    const float d = __fsub_rn(sq.x, sq.y);
+    cp[0] = make_float2(coef, jxy.x);
+    cp[1] = make_float2(jxy.y, jz);
+    cp[2] = make_float2(__fmul_rn(__fmul_rn(coef, 0.5f), d), __fmul_rn(jxy.x, uy));
+    cp[3] = __fmul2_rn(bc2(jz), uxy);
+}
+// Scaled pairs cs = fl(cf * S), their fast-range test and, for a fast
+// particle, the window bounds l1 += |cs| (as scale_fast, two fields at a time).
+template <int NP>
+__device__ __forceinline__ bool scale_fast2(const float2 (&cf)[NP], const float2 (&S)[NP], float2 (&cs)[NP],
+                                            float2 (&l1)[NP]) {
+    bool fast = true;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+        cs[i] = __fmul2_rn(cf[i], S[i]);
+        fast = fast && (fabsf(cs[i].x) < kFastLim) && (fabsf(cs[i].y) < kFastLim);
+    }
+    if (fast) {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) l1[i] = __fadd2_rn(l1[i], make_float2(fabsf(cs[i].x), fabsf(cs[i].y)));
+    }
+    return fast;
+}
+
 // Scaled coefficients cs = fl(cf * S) and whether every one is inside the fast
 // range (|cs| < 2^22; the CIC weights are <= 1, so every product is too). A
 // fast particle's |cs| are added to the thread's window bounds l1.
@@ -325,6 +358,40 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
 }
 
 // ---------------------------------------------------------------------------
+// The EM gather of the four corners' [Ex Ey Ez Bx | By Bz . .] records a[k],
+// b[k] with gather4_tile's arithmetic, fields in pairs: (Ex, Ey), (Ez, Bx),
+// (By, Bz).
+struct EB2 { float2 exy, ezbx, byz; };
+__device__ __forceinline__ EB2 gather_em_pairs(const Cic& s, const float4 (&a)[4], const float4 (&b)[4]) {
+    const float2 W[4] = {bc2(s.w0), bc2(s.w1), bc2(s.w2), bc2(s.w3)};
+    EB2 r;
+    r.exy  = gather4_tile2(W, lo2(a[0]), lo2(a[1]), lo2(a[2]), lo2(a[3]));
+    r.ezbx = gather4_tile2(W, hi2(a[0]), hi2(a[1]), hi2(a[2]), hi2(a[3]));
+    r.byz  = gather4_tile2(W, lo2(b[0]), lo2(b[1]), lo2(b[2]), lo2(b[3]));
+    return r;
+}
+// From the interleaved buffer gb[ncell][8] in global memory.
+__device__ __forceinline__ EB2 gather_em2(const float* __restrict__ gb, const Cic& s, const Geo& g) {
+    const int i0 = s.i0, i1 = wrap_once(s.i0 + 1, g.nx);
+    const int r0 = s.j0 * g.nx, r1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
+    const float4* q = reinterpret_cast<const float4*>(gb);
+    const int cc[4] = {r0 + i0, r0 + i1, r1 + i0, r1 + i1};
+    float4 a[4], b[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { a[k] = __ldg(q + 2 * cc[k]); b[k] = __ldg(q + 2 * cc[k] + 1); }
+    return gather_em_pairs(s, a, b);
+}
+// From the chunk's shared tile (W cells per row; (li, lj) the base cell in it).
+__device__ __forceinline__ EB2 gather_em_tile2(const float* __restrict__ tile, const Cic& s, int li, int lj, int W) {
+    const float4* q = reinterpret_cast<const float4*>(tile);
+    const int c0 = lj * W + li, c2 = c0 + W;
+    const int cc[4] = {c0, c0 + 1, c2, c2 + 1};
+    float4 a[4], b[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { a[k] = q[2 * cc[k]]; b[k] = q[2 * cc[k] + 1]; }
+    return gather_em_pairs(s, a, b);
+}
+
 // EM gather from the interleaved buffer gb[ncell][8] = Ex Ey Ez Bx | By Bz . .
 __device__ __forceinline__ void gather_em(const float* __restrict__ gb, const Cic& s, const Geo& g,
                                           float& ex, float& ey, float& ez,
@@ -515,17 +582,16 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
             if (in_grid(x, y, g)) {
                 const Cic c = cic(x, y);
                 bb.add(c.i0, c.j0, ir, jr, g);
-                float ex, ey, ez, bx, by, bz;
-                if (tl.use)
-                    gather_em_tile(tile, c, c.i0 - tl.i0, c.j0 - tl.j0, tl.W, ex, ey, ez, bx, by, bz);
-                else
-                    gather_em(gb, c, g, ex, ey, ez, bx, by, bz);
+                const EB2 eb = tl.use ? gather_em_tile2(tile, c, c.i0 - tl.i0, c.j0 - tl.j0, tl.W)
+                                      : gather_em2(gb, c, g);
+                const float bx = eb.ezbx.y, by = eb.byz.x, bz = eb.byz.y;
                 const float coef = __double2float_rn(qm2oa * static_cast<double>(w));
-                const float cx = __fmaf_rn(vy, bz, -__fmul_rn(vz, by));
-                const float cy = __fmaf_rn(vz, bx, -__fmul_rn(vx, bz));
+                // v x B: (cx, cy) = (vy bz - vz by, vz bx - vx bz) paired, cz = vx by - vy bx
+                const float2 nxy = __fmul2_rn(make_float2(vz, vx), make_float2(-by, -bz));
+                const float2 cxy = __ffma2_rn(make_float2(vy, vz), make_float2(bz, bx), nxy);
                 const float cz = __fmaf_rn(vx, by, -__fmul_rn(vy, bx));
-                const float cf[NF] = {__fmul_rn(coef, __fadd_rn(ex, cx)), __fmul_rn(coef, __fadd_rn(ey, cy)),
-                                      __fmul_rn(coef, __fadd_rn(ez, cz))};
+                const float2 cfxy = __fmul2_rn(bc2(coef), __fadd2_rn(eb.exy, cxy));
+                const float cf[NF] = {cfxy.x, cfxy.y, __fmul_rn(coef, __fadd_rn(eb.ezbx.x, cz))};
                 const bool fast = scale_fast<NF>(cf, S, cs, l1);
                 if (((c.i0 + c.j0) & 7) == 0) {   // rms sample: the particles of one cell in 8, any order
 #pragma unroll
@@ -727,9 +793,17 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
                 const int r0 = c.j0 * g.nx, r1 = wrap_once(c.j0 + 1, g.ny) * g.nx;
                 const float2 e0 = __ldg(q + r0 + c.i0), e1 = __ldg(q + r0 + i1);
                 const float2 e2 = __ldg(q + r1 + c.i0), e3 = __ldg(q + r1 + i1);
-                const float ex = gather4(c, e0.x, e1.x, e2.x, e3.x);
-                const float ey = gather4(c, e0.y, e1.y, e2.y, e3.y);
-                boris_es(ux, uy, uz, ex, ey, pp.qmh, pp.has_b0 != 0, pp.b0x, pp.b0y, pp.b0z);
+                // gather4 on the (Ex, Ey) pair, then the half kicks paired
+                float2 exy = __fmul2_rn(bc2(c.w0), e0);
+                exy = __ffma2_rn(bc2(c.w1), e1, exy);
+                exy = __ffma2_rn(bc2(c.w2), e2, exy);
+                exy = __ffma2_rn(bc2(c.w3), e3, exy);
+                const float2 Q = bc2(pp.qmh);
+                float2 uxy = __ffma2_rn(Q, exy, make_float2(ux, uy));
+                ux = uxy.x; uy = uxy.y;
+                if (pp.has_b0) boris_rotate(ux, uy, uz, pp.b0x, pp.b0y, pp.b0z, pp.qmh);
+                uxy = __ffma2_rn(Q, exy, make_float2(ux, uy));
+                ux = uxy.x; uy = uxy.y;
                 move_xy<POW2>(x, y, ux, uy, pp, g);
                 int ci, cj;
                 cell_ij(x, y, g, ci, cj);
@@ -802,6 +876,8 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
     float S[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) S[f] = st->S_next[f];
+    const float2 Sp[4] = {make_float2(S[0], S[1]), make_float2(S[2], S[3]), make_float2(S[4], S[5]),
+                          make_float2(S[6], S[7])};
     if (threadIdx.x == 0) nlist = 0;
     const ChunkSrc src{{p.x, p.y, p.w, p.ux, p.uy, p.uz}};
     float x0, y0;
@@ -828,10 +904,9 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
     if (tl.use && !load_tile8(tile, gb, tl, g, &tbar, st)) return;
 
     BBox bb;
-    float l1[NF] = {};
+    float2 l1p[4] = {}, sqp[4] = {};
     double ke = 0, px = 0, py = 0, pz = 0;
     float m0 = 0.f, m1 = 0.f, m2 = 0.f;
-    float sq[NF] = {};
     float nval = 0.f;
 #pragma unroll 2
     for (int it = 0; it < kPPT; ++it) {
@@ -844,12 +919,11 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
         if (s < cnt) {
             if (in_grid(x, y, g)) {
                 const Cic c = cic(x, y);
-                float ex, ey, ez, bx, by, bz;
-                if (tl.use)
-                    gather_em_tile(tile, c, c.i0 - tl.i0, c.j0 - tl.j0, tl.W, ex, ey, ez, bx, by, bz);
-                else
-                    gather_em(gb, c, g, ex, ey, ez, bx, by, bz);
-                boris_em(ux, uy, uz, ex, ey, ez, bx, by, bz, pp.qmh);
+                const EB2 eb = tl.use ? gather_em_tile2(tile, c, c.i0 - tl.i0, c.j0 - tl.j0, tl.W)
+                                      : gather_em2(gb, c, g);
+                float2 uxy = make_float2(ux, uy);
+                boris_em2(uxy, uz, eb.exy, eb.ezbx.x, eb.ezbx.y, eb.byz, pp.qmh);
+                ux = uxy.x; uy = uxy.y;
                 move_xy<POW2>(x, y, ux, uy, pp, g);
                 int ci, cj;
                 cell_ij(x, y, g, ci, cj);
@@ -859,13 +933,13 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
                 m0 = fmaxf(m0, fabsf(ux)); m1 = fmaxf(m1, fabsf(uy)); m2 = fmaxf(m2, fabsf(uz));
                 if (in_grid(x, y, g)) {
                     bb.add(ci, cj, ir, jr, g);
-                    float cf[NF], cs[NF];
+                    float2 cp[4], csp[4];
                     cf0 = __double2float_rn(qoa * static_cast<double>(w));
-                    src_coefs<SET_ALL>(cf0, ux, uy, uz, cf);
-                    const bool fast = scale_fast<NF>(cf, S, cs, l1);
+                    src_coefs8(cf0, ux, uy, uz, cp);
+                    const bool fast = scale_fast2<4>(cp, Sp, csp, l1p);
                     if (((ci + cj) & 7) == 0) {   // rms sample: the particles of one cell in 8, any order
 #pragma unroll
-                        for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
+                        for (int i = 0; i < 4; ++i) sqp[i] = __ffma2_rn(cp[i], cp[i], sqp[i]);
                         nval += 1.0f;
                     }
                     xs = __fadd_rn(x, 0.0f);
@@ -898,6 +972,9 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
         umx[1][threadIdx.x >> 5] = __float_as_uint(m1);
         umx[2][threadIdx.x >> 5] = __float_as_uint(m2);
     }
+    float l1[NF], sq[NF];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { l1[2 * i] = l1p[i].x; l1[2 * i + 1] = l1p[i].y; sq[2 * i] = sqp[i].x; sq[2 * i + 1] = sqp[i].y; }
     const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
     if (threadIdx.x < 3) {
         unsigned mx = 0;
@@ -905,10 +982,13 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
         atomicMax(&st->umax_bits[threadIdx.x], mx);
     }
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
-        float cf[NF];
-        src_coefs<SET_ALL>(a[2], a[3], a[4], a[5], cf);
+        float2 cp[4];
+        src_coefs8(a[2], a[3], a[4], a[5], cp);
 #pragma unroll
-        for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cf[f], S[f]);
+        for (int i = 0; i < 4; ++i) {
+            const float2 c = __fmul2_rn(cp[i], Sp[i]);
+            cs[2 * i] = c.x; cs[2 * i + 1] = c.y;
+        }
     };
     window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef, acc);
     close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);

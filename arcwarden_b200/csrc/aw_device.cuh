@@ -159,6 +159,41 @@ __device__ __forceinline__ float gather4_tile(const Cic& s, float a, float b, fl
 }
 
 // ---------------------------------------------------------------------------
+// Packed FP32 pairs. Blackwell issues two FP32 multiplies, adds or fused
+// multiply-adds as one instruction (__fmul2_rn, __fadd2_rn, __ffma2_rn); each
+// component rounds exactly like the scalar __fmul_rn / __fadd_rn / __fmaf_rn,
+// so pairing two independent operations of the same kind changes no bit.
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 lo2(const float4& v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 hi2(const float4& v) { return make_float2(v.z, v.w); }
+
+// CIC weights as corner pairs: w01 = (w0, w1), w23 = (w2, w3), the same
+// products as cic(): (gx gy, fx gy) and (gx fy, fx fy).
+struct Cic2 {
+    int    i0, j0;
+    float2 w01, w23;
+};
+__device__ __forceinline__ Cic2 cic2(float x, float y) {
+    Cic2 s;
+    s.i0 = static_cast<int>(x);
+    s.j0 = static_cast<int>(y);
+    const float2 f = __fadd2_rn(make_float2(x, y), make_float2(-static_cast<float>(s.i0), -static_cast<float>(s.j0)));
+    const float2 g = __fadd2_rn(make_float2(1.0f, 1.0f), make_float2(-f.x, -f.y));
+    const float2 gxfx = make_float2(g.x, f.x);
+    s.w01 = __fmul2_rn(gxfx, bc2(g.y));
+    s.w23 = __fmul2_rn(gxfx, bc2(f.y));
+    return s;
+}
+// gather4_tile on a pair of fields: corner values a..d hold the pair of each
+// corner, W0..W3 the weights broadcast to both halves.
+__device__ __forceinline__ float2 gather4_tile2(const float2 (&W)[4], float2 a, float2 b, float2 c, float2 d) {
+    float2 r = __ffma2_rn(W[0], a, __fmul2_rn(W[1], b));
+    r = __ffma2_rn(W[2], c, r);
+    r = __ffma2_rn(W[3], d, r);
+    return r;
+}
+
+// ---------------------------------------------------------------------------
 // Boris rotation about (bx,by,bz) with qmh = (q/m) dt/2 — pusher.hpp:85-97.
 __device__ __forceinline__ void boris_rotate(float& ux, float& uy, float& uz,
                                              float bx, float by, float bz, float qmh) {
@@ -189,6 +224,31 @@ __device__ __forceinline__ void boris_em(float& ux, float& uy, float& uz,
     ux = __fmaf_rn(qmh, ex, ux); uy = __fmaf_rn(qmh, ey, uy); uz = __fmaf_rn(qmh, ez, uz);
     boris_rotate(ux, uy, uz, bx, by, bz, qmh);
     ux = __fmaf_rn(qmh, ex, ux); uy = __fmaf_rn(qmh, ey, uy); uz = __fmaf_rn(qmh, ez, uz);
+}
+// The same push with the x-y components paired (the operations of boris_em
+// and boris_rotate, two at a time where they are independent).
+__device__ __forceinline__ void boris_em2(float2& uxy, float& uz, float2 exy, float ez, float bx, float2 byz,
+                                          float qmh) {
+    const float2 Q = bc2(qmh);
+    uxy = __ffma2_rn(Q, exy, uxy);
+    uz = __fmaf_rn(qmh, ez, uz);
+    const float tx = __fmul_rn(qmh, bx);
+    const float2 tyz = __fmul2_rn(Q, byz);
+    const float t2 = __fmaf_rn(tyz.y, tyz.y, __fmaf_rn(tyz.x, tyz.x, __fmul_rn(tx, tx)));
+    const float sf = __fdiv_rn(2.0f, __fadd_rn(1.0f, t2));
+    const float sx = __fmul_rn(sf, tx);
+    const float2 syz = __fmul2_rn(bc2(sf), tyz);
+    const float ux = uxy.x, uy = uxy.y;
+    // u' = u + u x t: (upx, upy) = (ux + (uy tz - uz ty), uy + (uz tx - ux tz))
+    const float2 pn = __fmul2_rn(make_float2(uz, ux), make_float2(-tyz.x, -tyz.y));   // -(uz ty), -(ux tz)
+    const float2 upxy = __fadd2_rn(uxy, __ffma2_rn(make_float2(uy, uz), make_float2(tyz.y, tx), pn));
+    const float upz = __fadd_rn(uz, __fmaf_rn(ux, tyz.x, -__fmul_rn(uy, tx)));
+    // u += u' x s: (ux + (upy sz - upz sy), uy + (upz sx - upx sz)), uz + (upx sy - upy sx)
+    const float2 qn = __fmul2_rn(make_float2(upz, upxy.x), make_float2(-syz.x, -syz.y));   // -(upz sy), -(upx sz)
+    uxy = __fadd2_rn(uxy, __ffma2_rn(make_float2(upxy.y, upz), make_float2(syz.y, sx), qn));
+    uz = __fadd_rn(uz, __fmaf_rn(upxy.x, syz.x, -__fmul_rn(upxy.y, sx)));
+    uxy = __ffma2_rn(Q, exy, uxy);
+    uz = __fmaf_rn(qmh, ez, uz);
 }
 // Move in cell units: x += float(double(u) * dt / dx) — pusher.hpp:126-127.
 __device__ __forceinline__ float move1(float x, float u, double dt, double d) {
@@ -567,6 +627,38 @@ __device__ __forceinline__ void slow_pass(const float* __restrict__ stage, const
     if (n) atomicAdd(&st->slow, static_cast<unsigned long long>(n));
 }
 
+// Grid cell of window cell (0, 0): the reference cell plus the minimum offsets,
+// wrapped (the window spans less than the grid plus one cell, so a valid
+// particle's cell lies in [o, o + W) modulo n).
+__device__ __forceinline__ int win_origin(int r, int m, int n) {
+    int o = r + m;
+    if (o < 0) o += n;
+    if (o >= n) o -= n;
+    return o;
+}
+// Window column (row) of a particle's base cell c, from the window origin o.
+__device__ __forceinline__ int win_col(int c, int o, int n) {
+    const int d = c - o;
+    return d < 0 ? d + n : d;
+}
+
+// The NF x 4 rounded contributions of one particle, two corners per packed
+// FMA: (q0, q1) from (w0, w1), (q2, q3) from (w2, w3), each exactly
+// quant(cs[f], w_k).
+template <int NF>
+__device__ __forceinline__ void quant_corners(const float (&cs)[NF], const Cic2& c, int (&v)[NF][4]) {
+    const float2 M2 = bc2(kMagic);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        const float2 C = bc2(cs[f]);
+        const float2 q01 = __ffma2_rn(C, c.w01, M2), q23 = __ffma2_rn(C, c.w23, M2);
+        v[f][0] = __float_as_int(q01.x) - kMagicBits;
+        v[f][1] = __float_as_int(q01.y) - kMagicBits;
+        v[f][2] = __float_as_int(q23.x) - kMagicBits;
+        v[f][3] = __float_as_int(q23.y) - kMagicBits;
+    }
+}
+
 // Window pass: lane l of warp w deposits the chunk slots 64 l + 8 w + k,
 // k = 0..7, one particle at a time: each of its NF x 4 rounded contributions is
 // one native 32-bit shared atomic into the window (field 0 wrap-tracked when
@@ -577,6 +669,7 @@ template <int NF, int NS, bool T0, bool TRACK_ALL, class CoefFn>
 __device__ __forceinline__ void window_particles(const float* __restrict__ stage, int* __restrict__ win,
                                                  const Win& wn, const Geo& g, CoefFn coef) {
     const int base = 64 * (threadIdx.x & 31) + 8 * (threadIdx.x >> 5);
+    const int oi = win_origin(wn.ir, wn.mi, g.nx), oj = win_origin(wn.jr, wn.mj, g.ny);
     const int offs[4] = {0, 1, wn.W, wn.W + 1};
 #pragma unroll 1
     for (int k = 0; k < kPPT; ++k) {
@@ -585,19 +678,19 @@ __device__ __forceinline__ void window_particles(const float* __restrict__ stage
 #pragma unroll
         for (int f = 0; f < NS; ++f) a[f] = stage[f * kChunk + d];
         if (__float_as_int(a[0]) < 0) continue;
-        const Cic c = cic(a[0], a[1]);
+        const Cic2 c = cic2(a[0], a[1]);
         float cs[NF];
         coef(a, cs);
-        const float wv[4] = {c.w0, c.w1, c.w2, c.w3};
-        const int cw = (win_off(c.j0, wn.jr, g.ny) - wn.mj) * wn.W + (win_off(c.i0, wn.ir, g.nx) - wn.mi);
+        int v[NF][4];
+        quant_corners<NF>(cs, c, v);
+        const int cw = win_col(c.j0, oj, g.ny) * wn.W + win_col(c.i0, oi, g.nx);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
             int* e = win + 2 * f * wn.WH + cw;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                const int v = quant(cs[f], wv[q]);
-                if (TRACK_ALL || (T0 && f == 0)) add_tracked(e + offs[q], wn.WH, v);
-                else atomicAdd(e + offs[q], v);
+                if (TRACK_ALL || (T0 && f == 0)) add_tracked(e + offs[q], wn.WH, v[f][q]);
+                else atomicAdd(e + offs[q], v[f][q]);
             }
         }
     }
@@ -610,23 +703,25 @@ template <int NF, int NS, bool T0, bool TRACK_ALL, class CoefFn>
 __device__ __forceinline__ void window_band(const float* __restrict__ stage, int* __restrict__ win,
                                             const Win& wn, int r0, const Geo& g, CoefFn coef) {
     const int base = 64 * (threadIdx.x & 31) + 8 * (threadIdx.x >> 5);
+    const int oi = win_origin(wn.ir, wn.mi, g.nx), oj = win_origin(wn.jr, wn.mj, g.ny);
 #pragma unroll 1
     for (int k = 0; k < kPPT; ++k) {
         const int d = stage_slot(base + k);
         const float x = stage[d];
         if (__float_as_int(x) < 0) continue;
         const float y = stage[kChunk + d];
-        const int rj = win_off(static_cast<int>(y), wn.jr, g.ny) - wn.mj - r0;
+        const int rj = win_col(static_cast<int>(y), oj, g.ny) - r0;
         if (rj < -1 || rj >= wn.Hb) continue;        // both rows outside the band
         float a[NS];
         a[0] = x; a[1] = y;
 #pragma unroll
         for (int f = 2; f < NS; ++f) a[f] = stage[f * kChunk + d];
-        const Cic c = cic(a[0], a[1]);
+        const Cic2 c = cic2(a[0], a[1]);
         float cs[NF];
         coef(a, cs);
-        const float wv[4] = {c.w0, c.w1, c.w2, c.w3};
-        const int ci = win_off(c.i0, wn.ir, g.nx) - wn.mi;
+        int v[NF][4];
+        quant_corners<NF>(cs, c, v);
+        const int ci = win_col(c.i0, oi, g.nx);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int row = rj + (q >> 1);                // corners 0, 1 in row rj; 2, 3 in rj + 1
@@ -634,10 +729,9 @@ __device__ __forceinline__ void window_band(const float* __restrict__ stage, int
             const int cw = row * wn.W + ci + (q & 1);
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
-                const int v = quant(cs[f], wv[q]);
                 int* t = win + 2 * f * wn.WH + cw;
-                if (TRACK_ALL || (T0 && f == 0)) add_tracked(t, wn.WH, v);
-                else atomicAdd(t, v);
+                if (TRACK_ALL || (T0 && f == 0)) add_tracked(t, wn.WH, v[f][q]);
+                else atomicAdd(t, v[f][q]);
             }
         }
     }
