@@ -61,7 +61,7 @@ template <> struct SetNF<SET_ALL>  { static constexpr int NF = 8, NS = 6; };
 // chunk of 2048 particles covers ~30-250 cells at 64 per cell; a chunk whose
 // window does not fit takes the exact slow path.
 constexpr int wmax_cells(int nf) {
-    return (nf == 1 || nf == 2) ? 2048 : (nf == 3 ? 896 : (nf == 4 ? 1536 : 320));
+    return nf == 1 ? 2048 : (nf == 2 ? 1920 : (nf == 3 ? 800 : (nf == 4 ? 1536 : 320)));
 }
 constexpr int kRedInts = kThreads / 32 * (4 + 8);
 // The fused ES kernel stages 5 planes and takes one of two rho windows. The ES
@@ -71,14 +71,14 @@ constexpr int kRedInts = kThreads / 32 * (4 + 8);
 // below that whole grid rows and their spread in y (3584 cells: 14 rows of 256,
 // 3 CTAs per SM).
 constexpr int kEsPlanes = 5, kEsWindowSmall = 1024, kEsWindowLarge = 3584;
-// stage [np][kChunk] f32 | window [2*nf][wmax] i32 | red ints | slow list u16[kChunk]
+// stage [np][kChunk] f32 | window [planes][wmax] i32 | red ints | slow list u16[kChunk]
 constexpr size_t win_offset(int np) { return static_cast<size_t>(np) * kChunk * 4; }
-constexpr size_t smem_bytes_w(int nf, int np, int wmax) {
-    return win_offset(np) + static_cast<size_t>(wmax) * nf * 8 + kRedInts * sizeof(int)
+constexpr size_t smem_bytes_w(int nf, int np, int wmax, int planes) {
+    return win_offset(np) + static_cast<size_t>(wmax) * planes * 4 + kRedInts * sizeof(int)
            + kChunk * sizeof(unsigned short);
 }
-constexpr size_t smem_bytes(int nf, int np) { return smem_bytes_w(nf, np, wmax_cells(nf)); }
-constexpr size_t es_smem_bytes(int wmax) { return smem_bytes_w(1, kEsPlanes, wmax); }
+constexpr size_t smem_bytes(int nf, int np) { return smem_bytes_w(nf, np, wmax_cells(nf), win_planes(nf)); }
+constexpr size_t es_smem_bytes(int wmax) { return smem_bytes_w(1, kEsPlanes, wmax, win_planes(1)); }
 
 struct Smem {
     float* stage;
@@ -86,11 +86,11 @@ struct Smem {
     int* red;
     unsigned short* slow;
 };
-__device__ __forceinline__ Smem carve(unsigned char* smem, int np, int nf, int wmaxc) {
+__device__ __forceinline__ Smem carve(unsigned char* smem, int np, int planes, int wmaxc) {
     Smem m;
     m.stage = reinterpret_cast<float*>(smem);
     m.win = reinterpret_cast<int*>(smem + win_offset(np));
-    m.red = m.win + static_cast<size_t>(wmaxc) * nf * 2;
+    m.red = m.win + static_cast<size_t>(wmaxc) * planes;
     m.slow = reinterpret_cast<unsigned short*>(m.red + kRedInts);
     return m;
 }
@@ -257,23 +257,23 @@ __device__ __forceinline__ void list_slow(unsigned short* list, int* nlist, int 
 }
 
 // Window set-up (syncs), zero, sync.
-template <int NF, bool T0>
+template <int NF, bool T0, int PC = 0>
 __device__ __forceinline__ Win open_window(const BBox& bb, int ir, int jr, int wmaxc, const Smem& m,
                                            const float (&l1)[NF]) {
     Win wn;
-    win_setup<NF, T0>(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, wmaxc, m.red, l1);
-    win_zero<NF>(m.win, wn);
+    win_setup<NF, T0>(wn, bb.lo_i, bb.lo_j, bb.hi_i, bb.hi_j, ir, jr, PC ? PC : wmaxc, m.red, l1);
+    win_zero<NF, T0, PC>(m.win, wn);
     __syncthreads();
     return wn;
 }
 
 // Block tail shared by every kernel: window flush, slow list, counters.
-template <int NF, int NS, bool T0, class CoefFn>
+template <int NF, int NS, bool T0, int PC = 0, class CoefFn>
 __device__ __forceinline__ void close_window(const Smem& m, const Win& wn, int nlist,
                                              unsigned long long* __restrict__ acc, const Geo& g, DevState* st,
                                              CoefFn coef) {
     __syncthreads();
-    if (wn.nb == 1) win_flush<NF, T0>(m.win, wn, acc, g);
+    if (wn.nb == 1) win_flush<NF, T0, PC>(m.win, wn, acc, g);
     slow_pass<NF, NS>(m.stage, m.slow, nlist, !wn.use, acc, g, st, coef);
     if (threadIdx.x == 0) {
         atomicAdd(&st->chunks, 1ull);
@@ -290,7 +290,7 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
     constexpr int NF = SetNF<SET>::NF, NS = SetNF<SET>::NS;
     constexpr bool T0 = SET != SET_AMU;      // field 0 is rho
     extern __shared__ __align__(16) unsigned char smem[];
-    const Smem m = carve(smem, NS, NF, wmaxc);
+    const Smem m = carve(smem, NS, win_planes(NF), wmaxc);
     __shared__ unsigned long long bar;
     __shared__ int nlist;
     __shared__ float ssq[(NF + 1) * (kThreads / 32)];
@@ -344,7 +344,8 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
 #pragma unroll
         for (int f = 1; f < NS; ++f) m.stage[f * kChunk + d] = a[f];
     }
-    const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
+    constexpr int PC = wmax_cells(NF);
+    const Win wn = open_window<NF, T0, PC>(bb, ir, jr, wmaxc, m, l1);
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
         float cf[NF];
         if constexpr (NS == 6) src_coefs<SET>(a[2], a[3], a[4], a[5], cf);
@@ -352,8 +353,8 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
 #pragma unroll
         for (int f = 0; f < NF; ++f) cs[f] = __fmul_rn(cf[f], S[f]);
     };
-    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef, acc);
-    close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
+    window_pass<NF, NS, T0, PC>(m.stage, m.win, wn, g, coef, acc);
+    close_window<NF, NS, T0, PC>(m, wn, nlist, acc, g, st, coef);
     if (psq) block_sumsq<NF>(sq, nval, psq, ssq, blockIdx.x);
 }
 
@@ -370,7 +371,7 @@ __device__ __forceinline__ EB2 gather_em_pairs(const Cic& s, const float4 (&a)[4
     r.byz  = gather4_tile2(W, lo2(b[0]), lo2(b[1]), lo2(b[2]), lo2(b[3]));
     return r;
 }
-// From the interleaved buffer gb[ncell][8] in global memory.
+// From the interleaved buffer gb[ncell][8] = Ex Ey Ez Bx | By Bz . . in global memory.
 __device__ __forceinline__ EB2 gather_em2(const float* __restrict__ gb, const Cic& s, const Geo& g) {
     const int i0 = s.i0, i1 = wrap_once(s.i0 + 1, g.nx);
     const int r0 = s.j0 * g.nx, r1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
@@ -390,25 +391,6 @@ __device__ __forceinline__ EB2 gather_em_tile2(const float* __restrict__ tile, c
 #pragma unroll
     for (int k = 0; k < 4; ++k) { a[k] = q[2 * cc[k]]; b[k] = q[2 * cc[k] + 1]; }
     return gather_em_pairs(s, a, b);
-}
-
-// EM gather from the interleaved buffer gb[ncell][8] = Ex Ey Ez Bx | By Bz . .
-__device__ __forceinline__ void gather_em(const float* __restrict__ gb, const Cic& s, const Geo& g,
-                                          float& ex, float& ey, float& ez,
-                                          float& bx, float& by, float& bz) {
-    const int i0 = s.i0, i1 = wrap_once(s.i0 + 1, g.nx);
-    const int r0 = s.j0 * g.nx, r1 = wrap_once(s.j0 + 1, g.ny) * g.nx;
-    const float4* q = reinterpret_cast<const float4*>(gb);
-    const float4 a0 = __ldg(q + 2 * (r0 + i0)), b0 = __ldg(q + 2 * (r0 + i0) + 1);
-    const float4 a1 = __ldg(q + 2 * (r0 + i1)), b1 = __ldg(q + 2 * (r0 + i1) + 1);
-    const float4 a2 = __ldg(q + 2 * (r1 + i0)), b2 = __ldg(q + 2 * (r1 + i0) + 1);
-    const float4 a3 = __ldg(q + 2 * (r1 + i1)), b3 = __ldg(q + 2 * (r1 + i1) + 1);
-    ex = gather4_tile(s, a0.x, a1.x, a2.x, a3.x);
-    ey = gather4_tile(s, a0.y, a1.y, a2.y, a3.y);
-    ez = gather4_tile(s, a0.z, a1.z, a2.z, a3.z);
-    bx = gather4_tile(s, a0.w, a1.w, a2.w, a3.w);
-    by = gather4_tile(s, b0.x, b1.x, b2.x, b3.x);
-    bz = gather4_tile(s, b0.y, b1.y, b2.y, b3.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -485,23 +467,6 @@ __device__ __forceinline__ bool load_tile8(float* tile, const float* __restrict_
     return true;
 }
 
-// The EM gather from a shared tile (same arithmetic as gather_em).
-__device__ __forceinline__ void gather_em_tile(const float* __restrict__ tile, const Cic& s, int li, int lj, int W,
-                                               float& ex, float& ey, float& ez, float& bx, float& by, float& bz) {
-    const float4* q = reinterpret_cast<const float4*>(tile);
-    const int c0 = lj * W + li, c2 = c0 + W;
-    const float4 a0 = q[2 * c0], b0 = q[2 * c0 + 1];
-    const float4 a1 = q[2 * c0 + 2], b1 = q[2 * c0 + 3];
-    const float4 a2 = q[2 * c2], b2 = q[2 * c2 + 1];
-    const float4 a3 = q[2 * c2 + 2], b3 = q[2 * c2 + 3];
-    ex = gather4_tile(s, a0.x, a1.x, a2.x, a3.x);
-    ey = gather4_tile(s, a0.y, a1.y, a2.y, a3.y);
-    ez = gather4_tile(s, a0.z, a1.z, a2.z, a3.z);
-    bx = gather4_tile(s, a0.w, a1.w, a2.w, a3.w);
-    by = gather4_tile(s, b0.x, b1.x, b2.x, b3.x);
-    bz = gather4_tile(s, b0.y, b1.y, b2.y, b3.y);
-}
-
 // dcu scales: |coef_dcu (E + v x B)| <= |qm| coef_max (Emax + 2 Umax Bmax); in
 // the fused step the bound per component is also capped at 8 x the rms the
 // previous step's dcu coefficients had.
@@ -533,7 +498,8 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
     constexpr int NF = 3, NS = 5, NIN = 6;
     constexpr bool T0 = false;
     extern __shared__ __align__(16) unsigned char smem[];
-    const Smem m = carve(smem, NIN, NF, wmaxc);
+    constexpr int PC = wmax_cells(NF);
+    const Smem m = carve(smem, NIN, win_planes(NF), PC);
     __shared__ unsigned long long bar, tbar;
     __shared__ int nlist;
     __shared__ float ssq[(NF + 1) * (kThreads / 32)];
@@ -563,7 +529,7 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
                 ymin = fminf(ymin, y); ymax = fmaxf(ymax, y);
             }
         }
-        tl = tile_of(xmin, xmax, ymin, ymax, g, wmaxc * NF / 4, m.red);
+        tl = tile_of(xmin, xmax, ymin, ymax, g, PC * win_planes(NF) / 8, m.red);
     }
     float* const tile = reinterpret_cast<float*>(m.win);
     if (tl.use && !load_tile8(tile, gb, tl, g, &tbar, st)) return;
@@ -612,10 +578,10 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
         m.stage[3 * kChunk + d] = cs[1];
         m.stage[4 * kChunk + d] = cs[2];
     }
-    const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
+    const Win wn = open_window<NF, T0, PC>(bb, ir, jr, wmaxc, m, l1);
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) { cs[0] = a[2]; cs[1] = a[3]; cs[2] = a[4]; };
-    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef, acc);
-    close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
+    window_pass<NF, NS, T0, PC>(m.stage, m.win, wn, g, coef, acc);
+    close_window<NF, NS, T0, PC>(m, wn, nlist, acc, g, st, coef);
     if (psq) block_sumsq<NF>(sq, nval, psq, ssq, chunk);}
 __global__ void __launch_bounds__(kThreads, 3) k_deposit_dcu(DcuArgs A) { deposit_dcu_chunk(A, blockIdx.x); }
 
@@ -637,14 +603,15 @@ __global__ void __launch_bounds__(kThreads, 3) k_deposit_dcu(DcuArgs A) { deposi
 // in place like x, y), lux, luy, luz into planes 4-6, which lie in the window
 // area, idle until the window opens after pass 1.
 constexpr int kAdjWindow = wmax_cells(2);
-static_assert(3 * kChunk * 4 <= kAdjWindow * 2 * 8, "the cotangent planes must fit the window area");
+static_assert(3 * kChunk * 4 <= kAdjWindow * win_planes(2) * 4, "the cotangent planes must fit the window area");
 __global__ void __launch_bounds__(kThreads, 3)
 k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ trajE, AdjDev* ad,
               unsigned long long* __restrict__ acc, int wmaxc, DevState* st) {
     constexpr int NF = 2, NS = 4, NIN = 7;
     constexpr bool T0 = false;
     extern __shared__ __align__(16) unsigned char smem[];
-    const Smem m = carve(smem, NS, NF, wmaxc);
+    constexpr int PC = kAdjWindow;
+    const Smem m = carve(smem, NS, win_planes(NF), PC);
     __shared__ unsigned long long bar;
     __shared__ int nlist;
 
@@ -716,10 +683,10 @@ k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ trajE, AdjDev* a
         m.stage[2 * kChunk + d] = cs[0];
         m.stage[3 * kChunk + d] = cs[1];
     }
-    const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
+    const Win wn = open_window<NF, T0, PC>(bb, ir, jr, wmaxc, m, l1);
     auto coef = [&](const float (&q)[NS], float (&c2)[NF]) { c2[0] = q[2]; c2[1] = q[3]; };
-    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef, acc);
-    close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
+    window_pass<NF, NS, T0, PC>(m.stage, m.win, wn, g, coef, acc);
+    close_window<NF, NS, T0, PC>(m, wn, nlist, acc, g, st, coef);
 }
 
 // ---------------------------------------------------------------------------
@@ -757,7 +724,7 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
     constexpr int NF = 1, NS = 3, NIN = 5;          // stage in: x y ux uy uz (w read from global)
     constexpr bool T0 = true;
     extern __shared__ __align__(16) unsigned char smem[];
-    const Smem m = carve(smem, NIN, NF, wmaxc);
+    const Smem m = carve(smem, NIN, win_planes(NF), wmaxc);
     __shared__ unsigned long long bar;
     __shared__ int nlist;
     __shared__ double dsh[4 * (kThreads / 32)];
@@ -864,7 +831,8 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
     constexpr int NF = 8, NS = 6;
     constexpr bool T0 = true;
     extern __shared__ __align__(16) unsigned char smem[];
-    const Smem m = carve(smem, NS, NF, wmaxc);
+    constexpr int PC = wmax_cells(NF);
+    const Smem m = carve(smem, NS, win_planes(NF), PC);
     __shared__ unsigned long long bar, tbar;
     __shared__ int nlist;
     __shared__ double dsh[4 * (kThreads / 32)];
@@ -898,7 +866,7 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
                 ymin = fminf(ymin, y); ymax = fmaxf(ymax, y);
             }
         }
-        tl = tile_of(xmin, xmax, ymin, ymax, g, wmaxc * NF / 4, m.red);
+        tl = tile_of(xmin, xmax, ymin, ymax, g, PC * win_planes(NF) / 8, m.red);
     }
     float* const tile = reinterpret_cast<float*>(m.win);
     if (tl.use && !load_tile8(tile, gb, tl, g, &tbar, st)) return;
@@ -975,7 +943,7 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
     float l1[NF], sq[NF];
 #pragma unroll
     for (int i = 0; i < 4; ++i) { l1[2 * i] = l1p[i].x; l1[2 * i + 1] = l1p[i].y; sq[2 * i] = sqp[i].x; sq[2 * i + 1] = sqp[i].y; }
-    const Win wn = open_window<NF, T0>(bb, ir, jr, wmaxc, m, l1);
+    const Win wn = open_window<NF, T0, PC>(bb, ir, jr, wmaxc, m, l1);
     if (threadIdx.x < 3) {
         unsigned mx = 0;
         for (int k = 0; k < kThreads / 32; ++k) mx = max(mx, umx[threadIdx.x][k]);
@@ -990,8 +958,8 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
             cs[2 * i] = c.x; cs[2 * i + 1] = c.y;
         }
     };
-    window_pass<NF, NS, T0>(m.stage, m.win, wn, g, coef, acc);
-    close_window<NF, NS, T0>(m, wn, nlist, acc, g, st, coef);
+    window_pass<NF, NS, T0, PC>(m.stage, m.win, wn, g, coef, acc);
+    close_window<NF, NS, T0, PC>(m, wn, nlist, acc, g, st, coef);
     block_sumsq<NF>(sq, nval, psq, ssq, chunk);
     block_sum4(ke, px, py, pz, part, dsh, chunk);
     if (threadIdx.x == 0 && chunk == 0) {
@@ -1269,8 +1237,8 @@ __device__ __forceinline__ void yee_window_pass(const float* __restrict__ stage,
         esirkepov_weights(x0, y0, x1, y1, ib, jb, [&](int f, int ni, int nj, float w) {
             const int v = quant(f == 0 ? a0 : f == 1 ? a1 : a2, w);
             if (v == 0) return;                    // prefix-sum residues that round to nothing
-            int* e = win + 2 * f * wn.WH + (cj + nj) * wn.W + (ci + ni);
-            if (wn.track_all) add_tracked(e, wn.WH, v);
+            int* e = win + f * wn.P + (cj + nj) * wn.W + (ci + ni);
+            if (wn.track_all) add_tracked(e, 3 * wn.P, v);
             else atomicAdd(e, v);
         });
     }
@@ -1322,7 +1290,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_push_esirkepov(YeeArgs A) {
     DevState* st = A.st;
     constexpr int NF = 3, NIN = 5;              // stage in: x y ux uy uz (w read from global)
     extern __shared__ __align__(16) unsigned char smem[];
-    const Smem m = carve(smem, kYeePlanes, NF, A.wmaxc);
+    const Smem m = carve(smem, kYeePlanes, 2 * NF, A.wmaxc);   // sums and carries: no count plane
     __shared__ unsigned long long bar;
     __shared__ int nlist;
     __shared__ double dsh[4 * (kThreads / 32)];
@@ -1426,9 +1394,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_push_esirkepov(YeeArgs A) {
     // the window of the nodes every move touches (4 x 4 stencils)
     // base offsets lo..hi, nodes to hi + 2: win_setup sizes W = hi - lo + 2, so pass hi + 1
     Win wn;
-    win_setup<NF, false>(wn, bb.lo_i, bb.lo_j, bb.hi_i + 1, bb.hi_j + 1, ir, jr, A.wmaxc, m.red, l1);
+    // unbiased adds: the Esirkepov pass skips zero weights, so no count argument
+    win_setup<NF, false, false>(wn, bb.lo_i, bb.lo_j, bb.hi_i + 1, bb.hi_j + 1, ir, jr, A.wmaxc, m.red, l1);
     if (wn.nb > 1) { wn.use = false; wn.WH = 0; }     // no bands on this path: the slow path takes the chunk
-    win_zero<NF>(m.win, wn);
+    win_zero<NF, false>(m.win, wn);
     if (threadIdx.x < 3) {
         unsigned mx = 0;
         for (int k = 0; k < kThreads / 32; ++k) mx = max(mx, umx[threadIdx.x][k]);
@@ -1563,7 +1532,7 @@ void launch_push_esirkepov(Ctx& c) {
     a.pump.ex = c.prm.pump_ex; a.pump.ey = c.prm.pump_ey; a.pump.ez = c.prm.pump_ez;
     a.pump.k0 = c.prm.pump_k0; a.pump.w0 = c.prm.pump_w0; a.pump.trmp = c.prm.pump_trmp; a.pump.toff = c.prm.pump_toff;
     a.acc = c.acc_src; a.wmaxc = kYeeWindow; a.part = c.part_p; a.st = c.st; a.write_cell = c.write_cell;
-    const size_t sh = smem_bytes_w(3, kYeePlanes, kYeeWindow);
+    const size_t sh = smem_bytes_w(3, kYeePlanes, kYeeWindow, 6);
     prep_smem(k_push_esirkepov, sh);
     k_push_esirkepov<<<nchunks(c.parts.n), kThreads, sh, c.stream>>>(a);
     AW_LAUNCH();

@@ -308,30 +308,54 @@ struct Parts {
 // when the whole box fits the shared capacity): each band is zeroed, takes the
 // corners of every particle that fall in its rows, and is flushed before the
 // next. A box that would need more than kMaxBands bands takes the slow path.
+//
+// Storage: int32 planes of P cells each (P = the window capacity, a
+// compile-time constant in the hot kernels, so every (field, corner) address of
+// a particle is one base register plus an immediate offset):
+//   plane f          (0 <= f < NF) the sums of field f;
+//   plane NF + f     the carries of field f when it is wrap-tracked;
+//   plane 2 NF       particles per base cell (biased chunks only).
+// Three ways to add a contribution q (|q| <= 2^22), all exact:
+//   tracked  the plane holds the sum modulo 2^32 and the carry plane the net
+//            number of times it wrapped past the int32 range: each add reads the
+//            old value back, so a crossing is seen by exactly the add that made
+//            it, and sum = (int32) plane + 2^32 carry;
+//   biased   the add is the quantising FMA's raw bits M + q (M = 0x4B400000,
+//            no subtraction per contribution); a node receives one add per field
+//            from every particle whose base cell is one of its four neighbours,
+//            so sum = plane - n M modulo 2^32 with n from the count plane, exact
+//            as a signed int32 when the chunk's bound proves |sum| < 2^31;
+//   plain    the add is q (chunks deposited in bands, and the Yee current).
+// Field 0 is tracked when T0 (the charge density: its chunk sums are large by
+// design); the other fields are biased (one band) or plain (bands) when the
+// chunk's bound fits int32, else every field is tracked.
 constexpr int kMaxBands = 8;
 struct Win {
     int ir, jr;      // reference cell
     int mi, mj;      // min wrapped offsets
     int W, H;        // extent in cells (incl. the +1 corner)
     int Hb, nb;      // rows per band, bands
-    int WH;          // W * Hb: the words of one plane
+    int WH;          // W * Hb: the cells of one plane in use
+    int P;           // plane stride (the capacity in cells)
     bool use;        // deposited in the shared window (in one or more bands)
     bool track_all;  // some field's chunk sums may leave int32: track every field
+    bool biased;     // the untracked fields add biased words (one band)
 };
+// Window planes for NF fields: sums and carries, plus the count plane when a
+// field can be biased (not for the charge density alone).
+__host__ __device__ constexpr int win_planes(int nf) { return nf == 1 ? 2 : 2 * nf + 1; }
 
 // Block-wide min/max of the offsets and sums of the per-field magnitude bounds,
 // then the window geometry. `l1[f]` is this thread's sum of |scaled coefficient|
 // of field f over its fast-path particles; `red` is (4 + NF) * warps ints of
 // shared scratch. Every thread of the block calls it.
 //
-// Window mode: a window entry receives at most one rounded contribution per
-// particle, |q| <= |cs| + 1/2, so sum_p (|cs_p| + 1) bounds it. Field 0 is
-// always wrap-tracked when T0 (the charge density: its chunk sums are large by
-// design); every other field is added with plain int32 atomics when that bound
-// is < 2^31 for all of them, else the chunk tracks every field (see below).
-// The thread bound is ceil(l1 (1 + 2^-20)) + kPPT (FP32 rounding of at most
-// kPPT additions, plus the +1 per particle).
-template <int NF, bool T0>
+// Bound: a window entry receives at most one rounded contribution per particle,
+// |q| <= |cs| + 1/2, so sum_p (|cs_p| + 1) bounds it; the untracked fields need
+// it below 2^31. The thread bound is ceil(l1 (1 + 2^-20)) + kPPT (FP32 rounding
+// of at most kPPT additions, plus the +1 per particle). BIASED_OK: the caller's
+// pass adds every corner of every particle (the count argument needs it).
+template <int NF, bool T0, bool BIASED_OK = true>
 __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, int hi_j, int ir, int jr,
                                           int wmaxc, int* red, const float (&l1)[NF]) {
     constexpr int NW = kThreads / 32;
@@ -372,6 +396,7 @@ __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, 
     w.mi = lo_i; w.mj = lo_j;
     w.W = hi_i - lo_i + 2;
     w.H = hi_j - lo_j + 2;
+    w.P = wmaxc;
     if (static_cast<long long>(w.W) * w.H <= wmaxc) {
         w.Hb = w.H;
         w.nb = 1;
@@ -382,58 +407,80 @@ __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, 
     w.use = w.nb <= kMaxBands;
     w.WH = w.use ? w.W * w.Hb : 0;
     w.track_all = track_all;
+    w.biased = BIASED_OK && w.use && w.nb == 1 && !track_all && (NF > (T0 ? 1 : 0));
 }
 
-// Window storage: field f owns planes 2f and 2f + 1 (W*H int32 words each).
-// Plain field (its chunk sums provably fit int32): plane 2f holds the sums,
-// added with plain 32-bit shared atomics. Tracked field: plane 2f holds the sum
-// modulo 2^32 and plane 2f + 1 the net number of times it wrapped past the
-// int32 range; each add reads the old value back (the atomic's return), so a
-// crossing is seen by exactly the add that made it (|v| < 2^22 crosses at most
-// once), and sum = (int32) plane_2f + 2^32 * plane_2f+1 exactly.
 template <bool T0>
 __device__ __forceinline__ bool tracked(const Win& w, int f) { return w.track_all || (T0 && f == 0); }
-__device__ __forceinline__ void add_tracked(int* e, int WH, int v) {
+// Tracked add; the carry word sits `coff` words after the sum word.
+__device__ __forceinline__ void add_tracked(int* e, int coff, int v) {
     const int old = atomicAdd(e, v);
     const int nw = static_cast<int>(static_cast<unsigned>(old) + static_cast<unsigned>(v));
-    if (((old ^ nw) & (v ^ nw)) < 0) atomicAdd(e + WH, v > 0 ? 1 : -1);
+    if (((old ^ nw) & (v ^ nw)) < 0) atomicAdd(e + coff, v > 0 ? 1 : -1);
 }
 
-// Zero the window; the caller syncs afterwards.
-template <int NF>
+// Zero the window cells in use (the sums, the carries of tracked fields, the
+// counts of a biased chunk); the caller syncs afterwards. PC: the plane stride
+// when known at compile time (0: w.P).
+template <int NF, bool T0, int PC = 0>
 __device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
-    const int m = 2 * NF * w.WH;
-    for (int i = threadIdx.x; i < m; i += kThreads) s[i] = 0;
+    const int P = PC ? PC : w.P;
+    const bool ta = w.track_all, bi = w.biased;
+    for (int c = threadIdx.x; c < w.WH; c += kThreads) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            s[f * P + c] = 0;
+            if (ta || (T0 && f == 0)) s[(NF + f) * P + c] = 0;
+        }
+        if (win_planes(NF) > 2 * NF && bi) s[2 * NF * P + c] = 0;
+    }
 }
 
 // Flush band `band` of the window into the global int64 accumulators
-// acc[f*ncell + cell]. The caller syncs before calling.
-template <int NF, bool T0>
+// acc[f*ncell + cell]; the caller syncs before calling. Cell-major: a thread
+// takes window cells t, t + 256, ..., maps each to its grid cell once and
+// flushes every field of it.
+template <int NF, bool T0, int PC = 0>
 __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& w,
                                           unsigned long long* __restrict__ acc, const Geo& g, int band = 0) {
     if (!w.use) return;            // the window was not used (its words are not zeroed)
-    // every thread takes (field, cell) items t, t + 256, ...: all warps work even
-    // when the window is one or two rows. The item -> (field, row, column) splits
-    // use float reciprocals: (t + 0.5) / n is at least 0.5 / n away from an
-    // integer, far more than the float error for t < 2^14. Window offsets are
-    // < nx, so one conditional add/subtract wraps them.
-    const int WH = w.WH, r0 = band * w.Hb, cells = w.W * min(w.Hb, w.H - r0), total = NF * cells;
-    const float inv_c = 1.0f / static_cast<float>(cells), inv_w = 1.0f / static_cast<float>(w.W);
-    for (int t = threadIdx.x; t < total; t += kThreads) {
-        const int f = static_cast<int>((static_cast<float>(t) + 0.5f) * inv_c);
-        const int c = t - f * cells;
-        const int wj = static_cast<int>((static_cast<float>(c) + 0.5f) * inv_w);
-        const int wi = c - wj * w.W;
-        int gj = w.jr + w.mj + r0 + wj;
-        if (gj < 0) gj += g.ny;
-        if (gj >= g.ny) gj -= g.ny;
-        int gi = w.ir + w.mi + wi;
-        if (gi < 0) gi += g.nx;
+    const int P = PC ? PC : w.P;
+    const int r0 = band * w.Hb, cells = w.W * min(w.Hb, w.H - r0);
+    int oi = w.ir + w.mi, oj = w.jr + w.mj + r0;
+    if (oi < 0) oi += g.nx;
+    if (oi >= g.nx) oi -= g.nx;
+    if (oj < 0) oj += g.ny;
+    if (oj >= g.ny) oj -= g.ny;
+    if (oj >= g.ny) oj -= g.ny;
+    const bool ta = w.track_all, bi = w.biased;
+    for (int c = threadIdx.x; c < cells; c += kThreads) {
+        const int wj = c / w.W, wi = c - wj * w.W;
+        int gi = oi + wi, gj = oj + wj;
         if (gi >= g.nx) gi -= g.nx;
-        long long v = s[2 * f * WH + c];
-        if (tracked<T0>(w, f)) v += static_cast<long long>(s[(2 * f + 1) * WH + c]) * 4294967296ll;
-        if (v != 0)
-            atomicAdd(acc + static_cast<size_t>(f) * g.ncell + gj * g.nx + gi, static_cast<unsigned long long>(v));
+        if (gj >= g.ny) gj -= g.ny;
+        unsigned long long* a = acc + (static_cast<size_t>(gj) * g.nx + gi);
+        unsigned nM = 0;
+        if (win_planes(NF) > 2 * NF && bi) {
+            const int* cn = s + 2 * NF * P;
+            int n = cn[c];
+            if (wi > 0) n += cn[c - 1];
+            if (wj > 0) {
+                n += cn[c - w.W];
+                if (wi > 0) n += cn[c - w.W - 1];
+            }
+            nM = static_cast<unsigned>(n) * kMagicU;
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f) {
+            long long v;
+            if (ta || (T0 && f == 0))
+                v = static_cast<long long>(s[f * P + c]) + static_cast<long long>(s[(NF + f) * P + c]) * 4294967296ll;
+            else if (bi)
+                v = static_cast<int>(static_cast<unsigned>(s[f * P + c]) - nM);
+            else
+                v = s[f * P + c];
+            if (v != 0) atomicAdd(a + static_cast<size_t>(f) * g.ncell, static_cast<unsigned long long>(v));
+        }
     }
 }
 
@@ -642,35 +689,38 @@ __device__ __forceinline__ int win_col(int c, int o, int n) {
     return d < 0 ? d + n : d;
 }
 
-// The NF x 4 rounded contributions of one particle, two corners per packed
-// FMA: (q0, q1) from (w0, w1), (q2, q3) from (w2, w3), each exactly
-// quant(cs[f], w_k).
+// The NF x 4 quantising FMAs of one particle, two corners per packed FMA:
+// (b0, b1) from (w0, w1), (b2, b3) from (w2, w3). b = the raw bits of
+// fl(cs w + 1.5 2^23) = kMagicBits + quant(cs[f], w_k) exactly.
 template <int NF>
-__device__ __forceinline__ void quant_corners(const float (&cs)[NF], const Cic2& c, int (&v)[NF][4]) {
+__device__ __forceinline__ void quant_bits(const float (&cs)[NF], const Cic2& c, int (&b)[NF][4]) {
     const float2 M2 = bc2(kMagic);
 #pragma unroll
     for (int f = 0; f < NF; ++f) {
         const float2 C = bc2(cs[f]);
         const float2 q01 = __ffma2_rn(C, c.w01, M2), q23 = __ffma2_rn(C, c.w23, M2);
-        v[f][0] = __float_as_int(q01.x) - kMagicBits;
-        v[f][1] = __float_as_int(q01.y) - kMagicBits;
-        v[f][2] = __float_as_int(q23.x) - kMagicBits;
-        v[f][3] = __float_as_int(q23.y) - kMagicBits;
+        b[f][0] = __float_as_int(q01.x);
+        b[f][1] = __float_as_int(q01.y);
+        b[f][2] = __float_as_int(q23.x);
+        b[f][3] = __float_as_int(q23.y);
     }
 }
 
-// Window pass: lane l of warp w deposits the chunk slots 64 l + 8 w + k,
-// k = 0..7, one particle at a time: each of its NF x 4 rounded contributions is
-// one native 32-bit shared atomic into the window (field 0 wrap-tracked when
-// T0; every field when the chunk needs it). Lanes sit 64 particles apart, so a
-// warp's atomics fall on different cells. Particles whose staged x has its sign
-// bit set (invalid, or listed for the slow pass) are skipped.
-template <int NF, int NS, bool T0, bool TRACK_ALL, class CoefFn>
+// Window pass of a one-band chunk: lane l of warp w deposits the chunk slots
+// 64 l + 8 w + k, k = 0..7, one particle at a time (lanes sit 64 particles
+// apart, so a warp's atomics fall on different cells). TRACK_ALL: every
+// contribution is a tracked add. Otherwise field 0 is tracked when T0 and the
+// other fields add the FMA's biased bits, one native 32-bit shared atomic per
+// contribution, and the particle counts itself in its base cell. Particles whose
+// staged x has its sign bit set (invalid, or listed for the slow pass) are
+// skipped. PC: the plane stride when known at compile time (0: wn.P).
+template <int NF, int NS, bool T0, bool TRACK_ALL, int PC, class CoefFn>
 __device__ __forceinline__ void window_particles(const float* __restrict__ stage, int* __restrict__ win,
                                                  const Win& wn, const Geo& g, CoefFn coef) {
+    constexpr bool kBiased = !TRACK_ALL && NF > (T0 ? 1 : 0);
+    const int P = PC ? PC : wn.P;
     const int base = 64 * (threadIdx.x & 31) + 8 * (threadIdx.x >> 5);
     const int oi = win_origin(wn.ir, wn.mi, g.nx), oj = win_origin(wn.jr, wn.mj, g.ny);
-    const int offs[4] = {0, 1, wn.W, wn.W + 1};
 #pragma unroll 1
     for (int k = 0; k < kPPT; ++k) {
         const int d = stage_slot(base + k);
@@ -681,16 +731,23 @@ __device__ __forceinline__ void window_particles(const float* __restrict__ stage
         const Cic2 c = cic2(a[0], a[1]);
         float cs[NF];
         coef(a, cs);
-        int v[NF][4];
-        quant_corners<NF>(cs, c, v);
-        const int cw = win_col(c.j0, oj, g.ny) * wn.W + win_col(c.i0, oi, g.nx);
+        int b[NF][4];
+        quant_bits<NF>(cs, c, b);
+        int* e0 = win + win_col(c.j0, oj, g.ny) * wn.W + win_col(c.i0, oi, g.nx);   // corners 0, 1
+        int* e2 = e0 + wn.W;                                                          // corners 2, 3
+        if (kBiased) atomicAdd(e0 + 2 * NF * P, 1);
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            int* e = win + 2 * f * wn.WH + cw;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                if (TRACK_ALL || (T0 && f == 0)) add_tracked(e + offs[q], wn.WH, v[f][q]);
-                else atomicAdd(e + offs[q], v[f][q]);
+            if (TRACK_ALL || (T0 && f == 0)) {
+                add_tracked(e0 + f * P, NF * P, b[f][0] - kMagicBits);
+                add_tracked(e0 + f * P + 1, NF * P, b[f][1] - kMagicBits);
+                add_tracked(e2 + f * P, NF * P, b[f][2] - kMagicBits);
+                add_tracked(e2 + f * P + 1, NF * P, b[f][3] - kMagicBits);
+            } else {
+                atomicAdd(e0 + f * P, b[f][0]);
+                atomicAdd(e0 + f * P + 1, b[f][1]);
+                atomicAdd(e2 + f * P, b[f][2]);
+                atomicAdd(e2 + f * P + 1, b[f][3]);
             }
         }
     }
@@ -698,10 +755,11 @@ __device__ __forceinline__ void window_particles(const float* __restrict__ stage
 
 // Banded window pass over rows [r0, r0 + Hb) of the box: a particle adds the
 // corners of its two rows that fall in the band (same contributions, same
-// integer sums per cell as one window).
-template <int NF, int NS, bool T0, bool TRACK_ALL, class CoefFn>
+// integer sums per cell as one window); unbiased adds.
+template <int NF, int NS, bool T0, bool TRACK_ALL, int PC, class CoefFn>
 __device__ __forceinline__ void window_band(const float* __restrict__ stage, int* __restrict__ win,
                                             const Win& wn, int r0, const Geo& g, CoefFn coef) {
+    const int P = PC ? PC : wn.P;
     const int base = 64 * (threadIdx.x & 31) + 8 * (threadIdx.x >> 5);
     const int oi = win_origin(wn.ir, wn.mi, g.nx), oj = win_origin(wn.jr, wn.mj, g.ny);
 #pragma unroll 1
@@ -719,19 +777,19 @@ __device__ __forceinline__ void window_band(const float* __restrict__ stage, int
         const Cic2 c = cic2(a[0], a[1]);
         float cs[NF];
         coef(a, cs);
-        int v[NF][4];
-        quant_corners<NF>(cs, c, v);
+        int b[NF][4];
+        quant_bits<NF>(cs, c, b);
         const int ci = win_col(c.i0, oi, g.nx);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int row = rj + (q >> 1);                // corners 0, 1 in row rj; 2, 3 in rj + 1
             if (row < 0 || row >= wn.Hb) continue;
-            const int cw = row * wn.W + ci + (q & 1);
+            int* t = win + row * wn.W + ci + (q & 1);
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
-                int* t = win + 2 * f * wn.WH + cw;
-                if (TRACK_ALL || (T0 && f == 0)) add_tracked(t, wn.WH, v[f][q]);
-                else atomicAdd(t, v[f][q]);
+                const int v = b[f][q] - kMagicBits;
+                if (TRACK_ALL || (T0 && f == 0)) add_tracked(t + f * P, NF * P, v);
+                else atomicAdd(t + f * P, v);
             }
         }
     }
@@ -739,26 +797,26 @@ __device__ __forceinline__ void window_band(const float* __restrict__ stage, int
 
 // The window pass. With one band the caller flushes (close_window); with
 // several, each band is flushed here, and the window is zeroed for the next.
-template <int NF, int NS, bool T0, class CoefFn>
+template <int NF, int NS, bool T0, int PC = 0, class CoefFn>
 __device__ __forceinline__ void window_pass(const float* __restrict__ stage, int* __restrict__ win,
                                             const Win& wn, const Geo& g, CoefFn coef,
                                             unsigned long long* __restrict__ acc) {
     if (!wn.use) return;
     if (wn.nb == 1) {
-        if (wn.track_all) window_particles<NF, NS, T0, true>(stage, win, wn, g, coef);
-        else window_particles<NF, NS, T0, false>(stage, win, wn, g, coef);
+        if (wn.track_all) window_particles<NF, NS, T0, true, PC>(stage, win, wn, g, coef);
+        else window_particles<NF, NS, T0, false, PC>(stage, win, wn, g, coef);
         return;
     }
 #pragma unroll 1
     for (int b = 0; b < wn.nb; ++b) {
         if (b > 0) {
-            win_zero<NF>(win, wn);
+            win_zero<NF, T0, PC>(win, wn);
             __syncthreads();
         }
-        if (wn.track_all) window_band<NF, NS, T0, true>(stage, win, wn, b * wn.Hb, g, coef);
-        else window_band<NF, NS, T0, false>(stage, win, wn, b * wn.Hb, g, coef);
+        if (wn.track_all) window_band<NF, NS, T0, true, PC>(stage, win, wn, b * wn.Hb, g, coef);
+        else window_band<NF, NS, T0, false, PC>(stage, win, wn, b * wn.Hb, g, coef);
         __syncthreads();
-        win_flush<NF, T0>(win, wn, acc, g, b);
+        win_flush<NF, T0, PC>(win, wn, acc, g, b);
         __syncthreads();
     }
 }
