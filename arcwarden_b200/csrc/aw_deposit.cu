@@ -458,13 +458,197 @@ __device__ __forceinline__ bool load_tile8(float* tile, const float* __restrict_
         }
     }
     __syncthreads();
-    const bool ok = mbar_wait_bounded(bar, 0u);
-    if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) set_err(st, 4u);     // AW_DEV_WAIT_LIMIT
-        mbar_wait_bounded(bar, 0u);
-        return false;
+    return mbar_wait_block(bar, st);
+}
+
+// ---------------------------------------------------------------------------
+// Single-pass chunks. When a chunk's deposit window - the box of its CURRENT
+// base cells, widened on every side by the cells a particle can cross in one
+// step, plus the +1 CIC corner - fits the shared capacity next to its gather
+// tile, the kernel pushes and deposits each particle in the same pass, from
+// registers: no second pass over the staged chunk, no per-particle re-read or
+// recomputation of the weights and coefficients. The new state is written back
+// into the stage in place and leaves with one bulk copy per array. A particle
+// that lands outside the window (it moved further than the margin) or whose
+// coefficients leave the fast range takes the exact slow path, as in the two-pass
+// kernels, so the sums are the same bits either way. Chunks that do not fit take
+// the two-pass path.
+
+// Slot of this thread's k-th particle: lanes sit 64 particles apart (in loader
+// order a warp's atomics then fall on different cells) and read the linear stage
+// without bank conflicts (lane l's slot is congruent to 8 w + k + l modulo 32).
+__device__ __forceinline__ int spread_slot(int k) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    return 64 * lane + ((8 * warp + k + lane) & 63);
+}
+
+// Block-wide box of the threads' BBoxes (empty: lo > hi). Ends with a barrier
+// after the scratch `red` is read.
+struct Box { int lo_i, hi_i, lo_j, hi_j; };
+__device__ __forceinline__ Box box_reduce(const BBox& bb, int* red) {
+    constexpr int NW = kThreads / 32;
+    const int v[4] = {__reduce_min_sync(0xffffffffu, bb.lo_i), __reduce_max_sync(0xffffffffu, bb.hi_i),
+                      __reduce_min_sync(0xffffffffu, bb.lo_j), __reduce_max_sync(0xffffffffu, bb.hi_j)};
+    const int warp = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) red[warp * 4 + k] = v[k];
+    __syncthreads();
+    Box b{red[0], red[1], red[2], red[3]};
+#pragma unroll
+    for (int k = 1; k < NW; ++k) {
+        b.lo_i = min(b.lo_i, red[k * 4 + 0]); b.hi_i = max(b.hi_i, red[k * 4 + 1]);
+        b.lo_j = min(b.lo_j, red[k * 4 + 2]); b.hi_j = max(b.hi_j, red[k * 4 + 3]);
     }
+    __syncthreads();
+    return b;
+}
+
+// True (block-uniformly) when some untracked field's chunk bound
+// sum_p (|cs_p| + 1) may reach 2^31 (win_setup's test): its biased int32 window
+// words may then have wrapped, and the chunk is deposited through the exact
+// slow path instead. Ends with a barrier after `red` is read.
+template <int NF, bool T0>
+__device__ __forceinline__ bool chunk_overflows(const float (&l1)[NF], int* red) {
+    constexpr int NW = kThreads / 32;
+    const int warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int f = T0 ? 1 : 0; f < NF; ++f) {
+        const float b = fminf(ceilf(__fmul_rn(l1[f], 1.00000095367431640625f)), 33554432.0f);
+        const unsigned w = __reduce_add_sync(0xffffffffu, static_cast<unsigned>(b) + static_cast<unsigned>(kPPT));
+        if ((threadIdx.x & 31) == 0) red[f * NW + warp] = static_cast<int>(w);
+    }
+    __syncthreads();
+    bool over = false;
+#pragma unroll
+    for (int f = T0 ? 1 : 0; f < NF; ++f) {
+        unsigned long long t = 0;
+#pragma unroll
+        for (int k = 0; k < NW; ++k) t += static_cast<unsigned>(red[f * NW + k]);
+        over = over || (t >= 2147483648ull);
+    }
+    __syncthreads();
+    return over;
+}
+
+// The window of a single-pass chunk: the box widened by `mg` cells, plus the
+// corner; biased, one band, plane stride P1. False when it does not fit.
+template <int NF, bool T0, int P1>
+__device__ __forceinline__ bool one_pass_window(Win& w, const Box& b, int ir, int jr, int mg) {
+    if (b.hi_i < b.lo_i) return false;
+    w.ir = ir; w.jr = jr;
+    w.mi = b.lo_i - mg; w.mj = b.lo_j - mg;
+    w.W = b.hi_i - b.lo_i + 2 + 2 * mg;
+    w.H = b.hi_j - b.lo_j + 2 + 2 * mg;
+    if (static_cast<long long>(w.W) * w.H > P1) return false;
+    w.Hb = w.H; w.nb = 1;
+    w.WH = w.W * w.H;
+    w.P = P1;
+    w.use = true;
+    w.track_all = false;
+    w.biased = NF > (T0 ? 1 : 0);
     return true;
+}
+
+// The gather tile of the box (its base cells plus the corner), from the
+// wrapped origin; use = false when it does not fit `cap` cells.
+__device__ __forceinline__ Tile box_tile(const Box& b, int ir, int jr, const Geo& g, int cap) {
+    Tile t;
+    t.i0 = ir + b.lo_i; if (t.i0 < 0) t.i0 += g.nx; if (t.i0 >= g.nx) t.i0 -= g.nx;
+    t.j0 = jr + b.lo_j; if (t.j0 < 0) t.j0 += g.ny; if (t.j0 >= g.ny) t.j0 -= g.ny;
+    t.W = b.hi_i - b.lo_i + 2;
+    t.H = b.hi_j - b.lo_j + 2;
+    t.use = b.hi_i >= b.lo_i && t.W <= g.nx && t.H <= g.ny && t.W * t.H <= cap;
+    return t;
+}
+
+// Write stage planes pl[0..NP) back to their arrays dst[0..NP) for the chunk
+// [c0, c0 + cnt): one bulk shared->global copy per plane for the 16-byte
+// aligned body (issued by thread 0, evict-first), plain stores for the ragged
+// tail and unaligned arrays. The caller has synced after writing the stage;
+// thread 0 must call bulk_store_wait before the block exits.
+template <int NP>
+__device__ __forceinline__ void bulk_store_planes(const float* stage, const int (&pl)[NP], float* const (&dst)[NP],
+                                                  long long c0, int cnt, bool vec) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    const int nbulk = vec ? (cnt & ~3) : 0;
+    if (threadIdx.x == 0 && nbulk > 0) {
+        unsigned long long pol;
+        asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+#pragma unroll
+        for (int k = 0; k < NP; ++k)
+            asm volatile("cp.async.bulk.global.shared::cta.bulk_group.L2::cache_hint [%0], [%1], %2, %3;"
+                         :: "l"(dst[k] + c0), "r"(smem_u32(stage + pl[k] * kChunk)),
+                            "r"(static_cast<unsigned>(nbulk) * 4u), "l"(pol) : "memory");
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+    const int rem = cnt - nbulk;
+    if (rem > 0)
+        for (int idx = threadIdx.x; idx < rem * NP; idx += blockDim.x) {
+            const int k = idx / rem, sl = nbulk + idx % rem;
+#pragma unroll
+            for (int q = 0; q < NP; ++q)
+                if (q == k) dst[q][c0 + sl] = stage[pl[q] * kChunk + sl];
+        }
+}
+__device__ __forceinline__ void bulk_store_wait() {
+    if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// Exact slow path of a single-pass chunk, from the linear stage: the listed
+// slots, or (redo: the window may have wrapped) every slot whose staged
+// position is in the grid. coef(s, cs) gives slot s's NF scaled coefficients.
+template <int NF, class CoefFn>
+__device__ __forceinline__ void slow_pass_linear(const float* __restrict__ stage, const unsigned short* __restrict__ list,
+                                                 int nlist, bool redo, int cnt, unsigned long long* __restrict__ gacc,
+                                                 const Geo& g, DevState* st, CoefFn coef) {
+    const int total = redo ? cnt : nlist;
+    unsigned n = 0;
+    for (int k = threadIdx.x; k < total; k += kThreads) {
+        const int sl = redo ? k : static_cast<int>(list[k]);
+        const float x = stage[sl], y = stage[kChunk + sl];
+        if (!in_grid(x, y, g)) continue;
+        float cs[NF];
+        coef(sl, cs);
+        bool finite = true;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) finite = finite && isfinite(cs[f]);
+        if (!finite) { set_err(st, 1u); continue; }      // AW_DEV_NONFINITE
+        const Cic c = cic(x, y);
+        const float wv[4] = {c.w0, c.w1, c.w2, c.w3};
+        deposit_global<NF>(c.i0, c.j0, wv, cs, gacc, g);
+        ++n;
+    }
+    if (n) atomicAdd(&st->slow, static_cast<unsigned long long>(n));
+}
+
+// The NF x 4 contributions of one particle into a single-pass window (plane
+// stride P1): the count of its base cell, field 0 tracked when T0, the others
+// as biased words.
+template <int NF, bool T0, int P1>
+__device__ __forceinline__ void one_pass_deposit(int* __restrict__ win, const Win& w, int di, int dj, float x, float y,
+                                                 const float (&cs)[NF]) {
+    const Cic2 c2 = cic2(x, y);
+    int b[NF][4];
+    quant_bits<NF>(cs, c2, b);
+    int* e0 = win + dj * w.W + di;
+    int* e2 = e0 + w.W;
+    if (NF > (T0 ? 1 : 0)) atomicAdd(e0 + 2 * NF * P1, 1);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        if (T0 && f == 0) {
+            add_tracked(e0, NF * P1, b[0][0] - kMagicBits);
+            add_tracked(e0 + 1, NF * P1, b[0][1] - kMagicBits);
+            add_tracked(e2, NF * P1, b[0][2] - kMagicBits);
+            add_tracked(e2 + 1, NF * P1, b[0][3] - kMagicBits);
+        } else {
+            atomicAdd(e0 + f * P1, b[f][0]);
+            atomicAdd(e0 + f * P1 + 1, b[f][1]);
+            atomicAdd(e2 + f * P1, b[f][2]);
+            atomicAdd(e2 + f * P1 + 1, b[f][3]);
+        }
+    }
 }
 
 // dcu scales: |coef_dcu (E + v x B)| <= |qm| coef_max (Emax + 2 Umax Bmax); in
@@ -516,6 +700,75 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
     int ir, jr;
     ref_of(x0, y0, g, ir, jr);
 
+    // ---- single pass when the window fits: the particles do not move, so the
+    // window is the box of their base cells plus the corner - the gather tile's box
+    constexpr int P1 = 352, kTileCap1 = (PC - P1) * win_planes(NF) / 8;
+    static_assert(kTileCap1 >= P1, "the tile of a single-pass window must fit beside it");
+    {
+        BBox cb;
+#pragma unroll 4
+        for (int it = 0; it < kPPT; ++it) {
+            const int sl = it * kThreads + threadIdx.x;
+            const float x = m.stage[sl], y = m.stage[kChunk + sl];
+            if (sl < cnt && in_grid(x, y, g)) cb.add(static_cast<int>(x), static_cast<int>(y), ir, jr, g);
+        }
+        const Box bx = box_reduce(cb, m.red);
+        Win w1;
+        if (one_pass_window<NF, T0, P1>(w1, bx, ir, jr, 0)) {
+            float* const tile1 = reinterpret_cast<float*>(m.win + P1 * win_planes(NF));
+            const Tile tl = A.use_tile ? box_tile(bx, ir, jr, g, kTileCap1) : Tile{};
+            if (tl.use && !load_tile8(tile1, gb, tl, g, &tbar, st)) return;
+            win_zero<NF, T0, P1>(m.win, w1);
+            __syncthreads();
+            const int oi = win_origin(ir, w1.mi, g.nx), oj = win_origin(jr, w1.mj, g.ny);
+            float l1[NF] = {}, sq[NF] = {};
+            float nval = 0.f;
+#pragma unroll 1
+            for (int k = 0; k < kPPT; ++k) {
+                const int sl = spread_slot(k);
+                if (sl >= cnt) continue;
+                const float x = m.stage[sl], y = m.stage[kChunk + sl];
+                if (!in_grid(x, y, g)) { set_err(st, AW_DEV_OUT_OF_GRID); continue; }
+                const float w = m.stage[2 * kChunk + sl];
+                const float vx = m.stage[3 * kChunk + sl], vy = m.stage[4 * kChunk + sl], vz = m.stage[5 * kChunk + sl];
+                const Cic c = cic(x, y);
+                const EB2 eb = tl.use ? gather_em_tile2(tile1, c, win_col(c.i0, tl.i0, g.nx), win_col(c.j0, tl.j0, g.ny), tl.W)
+                                      : gather_em2(gb, c, g);
+                const float bxf = eb.ezbx.y, by = eb.byz.x, bz = eb.byz.y;
+                const float coef = __double2float_rn(qm2oa * static_cast<double>(w));
+                const float2 nxy = __fmul2_rn(make_float2(vz, vx), make_float2(-by, -bz));
+                const float2 cxy = __ffma2_rn(make_float2(vy, vz), make_float2(bz, bxf), nxy);
+                const float cz = __fmaf_rn(vx, by, -__fmul_rn(vy, bxf));
+                const float2 cfxy = __fmul2_rn(bc2(coef), __fadd2_rn(eb.exy, cxy));
+                const float cf[NF] = {cfxy.x, cfxy.y, __fmul_rn(coef, __fadd_rn(eb.ezbx.x, cz))};
+                float cs[NF];
+                const bool fast = scale_fast<NF>(cf, S, cs, l1);
+                if (((c.i0 + c.j0) & 7) == 0) {   // rms sample: the particles of one cell in 8, any order
+#pragma unroll
+                    for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
+                    nval += 1.0f;
+                }
+                // the scaled coefficients replace w, vx, vy in the stage for the slow path
+                m.stage[2 * kChunk + sl] = cs[0]; m.stage[3 * kChunk + sl] = cs[1]; m.stage[4 * kChunk + sl] = cs[2];
+                const int di = win_col(c.i0, oi, g.nx), dj = win_col(c.j0, oj, g.ny);
+                if (fast && di <= w1.W - 2 && dj <= w1.H - 2) one_pass_deposit<NF, T0, P1>(m.win, w1, di, dj, x, y, cs);
+                else list_slow(m.slow, &nlist, sl);
+            }
+            const bool redo = chunk_overflows<NF, T0>(l1, m.red);     // (its barrier also ends the pass)
+            if (!redo) win_flush<NF, T0, P1>(m.win, w1, acc, g);
+            slow_pass_linear<NF>(m.stage, m.slow, nlist, redo, cnt, acc, g, st, [&](int sl, float (&cs)[NF]) {
+                cs[0] = m.stage[2 * kChunk + sl]; cs[1] = m.stage[3 * kChunk + sl]; cs[2] = m.stage[4 * kChunk + sl];
+            });
+            if (threadIdx.x == 0) {
+                atomicAdd(&st->chunks, 1ull);
+                if (redo) atomicAdd(&st->overflow, 1ull);
+            }
+            if (psq) block_sumsq<NF>(sq, nval, psq, ssq, chunk);
+            return;
+        }
+    }
+
+    // ---- two passes --------------------------------------------------------
     // the field tile of the chunk's positions, in the window area
     Tile tl{};
     if (A.use_tile) {
@@ -853,6 +1106,129 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
     int ir, jr;
     ref_of(x0, y0, g, ir, jr);
 
+    // ---- single pass when the window fits ----------------------------------
+    // Window planes of stride P1 (window capacity P1 cells), the gather tile after them.
+    constexpr int P1 = 224, kTileCap1 = (PC - P1) * win_planes(NF) / 8;
+    {
+        BBox cb;
+#pragma unroll 4
+        for (int it = 0; it < kPPT; ++it) {
+            const int sl = it * kThreads + threadIdx.x;
+            const float x = m.stage[sl], y = m.stage[kChunk + sl];
+            if (sl < cnt && in_grid(x, y, g)) cb.add(static_cast<int>(x), static_cast<int>(y), ir, jr, g);
+        }
+        const Box bx = box_reduce(cb, m.red);
+        // the cells a particle can cross in one step: twice the largest in-plane |u| of
+        // the current state times dt/dx (one further cell for the rounding)
+        const float uxy_max = fmaxf(__uint_as_float(st->ucur_bits[0]), __uint_as_float(st->ucur_bits[1]));
+        const float dmv = __fmul_rn(2.0f * uxy_max, static_cast<float>(fmax(pp.dtx, pp.dty)));
+        const int mg = (dmv >= 0.0f && dmv < 8.0f) ? 1 + static_cast<int>(dmv) : -1;
+        Win w1;
+        if (mg > 0 && one_pass_window<NF, T0, P1>(w1, bx, ir, jr, mg)) {
+            float* const tile1 = reinterpret_cast<float*>(m.win + P1 * win_planes(NF));
+            const Tile tl = A.use_tile ? box_tile(bx, ir, jr, g, kTileCap1) : Tile{};
+            if (tl.use && !load_tile8(tile1, gb, tl, g, &tbar, st)) return;
+            win_zero<NF, T0, P1>(m.win, w1);
+            __syncthreads();
+            const int oi = win_origin(ir, w1.mi, g.nx), oj = win_origin(jr, w1.mj, g.ny);
+            float2 l1p[4] = {}, sqp[4] = {};
+            double ke = 0, px = 0, py = 0, pz = 0;
+            float m0 = 0.f, m1 = 0.f, m2 = 0.f, nval = 0.f;
+#pragma unroll 1
+            for (int k = 0; k < kPPT; ++k) {
+                const int sl = spread_slot(k);
+                if (sl >= cnt) continue;
+                float x = m.stage[sl], y = m.stage[kChunk + sl];
+                if (!in_grid(x, y, g)) { set_err(st, AW_DEV_OUT_OF_GRID); continue; }
+                const float w = m.stage[2 * kChunk + sl];
+                float ux = m.stage[3 * kChunk + sl], uy = m.stage[4 * kChunk + sl], uz = m.stage[5 * kChunk + sl];
+                const Cic c = cic(x, y);
+                const EB2 eb = tl.use ? gather_em_tile2(tile1, c, win_col(c.i0, tl.i0, g.nx), win_col(c.j0, tl.j0, g.ny), tl.W)
+                                      : gather_em2(gb, c, g);
+                float2 uxy = make_float2(ux, uy);
+                boris_em2(uxy, uz, eb.exy, eb.ezbx.x, eb.ezbx.y, eb.byz, pp.qmh);
+                ux = uxy.x; uy = uxy.y;
+                move_xy<POW2>(x, y, ux, uy, pp, g);
+                int ci, cj;
+                cell_ij(x, y, g, ci, cj);
+                m.stage[sl] = x; m.stage[kChunk + sl] = y;
+                m.stage[3 * kChunk + sl] = ux; m.stage[4 * kChunk + sl] = uy; m.stage[5 * kChunk + sl] = uz;
+                if (pp.write_cell && p.cell) __stcs(p.cell + c0 + sl, cj * g.nx + ci);
+                m0 = fmaxf(m0, fabsf(ux)); m1 = fmaxf(m1, fabsf(uy)); m2 = fmaxf(m2, fabsf(uz));
+                if (in_grid(x, y, g)) {
+                    float2 cp[4], csp[4];
+                    const float cf0 = __double2float_rn(qoa * static_cast<double>(w));
+                    src_coefs8(cf0, ux, uy, uz, cp);
+                    const bool fast = scale_fast2<4>(cp, Sp, csp, l1p);
+                    if (((ci + cj) & 7) == 0) {   // rms sample: the particles of one cell in 8, any order
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) sqp[i] = __ffma2_rn(cp[i], cp[i], sqp[i]);
+                        nval += 1.0f;
+                    }
+                    const int di = win_col(ci, oi, g.nx), dj = win_col(cj, oj, g.ny);
+                    if (fast && di <= w1.W - 2 && dj <= w1.H - 2) {
+                        const float cs[NF] = {csp[0].x, csp[0].y, csp[1].x, csp[1].y,
+                                              csp[2].x, csp[2].y, csp[3].x, csp[3].y};
+                        one_pass_deposit<NF, T0, P1>(m.win, w1, di, dj, x, y, cs);
+                    } else {
+                        list_slow(m.slow, &nlist, sl);
+                    }
+                } else {
+                    set_err(st, AW_DEV_OUT_OF_GRID);
+                }
+                const double dw = w, du = ux, dv = uy, dz = uz;
+                ke += dw * (du * du + dv * dv + dz * dz);
+                px += dw * du; py += dw * dv; pz += dw * dz;
+            }
+            m0 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m0)));
+            m1 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m1)));
+            m2 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m2)));
+            if ((threadIdx.x & 31) == 0) {
+                umx[0][threadIdx.x >> 5] = __float_as_uint(m0);
+                umx[1][threadIdx.x >> 5] = __float_as_uint(m1);
+                umx[2][threadIdx.x >> 5] = __float_as_uint(m2);
+            }
+            // the new state leaves by bulk copy (x y ux uy uz: stage planes 0 1 3 4 5)
+            const int pl[5] = {0, 1, 3, 4, 5};
+            float* const dst[5] = {p.x, p.y, p.ux, p.uy, p.uz};
+            bulk_store_planes<5>(m.stage, pl, dst, c0, cnt, p.vec_ok != 0);
+            if (threadIdx.x < 3) {
+                unsigned mx = 0;
+                for (int k = 0; k < kThreads / 32; ++k) mx = max(mx, umx[threadIdx.x][k]);
+                atomicMax(&st->umax_bits[threadIdx.x], mx);
+            }
+            float l1[NF], sq[NF];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) { l1[2 * i] = l1p[i].x; l1[2 * i + 1] = l1p[i].y; sq[2 * i] = sqp[i].x; sq[2 * i + 1] = sqp[i].y; }
+            const bool redo = chunk_overflows<NF, T0>(l1, m.red);
+            if (!redo) win_flush<NF, T0, P1>(m.win, w1, acc, g);
+            slow_pass_linear<NF>(m.stage, m.slow, nlist, redo, cnt, acc, g, st, [&](int sl, float (&cs)[NF]) {
+                float2 cp[4];
+                src_coefs8(__double2float_rn(qoa * static_cast<double>(m.stage[2 * kChunk + sl])),
+                           m.stage[3 * kChunk + sl], m.stage[4 * kChunk + sl], m.stage[5 * kChunk + sl], cp);
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const float2 cc = __fmul2_rn(cp[i], Sp[i]);
+                    cs[2 * i] = cc.x; cs[2 * i + 1] = cc.y;
+                }
+            });
+            if (threadIdx.x == 0) {
+                atomicAdd(&st->chunks, 1ull);
+                if (redo) atomicAdd(&st->overflow, 1ull);
+            }
+            block_sumsq<NF>(sq, nval, psq, ssq, chunk);
+            block_sum4(ke, px, py, pz, part, dsh, chunk);
+            if (threadIdx.x == 0 && chunk == 0) {
+#pragma unroll
+                for (int f = 0; f < NF; ++f) st->S_pend[f] = S[f];
+                st->step += 1;
+            }
+            bulk_store_wait();
+            return;
+        }
+    }
+
+    // ---- two passes --------------------------------------------------------
     // the field tile of the chunk's current positions, in the window area
     Tile tl{};
     if (A.use_tile) {

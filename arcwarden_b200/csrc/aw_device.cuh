@@ -194,12 +194,20 @@ __device__ __forceinline__ float2 gather4_tile2(const float2 (&W)[4], float2 a, 
 }
 
 // ---------------------------------------------------------------------------
+// s = 2 / (1 + t^2) of the Boris rotation, correctly rounded like the
+// reference's IEEE divide: for d = 1 + t^2 >= 1 the quotient 2/d is 2 (1/d),
+// and scaling by 2 commutes with rounding (no overflow, no subnormal), so
+// RN(2/d) = 2 RN(1/d) bit for bit; the correctly rounded reciprocal is the
+// cheaper operation.
+__device__ __forceinline__ float boris_sf(float t2) {
+    return __fmul_rn(2.0f, __frcp_rn(__fadd_rn(1.0f, t2)));
+}
 // Boris rotation about (bx,by,bz) with qmh = (q/m) dt/2 — pusher.hpp:85-97.
 __device__ __forceinline__ void boris_rotate(float& ux, float& uy, float& uz,
                                              float bx, float by, float bz, float qmh) {
     const float tx = __fmul_rn(qmh, bx), ty = __fmul_rn(qmh, by), tz = __fmul_rn(qmh, bz);
     const float t2 = __fmaf_rn(tz, tz, __fmaf_rn(ty, ty, __fmul_rn(tx, tx)));
-    const float sf = __fdiv_rn(2.0f, __fadd_rn(1.0f, t2));
+    const float sf = boris_sf(t2);
     const float sx = __fmul_rn(sf, tx), sy = __fmul_rn(sf, ty), sz = __fmul_rn(sf, tz);
     const float upx = __fadd_rn(ux, __fmaf_rn(uy, tz, -__fmul_rn(uz, ty)));
     const float upy = __fadd_rn(uy, __fmaf_rn(uz, tx, -__fmul_rn(ux, tz)));
@@ -235,7 +243,7 @@ __device__ __forceinline__ void boris_em2(float2& uxy, float& uz, float2 exy, fl
     const float tx = __fmul_rn(qmh, bx);
     const float2 tyz = __fmul2_rn(Q, byz);
     const float t2 = __fmaf_rn(tyz.y, tyz.y, __fmaf_rn(tyz.x, tyz.x, __fmul_rn(tx, tx)));
-    const float sf = __fdiv_rn(2.0f, __fadd_rn(1.0f, t2));
+    const float sf = boris_sf(t2);
     const float sx = __fmul_rn(sf, tx);
     const float2 syz = __fmul2_rn(bc2(sf), tyz);
     const float ux = uxy.x, uy = uxy.y;
@@ -566,6 +574,24 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
     return false;
 }
 
+// Block-wide bounded wait on the phase-0 completion of `bar`: one warp polls
+// while the other warps sleep at the barrier (a polling warp takes issue
+// slots), then every thread takes the completed phase itself (one try_wait,
+// which orders its reads of the copied bytes after the copy). Returns false
+// (block-uniformly) when the wait gave up; the copies in flight are then given
+// a second bounded wait before the caller returns.
+__device__ __forceinline__ bool mbar_wait_block(unsigned long long* bar, DevState* st) {
+    bool ok = true;
+    if (threadIdx.x < 32) ok = mbar_wait_bounded(bar, 0u);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) set_err(st, 4u);     // AW_DEV_WAIT_LIMIT
+        mbar_wait_bounded(bar, 0u);                // let copies in flight land
+        return false;
+    }
+    mbar_wait_bounded(bar, 0u);                    // completed: returns at the first try
+    return true;
+}
+
 // Source arrays of a chunk load, in stage-plane order.
 struct ChunkSrc {
     const float* a[7];
@@ -598,15 +624,7 @@ __device__ __forceinline__ bool load_chunk(float* stage, const ChunkSrc& src, in
             stage[k * kChunk + s] = __ldg(src.at(k) + c0 + s);
         }
     __syncthreads();                        // barrier initialised; plain loads visible
-    bool ok = mbar_wait_bounded(bar, 0u);
-    *x0 = stage[0];
-    *y0 = stage[kChunk];
-    if (__syncthreads_or(!ok)) {
-        if (threadIdx.x == 0) set_err(st, 4u);     // AW_DEV_WAIT_LIMIT
-        mbar_wait_bounded(bar, 0u);                // let copies in flight land
-        return false;
-    }
-    return true;
+    return mbar_wait_block(bar, st) && (*x0 = stage[0], *y0 = stage[kChunk], true);
 }
 
 // Write planes [0, np) of the stage back to the chunk [c0, c0 + cnt) of their
