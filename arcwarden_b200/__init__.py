@@ -79,9 +79,13 @@ class CheckpointInfo(C.Structure):
                 ("eps_l", C.c_double), ("deck", C.c_char_p), ("git_hash", C.c_char_p)]
 
 
+class KernelPlan(C.Structure):
+    _fields_ = [("one_pass", C.c_int32), ("tile", C.c_int32), ("es_window", C.c_int32)]
+
+
 class Stats(C.Structure):
     _fields_ = [("chunks", C.c_int64), ("window_overflow", C.c_int64), ("slow_deposits", C.c_int64),
-                ("steps", C.c_int64), ("kernels_per_step", C.c_int64)]
+                ("steps", C.c_int64), ("kernels_per_step", C.c_int64), ("one_pass_chunks", C.c_int64)]
 
 
 # Exported symbols and their ctypes signatures (must match include/arcb200.h).
@@ -91,6 +95,8 @@ SIGNATURES = {
     "aw_ctx_destroy": [_P],
     "aw_set_stream": [_P, _P],
     "aw_set_params": [_P, C.POINTER(Params)],
+    "aw_set_kernel_plan": [_P, C.POINTER(KernelPlan)],
+    "aw_get_kernel_plan": [_P, C.POINTER(KernelPlan)],
     "aw_particles_bind": [_P, _P, _P, _P, _P, _P, _P, _P, _I64],
     "aw_sources_bind": [_P, C.POINTER(SourcePtrs)],
     "aw_fields_bind": [_P, C.POINTER(FieldPtrs)],
@@ -250,6 +256,15 @@ class Context:
     def set_resort(self, every: int):
         """Re-sort inside run() before every step n with n % every == 0 (0 = never)."""
         _check(self.lib.aw_set_resort(self.h, int(every)))
+
+    def set_kernel_plan(self, one_pass: int = -1, tile: int = -1, es_window: int = 0):
+        """The particle kernels' choices (-1 / 0: built in); results never change."""
+        _check(self.lib.aw_set_kernel_plan(self.h, C.byref(KernelPlan(one_pass, tile, es_window))))
+
+    def kernel_plan(self) -> dict:
+        k = KernelPlan()
+        _check(self.lib.aw_get_kernel_plan(self.h, C.byref(k)))
+        return {"one_pass": k.one_pass, "tile": k.tile, "es_window": k.es_window}
 
     def set_form_factor(self, ax: float = 0.0, ay: float = 0.0, cic_order: int = 0, k_filter: float = 0.0):
         """k-space form factor s(k) on every solve: exp(-((kx ax)^2 + (ky ay)^2)/2)

@@ -1028,6 +1028,27 @@ int aw_set_resort(aw_ctx* ctx, int32_t every) {
     });
 }
 
+int aw_set_kernel_plan(aw_ctx* ctx, const aw_kernel_plan* plan) {
+    return guarded([&] {
+        aw::need(ctx != nullptr && plan != nullptr, AW_ERR_ARG, "null argument");
+        aw::need(plan->one_pass >= -1 && plan->one_pass <= 1 && plan->tile >= -1 && plan->tile <= 1,
+                 AW_ERR_ARG, "set_kernel_plan: one_pass and tile are -1, 0 or 1");
+        aw::need(plan->es_window == 0 || (plan->es_window >= 256 && plan->es_window <= 4096), AW_ERR_ARG,
+                 "set_kernel_plan: es_window is 0 or 256..4096 cells");
+        Ctx& c = ctx->c;
+        if (std::memcmp(&c.plan, plan, sizeof(aw_kernel_plan)) == 0) return;
+        c.plan = *plan;
+        aw::drop_graph(c);     // the captured step holds the old kernel arguments
+    });
+}
+
+int aw_get_kernel_plan(aw_ctx* ctx, aw_kernel_plan* plan) {
+    return guarded([&] {
+        aw::need(ctx != nullptr && plan != nullptr, AW_ERR_ARG, "null argument");
+        *plan = ctx->c.plan;
+    });
+}
+
 int aw_resort(aw_ctx* ctx) {
     return guarded([&] {
         aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
@@ -1135,6 +1156,7 @@ int aw_stats(aw_ctx* ctx, aw_stats_t* out) {
         out->slow_deposits = static_cast<int64_t>(h.slow);
         out->steps = h.step;
         out->kernels_per_step = aw::kernels_per_step(c);
+        out->one_pass_chunks = static_cast<int64_t>(h.one_pass);
     });
 }
 

@@ -338,8 +338,7 @@ k_deposit_src(Parts p, Geo g, double qoa, const float* __restrict__ Sdev,
                 set_err(st, AW_DEV_OUT_OF_GRID);
             }
         }
-        __syncwarp();
-        const int d = stage_slot(s);
+        const int d = s;                     // in place: this thread's own slot
         m.stage[d] = xs;
 #pragma unroll
         for (int f = 1; f < NS; ++f) m.stage[f * kChunk + d] = a[f];
@@ -473,14 +472,6 @@ __device__ __forceinline__ bool load_tile8(float* tile, const float* __restrict_
 // coefficients leave the fast range takes the exact slow path, as in the two-pass
 // kernels, so the sums are the same bits either way. Chunks that do not fit take
 // the two-pass path.
-
-// Slot of this thread's k-th particle: lanes sit 64 particles apart (in loader
-// order a warp's atomics then fall on different cells) and read the linear stage
-// without bank conflicts (lane l's slot is congruent to 8 w + k + l modulo 32).
-__device__ __forceinline__ int spread_slot(int k) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    return 64 * lane + ((8 * warp + k + lane) & 63);
-}
 
 // Block-wide box of the threads' BBoxes (empty: lo > hi). Ends with a barrier
 // after the scratch `red` is read.
@@ -672,7 +663,7 @@ __device__ __forceinline__ void dcu_scales(const DevState* st, float abs_qm, boo
 // dcu deposit: input x y w ux uy uz; stage = x, y, ax, ay, az (scaled coefficients).
 struct DcuArgs {
     Parts p; Geo g; double qm2oa; float abs_qm; const float* gb; unsigned long long* acc; int wmaxc;
-    DevState* st; int use_rms; float* psq; int use_tile;
+    DevState* st; int use_rms; float* psq; int use_tile; int one_pass;
 };
 __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int chunk) {
     const Parts& p = A.p; const Geo& g = A.g;
@@ -704,7 +695,7 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
     // window is the box of their base cells plus the corner - the gather tile's box
     constexpr int P1 = 352, kTileCap1 = (PC - P1) * win_planes(NF) / 8;
     static_assert(kTileCap1 >= P1, "the tile of a single-pass window must fit beside it");
-    {
+    if (A.one_pass) {
         BBox cb;
 #pragma unroll 4
         for (int it = 0; it < kPPT; ++it) {
@@ -714,9 +705,9 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
         }
         const Box bx = box_reduce(cb, m.red);
         Win w1;
-        if (one_pass_window<NF, T0, P1>(w1, bx, ir, jr, 0)) {
+        if (A.one_pass && one_pass_window<NF, T0, P1>(w1, bx, ir, jr, 0)) {
             float* const tile1 = reinterpret_cast<float*>(m.win + P1 * win_planes(NF));
-            const Tile tl = A.use_tile ? box_tile(bx, ir, jr, g, kTileCap1) : Tile{};
+            const Tile tl = box_tile(bx, ir, jr, g, kTileCap1);
             if (tl.use && !load_tile8(tile1, gb, tl, g, &tbar, st)) return;
             win_zero<NF, T0, P1>(m.win, w1);
             __syncthreads();
@@ -761,6 +752,7 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
             });
             if (threadIdx.x == 0) {
                 atomicAdd(&st->chunks, 1ull);
+                atomicAdd(&st->one_pass, 1ull);
                 if (redo) atomicAdd(&st->overflow, 1ull);
             }
             if (psq) block_sumsq<NF>(sq, nval, psq, ssq, chunk);
@@ -787,16 +779,18 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
     float* const tile = reinterpret_cast<float*>(m.win);
     if (tl.use && !load_tile8(tile, gb, tl, g, &tbar, st)) return;
 
+    // Stage after pass 1, per slot: x (sign set: no deposit - listed for the slow
+    // path, or not in the grid), y (< 0: not in the grid), the unscaled
+    // coefficients; pass 2 (spread lanes) deposits and takes the rms sample over
+    // the same slots of each thread as the single pass.
     BBox bb;
     float l1[NF] = {};
-    float sq[NF] = {};
-    float nval = 0.f;
 #pragma unroll 2
     for (int it = 0; it < kPPT; ++it) {
         const int s = it * kThreads + threadIdx.x;
         const float x = m.stage[s], y = m.stage[kChunk + s], w = m.stage[2 * kChunk + s];
         const float vx = m.stage[3 * kChunk + s], vy = m.stage[4 * kChunk + s], vz = m.stage[5 * kChunk + s];
-        float xs = -1.0f, cs[NF] = {0.f, 0.f, 0.f};
+        float xs = -1.0f, ys = -1.0f, cfs[NF] = {0.f, 0.f, 0.f};
         if (s < cnt) {
             if (in_grid(x, y, g)) {
                 const Cic c = cic(x, y);
@@ -811,29 +805,53 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
                 const float cz = __fmaf_rn(vx, by, -__fmul_rn(vy, bx));
                 const float2 cfxy = __fmul2_rn(bc2(coef), __fadd2_rn(eb.exy, cxy));
                 const float cf[NF] = {cfxy.x, cfxy.y, __fmul_rn(coef, __fadd_rn(eb.ezbx.x, cz))};
+                float cs[NF];
                 const bool fast = scale_fast<NF>(cf, S, cs, l1);
-                if (((c.i0 + c.j0) & 7) == 0) {   // rms sample: the particles of one cell in 8, any order
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(cf[f], cf[f], sq[f]);
-                    nval += 1.0f;
-                }
                 xs = __fadd_rn(x, 0.0f);
+                ys = y;
+                cfs[0] = cf[0]; cfs[1] = cf[1]; cfs[2] = cf[2];
                 if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
             } else {
                 set_err(st, AW_DEV_OUT_OF_GRID);
             }
         }
-        __syncwarp();
-        const int d = stage_slot(s);
+        const int d = s;                     // in place: this thread's own slot
         m.stage[d] = xs;
-        m.stage[kChunk + d] = y;
-        m.stage[2 * kChunk + d] = cs[0];
-        m.stage[3 * kChunk + d] = cs[1];
-        m.stage[4 * kChunk + d] = cs[2];
+        m.stage[kChunk + d] = ys;
+        m.stage[2 * kChunk + d] = cfs[0];
+        m.stage[3 * kChunk + d] = cfs[1];
+        m.stage[4 * kChunk + d] = cfs[2];
     }
     const Win wn = open_window<NF, T0, PC>(bb, ir, jr, wmaxc, m, l1);
-    auto coef = [&](const float (&a)[NS], float (&cs)[NF]) { cs[0] = a[2]; cs[1] = a[3]; cs[2] = a[4]; };
-    window_pass<NF, NS, T0, PC>(m.stage, m.win, wn, g, coef, acc);
+    auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
+        cs[0] = __fmul_rn(a[2], S[0]); cs[1] = __fmul_rn(a[3], S[1]); cs[2] = __fmul_rn(a[4], S[2]);
+    };
+    float sq[NF] = {};
+    float nval = 0.f;
+    auto stats = [&](const float (&a)[NS]) {
+        if (a[1] >= 0.0f) {
+            const int ci = static_cast<int>(fabsf(a[0])), cj = static_cast<int>(a[1]);
+            if (((ci + cj) & 7) == 0) {   // rms sample: the particles of one cell in 8, any order
+#pragma unroll
+                for (int f = 0; f < NF; ++f) sq[f] = __fmaf_rn(a[2 + f], a[2 + f], sq[f]);
+                nval += 1.0f;
+            }
+        }
+    };
+    if (wn.use && wn.nb == 1) {
+        if (wn.track_all) window_particles<NF, NS, T0, true, PC>(m.stage, m.win, wn, g, coef, stats);
+        else window_particles<NF, NS, T0, false, PC>(m.stage, m.win, wn, g, coef, stats);
+    } else {
+#pragma unroll 1
+        for (int k = 0; k < kPPT; ++k) {
+            const int d = spread_slot(k);
+            float a[NS];
+#pragma unroll
+            for (int f = 0; f < NS; ++f) a[f] = m.stage[f * kChunk + d];
+            stats(a);
+        }
+        window_pass<NF, NS, T0, PC>(m.stage, m.win, wn, g, coef, acc);   // bands (or the slow path alone)
+    }
     close_window<NF, NS, T0, PC>(m, wn, nlist, acc, g, st, coef);
     if (psq) block_sumsq<NF>(sq, nval, psq, ssq, chunk);}
 __global__ void __launch_bounds__(kThreads, 3) k_deposit_dcu(DcuArgs A) { deposit_dcu_chunk(A, blockIdx.x); }
@@ -929,8 +947,7 @@ k_adj_scatter(AdjP a, Geo g, AdjK k, const float2* __restrict__ trajE, AdjDev* a
             xs = __fadd_rn(x, 0.0f);
             if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
         }
-        __syncwarp();
-        const int d = stage_slot(s);
+        const int d = s;                     // in place: this thread's own slot
         m.stage[d] = xs;
         m.stage[kChunk + d] = y;
         m.stage[2 * kChunk + d] = cs[0];
@@ -1048,8 +1065,7 @@ __device__ __forceinline__ void push_deposit_es_chunk(const EsArgs& A, const int
                 set_err(st, AW_DEV_OUT_OF_GRID);
             }
         }
-        __syncwarp();
-        const int d = stage_slot(s);
+        const int d = s;                     // in place: this thread's own slot
         m.stage[d] = xs;
         m.stage[kChunk + d] = y;
         m.stage[2 * kChunk + d] = cf0;
@@ -1073,7 +1089,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_push_deposit_es(EsArgs A) {
 // Fused Darwin step kernel: input x y w ux uy uz; stage = new x, y, coefficient, ux, uy, uz.
 struct EmArgs {
     Parts p; Geo g; PushP pp; const float* gb; double qoa; unsigned long long* acc; int wmaxc;
-    double* part; DevState* st; float* psq; int use_tile;
+    double* part; DevState* st; float* psq; int use_tile; int one_pass;
 };
 template <bool POW2>
 __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int chunk) {
@@ -1109,7 +1125,7 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
     // ---- single pass when the window fits ----------------------------------
     // Window planes of stride P1 (window capacity P1 cells), the gather tile after them.
     constexpr int P1 = 224, kTileCap1 = (PC - P1) * win_planes(NF) / 8;
-    {
+    if (A.one_pass) {
         BBox cb;
 #pragma unroll 4
         for (int it = 0; it < kPPT; ++it) {
@@ -1124,9 +1140,9 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
         const float dmv = __fmul_rn(2.0f * uxy_max, static_cast<float>(fmax(pp.dtx, pp.dty)));
         const int mg = (dmv >= 0.0f && dmv < 8.0f) ? 1 + static_cast<int>(dmv) : -1;
         Win w1;
-        if (mg > 0 && one_pass_window<NF, T0, P1>(w1, bx, ir, jr, mg)) {
+        if (A.one_pass && mg > 0 && one_pass_window<NF, T0, P1>(w1, bx, ir, jr, mg)) {
             float* const tile1 = reinterpret_cast<float*>(m.win + P1 * win_planes(NF));
-            const Tile tl = A.use_tile ? box_tile(bx, ir, jr, g, kTileCap1) : Tile{};
+            const Tile tl = box_tile(bx, ir, jr, g, kTileCap1);
             if (tl.use && !load_tile8(tile1, gb, tl, g, &tbar, st)) return;
             win_zero<NF, T0, P1>(m.win, w1);
             __syncthreads();
@@ -1153,7 +1169,6 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
                 cell_ij(x, y, g, ci, cj);
                 m.stage[sl] = x; m.stage[kChunk + sl] = y;
                 m.stage[3 * kChunk + sl] = ux; m.stage[4 * kChunk + sl] = uy; m.stage[5 * kChunk + sl] = uz;
-                if (pp.write_cell && p.cell) __stcs(p.cell + c0 + sl, cj * g.nx + ci);
                 m0 = fmaxf(m0, fabsf(ux)); m1 = fmaxf(m1, fabsf(uy)); m2 = fmaxf(m2, fabsf(uz));
                 if (in_grid(x, y, g)) {
                     float2 cp[4], csp[4];
@@ -1192,6 +1207,15 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
             const int pl[5] = {0, 1, 3, 4, 5};
             float* const dst[5] = {p.x, p.y, p.ux, p.uy, p.uz};
             bulk_store_planes<5>(m.stage, pl, dst, c0, cnt, p.vec_ok != 0);
+            if (pp.write_cell && p.cell)      // the owning cells, coalesced, from the staged new positions
+                for (int sl = threadIdx.x; sl < cnt; sl += kThreads) {
+                    const float x = m.stage[sl], y = m.stage[kChunk + sl];
+                    if (in_grid(x, y, g)) {
+                        int ci, cj;
+                        cell_ij(x, y, g, ci, cj);
+                        __stcs(p.cell + c0 + sl, cj * g.nx + ci);
+                    }
+                }
             if (threadIdx.x < 3) {
                 unsigned mx = 0;
                 for (int k = 0; k < kThreads / 32; ++k) mx = max(mx, umx[threadIdx.x][k]);
@@ -1214,6 +1238,7 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
             });
             if (threadIdx.x == 0) {
                 atomicAdd(&st->chunks, 1ull);
+                atomicAdd(&st->one_pass, 1ull);
                 if (redo) atomicAdd(&st->overflow, 1ull);
             }
             block_sumsq<NF>(sq, nval, psq, ssq, chunk);
@@ -1229,6 +1254,14 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
     }
 
     // ---- two passes --------------------------------------------------------
+    // Pass 1 (lanes on neighbouring particles) pushes, stores the new state and
+    // stages it in place; pass 2 (spread lanes) deposits and accumulates the
+    // step's kinetic energy, momentum and coefficient rms, over the same slots
+    // of each thread and in the same order as the single pass: the partial sums,
+    // and so the diagnostics and the next deposit's scales, do not depend on the
+    // path. Stage after pass 1, per slot: x (sign set: no deposit - listed for the
+    // slow path, or no new position in the grid), y (< 0: no new position in the
+    // grid), w (0 when the particle was not pushed), ux uy uz (0 when not pushed).
     // the field tile of the chunk's current positions, in the window area
     Tile tl{};
     if (A.use_tile) {
@@ -1248,10 +1281,8 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
     if (tl.use && !load_tile8(tile, gb, tl, g, &tbar, st)) return;
 
     BBox bb;
-    float2 l1p[4] = {}, sqp[4] = {};
-    double ke = 0, px = 0, py = 0, pz = 0;
+    float2 l1p[4] = {};
     float m0 = 0.f, m1 = 0.f, m2 = 0.f;
-    float nval = 0.f;
 #pragma unroll 2
     for (int it = 0; it < kPPT; ++it) {
         const int s = it * kThreads + threadIdx.x;
@@ -1259,7 +1290,8 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
         float x = m.stage[s], y = m.stage[kChunk + s];
         const float w = m.stage[2 * kChunk + s];
         float ux = m.stage[3 * kChunk + s], uy = m.stage[4 * kChunk + s], uz = m.stage[5 * kChunk + s];
-        float xs = -1.0f, cf0 = 0.0f;
+        float xs = -1.0f, ys = -1.0f, ws = 0.0f;
+        bool pushed = false;
         if (s < cnt) {
             if (in_grid(x, y, g)) {
                 const Cic c = cic(x, y);
@@ -1275,37 +1307,30 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
                 __stcs(p.x + i, x); __stcs(p.y + i, y); __stcs(p.ux + i, ux); __stcs(p.uy + i, uy); __stcs(p.uz + i, uz);
                 if (pp.write_cell && p.cell) __stcs(p.cell + i, cj * g.nx + ci);
                 m0 = fmaxf(m0, fabsf(ux)); m1 = fmaxf(m1, fabsf(uy)); m2 = fmaxf(m2, fabsf(uz));
+                pushed = true;
+                ws = w;
                 if (in_grid(x, y, g)) {
                     bb.add(ci, cj, ir, jr, g);
                     float2 cp[4], csp[4];
-                    cf0 = __double2float_rn(qoa * static_cast<double>(w));
-                    src_coefs8(cf0, ux, uy, uz, cp);
+                    src_coefs8(__double2float_rn(qoa * static_cast<double>(w)), ux, uy, uz, cp);
                     const bool fast = scale_fast2<4>(cp, Sp, csp, l1p);
-                    if (((ci + cj) & 7) == 0) {   // rms sample: the particles of one cell in 8, any order
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) sqp[i] = __ffma2_rn(cp[i], cp[i], sqp[i]);
-                        nval += 1.0f;
-                    }
                     xs = __fadd_rn(x, 0.0f);
+                    ys = y;
                     if (!fast) { xs = -xs; list_slow(m.slow, &nlist, s); }
                 } else {
                     set_err(st, AW_DEV_OUT_OF_GRID);
                 }
-                const double dw = w, du = ux, dv = uy, dz = uz;
-                ke += dw * (du * du + dv * dv + dz * dz);
-                px += dw * du; py += dw * dv; pz += dw * dz;
             } else {
                 set_err(st, AW_DEV_OUT_OF_GRID);
             }
         }
-        __syncwarp();
-        const int d = stage_slot(s);
+        const int d = s;                     // in place: this thread's own slot
         m.stage[d] = xs;
-        m.stage[kChunk + d] = y;
-        m.stage[2 * kChunk + d] = cf0;
-        m.stage[3 * kChunk + d] = ux;
-        m.stage[4 * kChunk + d] = uy;
-        m.stage[5 * kChunk + d] = uz;
+        m.stage[kChunk + d] = ys;
+        m.stage[2 * kChunk + d] = ws;
+        m.stage[3 * kChunk + d] = pushed ? ux : 0.0f;
+        m.stage[4 * kChunk + d] = pushed ? uy : 0.0f;
+        m.stage[5 * kChunk + d] = pushed ? uz : 0.0f;
     }
     // |u| maxima of the new state (next step's deposit scales): one atomic per block
     m0 = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(m0)));
@@ -1316,9 +1341,9 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
         umx[1][threadIdx.x >> 5] = __float_as_uint(m1);
         umx[2][threadIdx.x >> 5] = __float_as_uint(m2);
     }
-    float l1[NF], sq[NF];
+    float l1[NF];
 #pragma unroll
-    for (int i = 0; i < 4; ++i) { l1[2 * i] = l1p[i].x; l1[2 * i + 1] = l1p[i].y; sq[2 * i] = sqp[i].x; sq[2 * i + 1] = sqp[i].y; }
+    for (int i = 0; i < 4; ++i) { l1[2 * i] = l1p[i].x; l1[2 * i + 1] = l1p[i].y; }
     const Win wn = open_window<NF, T0, PC>(bb, ir, jr, wmaxc, m, l1);
     if (threadIdx.x < 3) {
         unsigned mx = 0;
@@ -1327,15 +1352,50 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
     }
     auto coef = [&](const float (&a)[NS], float (&cs)[NF]) {
         float2 cp[4];
-        src_coefs8(a[2], a[3], a[4], a[5], cp);
+        src_coefs8(__double2float_rn(qoa * static_cast<double>(a[2])), a[3], a[4], a[5], cp);
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
             const float2 c = __fmul2_rn(cp[i], Sp[i]);
             cs[2 * i] = c.x; cs[2 * i + 1] = c.y;
         }
     };
-    window_pass<NF, NS, T0, PC>(m.stage, m.win, wn, g, coef, acc);
+    // the step's sums, every slot (a pushed particle's KE, momentum; the rms sample)
+    float2 sqp[4] = {};
+    double ke = 0, px = 0, py = 0, pz = 0;
+    float nval = 0.f;
+    auto stats = [&](const float (&a)[NS]) {
+        const double dw = a[2], du = a[3], dv = a[4], dz = a[5];
+        ke += dw * (du * du + dv * dv + dz * dz);
+        px += dw * du; py += dw * dv; pz += dw * dz;
+        if (a[1] >= 0.0f) {
+            const int ci = static_cast<int>(fabsf(a[0])), cj = static_cast<int>(a[1]);
+            if (((ci + cj) & 7) == 0) {   // rms sample: the particles of one cell in 8, any order
+                float2 cp[4];
+                src_coefs8(__double2float_rn(qoa * static_cast<double>(a[2])), a[3], a[4], a[5], cp);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) sqp[q] = __ffma2_rn(cp[q], cp[q], sqp[q]);
+                nval += 1.0f;
+            }
+        }
+    };
+    if (wn.use && wn.nb == 1) {
+        if (wn.track_all) window_particles<NF, NS, T0, true, PC>(m.stage, m.win, wn, g, coef, stats);
+        else window_particles<NF, NS, T0, false, PC>(m.stage, m.win, wn, g, coef, stats);
+    } else {
+#pragma unroll 1
+        for (int k = 0; k < kPPT; ++k) {
+            const int d = spread_slot(k);
+            float a[NS];
+#pragma unroll
+            for (int f = 0; f < NS; ++f) a[f] = m.stage[f * kChunk + d];
+            stats(a);
+        }
+        window_pass<NF, NS, T0, PC>(m.stage, m.win, wn, g, coef, acc);   // bands (or the slow path alone)
+    }
     close_window<NF, NS, T0, PC>(m, wn, nlist, acc, g, st, coef);
+    float sq[NF];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { sq[2 * i] = sqp[i].x; sq[2 * i + 1] = sqp[i].y; }
     block_sumsq<NF>(sq, nval, psq, ssq, chunk);
     block_sum4(ke, px, py, pz, part, dsh, chunk);
     if (threadIdx.x == 0 && chunk == 0) {
@@ -1431,7 +1491,16 @@ PushP push_params(const Ctx& c) {
 // most 128 particles per cell on average (16 or more cells per chunk). Denser
 // chunks keep their few cells in L1, and the tile's pre-pass and copy only add
 // time (dcu at 64 per cell: -2%; at 256 per cell: +4.6%).
-bool use_tile(const Ctx& c) { return c.parts.n <= 128LL * c.geo.ncell; }
+bool use_tile(const Ctx& c) {
+    return c.plan.tile >= 0 ? c.plan.tile != 0 : c.parts.n <= 128LL * c.geo.ncell;
+}
+// The single pass pays where chunks are dense (few cells, the spread lanes of the
+// deposit share cells anyway); where a chunk spans many cells the two-pass
+// kernels gather with lanes on neighbouring particles, which read the same tile
+// cells.
+bool one_pass(const Ctx& c) {
+    return c.plan.one_pass >= 0 ? c.plan.one_pass != 0 : c.parts.n > 128LL * c.geo.ncell;
+}
 DcuArgs dcu_args(const Ctx& c, const float* gb, bool fused) {
     DcuArgs a{};
     a.p = c.parts; a.g = c.geo;
@@ -1440,9 +1509,11 @@ DcuArgs dcu_args(const Ctx& c, const float* gb, bool fused) {
     a.gb = gb; a.acc = c.acc_dcu; a.wmaxc = wmax_cells(3); a.st = c.st;
     a.use_rms = fused ? 1 : 0; a.psq = fused ? c.part_d : nullptr;
     a.use_tile = use_tile(c) ? 1 : 0;
+    a.one_pass = one_pass(c) ? 1 : 0;
     return a;
 }
 int es_window(const Ctx& c) {
+    if (c.plan.es_window > 0) return c.plan.es_window;
     return c.parts.n >= 32LL * c.geo.ncell ? kEsWindowSmall : kEsWindowLarge;
 }
 EsArgs es_args(const Ctx& c) {
@@ -1459,6 +1530,7 @@ EmArgs em_args(const Ctx& c) {
     a.qoa = c.prm.qm / (c.geo.dx * c.geo.dy);
     a.acc = c.acc_src; a.wmaxc = wmax_cells(8); a.part = c.part_p; a.st = c.st; a.psq = c.part_c;
     a.use_tile = use_tile(c) ? 1 : 0;
+    a.one_pass = one_pass(c) ? 1 : 0;
     return a;
 }
 bool pow2_geo(const Ctx& c) { return is_pow2(c.geo.dx) && is_pow2(c.geo.dy); }
@@ -1599,10 +1671,9 @@ __device__ __forceinline__ int wrap_node(int i, int n) {
 __device__ __forceinline__ void yee_window_pass(const float* __restrict__ stage, int* __restrict__ win,
                                                 const Win& wn, const Geo& g) {
     if (!wn.use) return;
-    const int base = 64 * (threadIdx.x & 31) + 8 * (threadIdx.x >> 5);
 #pragma unroll 1
     for (int k = 0; k < kPPT; ++k) {
-        const int d = stage_slot(base + k);
+        const int d = spread_slot(k);
         const float x0 = stage[d];
         if (__float_as_int(x0) < 0) continue;
         const float y0 = stage[kChunk + d], x1 = stage[2 * kChunk + d], y1 = stage[3 * kChunk + d];
@@ -1629,7 +1700,7 @@ __device__ __forceinline__ void yee_slow_pass(const float* __restrict__ stage, c
     unsigned n = 0;
     for (int k = threadIdx.x; k < total; k += kThreads) {
         const bool listed = k < nlist;
-        const int d = stage_slot(listed ? static_cast<int>(list[k]) : k - nlist);
+        const int d = listed ? static_cast<int>(list[k]) : k - nlist;
         float x0 = stage[d];
         if (listed) x0 = -x0;
         else if (__float_as_int(x0) < 0) continue;
@@ -1749,8 +1820,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_push_esirkepov(YeeArgs A) {
                 set_err(st, AW_DEV_OUT_OF_GRID);
             }
         }
-        __syncwarp();
-        const int d = stage_slot(s);
+        const int d = s;                     // in place: this thread's own slot
         m.stage[d] = xs;
         m.stage[kChunk + d] = y0;
         m.stage[2 * kChunk + d] = x1;

@@ -80,6 +80,7 @@ struct DevState {
     float     rms_dcu[4];      // rms of the dcu coefficients (unscaled)
     unsigned long long chunks, overflow, slow;
     unsigned  red_ticket;      // k_step_reduce blocks finished (reset by the last)
+    unsigned long long one_pass;   // chunks taken by the single-pass path
     double    rho_ref;         // mean charge density, subtracted from the fused solve's
                                // FFT input (the k = 0 mode is zeroed anyway): a large
                                // mean would otherwise put FP32 roundoff into every mode
@@ -495,12 +496,17 @@ __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& 
 // Wrapped offset of a cell from the window's reference cell.
 __device__ __forceinline__ int win_off(int c, int r, int n) { return wrap_signed(c - r, n); }
 
-// Stage layout: chunk slot s is stored at s ^ ((s >> 6) & 31). Pass 1 writes
-// 32 consecutive slots per warp instruction (one aligned group of 32, permuted
-// within itself: conflict-free, and a warp only ever touches its own groups, so
-// the rewrite can be done in place); pass 2 reads slot 64 l + c in lane l, which
-// lands in bank (c ^ l) mod 32: conflict-free as well.
-__device__ __forceinline__ int stage_slot(int s) { return s ^ ((s >> 6) & 31); }
+// The stage is linear: chunk slot s of plane f is stage[f * kChunk + s]. Pass 1
+// takes slots it * kThreads + t (lanes on neighbouring particles: coalesced
+// global accesses, and the gathers of a warp fall on few cells); the deposit
+// takes this thread's k-th slot below. Lanes sit 64 particles apart (in loader
+// order a warp's atomics then fall on different cells) and read the linear
+// stage without bank conflicts (lane l's slot is congruent to 8 w + k + l
+// modulo 32). Over k = 0..7 the 256 threads take every slot exactly once.
+__device__ __forceinline__ int spread_slot(int k) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    return 64 * lane + ((8 * warp + k + lane) & 63);
+}
 
 // Exact quantisation of a contribution: rint(a*b) with one FFMA against
 // 1.5*2^23 (exact for |a*b| < 2^22), read back as an integer.
@@ -672,7 +678,7 @@ __device__ __forceinline__ void slow_pass(const float* __restrict__ stage, const
     unsigned n = 0;
     for (int k = threadIdx.x; k < total; k += kThreads) {
         const bool listed = k < nlist;
-        const int d = stage_slot(listed ? static_cast<int>(list[k]) : k - nlist);
+        const int d = listed ? static_cast<int>(list[k]) : k - nlist;
         float a[NS];
 #pragma unroll
         for (int f = 0; f < NS; ++f) a[f] = stage[f * kChunk + d];
@@ -732,19 +738,22 @@ __device__ __forceinline__ void quant_bits(const float (&cs)[NF], const Cic2& c,
 // contribution, and the particle counts itself in its base cell. Particles whose
 // staged x has its sign bit set (invalid, or listed for the slow pass) are
 // skipped. PC: the plane stride when known at compile time (0: wn.P).
-template <int NF, int NS, bool T0, bool TRACK_ALL, int PC, class CoefFn>
+struct NoHook {
+    template <int NS> __device__ __forceinline__ void operator()(const float (&)[NS]) const {}
+};
+template <int NF, int NS, bool T0, bool TRACK_ALL, int PC, class CoefFn, class Hook = NoHook>
 __device__ __forceinline__ void window_particles(const float* __restrict__ stage, int* __restrict__ win,
-                                                 const Win& wn, const Geo& g, CoefFn coef) {
+                                                 const Win& wn, const Geo& g, CoefFn coef, Hook hook = Hook{}) {
     constexpr bool kBiased = !TRACK_ALL && NF > (T0 ? 1 : 0);
     const int P = PC ? PC : wn.P;
-    const int base = 64 * (threadIdx.x & 31) + 8 * (threadIdx.x >> 5);
     const int oi = win_origin(wn.ir, wn.mi, g.nx), oj = win_origin(wn.jr, wn.mj, g.ny);
 #pragma unroll 1
     for (int k = 0; k < kPPT; ++k) {
-        const int d = stage_slot(base + k);
+        const int d = spread_slot(k);
         float a[NS];
 #pragma unroll
         for (int f = 0; f < NS; ++f) a[f] = stage[f * kChunk + d];
+        hook(a);                                  // every slot, deposited or not
         if (__float_as_int(a[0]) < 0) continue;
         const Cic2 c = cic2(a[0], a[1]);
         float cs[NF];
@@ -778,11 +787,10 @@ template <int NF, int NS, bool T0, bool TRACK_ALL, int PC, class CoefFn>
 __device__ __forceinline__ void window_band(const float* __restrict__ stage, int* __restrict__ win,
                                             const Win& wn, int r0, const Geo& g, CoefFn coef) {
     const int P = PC ? PC : wn.P;
-    const int base = 64 * (threadIdx.x & 31) + 8 * (threadIdx.x >> 5);
     const int oi = win_origin(wn.ir, wn.mi, g.nx), oj = win_origin(wn.jr, wn.mj, g.ny);
 #pragma unroll 1
     for (int k = 0; k < kPPT; ++k) {
-        const int d = stage_slot(base + k);
+        const int d = spread_slot(k);
         const float x = stage[d];
         if (__float_as_int(x) < 0) continue;
         const float y = stage[kChunk + d];

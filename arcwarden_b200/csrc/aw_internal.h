@@ -131,6 +131,9 @@ struct Ctx {
     void* rs_temp = nullptr; size_t rs_temp_bytes = 0;
     int resort_every = 0;             // aw_run re-sorts before every step n with n % resort_every == 0
     int resort_tile = kChunk / 2;     // particles per re-sort tile (the ensemble autotuner sets it)
+    // Kernel choices of the particle kernels (aw_set_kernel_plan / aw_tune_kernels;
+    // -1 or 0: the built-in choice). None of them changes a result bit.
+    aw_kernel_plan plan{-1, -1, 0};
     // scales for unfused deposits
     bool have_static_scales = false;
 

@@ -115,6 +115,16 @@ typedef struct aw_diag {
     double eb;        /* 1/2 sum (Bx^2 + By^2 + Bz^2) dx dy  (Darwin)          */
 } aw_diag;
 
+/* Kernel choices of the particle kernels of one context. Every choice gives
+ * the same bits (the deposits are exact and order-free); they only change the
+ * speed. -1 (or 0 for es_window) selects the built-in choice. */
+typedef struct aw_kernel_plan {
+    int32_t one_pass;   /* Darwin push and dcu kernels: push and deposit in one pass over a
+                           chunk whose window fits (1), or always in two passes (0)        */
+    int32_t tile;       /* two-pass Darwin kernels stage a gather tile of the chunk (1/0) */
+    int32_t es_window;  /* electrostatic push: rho window capacity in cells (> 0)         */
+} aw_kernel_plan;
+
 /* Counters the fused kernels keep (read by aw_stats; a host sync). */
 typedef struct aw_stats_t {
     int64_t chunks;           /* particle chunks processed by window kernels   */
@@ -122,6 +132,7 @@ typedef struct aw_stats_t {
     int64_t slow_deposits;    /* contributions that took the exact slow path   */
     int64_t steps;            /* fused steps taken                             */
     int64_t kernels_per_step; /* this library's kernels in one fused step      */
+    int64_t one_pass_chunks;  /* chunks pushed/deposited in a single pass      */
 } aw_stats_t;
 
 typedef struct aw_ctx aw_ctx;
@@ -214,6 +225,13 @@ int aw_resort(aw_ctx* ctx);
  * particles by tile), 0 for the electrostatic model, whose reference path keeps
  * the particle order. */
 int aw_set_resort(aw_ctx* ctx, int32_t every);
+/* The context's kernel choices (see aw_kernel_plan). No counterpart in the
+ * reference, whose kernels take their tile sizes from compile-time policies
+ * (include/pic/config.hpp:61-66) and a fixed blocks-per-tile heuristic
+ * (depositor.hpp:354-360). Setting a different plan drops the captured step
+ * graph; results do not change. */
+int aw_set_kernel_plan(aw_ctx* ctx, const aw_kernel_plan* plan);
+int aw_get_kernel_plan(aw_ctx* ctx, aw_kernel_plan* plan);
 /* Yee contexts: `passes` (0-4) passes of the binomial current filter
  * [1,2,1] x [1,2,1] / 16 per step (RunParams::jfilter, k_binomial3x3,
  * include/pic/yee2d.hpp:471-487, simulation_maxwell.hpp:78-92), applied exactly

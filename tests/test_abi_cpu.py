@@ -63,7 +63,8 @@ def test_struct_layouts_match_header(aw):
     assert C.sizeof(aw.Diag) == 64
     assert C.sizeof(aw.SourcePtrs) == 11 * 8
     assert C.sizeof(aw.FieldPtrs) == 11 * 8
-    assert C.sizeof(aw.Stats) == 40
+    assert C.sizeof(aw.Stats) == 48
+    assert C.sizeof(aw.KernelPlan) == 12
 
 
 def test_product_does_not_import_the_oracle():
