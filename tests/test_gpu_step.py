@@ -248,8 +248,9 @@ def test_kernel_plans_give_identical_bits(setup, aw, ppc, B0, pump):
     diagnostics bit for bit over six graph-launched steps: the deposits are exact
     and order-free, and the per-thread partial sums (kinetic energy, momentum,
     the coefficient rms behind the deposit scales) cover the same particles in
-    the same order on both paths. At 16 particles per cell the chunks' windows do
-    not fit the single pass, which then falls back to two passes."""
+    the same order on both paths. At 16 particles per cell a chunk is two grid
+    rows: the push's window (with its motion margin) does not fit the single
+    pass and falls back to two passes, while the dcu deposit's window does fit."""
     nx, L = 64, 32.0
     sp = [dict(ppc=ppc, density=1.0, uth=(0.05, 0.05, 0.2), ufl=(0.0, 0.0, 0.0))]
     kw = dict(dt=0.05, B0=B0)
@@ -272,10 +273,7 @@ def test_kernel_plans_give_identical_bits(setup, aw, ppc, B0, pump):
         r["one_pass_chunks"] = st["one_pass_chunks"]
         assert s.ctx.error_word() == 0
         out.append(r)
-    if ppc >= 64:
-        assert out[2]["one_pass_chunks"] > 0 and out[0]["one_pass_chunks"] == 0
-    else:
-        assert out[2]["one_pass_chunks"] == 0      # the windows of 128 cells in a row do not fit
+    assert out[2]["one_pass_chunks"] > 0 and out[0]["one_pass_chunks"] == 0
     for r in out[1:]:
         assert r["diag"] == out[0]["diag"]
         for k in out[0]:
