@@ -535,6 +535,7 @@ __device__ __forceinline__ bool one_pass_window(Win& w, const Box& b, int ir, in
     w.Hb = w.H; w.nb = 1;
     w.WH = w.W * w.H;
     w.P = P1;
+    w.rep = w.WH * 4 <= P1 ? 4 : (w.WH * 2 <= P1 ? 2 : 1);
     w.use = true;
     w.track_all = false;
     w.biased = NF > (T0 ? 1 : 0);
@@ -623,7 +624,7 @@ __device__ __forceinline__ void one_pass_deposit(int* __restrict__ win, const Wi
     const Cic2 c2 = cic2(x, y);
     int b[NF][4];
     quant_bits<NF>(cs, c2, b);
-    int* e0 = win + dj * w.W + di;
+    int* e0 = win + (threadIdx.x & (w.rep - 1)) * w.WH + dj * w.W + di;   // this lane's copy
     int* e2 = e0 + w.W;
     if (NF > (T0 ? 1 : 0)) atomicAdd(e0 + 2 * NF * P1, 1);
 #pragma unroll

@@ -344,8 +344,11 @@ struct Win {
     int mi, mj;      // min wrapped offsets
     int W, H;        // extent in cells (incl. the +1 corner)
     int Hb, nb;      // rows per band, bands
-    int WH;          // W * Hb: the cells of one plane in use
+    int WH;          // W * Hb: the cells of one plane in use (one copy)
     int P;           // plane stride (the capacity in cells)
+    int rep;         // copies of the window in each plane: lane l adds to copy l mod rep
+                     // (dense chunks, whose neighbouring lanes share cells); the
+                     // flush sums them
     bool use;        // deposited in the shared window (in one or more bands)
     bool track_all;  // some field's chunk sums may leave int32: track every field
     bool biased;     // the untracked fields add biased words (one band)
@@ -406,6 +409,7 @@ __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, 
     w.W = hi_i - lo_i + 2;
     w.H = hi_j - lo_j + 2;
     w.P = wmaxc;
+    w.rep = 1;
     if (static_cast<long long>(w.W) * w.H <= wmaxc) {
         w.Hb = w.H;
         w.nb = 1;
@@ -435,7 +439,8 @@ template <int NF, bool T0, int PC = 0>
 __device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
     const int P = PC ? PC : w.P;
     const bool ta = w.track_all, bi = w.biased;
-    for (int c = threadIdx.x; c < w.WH; c += kThreads) {
+    const int used = w.WH * w.rep;
+    for (int c = threadIdx.x; c < used; c += kThreads) {
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
             s[f * P + c] = 0;
@@ -468,26 +473,35 @@ __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& 
         if (gi >= g.nx) gi -= g.nx;
         if (gj >= g.ny) gj -= g.ny;
         unsigned long long* a = acc + (static_cast<size_t>(gj) * g.nx + gi);
+        const int WHc = w.WH, R = w.rep;
         unsigned nM = 0;
         if (win_planes(NF) > 2 * NF && bi) {
-            const int* cn = s + 2 * NF * P;
-            int n = cn[c];
-            if (wi > 0) n += cn[c - 1];
-            if (wj > 0) {
-                n += cn[c - w.W];
-                if (wi > 0) n += cn[c - w.W - 1];
+            int n = 0;
+            for (int r = 0; r < R; ++r) {
+                const int* cn = s + 2 * NF * P + r * WHc;
+                n += cn[c];
+                if (wi > 0) n += cn[c - 1];
+                if (wj > 0) {
+                    n += cn[c - w.W];
+                    if (wi > 0) n += cn[c - w.W - 1];
+                }
             }
             nM = static_cast<unsigned>(n) * kMagicU;
         }
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
-            long long v;
-            if (ta || (T0 && f == 0))
-                v = static_cast<long long>(s[f * P + c]) + static_cast<long long>(s[(NF + f) * P + c]) * 4294967296ll;
-            else if (bi)
-                v = static_cast<int>(static_cast<unsigned>(s[f * P + c]) - nM);
-            else
-                v = s[f * P + c];
+            long long v = 0;
+            if (ta || (T0 && f == 0)) {
+                for (int r = 0; r < R; ++r)
+                    v += static_cast<long long>(s[f * P + r * WHc + c])
+                         + static_cast<long long>(s[(NF + f) * P + r * WHc + c]) * 4294967296ll;
+            } else if (bi) {
+                unsigned u = 0;
+                for (int r = 0; r < R; ++r) u += static_cast<unsigned>(s[f * P + r * WHc + c]);
+                v = static_cast<int>(u - nM);      // the copies' true sums add up to the chunk's, < 2^31
+            } else {
+                for (int r = 0; r < R; ++r) v += s[f * P + r * WHc + c];
+            }
             if (v != 0) atomicAdd(a + static_cast<size_t>(f) * g.ncell, static_cast<unsigned long long>(v));
         }
     }
