@@ -774,7 +774,8 @@ __device__ __forceinline__ void window_particles(const float* __restrict__ stage
         coef(a, cs);
         int b[NF][4];
         quant_bits<NF>(cs, c, b);
-        int* e0 = win + win_col(c.j0, oj, g.ny) * wn.W + win_col(c.i0, oi, g.nx);   // corners 0, 1
+        int* e0 = win + (threadIdx.x & (wn.rep - 1)) * wn.WH                       // this lane's copy
+                  + win_col(c.j0, oj, g.ny) * wn.W + win_col(c.i0, oi, g.nx);         // corners 0, 1
         int* e2 = e0 + wn.W;                                                          // corners 2, 3
         if (kBiased) atomicAdd(e0 + 2 * NF * P, 1);
 #pragma unroll
