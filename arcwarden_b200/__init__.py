@@ -96,6 +96,7 @@ SIGNATURES = {
     "aw_set_stream": [_P, _P],
     "aw_set_params": [_P, C.POINTER(Params)],
     "aw_set_kernel_plan": [_P, C.POINTER(KernelPlan)],
+    "aw_debug_wait": [_P, C.c_uint32, C.c_uint32],
     "aw_get_kernel_plan": [_P, C.POINTER(KernelPlan)],
     "aw_particles_bind": [_P, _P, _P, _P, _P, _P, _P, _P, _I64],
     "aw_sources_bind": [_P, C.POINTER(SourcePtrs)],
@@ -256,6 +257,10 @@ class Context:
     def set_resort(self, every: int):
         """Re-sort inside run() before every step n with n % every == 0 (0 = never)."""
         _check(self.lib.aw_set_resort(self.h, int(every)))
+
+    def debug_wait(self, extra_bytes: int = 0, poll_limit: int = 0):
+        """Make every chunk load's bounded wait run out (extra_bytes > 0) after poll_limit polls."""
+        _check(self.lib.aw_debug_wait(self.h, int(extra_bytes), int(poll_limit)))
 
     def set_kernel_plan(self, one_pass: int = -1, tile: int = -1, es_window: int = 0):
         """The particle kernels' choices (-1 / 0: built in); results never change."""

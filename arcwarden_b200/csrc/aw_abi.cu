@@ -1144,6 +1144,18 @@ int aw_error_word(aw_ctx* ctx, uint32_t* out) {
     });
 }
 
+int aw_debug_wait(aw_ctx* ctx, uint32_t extra_bytes, uint32_t poll_limit) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::need(extra_bytes % 16 == 0 && extra_bytes <= 4096, AW_ERR_ARG,
+                 "debug_wait: extra_bytes is a multiple of 16, at most 4096");
+        Ctx& c = ctx->c;
+        const unsigned v[2] = {poll_limit, extra_bytes};
+        AW_CUDA(cudaMemcpyAsync(&c.st->wait_polls, v, sizeof(v), cudaMemcpyHostToDevice, c.stream));
+        AW_CUDA(cudaStreamSynchronize(c.stream));
+    });
+}
+
 int aw_stats(aw_ctx* ctx, aw_stats_t* out) {
     return guarded([&] {
         aw::need(ctx && out, AW_ERR_ARG, "null argument");

@@ -81,6 +81,9 @@ struct DevState {
     unsigned long long chunks, overflow, slow;
     unsigned  red_ticket;      // k_step_reduce blocks finished (reset by the last)
     unsigned long long one_pass;   // chunks taken by the single-pass path
+    unsigned  wait_polls;      // polls before a bounded device wait gives up (0: kWaitLimit)
+    unsigned  dbg_extra_tx;    // bytes a chunk load's mbarrier expects beyond those issued
+                               // (aw_debug_wait: makes every load's wait run out; 0 in use)
     double    rho_ref;         // mean charge density, subtracted from the fused solve's
                                // FFT input (the k = 0 mode is zeroed anyway): a large
                                // mean would otherwise put FP32 roundoff into every mode
@@ -587,9 +590,10 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
                  : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
     return ok != 0;
 }
-constexpr int kWaitLimit = 1 << 22;    // try_wait rounds before a wait gives up
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (int k = 0; k < kWaitLimit; ++k)
+constexpr unsigned kWaitLimit = 1u << 22;    // try_wait rounds before a wait gives up
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  unsigned limit = kWaitLimit) {
+    for (unsigned k = 0; k < limit; ++k)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -601,14 +605,15 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
 // (block-uniformly) when the wait gave up; the copies in flight are then given
 // a second bounded wait before the caller returns.
 __device__ __forceinline__ bool mbar_wait_block(unsigned long long* bar, DevState* st) {
+    const unsigned lim = st->wait_polls ? st->wait_polls : kWaitLimit;
     bool ok = true;
-    if (threadIdx.x < 32) ok = mbar_wait_bounded(bar, 0u);
+    if (threadIdx.x < 32) ok = mbar_wait_bounded(bar, 0u, lim);
     if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) set_err(st, 4u);     // AW_DEV_WAIT_LIMIT
-        mbar_wait_bounded(bar, 0u);                // let copies in flight land
+        mbar_wait_bounded(bar, 0u, lim);           // let copies in flight land
         return false;
     }
-    mbar_wait_bounded(bar, 0u);                    // completed: returns at the first try
+    mbar_wait_bounded(bar, 0u, lim);               // completed: returns at the first try
     return true;
 }
 
@@ -632,7 +637,7 @@ __device__ __forceinline__ bool load_chunk(float* stage, const ChunkSrc& src, in
     const int nbulk = vec ? (cnt & ~3) : 0;
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
-        mbar_arrive_expect_tx(bar, static_cast<unsigned>(np * nbulk) * 4u);
+        mbar_arrive_expect_tx(bar, static_cast<unsigned>(np * nbulk) * 4u + st->dbg_extra_tx);
         if (nbulk > 0)
             for (int k = 0; k < np; ++k)
                 bulk_load(stage + k * kChunk, src.at(k) + c0, static_cast<unsigned>(nbulk) * 4u, bar);

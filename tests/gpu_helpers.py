@@ -27,7 +27,7 @@ class Setup:
 
     def __init__(self, torch, aw, nx, ny, Lx, Ly, n, model, **kw):
         self.torch = torch
-        self.dev = torch.device("cuda:0")
+        self.dev = torch.device("cuda", torch.cuda.current_device())
         self.nx, self.ny, self.Lx, self.Ly, self.n = nx, ny, Lx, Ly, n
         self.ctx = aw.Context(nx, ny, Lx, Ly, model=model, stream=torch.cuda.current_stream().cuda_stream, **kw)
         f32 = dict(dtype=torch.float32, device=self.dev)

@@ -523,3 +523,48 @@ def test_deposit_bit_exact_in_window_bands(setup, aw, oracle, op, fset, keys, ro
     fin = oracle.finalize(oracle.deposit(g, *(p[k] for k in PARTICLE_KEYS[:5]), p["w"], -1.0, S, fset), S)
     for i, k in enumerate(keys):
         assert np.array_equal(s.grid(k), fin[i]), k
+
+
+@pytest.mark.parametrize("model", [0, 1])
+def test_bounded_wait_gives_up_and_recovers(torch_cuda, aw, model):
+    """The chunk loads' bounded mbarrier waits: with aw_debug_wait every load's
+    barrier expects 16 bytes more than its copies deliver, so no wait can
+    complete; after 256 polls the kernels set AW_DEV_WAIT_LIMIT and return (no
+    hang, no fault: the copies themselves all land). With the option off, the
+    next step runs clean on the same context."""
+    sp = TWO_STREAM if model == aw.AW_MODEL_ES else WEIBEL
+    s = Setup(torch_cuda, aw, 8, 8, 8.0, 8.0, n_particles(sp, 8, 8), model, dt=0.05)
+    try:
+        s.ctx.load_species(sp, seed=5, noisy=True)
+        s.ctx.init()
+        assert s.ctx.error_word() == 0
+        s.ctx.debug_wait(16, 256)
+        s.ctx.step(0)                                   # returns: every wait gave up
+        assert s.ctx.error_word() & aw.AW_DEV_WAIT_LIMIT
+        s.ctx.debug_wait(0, 0)
+        s.ctx.step(1)
+        assert s.ctx.error_word() == 0
+        assert np.isfinite(s.grid("Ex")).all()
+    finally:
+        s.close()
+
+
+def test_contexts_on_every_device_launch_the_large_shared_memory_kernels(torch_cuda, aw):
+    """The dynamic shared-memory opt-in of the >48 KB particle kernels is made
+    per device: a Darwin context on each visible device (and two on device 0)
+    runs its fused steps without a launch error."""
+    made = []
+    try:
+        for dev in list(range(torch_cuda.cuda.device_count())) + [0]:
+            with torch_cuda.cuda.device(dev):
+                s = Setup(torch_cuda, aw, 32, 32, 16.0, 16.0, n_particles(WEIBEL, 32, 32), aw.AW_MODEL_DARWIN,
+                          dt=0.05)
+                made.append(s)
+                s.ctx.load_species(WEIBEL, seed=dev, noisy=True)
+                s.ctx.init()
+                s.ctx.run(0, 2, graph=False)
+                torch_cuda.cuda.synchronize(dev)
+                assert s.ctx.error_word() == 0
+    finally:
+        for s in made:
+            s.close()
