@@ -125,14 +125,6 @@ typedef struct aw_kernel_plan {
     int32_t es_window;  /* electrostatic push: rho window capacity in cells (> 0)         */
 } aw_kernel_plan;
 
-/* Failure-path check of the bounded device waits (no counterpart in the
- * reference). From now on every particle chunk load's mbarrier expects
- * `extra_bytes` more than the copies deliver, so its phase never completes, and
- * every bounded wait gives up after `poll_limit` polls (0: the built-in limit of
- * 2^22): the kernels set AW_DEV_WAIT_LIMIT, leave the chunk untouched and
- * return; nothing hangs and the context stays usable. aw_debug_wait(ctx, 0, 0)
- * restores normal operation. A debugging aid for tests; never on in a run. */
-int aw_debug_wait(aw_ctx* ctx, uint32_t extra_bytes, uint32_t poll_limit);
 
 /* Counters the fused kernels keep (read by aw_stats; a host sync). */
 typedef struct aw_stats_t {
@@ -234,6 +226,14 @@ int aw_resort(aw_ctx* ctx);
  * particles by tile), 0 for the electrostatic model, whose reference path keeps
  * the particle order. */
 int aw_set_resort(aw_ctx* ctx, int32_t every);
+/* Failure-path check of the bounded device waits (no counterpart in the
+ * reference). From now on every particle chunk load's mbarrier expects
+ * `extra_bytes` more than the copies deliver, so its phase never completes, and
+ * every bounded wait gives up after `poll_limit` polls (0: the built-in limit of
+ * 2^22): the kernels set AW_DEV_WAIT_LIMIT, leave the chunk untouched and
+ * return; nothing hangs and the context stays usable. aw_debug_wait(ctx, 0, 0)
+ * restores normal operation. A debugging aid for tests; never on in a run. */
+int aw_debug_wait(aw_ctx* ctx, uint32_t extra_bytes, uint32_t poll_limit);
 /* The context's kernel choices (see aw_kernel_plan). No counterpart in the
  * reference, whose kernels take their tile sizes from compile-time policies
  * (include/pic/config.hpp:61-66) and a fixed blocks-per-tile heuristic
