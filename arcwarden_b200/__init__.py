@@ -97,6 +97,7 @@ SIGNATURES = {
     "aw_set_params": [_P, C.POINTER(Params)],
     "aw_set_kernel_plan": [_P, C.POINTER(KernelPlan)],
     "aw_debug_wait": [_P, C.c_uint32, C.c_uint32],
+    "aw_tune_kernels": [_P, _I32, C.POINTER(KernelPlan)],
     "aw_get_kernel_plan": [_P, C.POINTER(KernelPlan)],
     "aw_particles_bind": [_P, _P, _P, _P, _P, _P, _P, _P, _I64],
     "aw_sources_bind": [_P, C.POINTER(SourcePtrs)],
@@ -265,6 +266,13 @@ class Context:
     def set_kernel_plan(self, one_pass: int = -1, tile: int = -1, es_window: int = 0):
         """The particle kernels' choices (-1 / 0: built in); results never change."""
         _check(self.lib.aw_set_kernel_plan(self.h, C.byref(KernelPlan(one_pass, tile, es_window))))
+
+    def tune_kernels(self, trial_steps: int = 8) -> dict:
+        """Time every kernel plan from the loaded initial state and keep the fastest
+        (aw_tune_kernels); leaves the context initialised."""
+        k = KernelPlan()
+        _check(self.lib.aw_tune_kernels(self.h, int(trial_steps), C.byref(k)))
+        return {"one_pass": k.one_pass, "tile": k.tile, "es_window": k.es_window}
 
     def kernel_plan(self) -> dict:
         k = KernelPlan()

@@ -1049,6 +1049,95 @@ int aw_get_kernel_plan(aw_ctx* ctx, aw_kernel_plan* plan) {
     });
 }
 
+namespace {
+// Tuned plans of this process, keyed by the run class (device, model, grid,
+// particle count): later contexts of the same class take the plan without trials.
+struct TuneKey {
+    int dev, model, nx, ny;
+    long long n;
+    bool operator==(const TuneKey& o) const {
+        return dev == o.dev && model == o.model && nx == o.nx && ny == o.ny && n == o.n;
+    }
+};
+std::mutex g_tune_mu;
+std::vector<std::pair<TuneKey, aw_kernel_plan>> g_tuned;
+// A failing entry point's status, rethrown with its message.
+void check_status(int rc) {
+    if (rc != AW_OK) throw aw::Error(rc, aw::g_last_error);
+}
+}  // namespace
+
+int aw_tune_kernels(aw_ctx* ctx, int32_t trial_steps, aw_kernel_plan* chosen) {
+    return guarded([&] {
+        aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");
+        aw::need(trial_steps >= 1 && trial_steps <= 1000, AW_ERR_ARG, "tune_kernels: trial_steps in 1..1000");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        aw::need(c.parts.x != nullptr && c.parts.w != nullptr, AW_ERR_STATE, "tune_kernels: particles not bound");
+        TuneKey key{0, c.model, c.geo.nx, c.geo.ny, c.parts.n};
+        AW_CUDA(cudaGetDevice(&key.dev));
+        std::vector<aw_kernel_plan> cands;
+        if (c.model == AW_MODEL_DARWIN)
+            cands = {{0, 0, 0}, {0, 1, 0}, {1, 0, 0}, {1, 1, 0}};
+        else if (c.model == AW_MODEL_ES)
+            cands = {{-1, -1, 1024}, {-1, -1, 2048}, {-1, -1, 3584}};
+        aw_kernel_plan best = c.plan;
+        bool cached = false;
+        {
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            for (const auto& e : g_tuned)
+                if (e.first == key) { best = e.second; cached = true; }
+        }
+        if (!cached && cands.size() > 1) {
+            // every trial starts from the caller's particles, restored from a snapshot
+            const size_t nb = sizeof(float) * static_cast<size_t>(c.parts.n);
+            float* snap = nullptr;
+            AW_CUDA(cudaMalloc(&snap, 6 * nb));
+            float* arr[6] = {c.parts.x, c.parts.y, c.parts.ux, c.parts.uy, c.parts.uz, c.parts.w};
+            auto copy = [&](bool save) {
+                for (int k = 0; k < 6; ++k)
+                    AW_CUDA(cudaMemcpyAsync(save ? snap + k * c.parts.n : arr[k], save ? arr[k] : snap + k * c.parts.n,
+                                            nb, cudaMemcpyDeviceToDevice, c.stream));
+            };
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            float bestms = 3.0e38f;
+            try {
+                copy(true);
+                AW_CUDA(cudaEventCreate(&e0));
+                AW_CUDA(cudaEventCreate(&e1));
+                for (const aw_kernel_plan& pl : cands) {
+                    copy(false);
+                    c.plan = pl;
+                    aw::init_impl(c);                    // drops the graph; synchronises
+                    check_status(aw_run(ctx, 0, 2, 1));    // capture + warm-up
+                    AW_CUDA(cudaEventRecord(e0, c.stream));
+                    check_status(aw_run(ctx, 2, trial_steps, 1));
+                    AW_CUDA(cudaEventRecord(e1, c.stream));
+                    AW_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    AW_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    if (ms < bestms) { bestms = ms; best = pl; }
+                }
+                copy(false);
+                AW_CUDA(cudaStreamSynchronize(c.stream));
+            } catch (...) {
+                if (e0) cudaEventDestroy(e0);
+                if (e1) cudaEventDestroy(e1);
+                cudaFree(snap);
+                throw;
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            cudaFree(snap);
+            std::lock_guard<std::mutex> lock(g_tune_mu);
+            g_tuned.push_back({key, best});
+        }
+        c.plan = best;
+        aw::init_impl(c);      // the caller's initial state, initialised as by aw_init
+        if (chosen) *chosen = best;
+    });
+}
+
 int aw_resort(aw_ctx* ctx) {
     return guarded([&] {
         aw::need(ctx != nullptr, AW_ERR_ARG, "null ctx");

@@ -307,7 +307,10 @@ def run_ours(args, wl, rank, world, dist):
     ctx.load_species(wl["species"], seed=seed, noisy=True)
     if wl["model"] == aw.AW_MODEL_YEE:
         ctx.set_current_filter(wl.get("jfilter", 0))
-    ctx.init()
+    # the kernel plan: trial runs of each candidate from this initial state (leaves it initialised)
+    t_tune = time.perf_counter()
+    plan = ctx.tune_kernels(8)
+    t_tune = time.perf_counter() - t_tune
 
     def barrier():
         if dist is not None:
@@ -390,6 +393,7 @@ def run_ours(args, wl, rank, world, dist):
         "data": f"synthetic: reference seeded loader streams (noisy load, seed {seed})",
         "config": bench_config(wl, n, world),
         "step": "one fused PIC step, replayed from a captured CUDA graph",
+        "kernel_plan": dict(plan, tuning_s=round(t_tune, 3)),
         "e2e": {"value": world * n * K / e2e_s, "unit": "particles/s",
                 "h2d_bytes_per_step": round(24 * n / K), "d2h_bytes_per_step": round(20 * n / K + 64),
                 "run": f"{K} steps: H2D of the particle state, aw_init, aw_run_diag (per-step FP64 diagnostics to "

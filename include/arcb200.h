@@ -241,6 +241,17 @@ int aw_debug_wait(aw_ctx* ctx, uint32_t extra_bytes, uint32_t poll_limit);
  * graph; results do not change. */
 int aw_set_kernel_plan(aw_ctx* ctx, const aw_kernel_plan* plan);
 int aw_get_kernel_plan(aw_ctx* ctx, aw_kernel_plan* plan);
+/* Kernel-plan autotuner (no counterpart in the reference, which sizes its tiles
+ * with a fixed heuristic, include/pic/depositor.hpp:354-360 and
+ * config.hpp:61-66). Call it with the particles bound and loaded, before
+ * aw_init: every candidate plan (Darwin: single/two-pass x gather tile;
+ * electrostatic: the rho window) runs init, 2 warm-up steps and `trial_steps`
+ * timed steps from the same initial state; the fastest is set (and written to
+ * *chosen when not NULL). The particles are restored and the context is left
+ * initialised, as after aw_init. Plans are cached for the process per (device,
+ * model, grid, particle count): a later context of the same class takes the
+ * cached plan without trials. Results never depend on the plan. Synchronises. */
+int aw_tune_kernels(aw_ctx* ctx, int32_t trial_steps, aw_kernel_plan* chosen);
 /* Yee contexts: `passes` (0-4) passes of the binomial current filter
  * [1,2,1] x [1,2,1] / 16 per step (RunParams::jfilter, k_binomial3x3,
  * include/pic/yee2d.hpp:471-487, simulation_maxwell.hpp:78-92), applied exactly

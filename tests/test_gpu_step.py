@@ -280,3 +280,38 @@ def test_kernel_plans_give_identical_bits(setup, aw, ppc, B0, pump):
             if k in ("diag", "one_pass_chunks"):
                 continue
             assert np.array_equal(r[k], out[0][k]), k
+
+
+@pytest.mark.parametrize("model", [0, 1])
+def test_tuned_kernel_plan_keeps_results(setup, aw, model):
+    """aw_tune_kernels: trial runs of every candidate plan from the loaded state,
+    the fastest kept, the particles restored and the context initialised. A run
+    after tuning equals a run with the built-in plan bit for bit; a second
+    context of the same class takes the cached plan."""
+    sp = [dict(ppc=64, density=1.0, uth=(0.05, 0.05, 0.2), ufl=(0.0, 0.0, 0.0))] if model else TWO_STREAM
+    nx, L = 64, 32.0
+    out = []
+    for tune in (True, False, True):
+        s = setup(nx, nx, L, L, n_particles(sp, nx, nx), model, dt=0.05)
+        s.ctx.load_species(sp, seed=7, noisy=True)
+        if tune:
+            plan = s.ctx.tune_kernels(3)
+            assert plan == s.ctx.kernel_plan()
+            if model == aw.AW_MODEL_DARWIN:
+                assert plan["one_pass"] in (0, 1) and plan["tile"] in (0, 1)
+            else:
+                assert plan["es_window"] in (1024, 2048, 3584)
+        else:
+            s.ctx.init()
+        s.ctx.run(0, 5, graph=True)
+        r = s.parts()
+        r["Ex"], r["rho"] = s.grid("Ex"), s.grid("rho")
+        r["diag"] = s.ctx.step_diag()
+        r["plan"] = s.ctx.kernel_plan()
+        assert s.ctx.error_word() == 0
+        out.append(r)
+    assert out[2]["plan"] == out[0]["plan"]
+    for r in out[1:]:
+        assert r["diag"] == out[0]["diag"]
+        for k in PARTICLE_KEYS + ("Ex", "rho"):
+            assert np.array_equal(r[k], out[0][k]), k
