@@ -98,6 +98,7 @@ SIGNATURES = {
     "aw_set_kernel_plan": [_P, C.POINTER(KernelPlan)],
     "aw_debug_wait": [_P, C.c_uint32, C.c_uint32],
     "aw_tune_kernels": [_P, _I32, C.POINTER(KernelPlan)],
+    "aw_grad_darwin": [_P, _I64, _I32, _P, _P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)],
     "aw_get_kernel_plan": [_P, C.POINTER(KernelPlan)],
     "aw_particles_bind": [_P, _P, _P, _P, _P, _P, _P, _P, _I64],
     "aw_sources_bind": [_P, C.POINTER(SourcePtrs)],
@@ -316,6 +317,14 @@ class Context:
         _check(self.lib.aw_grad_es(self.h, int(nsteps), int(checkpoint_every), _ptr(dux), _ptr(duy), _ptr(duz),
                                    C.byref(loss)))
         return loss.value
+
+    def grad_darwin(self, nsteps: int, checkpoint_every: int, dux, duy, duz):
+        """(loss, d loss / d pump amplitude) with d loss / d u0 written into dux,
+        duy, duz (aw_grad_darwin)."""
+        loss, dp = C.c_double(), C.c_double()
+        _check(self.lib.aw_grad_darwin(self.h, int(nsteps), int(checkpoint_every), _ptr(dux), _ptr(duy), _ptr(duz),
+                                       C.byref(dp), C.byref(loss)))
+        return loss.value, dp.value
 
     def tile_bins(self):
         off, idx, nt, ntx = C.c_void_p(), C.c_void_p(), C.c_int32(), C.c_int32()

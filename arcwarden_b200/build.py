@@ -18,7 +18,7 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libarcb200.so"
-SOURCES = ["aw_abi.cu", "aw_particles.cu", "aw_deposit.cu", "aw_spectral.cu", "aw_noalloc.cu", "aw_resort.cu", "aw_adjoint.cu", "aw_ensemble.cu", "aw_checkpoint.cu"]
+SOURCES = ["aw_abi.cu", "aw_particles.cu", "aw_deposit.cu", "aw_spectral.cu", "aw_noalloc.cu", "aw_resort.cu", "aw_adjoint.cu", "aw_adjoint_darwin.cu", "aw_ensemble.cu", "aw_checkpoint.cu"]
 HEADERS = ["aw_device.cuh", "aw_internal.h"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -302,6 +302,16 @@ cudaGraphExec_t capture_exec(Ctx& c, F body) {
     return e;
 }
 
+}  // namespace
+// aw_init's sequence and one fused step (graph launch) for the Darwin adjoint.
+void init_impl_for_adjoint(Ctx& c) { init_impl(c); }
+void run_step_for_adjoint(Ctx& c) {
+    if (!c.gexec) c.gexec = capture_exec(c, [&] { step_body(c); });
+    AW_CUDA(cudaGraphLaunch(c.gexec, c.stream));
+}
+double grad_darwin_impl(Ctx& c, long long nsteps, int every, float* dux, float* duy, float* duz, double* dpump);
+namespace {
+
 // Forward run with checkpoints, then the backward sweep segment by segment
 // (recompute the segment from its checkpoint, then transpose its steps in
 // reverse). A checkpoint holds the particle state, the pending rho accumulator
@@ -946,6 +956,19 @@ int aw_grad_es(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux
         aw::need(nsteps >= 1 && checkpoint_every >= 1, AW_ERR_ARG, "grad_es: nsteps and checkpoint_every >= 1");
         aw::need(c.prm.pump == 0, AW_ERR_ARG, "grad_es: no pump in the ES step");
         *loss = aw::grad_es_impl(c, nsteps, checkpoint_every, dux, duy, duz);
+    });
+}
+
+int aw_grad_darwin(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux, float* duy, float* duz,
+                   double* dpump, double* loss) {
+    return guarded([&] {
+        aw::need(ctx && dux && duy && duz && dpump && loss, AW_ERR_ARG, "null argument");
+        Ctx& c = ctx->c;
+        aw::require_parts(c);
+        aw::need(c.model == AW_MODEL_DARWIN, AW_ERR_STATE, "grad_darwin: Darwin contexts only");
+        aw::need(c.parts.n > 0, AW_ERR_ARG, "grad_darwin: no particles");
+        aw::need(nsteps >= 1 && checkpoint_every >= 1, AW_ERR_ARG, "grad_darwin: nsteps and checkpoint_every >= 1");
+        *loss = aw::grad_darwin_impl(c, nsteps, checkpoint_every, dux, duy, duz, dpump);
     });
 }
 

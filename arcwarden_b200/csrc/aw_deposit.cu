@@ -1536,6 +1536,73 @@ EmArgs em_args(const Ctx& c) {
 }
 bool pow2_geo(const Ctx& c) { return is_pow2(c.geo.dx) && is_pow2(c.geo.dy); }
 
+// ---- exact scatter of per-particle values (the Darwin adjoint's gather transposes)
+// acc[f][cell] += sum_p W(x_p) v_f,p for NF = 6 value planes, in exact int64 fixed
+// point on the window engine: the scale of field f comes from the maximum |v_f|
+// (vmax, float bits, written by the producing kernel) and is stored to Sout
+// (block 0) for the finaliser. Stage: x, y, then the six scaled values.
+constexpr int kScatterNF = 6;
+__global__ void __launch_bounds__(kThreads, 2)
+k_scatter6(const float* __restrict__ xs, const float* __restrict__ ys, const float* __restrict__ vals, long long n,
+           Geo g, const unsigned* __restrict__ vmax, float* __restrict__ Sout,
+           unsigned long long* __restrict__ acc, DevState* st, int vec_ok) {
+    constexpr int NF = kScatterNF, NS = 2 + NF;
+    constexpr bool T0 = false;
+    constexpr int PC = wmax_cells(NF);
+    extern __shared__ __align__(16) unsigned char smem[];
+    const Smem m = carve(smem, NS, win_planes(NF), PC);
+    __shared__ unsigned long long bar;
+    __shared__ int nlist;
+    const long long c0 = static_cast<long long>(blockIdx.x) * kChunk;
+    const int cnt = static_cast<int>(min(static_cast<long long>(kChunk), n - c0));
+    float S[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) S[f] = scale_for_bound(__fmul_rn(__uint_as_float(vmax[f]), 1.0001f));
+    if (blockIdx.x == 0 && threadIdx.x < NF) Sout[threadIdx.x] = S[threadIdx.x];
+    if (threadIdx.x == 0) nlist = 0;
+    const ChunkSrc src{{xs, ys, vals, vals + n, vals + 2 * n, vals + 3 * n, vals + 4 * n}};
+    float x0, y0;
+    // planes 0..6 by bulk copy; the sixth value plane by plain loads below
+    if (!load_chunk(m.stage, src, 7, c0, cnt, vec_ok != 0, &bar, st, &x0, &y0)) return;
+    for (int sl = threadIdx.x; sl < cnt; sl += kThreads) m.stage[7 * kChunk + sl] = vals[5 * n + c0 + sl];
+    __syncthreads();
+    int ir, jr;
+    ref_of(x0, y0, g, ir, jr);
+    BBox bb;
+    float l1[NF] = {};
+#pragma unroll 1
+    for (int it = 0; it < kPPT; ++it) {
+        const int sl = it * kThreads + threadIdx.x;
+        const float x = m.stage[sl], y = m.stage[kChunk + sl];
+        float xsv = -1.0f, cs[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) cs[f] = 0.0f;
+        if (sl < cnt) {
+            if (in_grid(x, y, g)) {
+                float v[NF];
+#pragma unroll
+                for (int f = 0; f < NF; ++f) v[f] = m.stage[(2 + f) * kChunk + sl];
+                bb.add(static_cast<int>(x), static_cast<int>(y), ir, jr, g);
+                const bool fast = scale_fast<NF>(v, S, cs, l1);
+                xsv = __fadd_rn(x, 0.0f);
+                if (!fast) { xsv = -xsv; list_slow(m.slow, &nlist, sl); }
+            } else {
+                set_err(st, AW_DEV_OUT_OF_GRID);
+            }
+        }
+        m.stage[sl] = xsv;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) m.stage[(2 + f) * kChunk + sl] = cs[f];
+    }
+    const Win wn = open_window<NF, T0, PC>(bb, ir, jr, PC, m, l1);
+    auto coef = [&](const float (&a)[NS], float (&c)[NF]) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) c[f] = a[2 + f];
+    };
+    window_pass<NF, NS, T0, PC>(m.stage, m.win, wn, g, coef, acc);
+    close_window<NF, NS, T0, PC>(m, wn, nlist, acc, g, st, coef);
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1551,6 +1618,17 @@ void launch_deposit_src(Ctx& c, int which) {
 }
 
 void prep_adj_scatter() { prep_smem(k_adj_scatter, smem_bytes(2, 4)); }
+
+void launch_scatter6(Ctx& c, cudaStream_t s, const float* xs, const float* ys, const float* vals, long long n,
+                     const unsigned* vmax, float* Sout, unsigned long long* acc, DevState* st) {
+    if (n == 0) return;
+    const size_t sh = smem_bytes(kScatterNF, 2 + kScatterNF);
+    prep_smem(k_scatter6, sh);
+    const int vec = (n % 4 == 0 && (reinterpret_cast<uintptr_t>(xs) & 15) == 0 &&
+                     (reinterpret_cast<uintptr_t>(ys) & 15) == 0 && (reinterpret_cast<uintptr_t>(vals) & 15) == 0) ? 1 : 0;
+    k_scatter6<<<nchunks(n), kThreads, sh, s>>>(xs, ys, vals, n, c.geo, vmax, Sout, acc, st, vec);
+    AW_LAUNCH();
+}
 
 void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE, AdjDev* ad,
                         unsigned long long* acc, DevState* st) {

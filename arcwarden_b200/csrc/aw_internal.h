@@ -264,6 +264,10 @@ void launch_push_esirkepov(Ctx& c);
 void launch_adj_scatter(Ctx& c, const AdjP& a, const AdjK& k, const float* trajE, AdjDev* ad,
                         unsigned long long* acc, DevState* st);
 void prep_adj_scatter();   // its shared-memory opt-in (before any capture)
+// acc[6][ncell] += the exact CIC scatter of the six value planes vals[f * n + p] at
+// the positions (xs, ys); scales from the maxima vmax[6] (float bits), stored to Sout.
+void launch_scatter6(Ctx& c, cudaStream_t s, const float* xs, const float* ys, const float* vals, long long n,
+                     const unsigned* vmax, float* Sout, unsigned long long* acc, DevState* st);
 // Multi-run particle phases (batched ensembles): one launch over the chunks of
 // several runs of one kind. The run table is built once (device copies of each
 // run's kernel arguments); the runs' buffers must stay bound while it lives.

@@ -318,6 +318,19 @@ int aw_tile_bins(aw_ctx* ctx, const int32_t** off, const int32_t** idx,
  * dux/duy/duz (device, n floats each) = dloss/du0. Synchronises. */
 int aw_grad_es(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux, float* duy, float* duz,
                double* loss);
+/* The discrete adjoint of the fused Darwin step (no counterpart in the
+ * reference). With the particles bound holding the initial state:
+ * *loss = 0.5 eps0 dx dy sum (Ex^2 + Ey^2) of the last of `nsteps` steps (the
+ * ee diagnostic of that run), d loss / d(initial ux, uy, uz) into the device
+ * arrays dux, duy, duz (n floats each), and d loss / d a into *dpump, where the
+ * pump field (include/pic/pump.hpp:27-54) is scaled as a (pump_ex, pump_ey,
+ * pump_ez), taken at a = 1. The forward run is kept in checkpoints every
+ * `checkpoint_every` steps and each segment is recomputed for its backward
+ * steps; the transposed scatters are exact fixed point, so the result does not
+ * depend on the interval and repeats bit for bit. The bound particles hold the
+ * initial state again on return. Synchronises. */
+int aw_grad_darwin(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux, float* duy, float* duz,
+                   double* dpump, double* loss);
 
 /* ---- batched ensemble (no counterpart in the reference, which runs one
  * Simulation at a time) -------------------------------------------------------

@@ -122,3 +122,93 @@ def test_grad_rejects_darwin_and_bad_arguments(torch_cuda, aw):
             s.ctx.grad_es(4, 0, d, d, d)
     finally:
         s.close()
+
+
+# ---- the Darwin adjoint (aw_grad_darwin) ------------------------------------------
+DARWIN_PUMP = dict(ex=2e-2, ey=3e-2, ez=-1e-2, k0=2 * np.pi * 2 / 16.0, w0=0.3, trmp=0.2, toff=100.0)
+WEIBEL_SMALL = [dict(ppc=8, density=1.0, uth=(0.05, 0.05, 0.2), ufl=(0.0, 0.0, 0.0))]
+
+
+def _darwin(torch, aw, B0, pump, seed=0):
+    nx, ny, Lx, Ly = 32, 16, 16.0, 8.0
+    s = Setup(torch, aw, nx, ny, Lx, Ly, n_particles(WEIBEL_SMALL, nx, ny), aw.AW_MODEL_DARWIN, dt=0.05, B0=B0,
+              pump=pump)
+    s.ctx.load_species(WEIBEL_SMALL, seed=seed, noisy=True)
+    return s
+
+
+def _grad_darwin(torch, s, nsteps, every):
+    du = [torch.zeros(s.n, dtype=torch.float32, device=s.dev) for _ in range(3)]
+    loss, dpump = s.ctx.grad_darwin(nsteps, every, *du)
+    torch.cuda.synchronize()
+    return loss, dpump, np.stack([d.cpu().numpy().astype(np.float64) for d in du], axis=1)
+
+
+@pytest.mark.parametrize("B0, pump", [((0.0, 0.0, 0.0), None), ((0.3, 0.2, 0.4), DARWIN_PUMP)])
+def test_darwin_grad_matches_fp64_reference(torch_cuda, aw, B0, pump):
+    """aw_grad_darwin against the FP64 Darwin adjoint (oracle/darwin_adjoint64.py,
+    itself checked against FP64 central differences): 32 x 16 cells, 8 ppc,
+    10 steps, with and without B0 and the whistler pump. Bars: the loss within
+    1e-4, the velocity gradient within 2e-3 (relative 2-norm), the pump
+    amplitude gradient within 2e-3; the bound particles restored."""
+    from oracle.darwin_adjoint64 import DarwinCase
+    nsteps = 10
+    s = _darwin(torch_cuda, aw, B0, pump)
+    try:
+        p0 = s.parts()
+        loss, dpump, g = _grad_darwin(torch_cuda, s, nsteps, 4)
+        p1 = s.parts()
+        for k in PARTICLE_KEYS:
+            assert np.array_equal(p0[k], p1[k]), k
+        assert s.ctx.error_word() == 0
+        case = DarwinCase(32, 16, 16.0, 8.0, 0.05, B0=B0, pump=pump)
+        u0 = np.stack([p0["ux"], p0["uy"], p0["uz"]], axis=1).astype(np.float64)
+        L64, g64, dp64 = case.gradient(p0["x"].astype(np.float64), p0["y"].astype(np.float64), u0,
+                                       p0["w"].astype(np.float64), nsteps)
+        rel = np.linalg.norm(g - g64) / np.linalg.norm(g64)
+        print(f"B0={B0} pump={bool(pump)}: loss {loss:.8g} vs {L64:.8g}; |g-g64|/|g64| = {rel:.2e}; "
+              f"dL/da {dpump:.6g} vs {dp64:.6g}")
+        assert abs(loss - L64) <= 1e-4 * abs(L64), (loss, L64)
+        assert rel < 2e-3, rel
+        if pump:
+            assert abs(dpump - dp64) <= 2e-3 * abs(dp64), (dpump, dp64)
+        else:
+            assert dpump == 0.0
+    finally:
+        s.close()
+
+
+def test_darwin_grad_is_bit_identical_across_runs_and_checkpoint_intervals(torch_cuda, aw):
+    s = _darwin(torch_cuda, aw, (0.3, 0.2, 0.4), DARWIN_PUMP, seed=2)
+    try:
+        ref = _grad_darwin(torch_cuda, s, 7, 7)
+        for every in (1, 3, 7):
+            got = _grad_darwin(torch_cuda, s, 7, every)
+            assert got[0] == ref[0] and got[1] == ref[1], every
+            assert np.array_equal(got[2], ref[2]), every
+    finally:
+        s.close()
+
+
+def test_autograd_harness_returns_the_library_gradients(torch_cuda, aw):
+    """arcwarden_b200.autograd.field_energy: loss.backward() hands back the
+    adjoint's velocity and pump-amplitude gradients; a finite difference of the
+    harness's own loss in the amplitude agrees with its gradient."""
+    from arcwarden_b200.autograd import FieldEnergyRun, field_energy
+    torch = torch_cuda
+    s = _darwin(torch, aw, (0.3, 0.2, 0.4), DARWIN_PUMP, seed=4)
+    try:
+        run = FieldEnergyRun(s.ctx, s.P, nsteps=6, checkpoint_every=3, pump=DARWIN_PUMP)
+        u0 = torch.stack([s.P["ux"], s.P["uy"], s.P["uz"]], dim=1).clone().requires_grad_(True)
+        a = torch.tensor(1.0, dtype=torch.float64, device=s.dev, requires_grad=True)
+        loss = field_energy(run, u0, a)
+        loss.backward()
+        _, dp, g = _grad_darwin(torch, s, 6, 3)
+        assert np.array_equal(u0.grad.cpu().numpy().astype(np.float64), g)
+        assert float(a.grad) == dp
+        h = 1e-2
+        lp = float(field_energy(run, u0.detach(), torch.tensor(1 + h, dtype=torch.float64, device=s.dev)))
+        lm = float(field_energy(run, u0.detach(), torch.tensor(1 - h, dtype=torch.float64, device=s.dev)))
+        assert abs((lp - lm) / (2 * h) - dp) <= 2e-2 * abs(dp), ((lp - lm) / (2 * h), dp)
+    finally:
+        s.close()
