@@ -67,6 +67,11 @@ struct Particles {
     DeviceArray<double> wdd;
     int wprec = 0;
 
+    // The stream the particles were last loaded on (an addition to the
+    // reference's members): the deck diagnostics enqueue their device work on
+    // it. nullptr = the legacy default stream.
+    cudaStream_t stream = nullptr;
+
     Particles() = default;
 
     void enable_deltaf(cudaStream_t s, int wprec_ = 0) {
@@ -107,6 +112,7 @@ struct Particles {
     // Single-species RunParams load (aw_load_legacy).
     void initialize(const RunParams& rp, const Grid& g, cudaStream_t s) {
         if (n == 0) allocate(g, rp.ppc);
+        stream = s;
         aw_ctx* c = shim::prepare(g, rp, true, s);
         bind(c);
         aw_legacy_load L{};
@@ -126,6 +132,7 @@ struct Particles {
         for (const auto& q : sp) total += static_cast<std::size_t>(q.ppc) * g.real_size();
         if (total == 0) return;
         allocate_n(total);
+        stream = s;
         std::vector<aw_species> a;
         for (const auto& q : sp) {
             aw_species e{};

@@ -1,0 +1,190 @@
+"""The deck diagnostics of the reference's runner (tools/arcsim.cu) on the shim's
+modules (arcwarden_b200/shim/pic/diag: device reductions and histograms, copies
+into pinned buffers, files written by a writer thread), against the reference's
+own runner built from its unchanged headers (_build/ref_arcsim), and the step
+rate with every module enabled against the same deck with none.
+
+The programs are built by `make -C arcwarden_b200/shim all ref` where the
+reference sources are available; a test is skipped when its program is absent.
+"""
+import math
+import re
+import subprocess
+import time
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+BUILD = ROOT / "arcwarden_b200" / "shim" / "_build"
+DECK = ROOT / "arcwarden_b200" / "shim" / "decks" / "whistler_diag_1024x128.ini"
+
+
+def _exe(name):
+    exe = BUILD / name
+    if not exe.exists():
+        pytest.skip(f"{name} not built (make -C arcwarden_b200/shim all ref)")
+    return exe
+
+
+def _deck(tmp_path, name, subs):
+    text = DECK.read_text()
+    for old, new in subs:
+        assert re.search(old, text, flags=re.M), old
+        text = re.sub(old, new, text, flags=re.M)
+    p = tmp_path / name
+    p.write_text(text)
+    return p
+
+
+def _run(exe, deck, outdir, timeout=900):
+    t = time.perf_counter()
+    r = subprocess.run([str(exe), str(deck), str(outdir)], capture_output=True, text=True, timeout=timeout)
+    dt = time.perf_counter() - t
+    assert r.returncode == 0, (r.stdout[-2000:], r.stderr[-2000:])
+    return r.stdout, dt
+
+
+# 64 x 32 cells x 32 per cell = 65,536 particles: under the frames' 100k cap, so a
+# frame holds every particle, whatever order the two runners keep them in. The
+# runner's --nsteps flag ignores 0, so the deck itself says nsteps = 0: the
+# loop samples step 0 only (the snapshot fires there, at the last step).
+SMALL = [(r"^nx = .*$", "nx = 64"), (r"^ny = .*$", "ny = 32"), (r"^Lx = .*$", "Lx = 16.0"),
+         (r"^Ly = .*$", "Ly = 8.0"), (r"^ppc .*$", "ppc     = 32"), (r"^nsteps = .*$", "nsteps = 0")]
+ZERO = [(r"^nsteps = .*$", "nsteps = 0")]
+
+
+def _rows(path):
+    lines = path.read_text().splitlines()
+    return lines[0], sorted(lines[1:])
+
+
+def _floats(line):
+    return [float(v) for v in re.findall(r"[-+]?\d+\.?\d*(?:e[-+]?\d+)?", line)]
+
+
+def test_step0_outputs_match_the_reference_runner(tmp_path):
+    """At step 0 both runners hold the same loaded particles (the library's loader
+    reproduces the reference's) in different orders: every order-independent
+    output is the same bytes (the frame's rows as a multiset, the FP64 snapshot
+    histogram, the metadata), the FP32 video histogram the same counts, and the
+    field outputs agree to FP32 solve accuracy."""
+    ours, ref = _exe("arcsim"), _exe("ref_arcsim")
+    deck = _deck(tmp_path, "small.ini", SMALL)
+    a, b = tmp_path / "a", tmp_path / "b"
+    a.mkdir()
+    b.mkdir()
+    out_a, _ = _run(ours, deck, a)
+    out_b, _ = _run(ref, deck, b)
+
+    # phase frame 0: every particle, same text
+    ha, ra = _rows(a / "frame_0000.csv")
+    hb, rb = _rows(b / "frame_0000.csv")
+    assert ha == hb == "x,vx"
+    assert len(ra) == 64 * 32 * 32
+    assert ra == rb
+    assert (a / "manifest.csv").read_text() == (b / "manifest.csv").read_text()
+
+    # snapshot histogram (FP64 binning of every particle) and metadata
+    pre = "whistler_diag_"
+    fa = np.fromfile(a / (pre + "fhist.bin"), dtype=np.float32)
+    fb = np.fromfile(b / (pre + "fhist.bin"), dtype=np.float32)
+    assert fa.size == fb.size == 512 * 480
+    assert fa.sum() == fb.sum() == 64 * 32 * 32
+    assert np.array_equal(fa, fb), np.count_nonzero(fa != fb)
+    for meta in ("fhist.meta", "vid.meta", "kt.meta"):
+        assert (a / (pre + meta)).read_text() == (b / (pre + meta)).read_text(), meta
+
+    # video histogram (FP32 binning): the same counts; the reference's compiled
+    # kernel may contract v_par's sum into an FMA, which could move a particle
+    # lying within an ulp of a bin edge, so equality is asserted on the total
+    # and on all but a handful of bins
+    va = np.fromfile(a / (pre + "vid_phase.bin"), dtype=np.float32)
+    vb = np.fromfile(b / (pre + "vid_phase.bin"), dtype=np.float32)
+    assert va.size == vb.size == 256 * 200
+    assert va.sum() == vb.sum()
+    assert np.count_nonzero(va != vb) <= 4, np.count_nonzero(va != vb)
+
+    # field outputs at t = 0: FP32 fields from the two solvers
+    def close(x, y, rel):
+        x, y = np.asarray(x, np.float64), np.asarray(y, np.float64)
+        scale = max(np.abs(y).max(), 1e-30)
+        return np.abs(x - y).max() <= rel * scale
+
+    ka = np.fromfile(a / (pre + "kt.bin"), dtype=np.float32)
+    kb = np.fromfile(b / (pre + "kt.bin"), dtype=np.float32)
+    assert ka.size == kb.size == 64
+    assert close(ka, kb, 1e-4)
+    fla = np.fromfile(a / (pre + "vid_field.bin"), dtype=np.float32)
+    flb = np.fromfile(b / (pre + "vid_field.bin"), dtype=np.float32)
+    assert fla.size == flb.size == 3 * 64
+    for k in range(3):
+        assert close(fla[64 * k:64 * (k + 1)], flb[64 * k:64 * (k + 1)], 1e-4), k
+    ca = np.loadtxt(a / (pre + "fields.csv"), delimiter=",", skiprows=1)
+    cb = np.loadtxt(b / (pre + "fields.csv"), delimiter=",", skiprows=1)
+    assert ca.shape == cb.shape == (64, 6)
+    assert np.array_equal(ca[:, 0], cb[:, 0])
+    for k in range(1, 6):
+        assert close(ca[:, k], cb[:, k], 1e-4), k
+    ea = np.loadtxt(a / (pre + "emenergy.csv"), delimiter=",", skiprows=1)
+    eb = np.loadtxt(b / (pre + "emenergy.csv"), delimiter=",", skiprows=1)
+    assert ea.shape == eb.shape == (5,)
+    assert np.allclose(ea, eb, rtol=1e-4, atol=0)
+
+    # the spectrum line
+    la = [ln for ln in out_a.splitlines() if ln.startswith("t=")]
+    lb = [ln for ln in out_b.splitlines() if ln.startswith("t=")]
+    assert len(la) == len(lb) == 1
+    xa, xb = _floats(la[0]), _floats(lb[0])
+    assert len(xa) == len(xb)
+    assert np.allclose(xa, xb, rtol=1e-3, atol=1e-12), (la, lb)
+
+
+def test_every_module_keeps_the_step_rate(tmp_path):
+    """The full deck (33.5 M particles, 2000 steps, all six modules: 101 frames
+    of 100k points, 154 video frames, 401 E_L rows, 41 spectra and energy rows,
+    the snapshot) steps within 10% of the same deck with no module. Loop time =
+    process wall time at 2000 steps minus that of the same deck at 0 steps
+    (start-up, load and one sample), best of two."""
+    ours = _exe("arcsim")
+    off_text = [(r"^enable  = .*$", "enable  = none")]
+    decks = {"on": (DECK, _deck(tmp_path, "on0.ini", ZERO)),
+             "off": (_deck(tmp_path, "off.ini", off_text), _deck(tmp_path, "off0.ini", off_text + ZERO))}
+
+    def loop(tag):
+        full, zero = decks[tag]
+        best = math.inf
+        for rep in range(2):
+            d = tmp_path / f"{tag}{rep}"
+            d0 = tmp_path / f"{tag}{rep}_0"
+            d.mkdir()
+            d0.mkdir()
+            _, t_full = _run(ours, full, d)
+            _, t_zero = _run(ours, zero, d0)
+            best = min(best, t_full - t_zero)
+        return best, d
+
+    t_off, _ = loop("off")
+    t_on, d = loop("on")
+    print(f"\nloop time: {t_on:.3f} s with every module, {t_off:.3f} s with none ({t_on / t_off:.3f}x)")
+
+    pre = "whistler_diag_"
+    frames = sorted(d.glob("frame_*.csv"))
+    assert len(frames) == 101
+    with open(frames[-1]) as f:
+        assert sum(1 for _ in f) == 100001
+    assert len((d / "manifest.csv").read_text().splitlines()) == 102
+    assert (d / (pre + "vid_phase.bin")).stat().st_size == 154 * 256 * 200 * 4
+    assert (d / (pre + "kt.bin")).stat().st_size == 401 * 1024 * 4
+    assert len((d / (pre + "emenergy.csv")).read_text().splitlines()) == 42
+    n = 1024 * 128 * 256
+    hist = np.fromfile(d / (pre + "fhist.bin"), dtype=np.float32)
+    assert hist.size == 512 * 480
+    assert 0.99 * n <= hist.sum() <= n
+    vid = np.fromfile(d / (pre + "vid_phase.bin"), dtype=np.float32).reshape(154, -1)
+    assert np.all(vid.sum(axis=1) <= n)
+    assert np.all(vid.sum(axis=1) >= 0.99 * n)
+    assert t_on <= 1.10 * t_off, (t_on, t_off)
