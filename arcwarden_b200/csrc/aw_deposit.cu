@@ -523,14 +523,18 @@ __device__ __forceinline__ bool chunk_overflows(const float (&l1)[NF], int* red)
 }
 
 // The window of a single-pass chunk: the box widened by `mg` cells, plus the
-// corner; biased, one band, plane stride P1. False when it does not fit.
+// corner; biased, one band, plane stride P1. False when it does not fit, or
+// when it spans more than n + 1 cells of a grid dimension n (a margin too wide
+// for the grid, e.g. ny = 1): the origin and the flush wrap each index once,
+// which is exact while W <= nx + 1 and H <= ny + 1.
 template <int NF, bool T0, int P1>
-__device__ __forceinline__ bool one_pass_window(Win& w, const Box& b, int ir, int jr, int mg) {
+__device__ __forceinline__ bool one_pass_window(Win& w, const Box& b, int ir, int jr, int mg, const Geo& g) {
     if (b.hi_i < b.lo_i) return false;
     w.ir = ir; w.jr = jr;
     w.mi = b.lo_i - mg; w.mj = b.lo_j - mg;
     w.W = b.hi_i - b.lo_i + 2 + 2 * mg;
     w.H = b.hi_j - b.lo_j + 2 + 2 * mg;
+    if (w.W > g.nx + 1 || w.H > g.ny + 1) return false;
     if (static_cast<long long>(w.W) * w.H > P1) return false;
     w.Hb = w.H; w.nb = 1;
     w.WH = w.W * w.H;
@@ -706,7 +710,7 @@ __device__ __forceinline__ void deposit_dcu_chunk(const DcuArgs& A, const int ch
         }
         const Box bx = box_reduce(cb, m.red);
         Win w1;
-        if (A.one_pass && one_pass_window<NF, T0, P1>(w1, bx, ir, jr, 0)) {
+        if (A.one_pass && one_pass_window<NF, T0, P1>(w1, bx, ir, jr, 0, g)) {
             float* const tile1 = reinterpret_cast<float*>(m.win + P1 * win_planes(NF));
             const Tile tl = box_tile(bx, ir, jr, g, kTileCap1);
             if (tl.use && !load_tile8(tile1, gb, tl, g, &tbar, st)) return;
@@ -1141,7 +1145,7 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
         const float dmv = __fmul_rn(2.0f * uxy_max, static_cast<float>(fmax(pp.dtx, pp.dty)));
         const int mg = (dmv >= 0.0f && dmv < 8.0f) ? 1 + static_cast<int>(dmv) : -1;
         Win w1;
-        if (A.one_pass && mg > 0 && one_pass_window<NF, T0, P1>(w1, bx, ir, jr, mg)) {
+        if (A.one_pass && mg > 0 && one_pass_window<NF, T0, P1>(w1, bx, ir, jr, mg, g)) {
             float* const tile1 = reinterpret_cast<float*>(m.win + P1 * win_planes(NF));
             const Tile tl = box_tile(bx, ir, jr, g, kTileCap1);
             if (tl.use && !load_tile8(tile1, gb, tl, g, &tbar, st)) return;
