@@ -1925,7 +1925,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_push_esirkepov(YeeArgs A) {
     Win wn;
     // unbiased adds: the Esirkepov pass skips zero weights, so no count argument
     win_setup<NF, false, false>(wn, bb.lo_i, bb.lo_j, bb.hi_i + 1, bb.hi_j + 1, ir, jr, A.wmaxc, m.red, l1);
-    if (wn.nb > 1) { wn.use = false; wn.WH = 0; }     // no bands on this path: the slow path takes the chunk
+    // no bands on this path, and a window that spans more than n + 1 cells of a
+    // grid dimension n (the stencil is 3 nodes wide: a one-row grid) would wrap
+    // more than once at the flush: the slow path takes such chunks
+    if (wn.nb > 1 || wn.W > g.nx + 1 || wn.H > g.ny + 1) { wn.use = false; wn.WH = 0; }
     win_zero<NF, false>(m.win, wn);
     if (threadIdx.x < 3) {
         unsigned mx = 0;
