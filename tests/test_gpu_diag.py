@@ -48,12 +48,18 @@ def _run(exe, deck, outdir, timeout=900):
     return r.stdout, dt
 
 
-# 64 x 32 cells x 32 per cell = 65,536 particles: under the frames' 100k cap, so a
-# frame holds every particle, whatever order the two runners keep them in. The
-# runner's --nsteps flag ignores 0, so the deck itself says nsteps = 0: the
-# loop samples step 0 only (the snapshot fires there, at the last step).
-SMALL = [(r"^nx = .*$", "nx = 64"), (r"^ny = .*$", "ny = 32"), (r"^Lx = .*$", "Lx = 16.0"),
-         (r"^Ly = .*$", "Ly = 8.0"), (r"^ppc .*$", "ppc     = 32"), (r"^nsteps = .*$", "nsteps = 0")]
+# The deck cut to a small grid. The runner's --nsteps flag ignores 0, so the
+# deck itself says nsteps = 0: the loop samples step 0 only (the snapshot fires
+# there, at the last step).
+def _small(nx, ny, Lx, Ly, ppc):
+    return [(r"^nx = .*$", f"nx = {nx}"), (r"^ny = .*$", f"ny = {ny}"), (r"^Lx = .*$", f"Lx = {Lx}"),
+            (r"^Ly = .*$", f"Ly = {Ly}"), (r"^ppc .*$", f"ppc     = {ppc}"), (r"^nsteps = .*$", "nsteps = 0")]
+
+
+# (nx, ny, Lx, Ly, ppc): a 2D grid, and one cell high as the reference's whistler
+# decks run; 65,536 particles each, under the frames' 100k cap, so a frame holds
+# every particle, whatever order the two runners keep them in
+SMALL = [(64, 32, 16.0, 8.0, 32), (256, 1, 512.0, 2.0, 256)]
 ZERO = [(r"^nsteps = .*$", "nsteps = 0")]
 
 
@@ -66,14 +72,17 @@ def _floats(line):
     return [float(v) for v in re.findall(r"[-+]?\d+\.?\d*(?:e[-+]?\d+)?", line)]
 
 
-def test_step0_outputs_match_the_reference_runner(tmp_path):
+@pytest.mark.parametrize("grid", SMALL, ids=["64x32", "256x1"])
+def test_step0_outputs_match_the_reference_runner(tmp_path, grid):
     """At step 0 both runners hold the same loaded particles (the library's loader
     reproduces the reference's) in different orders: every order-independent
     output is the same bytes (the frame's rows as a multiset, the FP64 snapshot
     histogram, the metadata), the FP32 video histogram the same counts, and the
     field outputs agree to FP32 solve accuracy."""
     ours, ref = _exe("arcsim"), _exe("ref_arcsim")
-    deck = _deck(tmp_path, "small.ini", SMALL)
+    nx, ny, _, _, ppc = grid
+    npart = nx * ny * ppc
+    deck = _deck(tmp_path, "small.ini", _small(*grid))
     a, b = tmp_path / "a", tmp_path / "b"
     a.mkdir()
     b.mkdir()
@@ -84,7 +93,7 @@ def test_step0_outputs_match_the_reference_runner(tmp_path):
     ha, ra = _rows(a / "frame_0000.csv")
     hb, rb = _rows(b / "frame_0000.csv")
     assert ha == hb == "x,vx"
-    assert len(ra) == 64 * 32 * 32
+    assert len(ra) == npart
     assert ra == rb
     assert (a / "manifest.csv").read_text() == (b / "manifest.csv").read_text()
 
@@ -93,7 +102,7 @@ def test_step0_outputs_match_the_reference_runner(tmp_path):
     fa = np.fromfile(a / (pre + "fhist.bin"), dtype=np.float32)
     fb = np.fromfile(b / (pre + "fhist.bin"), dtype=np.float32)
     assert fa.size == fb.size == 512 * 480
-    assert fa.sum() == fb.sum() == 64 * 32 * 32
+    assert fa.sum() == fb.sum() == npart
     assert np.array_equal(fa, fb), np.count_nonzero(fa != fb)
     for meta in ("fhist.meta", "vid.meta", "kt.meta"):
         assert (a / (pre + meta)).read_text() == (b / (pre + meta)).read_text(), meta
@@ -116,16 +125,16 @@ def test_step0_outputs_match_the_reference_runner(tmp_path):
 
     ka = np.fromfile(a / (pre + "kt.bin"), dtype=np.float32)
     kb = np.fromfile(b / (pre + "kt.bin"), dtype=np.float32)
-    assert ka.size == kb.size == 64
+    assert ka.size == kb.size == nx
     assert close(ka, kb, 1e-4)
     fla = np.fromfile(a / (pre + "vid_field.bin"), dtype=np.float32)
     flb = np.fromfile(b / (pre + "vid_field.bin"), dtype=np.float32)
-    assert fla.size == flb.size == 3 * 64
+    assert fla.size == flb.size == 3 * nx
     for k in range(3):
-        assert close(fla[64 * k:64 * (k + 1)], flb[64 * k:64 * (k + 1)], 1e-4), k
+        assert close(fla[nx * k:nx * (k + 1)], flb[nx * k:nx * (k + 1)], 1e-4), k
     ca = np.loadtxt(a / (pre + "fields.csv"), delimiter=",", skiprows=1)
     cb = np.loadtxt(b / (pre + "fields.csv"), delimiter=",", skiprows=1)
-    assert ca.shape == cb.shape == (64, 6)
+    assert ca.shape == cb.shape == (nx, 6)
     assert np.array_equal(ca[:, 0], cb[:, 0])
     for k in range(1, 6):
         assert close(ca[:, k], cb[:, k], 1e-4), k
