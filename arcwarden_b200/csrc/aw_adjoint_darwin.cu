@@ -143,12 +143,27 @@ __device__ __forceinline__ void cross(const float (&a)[3], const float (&b)[3], 
     r[1] = a[2] * b[0] - a[0] * b[2];
     r[2] = a[0] * b[1] - a[1] * b[0];
 }
-// Block max of |v_f| into vmax[f] (float bits; non-negative floats order as unsigned).
-__device__ __forceinline__ void vmax_add(const float (&v)[6], unsigned* vmax) {
+// Running max of |v_f| per thread, and at the end of a kernel the block max
+// into vmax[f] (float bits; non-negative floats order as unsigned): one global
+// atomic per field and block (a per-iteration warp atomic on the same six
+// words serialises in L2). Every thread of the block calls vmax_flush.
+__device__ __forceinline__ void vmax_keep(const float (&v)[6], float (&m)[6]) {
+#pragma unroll
+    for (int f = 0; f < 6; ++f) m[f] = fmaxf(m[f], fabsf(v[f]));
+}
+__device__ __forceinline__ void vmax_flush(const float (&m)[6], unsigned* vmax) {
+    __shared__ unsigned sh[6][8];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        const unsigned m = __reduce_max_sync(0xffffffffu, __float_as_uint(fabsf(v[f])));
-        if ((threadIdx.x & 31) == 0 && m) atomicMax(vmax + f, m);
+        const unsigned w = __reduce_max_sync(0xffffffffu, __float_as_uint(m[f]));
+        if (lane == 0) sh[f][warp] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        unsigned b = 0;
+        for (int k = 0; k < static_cast<int>(blockDim.x >> 5); ++k) b = max(b, sh[threadIdx.x][k]);
+        if (b) atomicMax(vmax + threadIdx.x, b);
     }
 }
 
@@ -159,7 +174,7 @@ struct PArgs { const float* X; const float* w; float* lam; float* vals; unsigned
 __global__ void __launch_bounds__(256) k_dadj_push(PArgs a, const float* __restrict__ gbp, float h, float dtx,
                                                    float dty) {
     const long long n = a.n;
-    // block-uniform trip count: every lane reaches the warp-wide max in vmax_add
+    float vm[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (long long p0 = blockIdx.x * static_cast<long long>(blockDim.x); p0 < n;
          p0 += static_cast<long long>(gridDim.x) * blockDim.x) {
         const long long p = p0 + threadIdx.x;
@@ -199,8 +214,9 @@ __global__ void __launch_bounds__(256) k_dadj_push(PArgs a, const float* __restr
         }
         if (p < n)
             for (int d = 0; d < 6; ++d) a.vals[d * n + p] = v[d];
-        vmax_add(v, a.vmax);
+        vmax_keep(v, vm);
     }
+    vmax_flush(vm, a.vmax);
 }
 
 // Backward dcu deposit: g = G(ldcu); the scatter values (c g, c (g x u));
@@ -209,6 +225,7 @@ __global__ void __launch_bounds__(256) k_dadj_dcu(PArgs a, const float* __restri
                                                   double qm2oa) {
     const long long n = a.n;
     const int nc = a.g.ncell;
+    float vm[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     for (long long p0 = blockIdx.x * static_cast<long long>(blockDim.x); p0 < n;
          p0 += static_cast<long long>(gridDim.x) * blockDim.x) {
         const long long p = p0 + threadIdx.x;
@@ -243,8 +260,9 @@ __global__ void __launch_bounds__(256) k_dadj_dcu(PArgs a, const float* __restri
         }
         if (p < n)
             for (int d = 0; d < 6; ++d) a.vals[d * n + p] = v[d];
-        vmax_add(v, a.vmax);
+        vmax_keep(v, vm);
     }
+    vmax_flush(vm, a.vmax);
 }
 
 // Backward source deposit: from lsrc [ncell][8] = (lrho, lJ, lamu).

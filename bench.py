@@ -2,7 +2,7 @@
 """Benchmark of the B200 PIC hot path: particles/s per full PIC step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W]
-                    [--workload weibel512|es256|whistler1024|adjoint256|ensemble64|yee625]
+                    [--workload whistler1024|weibel512|es256|adjoint256|adjoint_darwin256|ensemble64|yee625]
                     [--impl ours|reference] [--no-cpu-baseline] [--dump-grad FILE]
 
 Workloads (synthetic, seeded; the reference's own seeded loader streams):
@@ -21,6 +21,8 @@ Workloads (synthetic, seeded; the reference's own seeded loader streams):
                 two-stream run (256x256, 2 x 8 ppc = 1,048,576) with respect
                 to every initial velocity, checkpoint every 20 steps; a bench
                 step is one gradient evaluation (forward + backward sweep)
+  adjoint_darwin256  the same for the Darwin step (256x256, 16 ppc, B0 and
+                the pump), with the pump-amplitude gradient
 
 `value` is the device-timed rate (K graph-launched steps bracketed by a
 barrier and a synchronize, CUDA events on the step's stream, max over ranks).
@@ -109,6 +111,18 @@ def workload(name: str) -> dict:
                              dict(ppc=8, density=0.5, uth=(0.01,) * 3, ufl=(-0.2, 0.0, 0.0))],
                     desc="adjoint of the electrostatic two-stream 256x256 dx=1 2x8ppc v0=+-0.2 vth=0.01 dt=0.1, "
                          "200 steps, checkpoint every 20, loss = final field energy")
+    if name == "adjoint_darwin256":
+        # the Darwin adjoint (pump-amplitude gradient included) at the config-3 size: a magnetised Weibel-type
+        # load with the whistler pump, 256^2 cells, 16 ppc
+        th = math.radians(30.0)
+        pump = dict(ex=1e-3, ey=2e-3, ez=-2e-3, k0=2 * math.pi * 4 / 128.0, w0=0.05, trmp=1.0, toff=1.0e9)
+        return dict(name=name, model=1, nx=256, ny=256, Lx=128.0, Ly=128.0, dt=0.05, c=1.0, n0=1.0,
+                    B0=(0.3 * math.cos(th), 0.0, 0.3 * math.sin(th)), pump=pump, run_steps=200, every=20,
+                    dom="push_deposit_em", adjoint=True,
+                    species=[dict(ppc=16, density=1.0, uth=(0.05, 0.05, 0.2), ufl=(0.0, 0.0, 0.0))],
+                    desc="Darwin adjoint: magnetised Weibel load 256x256 dx=0.5 ppc16 vth=(0.05,0.05,0.2), "
+                         "B0=0.3@30deg in x-z, pump M=4, c=1, dt=0.05, 200 steps, checkpoint every 20, "
+                         "loss = final field energy, gradients in u0 and the pump amplitude")
     if name == "yee625":
         # the reference's Yee benchmark (its published case 7, decks/eaw_case7_tiled.ini): whistler anisotropy
         # instability, 625^2 cells over 13.5 c/wpe, 400 particles per cell, wce/wpe = 0.25 along x, three
@@ -430,7 +444,10 @@ def profile_case(wl, steps):
     if wl.get("adjoint"):
         # one gradient of K steps (checkpoint interval as the workload's, at most K)
         du = [torch.zeros(n, dtype=torch.float32, device=dev) for _ in range(3)]
-        ctx.grad_es(steps, min(wl["every"], steps), *du)
+        if wl["model"] == aw.AW_MODEL_DARWIN:
+            ctx.grad_darwin(steps, min(wl["every"], steps), *du)
+        else:
+            ctx.grad_es(steps, min(wl["every"], steps), *du)
     else:
         ctx.init()
         for s in range(steps):
@@ -462,6 +479,25 @@ def adj_launches(nsteps, every):
     return 13 + 5 * nsteps + 4 * (nsteps - last) + 4 * nsteps + 2 * nseg + 2
 
 
+def adj_darwin_bytes_per_particle_step():
+    """Algorithmic bytes per particle per PIC step of one Darwin gradient: the
+    forward step (44 push + 24 dcu read), its recompute (68), the saved state
+    (20 read + 20 written) and three transposed particle passes (push, dcu and
+    source deposit), each reading the saved state x y ux uy uz and w (24) and
+    reading and writing the five cotangents (40)."""
+    return 68.0 + 68.0 + 40.0 + 3 * 64.0
+
+
+def adj_darwin_launches(nsteps, every):
+    """Kernels of this library one Darwin gradient launches: aw_init's 13; 9 per
+    forward step; per segment a restored state and its recompute (9 per step);
+    11 per backward step (push transpose, two 6-field scatters and their
+    conversions, the E_T and E_L/B transposes, the pump sum, the source pack and
+    transpose); the output."""
+    nseg = math.ceil(nsteps / every)
+    return 13 + 9 * nsteps + 9 * nsteps + 11 * nsteps + nseg + 1
+
+
 def run_adjoint(args, wl, rank, world, dist):
     import torch
     import arcwarden_b200 as aw
@@ -471,13 +507,15 @@ def run_adjoint(args, wl, rank, world, dist):
     n = nparticles(wl)
     N, every = wl["run_steps"], wl["every"]
     stream = torch.cuda.Stream(dev)
+    darwin = wl["model"] == aw.AW_MODEL_DARWIN
     ctx = aw.Context(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], dt=wl["dt"], c=wl["c"], n0=wl["n0"], B0=wl["B0"],
-                     model=wl["model"], stream=stream.cuda_stream)
+                     model=wl["model"], stream=stream.cuda_stream, pump=wl.get("pump"))
     P = {k: torch.empty(n, dtype=torch.float32, device=dev) for k in ("x", "y", "ux", "uy", "uz", "w")}
     cell = torch.empty(n, dtype=torch.int32, device=dev)
     ctx.bind_particles(P["x"], P["y"], P["ux"], P["uy"], P["uz"], P["w"], cell)
     ctx.load_species(wl["species"], seed=0, noisy=True)
     p0 = {k: v.clone() for k, v in P.items()}
+    dpump = [0.0]
     du = [torch.zeros(n, dtype=torch.float32, device=dev) for _ in range(3)]
 
     def barrier():
@@ -506,7 +544,10 @@ def run_adjoint(args, wl, rank, world, dist):
     loss = [0.0]
 
     def grad():
-        loss[0] = ctx.grad_es(N, every, *du)
+        if darwin:
+            loss[0], dpump[0] = ctx.grad_darwin(N, every, *du)
+        else:
+            loss[0] = ctx.grad_es(N, every, *du)
 
     for _ in range(max(args.warmup, 3)):
         forward()
@@ -545,9 +586,9 @@ def run_adjoint(args, wl, rank, world, dist):
     e2e_s = max_over_ranks((time.perf_counter() - t0) / reps, dist, dev)
 
     peak, peak_kind = measured_peak_gbs()
-    bpp = adj_bytes_per_particle_step(N, every)
+    bpp = adj_darwin_bytes_per_particle_step() if darwin else adj_bytes_per_particle_step(N, every)
     achieved = n * N * bpp / (grad_ms * 1e-3) / 1e9
-    launches = adj_launches(N, every)
+    launches = adj_darwin_launches(N, every) if darwin else adj_launches(N, every)
     res = {
         "metric": "particles/s/step (gradient: forward + checkpointed backward)",
         "value": world * n * N / (grad_ms * 1e-3),
@@ -557,7 +598,8 @@ def run_adjoint(args, wl, rank, world, dist):
         "dtype": "f32",
         "numerics": "f32 forward and cotangents; deposits and the cotangent scatter exact int64 fixed point",
         "data": "synthetic: reference seeded loader streams (noisy load, seed 0)",
-        "config": {"workload": wl["desc"], "field_model": "electrostatic", "grid": [wl["nx"], wl["ny"]],
+        "config": {"workload": wl["desc"], "field_model": "darwin" if darwin else "electrostatic",
+                   "grid": [wl["nx"], wl["ny"]],
                    "particles_per_gpu": n, "pic_steps_per_gradient": N, "checkpoint_every": every,
                    "bench_step": "one gradient evaluation", "parallelism": f"replicas x{world}",
                    "l2": "inputs > L2 per gradient (trajectory and checkpoints, ~400 MB)"},
@@ -566,9 +608,11 @@ def run_adjoint(args, wl, rank, world, dist):
         "gradient_over_forward": grad_ms / fwd_ms,
         "backward_over_forward": (grad_ms - fwd_ms) / fwd_ms,
         "loss": loss[0],
+        "dloss_dpump": dpump[0] if darwin else None,
         "e2e": {"value": world * n * N / e2e_s, "unit": "particles/s", "h2d_bytes_per_step": 24 * n,
                 "d2h_bytes_per_step": 12 * n,
-                "run": "H2D of the initial state from pinned memory, aw_grad_es, D2H of dL/du0"},
+                "run": "H2D of the initial state from pinned memory, "
+                       f"{'aw_grad_darwin' if darwin else 'aw_grad_es'}, D2H of dL/du0"},
         "roofline": {"bound": "hbm", "kernel": "whole gradient", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                      "algorithmic_bytes_per_particle_step": bpp},
@@ -584,10 +628,15 @@ def adjoint_cpu_baseline(wl, budget_steps=8):
     budget_steps PIC steps of the same particles, forward and adjoint."""
     import numpy as np
     from oracle import oracle as O
-    from oracle.adjoint64 import Case
     g = O.geo(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"])
     p = O.load_species(g, wl["species"], seed=0, noisy=True)
-    case = Case(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], wl["dt"], B0=wl["B0"])
+    if wl["model"] == 1:
+        from oracle.darwin_adjoint64 import DarwinCase
+        case = DarwinCase(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], wl["dt"], B0=wl["B0"], pump=wl.get("pump"))
+        budget_steps = min(budget_steps, 4)
+    else:
+        from oracle.adjoint64 import Case
+        case = Case(wl["nx"], wl["ny"], wl["Lx"], wl["Ly"], wl["dt"], B0=wl["B0"])
     u = np.stack([p["ux"], p["uy"], p["uz"]], axis=1).astype(np.float64)
     n = len(p["x"])
     t0 = time.perf_counter()
