@@ -65,10 +65,16 @@ struct DAdj {
                                          // transpose's 5 inputs and its 4 outputs after them
     double* dpump = nullptr;             // running dL/da
     DevState* st = nullptr;              // error word and counters of the sweep
+    long long* slot = nullptr;           // [2] the current trajectory slot and step
+    unsigned* ticket = nullptr;          // [1] last-block counter of k_dadj_save_gb
+    float* X = nullptr;                  // [5][n] the backward step's saved state
+    float* gbs = nullptr;                // [2][ncell][8] its gather buffers
     cufftHandle r2c3 = 0, c2r7 = 0, r2c5 = 0, c2r4 = 0;
+    cudaGraphExec_t back = nullptr;      // one backward step
     ~DAdj() {
+        if (back) cudaGraphExecDestroy(back);
         void* b[] = {init, ck, ck_acc, ck_st, traj, traj_gb, lam, vals, vmax, S, acc, lEB, l5, l7, l4, lsrc, k3, k7,
-                     dpump, st};
+                     dpump, st, slot, ticket, X, gbs};
         for (void* p : b) if (p) cudaFree(p);
         cufftHandle h[] = {r2c3, c2r7, r2c5, c2r4};
         for (cufftHandle x : h) if (x) cufftDestroy(x);
@@ -314,10 +320,16 @@ __device__ __forceinline__ void pump_at(const PumpD& pd, int i, double t, double
 // plus eps0 dx dy (Ex, Ey) of gbp when `seed`. mode 1 (dcu): out5 = (lE_xy + lFd_xy,
 // lBt + lBt'), from the push's lEB; the pump term sum (lE + lFd) . P into a
 // fixed-order block partial, reduced by k_dadj_pump.
+// The step comes from slot[1]: the seed applies at step `last`, the pump at
+// t = step dt.
 __global__ void __launch_bounds__(256) k_dadj_fin(unsigned long long* __restrict__ acc, const float* __restrict__ S,
                                                   int ncell, int nx, int mode, float* __restrict__ out,
                                                   const float* __restrict__ lEB, const float* __restrict__ gbp,
-                                                  float seed, PumpD pd, double t, double* __restrict__ part) {
+                                                  float seedv, long long last, const long long* __restrict__ slot,
+                                                  PumpD pd, double dt, double* __restrict__ part) {
+    const long long step = slot[1];
+    const float seed = step == last ? seedv : 0.0f;
+    const double t = static_cast<double>(step) * dt;
     double sp = 0.0;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
         float v[6];
@@ -445,6 +457,79 @@ __global__ void k_dadj_pack(const float* __restrict__ l4, const float* __restric
 
 int grid_blocks(long long n) { return static_cast<int>(std::min<long long>(4 * 148, (n + 255) / 256)); }
 
+// `body`'s work on stream s, captured into an instantiated graph.
+template <class F>
+cudaGraphExec_t capture_graph(cudaStream_t s, F body) {
+    cudaGraph_t g = nullptr;
+    AW_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    try {
+        body();
+    } catch (...) {
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    AW_CUDA(cudaStreamEndCapture(s, &g));
+    cudaGraphExec_t e = nullptr;
+    const cudaError_t r = cudaGraphInstantiate(&e, g, 0);
+    cudaGraphDestroy(g);
+    AW_CUDA(r);
+    return e;
+}
+
+// ---- the trajectory slot of the current step, on the device ---------------------
+// slot[0] = the step's index in its segment's trajectory, slot[1] = the step.
+// The recompute and backward steps address their trajectory slot through it, so
+// one captured backward graph (fixed pointers) serves every step.
+__global__ void k_dadj_set_slot(long long* slot, long long s, long long step) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) { slot[0] = s; slot[1] = step; }
+}
+// The five state arrays into trajectory slot slot[0] (before a recompute step).
+__global__ void k_dadj_save(const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ ux,
+                            const float* __restrict__ uy, const float* __restrict__ uz, long long n,
+                            float* __restrict__ traj, const long long* __restrict__ slot) {
+    float* t = traj + slot[0] * 5 * n;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        t[i] = x[i]; t[n + i] = y[i]; t[2 * n + i] = ux[i]; t[3 * n + i] = uy[i]; t[4 * n + i] = uz[i];
+    }
+}
+// The step's two gather buffers into slot slot[0] (after the recompute step);
+// then the next slot. The last block to finish moves the slot on.
+__global__ void k_dadj_save_gb(const float4* __restrict__ gbd, const float4* __restrict__ gbp, int nc,
+                               float4* __restrict__ traj_gb, long long* slot, unsigned* ticket) {
+    float4* t = traj_gb + slot[0] * 4 * nc;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 2 * nc; i += gridDim.x * blockDim.x) {
+        t[i] = gbd[i];
+        t[2 * nc + i] = gbp[i];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(ticket, 1u) == gridDim.x - 1) {
+            slot[0] += 1;
+            *ticket = 0u;
+        }
+    }
+}
+// Trajectory slot slot[0] (state and gather buffers) into the fixed buffers the
+// backward step reads.
+__global__ void k_dadj_load(const float* __restrict__ traj, const float4* __restrict__ traj_gb,
+                            const long long* __restrict__ slot, long long n, int nc, float* __restrict__ X,
+                            float4* __restrict__ gbs) {
+    const float* t = traj + slot[0] * 5 * n;
+    const float4* tg = traj_gb + slot[0] * 4 * nc;
+    const long long stride = static_cast<long long>(gridDim.x) * blockDim.x;
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < 5 * n; i += stride)
+        X[i] = t[i];
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < 4LL * nc; i += stride)
+        gbs[i] = tg[i];
+}
+// The previous step: slot[0] -= 1, slot[1] -= 1 (the end of a backward step).
+__global__ void k_dadj_prev(long long* slot) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) { slot[0] -= 1; slot[1] -= 1; }
+}
+
 }  // namespace
 
 // The gradient of the last step's field energy with respect to every initial
@@ -477,6 +562,10 @@ double grad_darwin_impl(Ctx& c, long long nsteps, int every, float* dux, float* 
     dmalloc(w.k7, 9 * nk);
     dmalloc(w.dpump, 1);
     dmalloc(w.st, 1);
+    dmalloc(w.slot, 2);
+    dmalloc(w.ticket, 1);
+    dmalloc(w.X, 5 * static_cast<size_t>(n));
+    dmalloc(w.gbs, 16 * static_cast<size_t>(nc));
     double* part = nullptr;
     const int fin_blocks = 148;
     dmalloc(part, fin_blocks);
@@ -502,16 +591,40 @@ double grad_darwin_impl(Ctx& c, long long nsteps, int every, float* dux, float* 
     };
     save_parts(w.init);
     init_impl_for_adjoint(c);
-    // forward run, checkpoints at the segment starts
+    const int pb = grid_blocks(n), gbk = std::min(fin_blocks, (nc + 255) / 256);
+    const int gbk2 = std::min(4 * 148, (2 * nc + 255) / 256);
+    AW_CUDA(cudaMemsetAsync(w.ticket, 0, sizeof(unsigned), c.stream));
+    // one recorded step: its state into trajectory slot w.slot[0], the step, its
+    // gather buffers into the same slot (then the next slot)
+    auto record_step = [&] {
+        k_dadj_save<<<pb, 256, 0, c.stream>>>(P[0], P[1], P[2], P[3], P[4], n, w.traj, w.slot);
+        AW_LAUNCH();
+        run_step_for_adjoint(c);
+        k_dadj_save_gb<<<gbk2, 256, 0, c.stream>>>(reinterpret_cast<const float4*>(c.gb_dcu),
+                                                   reinterpret_cast<const float4*>(c.gb_push), nc,
+                                                   reinterpret_cast<float4*>(w.traj_gb), w.slot, w.ticket);
+        AW_LAUNCH();
+    };
+    const long long last_seg = static_cast<long long>(nck - 1) * every;
+    // forward run, checkpoints at the segment starts but the last
     for (long long s = 0; s < nsteps; ++s) {
-        if (s % every == 0) {
+        if (s % every == 0 && s < last_seg) {
             const int k = static_cast<int>(s / every);
             save_parts(w.ck + static_cast<size_t>(k) * 5 * n);
             AW_CUDA(cudaMemcpyAsync(w.ck_acc + static_cast<size_t>(k) * 8 * nc, c.acc_src,
                                     sizeof(unsigned long long) * 8 * nc, cudaMemcpyDeviceToDevice, c.stream));
             AW_CUDA(cudaMemcpyAsync(w.ck_st + k, c.st, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
         }
-        run_step_for_adjoint(c);
+        if (s < last_seg) {
+            run_step_for_adjoint(c);
+            continue;
+        }
+        // the last segment is recorded by the forward run itself: no recompute
+        if (s == last_seg) {
+            k_dadj_set_slot<<<1, 32, 0, c.stream>>>(w.slot, 0, s);
+            AW_LAUNCH();
+        }
+        record_step();
     }
     aw_diag d{};
     AW_CUDA(cudaMemcpyAsync(&d, c.diag, sizeof(aw_diag), cudaMemcpyDeviceToHost, c.stream));
@@ -525,42 +638,44 @@ double grad_darwin_impl(Ctx& c, long long nsteps, int every, float* dux, float* 
     PumpD pd{c.prm.pump, c.prm.pump_ex, c.prm.pump_ey, c.prm.pump_ez, c.prm.pump_k0, c.prm.pump_w0, c.prm.pump_trmp,
              c.prm.pump_toff, c.geo.dx};
     const float seed = static_cast<float>(c.prm.eps0 * c.geo.dx * c.geo.dy);
-    const int pb = grid_blocks(n), gbk = std::min(fin_blocks, (nc + 255) / 256);
-    for (int k = nck - 1; k >= 0; --k) {
-        const long long s0 = static_cast<long long>(k) * every;
-        const int m = static_cast<int>(std::min<long long>(nsteps, s0 + every) - s0);
-        // recompute the segment, copying each step's state and gather buffers
-        load_parts(w.ck + static_cast<size_t>(k) * 5 * n);
-        AW_CUDA(cudaMemcpyAsync(c.acc_src, w.ck_acc + static_cast<size_t>(k) * 8 * nc,
-                                sizeof(unsigned long long) * 8 * nc, cudaMemcpyDeviceToDevice, c.stream));
-        AW_CUDA(cudaMemcpyAsync(c.st, w.ck_st + k, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
-        c.pending_valid = true;
-        for (int s = 0; s < m; ++s) {
-            save_parts(w.traj + static_cast<size_t>(s) * 5 * n);
-            run_step_for_adjoint(c);
-            float* tg = w.traj_gb + static_cast<size_t>(s) * 16 * nc;
-            AW_CUDA(cudaMemcpyAsync(tg, c.gb_dcu, sizeof(float) * 8 * nc, cudaMemcpyDeviceToDevice, c.stream));
-            AW_CUDA(cudaMemcpyAsync(tg + 8 * nc, c.gb_push, sizeof(float) * 8 * nc, cudaMemcpyDeviceToDevice,
-                                    c.stream));
-        }
-        // the segment's backward steps, in reverse
-        for (int s = m - 1; s >= 0; --s) {
-            const long long step = s0 + s;
-            const float* X = w.traj + static_cast<size_t>(s) * 5 * n;
-            const float* gbd = w.traj_gb + static_cast<size_t>(s) * 16 * nc;
-            const float* gbp = gbd + 8 * nc;
-            PArgs a{X, c.parts.w, w.lam, w.vals, w.vmax, n, c.geo};
+    // k_dadj_src holds more registers: its grid is the blocks that fit at once
+    // (one wave), each looping over particles
+    int sms = 148, per_sm = 3;
+    {
+        int dev = 0;
+        AW_CUDA(cudaGetDevice(&dev));
+        AW_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        AW_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_dadj_src, 256, 0));
+    }
+    const int pb_src = static_cast<int>(std::max<long long>(1, std::min<long long>(static_cast<long long>(sms) *
+                                                                                    std::max(per_sm, 1),
+                                                                                    (n + 255) / 256)));
+    // One backward step, captured once: it copies trajectory slot w.slot[0] into
+    // the fixed buffers w.X, w.gbs, reads its step from w.slot[1] and moves the
+    // slot one step back, so the same graph replays every step.
+    prepare_scatter6();
+    {
+        const float* X = w.X;
+        const float* gbd = w.gbs;
+        const float* gbp = w.gbs + 8 * static_cast<size_t>(nc);
+        const PArgs a{X, c.parts.w, w.lam, w.vals, w.vmax, n, c.geo};
+        const long long last = nsteps - 1;
+        w.back = capture_graph(c.stream, [&] {
+            k_dadj_load<<<pb, 256, 0, c.stream>>>(w.traj, reinterpret_cast<const float4*>(w.traj_gb), w.slot, n, nc,
+                                                  w.X, reinterpret_cast<float4*>(w.gbs));
+            AW_LAUNCH();
             // push transpose -> lE, lBt
             AW_CUDA(cudaMemsetAsync(w.vmax, 0, 6 * sizeof(unsigned), c.stream));
             k_dadj_push<<<pb, 256, 0, c.stream>>>(a, gbp, h, dtx, dty);
             AW_LAUNCH();
             launch_scatter6(c, c.stream, X, X + n, w.vals, n, w.vmax, w.S, w.acc, w.st);
-            k_dadj_fin<<<gbk, 256, 0, c.stream>>>(w.acc, w.S, nc, c.geo.nx, 0, w.lEB, nullptr, gbp,
-                                                  step == nsteps - 1 ? seed : 0.0f, pd, 0.0, nullptr);
+            k_dadj_fin<<<gbk, 256, 0, c.stream>>>(w.acc, w.S, nc, c.geo.nx, 0, w.lEB, nullptr, gbp, seed, last, w.slot,
+                                                  pd, c.prm.dt, nullptr);
             AW_LAUNCH();
             // E_T transpose -> ldcu, lamu
             AW_CUFFT(cufftExecR2C(w.r2c3, w.lEB, w.k3));
-            k_dadj_et_T<<<(c.sg.nk + 255) / 256, 256, 0, c.stream>>>(w.k3, w.k7, c.sg, c.prm.eps0, c.prm.c, c.prm.n0);
+            k_dadj_et_T<<<(c.sg.nk + 255) / 256, 256, 0, c.stream>>>(w.k3, w.k7, c.sg, c.prm.eps0, c.prm.c,
+                                                                     c.prm.n0);
             AW_LAUNCH();
             AW_CUFFT(cufftExecC2R(w.c2r7, w.k7, w.l7));
             // dcu transpose -> lFd, lBt'; combined with lE, lBt into (lE_L, lB); the pump term
@@ -568,8 +683,8 @@ double grad_darwin_impl(Ctx& c, long long nsteps, int every, float* dux, float* 
             k_dadj_dcu<<<pb, 256, 0, c.stream>>>(a, gbd, w.l7, qm2oa);
             AW_LAUNCH();
             launch_scatter6(c, c.stream, X, X + n, w.vals, n, w.vmax, w.S, w.acc, w.st);
-            k_dadj_fin<<<gbk, 256, 0, c.stream>>>(w.acc, w.S, nc, c.geo.nx, 1, w.l5, w.lEB, nullptr, 0.0f, pd,
-                                                  static_cast<double>(step) * c.prm.dt, part);
+            k_dadj_fin<<<gbk, 256, 0, c.stream>>>(w.acc, w.S, nc, c.geo.nx, 1, w.l5, w.lEB, nullptr, 0.0f, last,
+                                                  w.slot, pd, c.prm.dt, part);
             AW_LAUNCH();
             k_dadj_pump<<<1, 32, 0, c.stream>>>(part, gbk, w.dpump);
             AW_LAUNCH();
@@ -581,9 +696,31 @@ double grad_darwin_impl(Ctx& c, long long nsteps, int every, float* dux, float* 
             AW_CUFFT(cufftExecC2R(w.c2r4, w.k7 + 5 * nk, w.l4));
             k_dadj_pack<<<gbk, 256, 0, c.stream>>>(w.l4, w.l7 + 3 * static_cast<size_t>(nc), nc, w.lsrc);
             AW_LAUNCH();
-            k_dadj_src<<<pb, 256, 0, c.stream>>>(a, w.lsrc, qoa);
+            k_dadj_src<<<pb_src, 256, 0, c.stream>>>(a, w.lsrc, qoa);
             AW_LAUNCH();
+            k_dadj_prev<<<1, 32, 0, c.stream>>>(w.slot);
+            AW_LAUNCH();
+        });
+    }
+    for (int k = nck - 1; k >= 0; --k) {
+        const long long s0 = static_cast<long long>(k) * every;
+        const int m = static_cast<int>(std::min<long long>(nsteps, s0 + every) - s0);
+        // recompute the segment (the last one was recorded by the forward run),
+        // saving each step's state and gather buffers into slots 0 .. m - 1
+        if (k < nck - 1) {
+            load_parts(w.ck + static_cast<size_t>(k) * 5 * n);
+            AW_CUDA(cudaMemcpyAsync(c.acc_src, w.ck_acc + static_cast<size_t>(k) * 8 * nc,
+                                    sizeof(unsigned long long) * 8 * nc, cudaMemcpyDeviceToDevice, c.stream));
+            AW_CUDA(cudaMemcpyAsync(c.st, w.ck_st + k, sizeof(DevState), cudaMemcpyDeviceToDevice, c.stream));
+            c.pending_valid = true;
+            k_dadj_set_slot<<<1, 32, 0, c.stream>>>(w.slot, 0, s0);
+            AW_LAUNCH();
+            for (int s = 0; s < m; ++s) record_step();
         }
+        // the segment's backward steps, in reverse
+        k_dadj_set_slot<<<1, 32, 0, c.stream>>>(w.slot, m - 1, s0 + m - 1);
+        AW_LAUNCH();
+        for (int s = m - 1; s >= 0; --s) AW_CUDA(cudaGraphLaunch(w.back, c.stream));
     }
     // outputs, the initial state back in the caller's arrays, the sweep's errors
     for (int k = 0; k < 3; ++k) {

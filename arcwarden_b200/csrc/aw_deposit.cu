@@ -1623,6 +1623,7 @@ void launch_deposit_src(Ctx& c, int which) {
 
 void prep_adj_scatter() { prep_smem(k_adj_scatter, smem_bytes(2, 4)); }
 
+void prepare_scatter6() { prep_smem(k_scatter6, smem_bytes(kScatterNF, 2 + kScatterNF)); }
 void launch_scatter6(Ctx& c, cudaStream_t s, const float* xs, const float* ys, const float* vals, long long n,
                      const unsigned* vmax, float* Sout, unsigned long long* acc, DevState* st) {
     if (n == 0) return;

@@ -268,6 +268,9 @@ void prep_adj_scatter();   // its shared-memory opt-in (before any capture)
 // the positions (xs, ys); scales from the maxima vmax[6] (float bits), stored to Sout.
 void launch_scatter6(Ctx& c, cudaStream_t s, const float* xs, const float* ys, const float* vals, long long n,
                      const unsigned* vmax, float* Sout, unsigned long long* acc, DevState* st);
+// The shared-memory opt-in of k_scatter6 on the current device (before a
+// stream capture that launches it).
+void prepare_scatter6();
 // Multi-run particle phases (batched ensembles): one launch over the chunks of
 // several runs of one kind. The run table is built once (device copies of each
 // run's kernel arguments); the runs' buffers must stay bound while it lives.
