@@ -246,7 +246,8 @@ int aw_get_kernel_plan(aw_ctx* ctx, aw_kernel_plan* plan);
  * config.hpp:61-66). Call it with the particles bound and loaded, before
  * aw_init: every candidate plan (Darwin: single/two-pass x gather tile;
  * electrostatic: the rho window) runs init, 2 warm-up steps and `trial_steps`
- * timed steps from the same initial state; the fastest is set (and written to
+ * timed steps from the same initial state, twice (the second round in reverse
+ * order; each plan keeps its faster trial); the fastest is set (and written to
  * *chosen when not NULL). The particles are restored and the context is left
  * initialised, as after aw_init. Plans are cached for the process per (device,
  * model, grid, particle count): a later context of the same class takes the
