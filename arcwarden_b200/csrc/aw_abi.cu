@@ -85,6 +85,7 @@ void make_plan(cufftHandle& h, int ny, int nx, cufftType type, int batch, size_t
 void free_all(Ctx& c) {
     free_checkpoint(c);
     free_adjoint(c);
+    free_dadj(c);
     if (c.gexec) cudaGraphExecDestroy(c.gexec);
     if (c.graph) cudaGraphDestroy(c.graph);
     cufftHandle* plans[] = {&c.p_r2c1, &c.p_c2r1, &c.p_r2cS, &c.p_c2rO, &c.p_r2c3, &c.p_c2r3, &c.p_r2c4};

@@ -32,6 +32,7 @@
 #include "aw_internal.h"
 
 #include <cmath>
+#include <memory>
 #include <vector>
 
 namespace aw {
@@ -39,9 +40,9 @@ namespace aw {
 void init_impl_for_adjoint(Ctx& c);     // aw_abi.cu: aw_init's sequence
 void run_step_for_adjoint(Ctx& c);      // aw_abi.cu: one fused step on the context's stream
 
-namespace {
-
-struct DAdj {
+// Workspace of the Darwin adjoint sweep (aw_grad_darwin), kept by the context
+// between gradients of the same shape (particles, interval, segments, grid).
+struct DAdjWS {
     long long n = 0;
     int every = 0, nck = 0, ncell = 0;
     float* init = nullptr;               // [5][n] the initial x y ux uy uz
@@ -71,15 +72,23 @@ struct DAdj {
     float* gbs = nullptr;                // [2][ncell][8] its gather buffers
     cufftHandle r2c3 = 0, c2r7 = 0, r2c5 = 0, c2r4 = 0;
     cudaGraphExec_t back = nullptr;      // one backward step
-    ~DAdj() {
+    double* part = nullptr;              // [148] pump-term block partials
+    ~DAdjWS() {
         if (back) cudaGraphExecDestroy(back);
         void* b[] = {init, ck, ck_acc, ck_st, traj, traj_gb, lam, vals, vmax, S, acc, lEB, l5, l7, l4, lsrc, k3, k7,
-                     dpump, st, slot, ticket, X, gbs};
+                     dpump, st, slot, ticket, X, gbs, part};
         for (void* p : b) if (p) cudaFree(p);
         cufftHandle h[] = {r2c3, c2r7, r2c5, c2r4};
         for (cufftHandle x : h) if (x) cufftDestroy(x);
     }
 };
+
+void free_dadj(Ctx& c) {
+    delete c.dadj;
+    c.dadj = nullptr;
+}
+
+namespace {
 
 template <class T>
 void dmalloc(T*& p, size_t n) { AW_CUDA(cudaMalloc(reinterpret_cast<void**>(&p), n * sizeof(T))); }
@@ -540,40 +549,50 @@ double grad_darwin_impl(Ctx& c, long long nsteps, int every, float* dux, float* 
     const size_t nk = static_cast<size_t>(c.sg.nk);
     every = static_cast<int>(std::min<long long>(every, nsteps));
     const int nck = static_cast<int>((nsteps + every - 1) / every);
-    DAdj w;
-    w.n = n; w.every = every; w.nck = nck; w.ncell = nc;
-    dmalloc(w.init, 5 * static_cast<size_t>(n));
-    dmalloc(w.ck, static_cast<size_t>(nck) * 5 * n);
-    dmalloc(w.ck_acc, static_cast<size_t>(nck) * 8 * nc);
-    dmalloc(w.ck_st, static_cast<size_t>(nck));
-    dmalloc(w.traj, static_cast<size_t>(every) * 5 * n);
-    dmalloc(w.traj_gb, static_cast<size_t>(every) * 16 * nc);
-    dmalloc(w.lam, 5 * static_cast<size_t>(n));
-    dmalloc(w.vals, 6 * static_cast<size_t>(n));
-    dmalloc(w.vmax, 6);
-    dmalloc(w.S, 6);
-    dmalloc(w.acc, 6 * static_cast<size_t>(nc));
-    dmalloc(w.lEB, 6 * static_cast<size_t>(nc));
-    dmalloc(w.l5, 5 * static_cast<size_t>(nc));
-    dmalloc(w.l7, 7 * static_cast<size_t>(nc));
-    dmalloc(w.l4, 4 * static_cast<size_t>(nc));
-    dmalloc(w.lsrc, 8 * static_cast<size_t>(nc));
-    dmalloc(w.k3, 3 * nk);
-    dmalloc(w.k7, 9 * nk);
-    dmalloc(w.dpump, 1);
-    dmalloc(w.st, 1);
-    dmalloc(w.slot, 2);
-    dmalloc(w.ticket, 1);
-    dmalloc(w.X, 5 * static_cast<size_t>(n));
-    dmalloc(w.gbs, 16 * static_cast<size_t>(nc));
-    double* part = nullptr;
     const int fin_blocks = 148;
-    dmalloc(part, fin_blocks);
-    struct Free { double* p; ~Free() { if (p) cudaFree(p); } } fp{part};
-    plan(w.r2c3, c.geo.ny, c.geo.nx, CUFFT_R2C, 3);
-    plan(w.c2r7, c.geo.ny, c.geo.nx, CUFFT_C2R, 7);
-    plan(w.r2c5, c.geo.ny, c.geo.nx, CUFFT_R2C, 5);
-    plan(w.c2r4, c.geo.ny, c.geo.nx, CUFFT_C2R, 4);
+    if (c.dadj && !(c.dadj->n == n && c.dadj->every == every && c.dadj->nck == nck && c.dadj->ncell == nc))
+        free_dadj(c);
+    if (!c.dadj) {
+        std::unique_ptr<DAdjWS> ws(new DAdjWS());
+        DAdjWS& w = *ws;
+        w.n = n; w.every = every; w.nck = nck; w.ncell = nc;
+        dmalloc(w.init, 5 * static_cast<size_t>(n));
+        dmalloc(w.ck, static_cast<size_t>(nck) * 5 * n);
+        dmalloc(w.ck_acc, static_cast<size_t>(nck) * 8 * nc);
+        dmalloc(w.ck_st, static_cast<size_t>(nck));
+        dmalloc(w.traj, static_cast<size_t>(every) * 5 * n);
+        dmalloc(w.traj_gb, static_cast<size_t>(every) * 16 * nc);
+        dmalloc(w.lam, 5 * static_cast<size_t>(n));
+        dmalloc(w.vals, 6 * static_cast<size_t>(n));
+        dmalloc(w.vmax, 6);
+        dmalloc(w.S, 6);
+        dmalloc(w.acc, 6 * static_cast<size_t>(nc));
+        dmalloc(w.lEB, 6 * static_cast<size_t>(nc));
+        dmalloc(w.l5, 5 * static_cast<size_t>(nc));
+        dmalloc(w.l7, 7 * static_cast<size_t>(nc));
+        dmalloc(w.l4, 4 * static_cast<size_t>(nc));
+        dmalloc(w.lsrc, 8 * static_cast<size_t>(nc));
+        dmalloc(w.k3, 3 * nk);
+        dmalloc(w.k7, 9 * nk);
+        dmalloc(w.dpump, 1);
+        dmalloc(w.st, 1);
+        dmalloc(w.slot, 2);
+        dmalloc(w.ticket, 1);
+        dmalloc(w.X, 5 * static_cast<size_t>(n));
+        dmalloc(w.gbs, 16 * static_cast<size_t>(nc));
+        dmalloc(w.part, fin_blocks);
+        plan(w.r2c3, c.geo.ny, c.geo.nx, CUFFT_R2C, 3);
+        plan(w.c2r7, c.geo.ny, c.geo.nx, CUFFT_C2R, 7);
+        plan(w.r2c5, c.geo.ny, c.geo.nx, CUFFT_R2C, 5);
+        plan(w.c2r4, c.geo.ny, c.geo.nx, CUFFT_C2R, 4);
+        c.dadj = ws.release();
+    }
+    DAdjWS& w = *c.dadj;
+    double* const part = w.part;
+    if (w.back) {                      // captured with the previous call's parameters
+        cudaGraphExecDestroy(w.back);
+        w.back = nullptr;
+    }
     cufftHandle hs[] = {w.r2c3, w.c2r7, w.r2c5, w.c2r4};
     for (cufftHandle h : hs) AW_CUFFT(cufftSetStream(h, c.stream));
     AW_CUDA(cudaMemsetAsync(w.acc, 0, sizeof(unsigned long long) * 6 * nc, c.stream));

@@ -167,6 +167,9 @@ struct Ctx {
 
     // discrete adjoint of the ES step (aw_adjoint.cu; allocated by aw_grad_es)
     struct AdjWS* adj = nullptr;
+    // discrete adjoint of the Darwin step (aw_adjoint_darwin.cu; kept between
+    // gradients of the same shape, released with the context)
+    struct DAdjWS* dadj = nullptr;
     // Trajectory recording, set only while the adjoint's recording ES step is
     // captured: the step's finalize advances rec_ad->rec_slot, the fused push
     // writes x_n, y_n and the field kernel E_n into that slot.
@@ -336,6 +339,7 @@ void free_checkpoint(Ctx& c);
 AdjK adj_constants(const Ctx& c, float dt_scale);
 void adj_prepare(Ctx& c, long long nsteps, int every);   // (re)allocates c.adj
 void free_adjoint(Ctx& c);
+void free_dadj(Ctx& c);      // aw_adjoint_darwin.cu: releases c.dadj
 // lE = acc / S + ad->ext_scale * E_slot (E of the slot's step, interleaved
 // [ncell][2]); acc is zeroed.
 void launch_adj_finalize(Ctx& c);

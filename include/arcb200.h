@@ -329,7 +329,9 @@ int aw_grad_es(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux
  * `checkpoint_every` steps and each segment is recomputed for its backward
  * steps; the transposed scatters are exact fixed point, so the result does not
  * depend on the interval and repeats bit for bit. The bound particles hold the
- * initial state again on return. Synchronises. */
+ * initial state again on return. The sweep's workspace (checkpoints, one
+ * segment's trajectory, FFT plans) stays with the context for the next
+ * gradient of the same shape and is released with it. Synchronises. */
 int aw_grad_darwin(aw_ctx* ctx, int64_t nsteps, int32_t checkpoint_every, float* dux, float* duy, float* duz,
                    double* dpump, double* loss);
 
