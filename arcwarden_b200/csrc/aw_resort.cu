@@ -5,14 +5,19 @@
 // start with compact chunks, but thermal motion mixes them: after a few
 // thousand steps a chunk's cells span the grid, its window no longer fits and
 // every deposit takes the exact (global-atomic) slow path. Re-sorting the
-// particles by small tiles every few dozen steps keeps chunks compact. The
+// particles by small tiles every few dozen steps keeps chunks compact; within a
+// tile they are ordered by cell, as the loader leaves them, so the deposit's
+// lanes (64 particles apart) fall on different cells (a tile-only order
+// interleaves the tile's cells and slowed the whistler1024 particle kernels by
+// 17-35%). The
 // reference's Darwin path reorders its particles by 16x16 tile every step
 // (Particles::sort_by_tile, include/pic/particles.hpp:678-726); here the sort
 // is by tiles of ~kChunk/2 particles, occasional, and stable, so runs stay
 // bit-reproducible. Results do not depend on the order: the deposits are exact
 // sums and the push is per particle.
 //
-// The sort is an LSD radix sort of (tile key, index) pairs, 8 key bits per pass.
+// The sort is an LSD radix sort of (key, index) pairs, 8 key bits per pass; the
+// key is the tile, then the cell within the tile (row-major).
 // Each warp owns a contiguous range of kRsItems elements. A pass counts the
 // digits of every range (warp-private shared counters), turns the counts into
 // exclusive offsets in digit-major, range-minor order (one block per digit),
@@ -28,17 +33,19 @@
 namespace aw {
 namespace {
 
-// Tile key of every particle from its position (positions outside the grid go
-// last), and the identity permutation.
+// Key of every particle from its position: tile * tx * ty + the cell's row-major
+// index in the tile (positions outside the grid go last), and the identity
+// permutation.
 __global__ void k_resort_keys(const float* __restrict__ x, const float* __restrict__ y, long long n, Geo g,
                               int tx, int ty, int ntx, int ntiles, int* __restrict__ key, int* __restrict__ idx) {
     const long long stride = static_cast<long long>(blockDim.x) * gridDim.x;
+    const int tcells = tx * ty;
     for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride) {
         const float xi = x[i], yi = y[i];
-        int k = ntiles;
+        int k = ntiles * tcells;
         if (xi >= 0.0f && xi < g.nxf && yi >= 0.0f && yi < g.nyf) {
             const int ci = min(static_cast<int>(xi), g.nx - 1), cj = min(static_cast<int>(yi), g.ny - 1);
-            k = (cj / ty) * ntx + ci / tx;
+            k = ((cj / ty) * ntx + ci / tx) * tcells + (cj % ty) * tx + ci % tx;
         }
         key[i] = k;
         idx[i] = static_cast<int>(i);
@@ -217,7 +224,7 @@ void launch_resort(Ctx& c) {
     int* keys_out = c.rs_buf + n;
     int* vals_in = c.rs_buf + 2 * n;
     int* vals_out = c.rs_buf + 3 * n;
-    const int end_bit = bits_for(ntiles);
+    const int end_bit = bits_for(ntiles * tx * ty);
     const int blocks = static_cast<int>(std::min<long long>((n + kThreads - 1) / kThreads, 148LL * 16));
     k_resort_keys<<<blocks, kThreads, 0, c.stream>>>(c.parts.x, c.parts.y, n, c.geo, tx, ty, ntx, ntiles,
                                                       keys_in, vals_in);

@@ -215,8 +215,9 @@ int aw_migrate(aw_ctx* ctx);
  * The permutation (physical == 0) or the tile offsets are kept in the context. */
 int aw_sort_tiles(aw_ctx* ctx, int32_t tx, int32_t ty, int32_t physical);
 /* Stable spatial re-sort of the bound particle SoA (x, y, ux, uy, uz, w and
- * cell are permuted together, in place) by tiles of about 1024 particles.
- * Keeps the fused kernels' per-chunk cell windows compact as particles mix;
+ * cell are permuted together, in place) by tiles of about 1024 particles and,
+ * within a tile, by cell. Keeps the fused kernels' per-chunk cell windows
+ * compact as particles mix;
  * results do not depend on particle order. The reference reorders its Darwin
  * particles by tile every step (Particles::sort_by_tile,
  * include/pic/particles.hpp:678-726); this sort is deterministic. */

@@ -200,16 +200,16 @@ def test_resort_only_permutes(setup, aw, model):
 
 @pytest.mark.parametrize("nx, ny, ppc", [(96, 64, 16), (512, 256, 4), (40, 24, 1)])
 def test_resort_is_the_stable_sort_by_tile(setup, aw, nx, ny, ppc):
-    """aw_resort permutes the particles into the stable order of their tile keys
-    (tiles of ~1024 particles, out-of-grid last): the hand-written LSD radix sort
-    against numpy's stable argsort, element for element. 512 x 256 x 4 needs two
-    8-bit passes."""
+    """aw_resort permutes the particles into the stable order of their keys
+    (tiles of ~1024 particles, then the cell within the tile, row-major;
+    out-of-grid last): the hand-written LSD radix sort against numpy's stable
+    argsort, element for element. 512 x 256 x 4 needs three 8-bit passes."""
     n = nx * ny * ppc
     s = setup(nx, ny, float(nx), float(ny), n, aw.AW_MODEL_DARWIN, dt=0.05)
     rng = np.random.default_rng(nx + ppc)
     x = rng.uniform(0, nx, n).astype(np.float32)
     y = rng.uniform(0, ny, n).astype(np.float32)
-    x[::97] = -1.0                                    # out of the grid: key ntiles, sorted last
+    x[::97] = -1.0                                    # out of the grid: sorted last
     s.put("x", x)
     s.put("y", y)
     s.put("w", np.arange(n, dtype=np.float32))        # tags (exact below 2^24)
@@ -225,7 +225,8 @@ def test_resort_is_the_stable_sort_by_tile(setup, aw, nx, ny, ppc):
     inside = (x >= 0) & (x < nx) & (y >= 0) & (y < ny)
     ci = np.minimum(x.astype(np.int64), nx - 1)
     cj = np.minimum(y.astype(np.int64), ny - 1)
-    key = np.where(inside, (cj // ty) * ntx + ci // tx, ntx * nty)
+    tcells = tx * ty
+    key = np.where(inside, ((cj // ty) * ntx + ci // tx) * tcells + (cj % ty) * tx + ci % tx, ntx * nty * tcells)
     order = np.argsort(key, kind="stable")
     assert np.array_equal(got["w"].astype(np.int64), order)
     assert np.array_equal(got["x"], x[order]) and np.array_equal(got["y"], y[order])
