@@ -539,7 +539,13 @@ __device__ __forceinline__ bool one_pass_window(Win& w, const Box& b, int ir, in
     w.Hb = w.H; w.nb = 1;
     w.WH = w.W * w.H;
     w.P = P1;
-    w.rep = w.WH * 4 <= P1 ? 4 : (w.WH * 2 <= P1 ? 2 : 1);
+    // as many copies (4, 2, 1) as fit, each rep copies CS cells apart, CS the
+    // first stride >= WH congruent to 32 / rep modulo 32: a cell's copies then
+    // fall in banks 32 / rep apart
+    const int cs4 = w.WH + (((8 - w.WH) % 32) + 32) % 32, cs2 = w.WH + (((16 - w.WH) % 32) + 32) % 32;
+    if (4 * cs4 <= P1) { w.rep = 4; w.CS = cs4; }
+    else if (2 * cs2 <= P1) { w.rep = 2; w.CS = cs2; }
+    else { w.rep = 1; w.CS = w.WH; }
     w.use = true;
     w.track_all = false;
     w.biased = NF > (T0 ? 1 : 0);
@@ -628,7 +634,7 @@ __device__ __forceinline__ void one_pass_deposit(int* __restrict__ win, const Wi
     const Cic2 c2 = cic2(x, y);
     int b[NF][4];
     quant_bits<NF>(cs, c2, b);
-    int* e0 = win + (threadIdx.x & (w.rep - 1)) * w.WH + dj * w.W + di;   // this lane's copy
+    int* e0 = win + (threadIdx.x & (w.rep - 1)) * w.CS + dj * w.W + di;   // this lane's copy
     int* e2 = e0 + w.W;
     if (NF > (T0 ? 1 : 0)) atomicAdd(e0 + 2 * NF * P1, 1);
 #pragma unroll
@@ -1129,7 +1135,7 @@ __device__ __forceinline__ void push_deposit_em_chunk(const EmArgs& A, const int
 
     // ---- single pass when the window fits ----------------------------------
     // Window planes of stride P1 (window capacity P1 cells), the gather tile after them.
-    constexpr int P1 = 224, kTileCap1 = (PC - P1) * win_planes(NF) / 8;
+    constexpr int P1 = 288, kTileCap1 = (PC - P1) * win_planes(NF) / 8;
     if (A.one_pass) {
         BBox cb;
 #pragma unroll 4

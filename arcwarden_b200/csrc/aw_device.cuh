@@ -352,6 +352,9 @@ struct Win {
     int rep;         // copies of the window in each plane: lane l adds to copy l mod rep
                      // (dense chunks, whose neighbouring lanes share cells); the
                      // flush sums them
+    int CS;          // the copies' stride in cells (>= WH; with rep copies, congruent
+                     // to 32 / rep modulo 32, so that the copies of a cell sit in
+                     // different shared-memory banks)
     bool use;        // deposited in the shared window (in one or more bands)
     bool track_all;  // some field's chunk sums may leave int32: track every field
     bool biased;     // the untracked fields add biased words (one band)
@@ -422,6 +425,7 @@ __device__ __forceinline__ void win_setup(Win& w, int lo_i, int lo_j, int hi_i, 
     }
     w.use = w.nb <= kMaxBands;
     w.WH = w.use ? w.W * w.Hb : 0;
+    w.CS = w.WH;
     w.track_all = track_all;
     w.biased = BIASED_OK && w.use && w.nb == 1 && !track_all && (NF > (T0 ? 1 : 0));
 }
@@ -442,7 +446,7 @@ template <int NF, bool T0, int PC = 0>
 __device__ __forceinline__ void win_zero(int* __restrict__ s, const Win& w) {
     const int P = PC ? PC : w.P;
     const bool ta = w.track_all, bi = w.biased;
-    const int used = w.WH * w.rep;
+    const int used = w.rep > 1 ? w.CS * w.rep : w.WH;
     for (int c = threadIdx.x; c < used; c += kThreads) {
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
@@ -476,7 +480,7 @@ __device__ __forceinline__ void win_flush(const int* __restrict__ s, const Win& 
         if (gi >= g.nx) gi -= g.nx;
         if (gj >= g.ny) gj -= g.ny;
         unsigned long long* a = acc + (static_cast<size_t>(gj) * g.nx + gi);
-        const int WHc = w.WH, R = w.rep;
+        const int WHc = w.CS, R = w.rep;     // copy r of cell c: r * CS + c
         unsigned nM = 0;
         if (win_planes(NF) > 2 * NF && bi) {
             int n = 0;
@@ -779,7 +783,7 @@ __device__ __forceinline__ void window_particles(const float* __restrict__ stage
         coef(a, cs);
         int b[NF][4];
         quant_bits<NF>(cs, c, b);
-        int* e0 = win + (threadIdx.x & (wn.rep - 1)) * wn.WH                       // this lane's copy
+        int* e0 = win + (threadIdx.x & (wn.rep - 1)) * wn.CS                       // this lane's copy
                   + win_col(c.j0, oj, g.ny) * wn.W + win_col(c.i0, oi, g.nx);         // corners 0, 1
         int* e2 = e0 + wn.W;                                                          // corners 2, 3
         if (kBiased) atomicAdd(e0 + 2 * NF * P, 1);
