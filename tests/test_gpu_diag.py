@@ -197,3 +197,42 @@ def test_every_module_keeps_the_step_rate(tmp_path):
     assert np.all(vid.sum(axis=1) <= n)
     assert np.all(vid.sum(axis=1) >= 0.99 * n)
     assert t_on <= 1.10 * t_off, (t_on, t_off)
+
+
+def test_one_row_run_matches_the_reference_runner(tmp_path):
+    """The whistler deck on a grid one cell high (512 x 1 cells, dx = 2, 512 per
+    cell: the geometry of the reference's whistler decks) for 200 steps through
+    both runners: the energy rows (kinetic, field, total, charge, max |E|) and
+    the Darwin field energies agree along the run. The two implementations
+    differ by float rounding (FP32 atomics there, exact sums here), which the
+    run amplifies slowly (measured over 200 steps: kinetic 7e-6, field 5e-5,
+    E_total 3e-5, E_T 1.2e-5 relative, charge and B exactly), so the bars are
+    relative with a margin."""
+    ours, ref = _exe("arcsim"), _exe("ref_arcsim")
+    deck = _deck(tmp_path, "row.ini", [(r"^nx = .*$", "nx = 512"), (r"^ny = .*$", "ny = 1"),
+                                       (r"^Lx = .*$", "Lx = 1024.0"), (r"^Ly = .*$", "Ly = 2.0"),
+                                       (r"^ppc .*$", "ppc     = 512"), (r"^nsteps = .*$", "nsteps = 200"),
+                                       (r"^enable  = .*$", "enable  = em_energy")])
+    a, b = tmp_path / "a", tmp_path / "b"
+    a.mkdir()
+    b.mkdir()
+    _run(ours, deck, a)
+    _run(ref, deck, b)
+    ea = np.loadtxt(a / "energy.csv", delimiter=",", skiprows=1)
+    eb = np.loadtxt(b / "energy.csv", delimiter=",", skiprows=1)
+    assert ea.shape == eb.shape and ea.shape[0] >= 100
+    assert np.array_equal(ea[:, 0], eb[:, 0])
+    rel = lambda x, y: float(np.max(np.abs(x - y) / np.maximum(np.abs(y), 1e-300)))
+    print(f"\nke {rel(ea[:, 2], eb[:, 2]):.2e} ee {rel(ea[:, 3], eb[:, 3]):.2e} "
+          f"charge {rel(ea[:, 5], eb[:, 5]):.2e} max_e {rel(ea[:, 6], eb[:, 6]):.2e}")
+    assert rel(ea[:, 2], eb[:, 2]) < 5e-5          # kinetic energy
+    assert rel(ea[:, 4], eb[:, 4]) < 5e-5          # total
+    assert rel(ea[:, 5], eb[:, 5]) < 1e-5          # charge
+    assert rel(ea[:, 3], eb[:, 3]) < 1e-3          # field energy (noise level)
+    pa = np.loadtxt(a / "whistler_diag_emenergy.csv", delimiter=",", skiprows=1)
+    pb = np.loadtxt(b / "whistler_diag_emenergy.csv", delimiter=",", skiprows=1)
+    assert pa.shape == pb.shape
+    print(f"E_total {rel(pa[:, 2], pb[:, 2]):.2e} B {rel(pa[:, 3], pb[:, 3]):.2e} E_T {rel(pa[:, 4], pb[:, 4]):.2e}")
+    assert rel(pa[:, 3], pb[:, 3]) < 1e-5          # magnetic energy (B0 dominates)
+    assert rel(pa[:, 2], pb[:, 2]) < 1e-3
+    assert rel(pa[:, 4], pb[:, 4]) < 1e-3
