@@ -4,6 +4,10 @@
 // aw_init; every step() is one replay of the captured step graph (aw_run),
 // and a dump step enqueues an asynchronous copy of the step's GPU-reduced
 // diagnostics (the shim's pic/diagnostics.hpp), with no host sync.
+// With ARCB200_LOOP_TIME set in the environment, the destructor prints to
+// stderr the wall time from the first step() to its own start, after a stream
+// sync: the step loop and whatever the caller did between and after the steps
+// (a runner's diagnostics and their files), without the start-up.
 #ifndef ARC_PIC_SIMULATION_HPP
 #define ARC_PIC_SIMULATION_HPP
 
@@ -24,6 +28,9 @@
 
 #include "../arcb200_shim.hpp"
 
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <string>
 
 namespace arc {
@@ -40,6 +47,11 @@ public:
         diag_.set_geometry(g.dx, g.dy);
     }
     ~Simulation() {
+        if (steps_ > 0 && std::getenv("ARCB200_LOOP_TIME")) try {
+            stream_.synchronize();
+            const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - first_step_).count();
+            std::fprintf(stderr, "arcb200 loop: %ld steps in %.6f s\n", steps_, s);
+        } catch (...) {}
         if (ctx_) aw_ctx_destroy(ctx_);
     }
     Simulation(const Simulation&) = delete;
@@ -74,6 +86,7 @@ public:
     // One PIC step (the fused graph), then the diagnostics when due
     // (Diagnostics::maybe_compute's cadence: dump_every <= 0 means every step).
     void step(long n) {
+        if (steps_++ == 0) first_step_ = std::chrono::steady_clock::now();
         shim::check(aw_run(ctx_, n, 1, 1), "run");
         if (p_.dump_every <= 0 || n % p_.dump_every == 0) diag_.record_async(n, n * p_.dt, dev_diag_, stream_);
     }
@@ -123,6 +136,8 @@ private:
     CudaStream     stream_;
     aw_ctx*        ctx_ = nullptr;
     const aw_diag* dev_diag_ = nullptr;
+    long           steps_ = 0;
+    std::chrono::steady_clock::time_point first_step_{};
 };
 
 }  // namespace arc
