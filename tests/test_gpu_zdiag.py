@@ -172,6 +172,9 @@ def test_every_module_keeps_the_step_rate(tmp_path):
     diagnostics."""
     ours = _exe("arcsim")
     shm = os.path.isdir("/dev/shm") and os.access("/dev/shm", os.W_OK)
+    if shm:            # two runs' files (2 x 215 MB) at a time, with room to spare
+        st = os.statvfs("/dev/shm")
+        shm = st.f_bavail * st.f_frsize >= (1 << 30)
     work = Path(tempfile.mkdtemp(prefix="aw_diag_", dir="/dev/shm")) if shm else tmp_path
     try:
         _step_rate_case(ours, work)
